@@ -1,0 +1,147 @@
+/*
+ * csd_b200.h -- C ABI of the B200-native single-shell constrained spherical
+ * deconvolution (CSD) library, libcsd_b200.so.
+ *
+ * It replaces the hot path of MRtrix3's `dwi2fod csd`:
+ *   MR::DWI::SDeconv::CSD::Shared (src/dwi/sdeconv/csd.h:46-212) -> csd_shared_*
+ *   MR::DWI::SDeconv::CSD set/iterate/FOD (csd.h:221-271)         -> csd_state_*
+ *   the ThreadedLoop over voxels in cmd/dwi2fod.cpp:275-281
+ *     with CSD_Processor (cmd/dwi2fod.cpp:120-176)                -> csd_solve,
+ *                                                                    csd_dwi2fod_host
+ * Plain pointers and sizes only.  Device pointers are CUDA global memory on
+ * the current device; a `stream` argument is a cudaStream_t (NULL = legacy
+ * default stream).  All functions return 0 on success or a negative CSD_ERR_*
+ * code; csd_last_error() then describes the failure (thread-local).
+ */
+#ifndef CSD_B200_H
+#define CSD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSD_OK 0
+#define CSD_ERR_INVALID (-1)     /* invalid argument (the reference throws MR::Exception) */
+#define CSD_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define CSD_ERR_TIMEOUT (-3)     /* a bounded device wait gave up */
+#define CSD_ERR_NOMEM (-4)       /* device allocation failed */
+#define CSD_ERR_UNSUPPORTED (-5) /* e.g. lmax above the compiled maximum */
+
+/* Per-voxel status byte (low nibble = outcome, high bits = flags).  The
+ * reference reports non-convergence only as an INFO log
+ * (cmd/dwi2fod.cpp:142-144) and never checks the LLT status (csd.h:264). */
+#define CSD_STATUS_MASKED 0       /* outside the mask: FOD written as zeros (dwi2fod.cpp:130-133) */
+#define CSD_STATUS_CONVERGED 1    /* iterate() returned true within niter */
+#define CSD_STATUS_NITER 2        /* niter iterate() calls without convergence */
+#define CSD_STATUS_NONFINITE 3    /* a non-finite sample: FOD zeros (dwi2fod.cpp:166-167) */
+#define CSD_STATUS_FP64 0x10      /* flag: a factorisation was redone in FP64 */
+#define CSD_STATUS_CHOLFAIL 0x20  /* flag: the normal matrix was not positive definite */
+#define CSD_STATUS_WARM_RESTART 0x40 /* flag: warm start abandoned, re-solved from the plain start */
+
+#define CSD_MAX_LMAX 12           /* largest lmax compiled (91 coefficients) */
+
+/* Options of `dwi2fod csd` (src/dwi/sdeconv/csd.cpp:318-346,
+ * cmd/dwi2fod.cpp:38-59) and the two config-file keys the path reads. */
+typedef struct csd_params {
+  int lmax;                 /* -lmax; 0 = min(lmax of response, 8) (csd.h:127) */
+  int niter;                /* -niter, default 50 (csd.h:35) */
+  double neg_lambda;        /* -neg_lambda, default 1 (csd.h:32) */
+  double norm_lambda;       /* -norm_lambda, default 1 (csd.h:33) */
+  double threshold;         /* -threshold, default 0 (csd.h:34) */
+  const double* filter;     /* -filter (NULL = [1 1 1], csd.h:136-137) */
+  int n_filter;
+  double bzero_threshold;   /* config BZeroThreshold, default 10 (dwi/gradient.cpp:92-95) */
+  double bvalue_epsilon;    /* config BValueEpsilon, default 80 (dwi/shells.cpp:43-46) */
+  double fp64_condition;    /* GPU only: condition estimate above which a voxel's
+                               factorisation is redone in FP64 (default 1e6) */
+} csd_params;
+
+typedef struct csd_shared csd_shared;  /* immutable after creation, like CSD::Shared after init() */
+
+/* Fill *p with the reference defaults. */
+void csd_params_init(csd_params* p);
+
+/* CSD::Shared(header) + parse_cmdline_options() + set_response() + init()
+ * (csd.h:52-198).  grad: [n_volumes][4] host doubles (x y z b), as
+ * DWI::get_DW_scheme reads them (dwi/gradient.cpp:280).  response: zonal SH
+ * coefficients l=0,2,..  hr_dirs: [n_hr][2] azimuth/elevation, or NULL for
+ * the built-in 300 directions (csd.h:54, -directions at csd.h:84-86).
+ * Uploads the tables to the current device. */
+int csd_shared_create(const csd_params* p, const double* grad, int n_volumes, const double* response,
+                      int n_response, const double* hr_dirs, int n_hr, csd_shared** out);
+void csd_shared_destroy(csd_shared* s);
+
+/* CSD::Shared::nSH() (csd.h:200-202). */
+int csd_shared_nsh(const csd_shared* s);
+/* info[8] = lmax, lmax_response, lmax_data, nSH, n_init, n_dw, n_hr, niter */
+int csd_shared_info(const csd_shared* s, int* info);
+/* The `dwis` member (csd.h:62): volume indices of the selected shell [n_dw]. */
+int csd_shared_dwis(const csd_shared* s, int* out);
+/* Host FP64 copies of the public matrices: which = 0 rconv [n_init][n_dw],
+ * 1 M [n_dw][nSH], 2 Mt_M [nSH][nSH] (symmetric, with norm_lambda),
+ * 3 HR_trans [n_hr][nSH], 4 scalars [threshold, norm_lambda, neg_lambda]. */
+int csd_shared_matrix(const csd_shared* s, int which, double* out);
+
+/* One image to deconvolve.  dwi[v*voxel_stride + t*volume_stride] is volume
+ * t of voxel v (float32, the layout `with_direct_io(3)` gives when
+ * voxel_stride = n_volumes and volume_stride = 1, dwi2fod.cpp:279).
+ * All pointers are device pointers; optional ones may be NULL. */
+typedef struct csd_volume {
+  const float* dwi;
+  int64_t n_voxels;
+  int64_t voxel_stride;
+  int64_t volume_stride;
+  const uint8_t* mask;            /* optional [n_voxels], 0 = skip (dwi2fod.cpp:158-162) */
+  const uint32_t* warm_negmask;   /* optional [n_voxels][ceil(n_hr/32)] first negative set */
+  float* fod;                     /* [n_voxels][fod_stride] output, first nSH used */
+  int64_t fod_stride;
+  uint8_t* status;                /* optional [n_voxels] CSD_STATUS_* */
+  uint8_t* iterations;            /* optional [n_voxels] iterate() calls (saturates at 255) */
+  uint32_t* negmask;              /* optional [n_voxels][ceil(n_hr/32)] final negative set */
+} csd_volume;
+
+/* Deconvolve n_volumes images in ONE persistent launch: volumes[i] uses
+ * shared[i] (each may have its own gradient scheme, but all must share nSH
+ * and n_hr).  Warps pull voxels from a device work queue; converged voxels
+ * free their warp for the next.  Equivalent to running CSD_Processor over
+ * every voxel (dwi2fod.cpp:128-147).  Asynchronous on `stream`. */
+int csd_solve(const csd_shared* const* shared, const csd_volume* volumes, int n_volumes, void* stream);
+
+/* End-to-end call on HOST buffers: dwi [n_voxels][n_volumes] float32,
+ * voxel-interleaved; mask optional; fod [n_voxels][nSH].  Stages through
+ * pinned memory in slabs with copies overlapped with the solve.  Synchronous. */
+int csd_dwi2fod_host(const csd_shared* s, const float* dwi, int64_t n_voxels, const uint8_t* mask,
+                     float* fod, uint8_t* status, uint8_t* iterations);
+
+/* ---- per-step surface: CSD::set / iterate / FOD (csd.h:237-271) over a
+ *      batch of voxels (the reference object is one voxel: a batch of 1).
+ *      The plain GPU method drives these phases from the host, one pass per
+ *      iterate(): projection of all still-active voxels, compaction, then
+ *      assembly + factorisation of the voxels whose negative set changed. */
+typedef struct csd_state csd_state;
+int csd_state_create(const csd_shared* s, int64_t capacity, csd_state** out);
+void csd_state_destroy(csd_state* st);
+/* CSD::set for n_voxels voxels (clamps <0 to 0; non-finite or masked voxels
+ * are marked done with a zero FOD).  Resets the iteration state. */
+int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, int64_t voxel_stride,
+                  int64_t volume_stride, const uint8_t* mask, void* stream);
+/* Replace the first negative set of every active voxel (warm start). */
+int csd_state_warm(csd_state* st, const uint32_t* negmask, void* stream);
+/* One CSD::iterate() on every active voxel.  *n_active receives how many
+ * voxels are still iterating afterwards (synchronises the stream). */
+int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream);
+/* CSD::FOD(): copy F (float) out, plus optional status/iterations/negmask. */
+int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride, uint8_t* status,
+                  uint8_t* iterations, uint32_t* negmask, void* stream);
+
+/* Thread-local description of the last failure. */
+const char* csd_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CSD_B200_H */

@@ -1,0 +1,935 @@
+// libcsd_b200: kernels and C ABI of the B200-native single-shell CSD.
+//
+// Replaces the per-voxel ThreadedLoop of MRtrix3 `dwi2fod csd`
+// (cmd/dwi2fod.cpp:275-281, core/algo/threaded_loop.h:324-362): instead of
+// CPU threads taking rows of voxels under a mutex, persistent warps take
+// voxels from a device work counter.  A warp that finishes a voxel (whatever
+// its iteration count) immediately takes the next one, so unconverged voxels
+// never hold back converged ones and volumes of uneven size share one launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/csd_b200.h"
+#include "csd_device.cuh"
+#include "shared_init.hpp"
+
+using namespace csdb200;
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (expr);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(CSD_ERR_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" const char* csd_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------------------
+// kernels
+
+namespace csdb200 {
+
+// Solve voxel v of volume V with one warp (CSD_Processor::operator(),
+// cmd/dwi2fod.cpp:128-147, with CSD::set/iterate, csd.h:237-269).
+template <int N>
+__device__ void solve_voxel(const VolumeDesc& V, long long v, const float* Hs, int nhr, int nw,
+                            float cond_thr, int refine, const WarpWS<N>& w, int lane, double* slot) {
+  const Scheme& sc = V.sc;
+  const bool masked = V.mask && !V.mask[v];
+  const float* dwi = V.dwi + v * V.vox_stride;
+  float* out = V.fod + v * V.fod_stride;
+  int st = voxel_set<N>(sc, dwi, V.vol_stride, masked, w, lane);
+  if (st != 0) {
+    for (int c = lane; c < N; c += 32) out[c] = 0.f;
+    if (lane == 0) {
+      if (V.status) V.status[v] = (uint8_t)(st == 1 ? CSD_STATUS_MASKED : CSD_STATUS_NONFINITE);
+      if (V.iters) V.iters[v] = 0;
+    }
+    if (V.negmask)
+      for (int p = lane; p < nw; p += 32) V.negmask[v * nw + p] = 0u;
+    return;
+  }
+  uint32_t bits[kMaxWords], old[kMaxWords];
+#pragma unroll
+  for (int p = 0; p < kMaxWords; ++p) old[p] = 0u;
+  int flags = 0, it = 0;
+  bool conv = false, use_warm = V.warm != nullptr;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    bool have_old = false;
+    conv = false;
+#pragma unroll 1
+    for (it = 0; it < sc.niter; ++it) {
+      if (it == 0 && use_warm) {
+        // warm start: the first negative set is supplied instead of projected
+#pragma unroll
+        for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < nw) ? __ldg(V.warm + v * nw + p) : 0u;
+        if (nhr & 31) bits[nw - 1] &= (1u << (nhr & 31)) - 1u;
+      } else {
+        project_mask<N>(Hs, nhr, nw, sc.threshold, w, lane, bits);
+        if (have_old) {
+          bool same = true;
+#pragma unroll
+          for (int p = 0; p < kMaxWords; ++p)
+            if (p < nw) same = same && (bits[p] == old[p]);
+          if (same) {  // csd.h:252-253
+            conv = true;
+            ++it;
+            break;
+          }
+        }
+      }
+      const int k = mask_to_list(bits, nw, w.neg, lane);
+      flags |= assemble_solve<N>(sc, Hs, k, w, lane, cond_thr, refine, slot);
+#pragma unroll
+      for (int p = 0; p < kMaxWords; ++p) old[p] = bits[p];
+      have_old = true;
+    }
+    if (conv || !use_warm || sc.niter == 0) break;
+    // the warm-started iteration did not reach a fixed point: restart the
+    // voxel from the plain start
+    flags |= CSD_STATUS_WARM_RESTART;
+    use_warm = false;
+#pragma unroll
+    for (int p = 0; p < kMaxWords; ++p) old[p] = 0u;
+    voxel_set<N>(sc, dwi, V.vol_stride, false, w, lane);
+  }
+  for (int c = lane; c < N; c += 32) out[c] = w.F[c];
+  if (lane == 0) {
+    const int outcome = (conv || sc.niter == 0) ? CSD_STATUS_CONVERGED : CSD_STATUS_NITER;
+    if (V.status) V.status[v] = (uint8_t)(outcome | flags);
+    if (V.iters) V.iters[v] = (uint8_t)(it > 255 ? 255 : it);
+  }
+  if (V.negmask) {
+#pragma unroll
+    for (int p = 0; p < kMaxWords; ++p)
+      if (p < nw && p == lane) V.negmask[v * nw + p] = old[p];
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_persistent_kernel(const __grid_constant__ SolveParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int HS = Dims<N>::HS;
+  float* Hs = reinterpret_cast<float*>(smem);
+  const int nhr = P.nhr;
+  {
+    const float4* src = reinterpret_cast<const float4*>(P.vol[0].sc.H32);
+    float4* dst = reinterpret_cast<float4*>(Hs);
+    for (int i = threadIdx.x; i < nhr * HS / 4; i += blockDim.x) dst[i] = __ldg(src + i);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int hbytes = ((nhr * HS * 4 + 15) / 16) * 16;
+  WarpWS<N> w = carve_ws<N>(smem + hbytes + warp * warp_ws_bytes<N>());
+  double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
+  for (;;) {
+    unsigned long long g = 0;
+    if (lane == 0) g = atomicAdd(P.queue, 1ULL);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= (unsigned long long)P.total) break;
+    int vi = 0;
+    while (vi + 1 < P.n_vol && (long long)g >= P.vol[vi + 1].first) ++vi;
+    const VolumeDesc& V = P.vol[vi];
+    solve_voxel<N>(V, (long long)g - V.first, Hs, nhr, P.nw, P.cond_thr, P.refine, w, lane, slot);
+  }
+}
+
+
+// ---- phased kernels behind the csd_state_* surface ------------------------
+
+struct StateParams {
+  Scheme sc;
+  int nhr, nw, refine, n_in, use_warm;
+  float cond_thr;
+  float* F;             // [cap][HS]
+  double* b;            // [cap][N]
+  uint32_t* old;        // [cap][nw]
+  const uint32_t* warm; // [cap][nw] or NULL
+  uint8_t* status;      // [cap]
+  uint16_t* iters;      // [cap] iterate() calls made
+  const int* act_in;    // [n_in] active voxel ids
+  int* act_out;         // compacted survivors
+  int* n_out;
+  double* fp64_scratch;
+  // set() inputs
+  const float* dwi;
+  long long vox_stride, vol_stride;
+  const uint8_t* mask;
+};
+
+// CSD::set for every voxel (csd.h:237-243); voxels that are masked out or
+// hold a non-finite sample are finished immediately with F = 0.
+template <int N>
+__global__ void __launch_bounds__(256) csd_state_set_kernel(const __grid_constant__ StateParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpWS<N> w = carve_ws<N>(smem + warp * warp_ws_bytes<N>());
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+  const long long nwt = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long v = gw; v < P.n_in; v += nwt) {
+    const bool masked = P.mask && !P.mask[v];
+    const int st = voxel_set<N>(P.sc, P.dwi + v * P.vox_stride, P.vol_stride, masked, w, lane);
+    float* F = P.F + v * Dims<N>::HS;
+    for (int c = lane; c < Dims<N>::HS; c += 32) F[c] = st ? 0.f : w.F[c];
+    for (int c = lane; c < N; c += 32) P.b[v * N + c] = st ? 0.0 : w.b[c];
+    for (int p = lane; p < P.nw; p += 32) P.old[v * P.nw + p] = 0u;
+    if (lane == 0) {
+      P.iters[v] = 0;
+      if (st) {
+        P.status[v] = (uint8_t)(st == 1 ? CSD_STATUS_MASKED : CSD_STATUS_NONFINITE);
+      } else if (P.sc.niter == 0) {
+        P.status[v] = CSD_STATUS_CONVERGED;
+      } else {
+        P.status[v] = 0xFF;  // active
+        P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
+      }
+    }
+  }
+}
+
+// One CSD::iterate() (csd.h:245-269) on each listed voxel; voxels that
+// converge or exhaust niter drop out, the others are appended to act_out.
+template <int N>
+__global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_state_iterate_kernel(const __grid_constant__ StateParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int HS = Dims<N>::HS;
+  float* Hs = reinterpret_cast<float*>(smem);
+  {
+    const float4* src = reinterpret_cast<const float4*>(P.sc.H32);
+    float4* dst = reinterpret_cast<float4*>(Hs);
+    for (int i = threadIdx.x; i < P.nhr * HS / 4; i += blockDim.x) dst[i] = __ldg(src + i);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int hbytes = ((P.nhr * HS * 4 + 15) / 16) * 16;
+  WarpWS<N> w = carve_ws<N>(smem + hbytes + warp * warp_ws_bytes<N>());
+  double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
+  const int gw = blockIdx.x * nwarps + warp, nwt = gridDim.x * nwarps;
+  for (int e = gw; e < P.n_in; e += nwt) {
+    const long long v = P.act_in[e];
+    for (int c = lane; c < HS; c += 32) w.F[c] = P.F[v * HS + c];
+    for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
+    __syncwarp();
+    const int it = P.iters[v];
+    uint32_t bits[kMaxWords];
+    if (it == 0 && P.use_warm && P.warm) {
+#pragma unroll
+      for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.warm[v * P.nw + p] : 0u;
+      if (P.nhr & 31) bits[P.nw - 1] &= (1u << (P.nhr & 31)) - 1u;
+    } else {
+      project_mask<N>(Hs, P.nhr, P.nw, P.sc.threshold, w, lane, bits);
+      if (it > 0) {
+        bool same = true;
+#pragma unroll
+        for (int p = 0; p < kMaxWords; ++p)
+          if (p < P.nw) same = same && (bits[p] == P.old[v * P.nw + p]);
+        if (same) {
+          if (lane == 0) {
+            P.iters[v] = (uint16_t)(it + 1);
+            P.status[v] = (uint8_t)(CSD_STATUS_CONVERGED | (P.status[v] == 0xFF ? 0 : (P.status[v] & 0xF0)));
+          }
+          continue;
+        }
+      }
+    }
+    const int k = mask_to_list(bits, P.nw, w.neg, lane);
+    const int fl = assemble_solve<N>(P.sc, Hs, k, w, lane, P.cond_thr, P.refine, slot);
+    for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
+#pragma unroll
+    for (int p = 0; p < kMaxWords; ++p)
+      if (p < P.nw && p == lane) P.old[v * P.nw + p] = bits[p];
+    if (lane == 0) {
+      const int nit = it + 1;
+      P.iters[v] = (uint16_t)nit;
+      // status holds 0xFF while active with no flags; flags accumulate in the high nibble
+      uint8_t stv = P.status[v];
+      uint8_t flags = (uint8_t)((stv == 0xFF ? 0 : (stv & 0xF0)) | fl);
+      if (nit >= P.sc.niter) {
+        P.status[v] = (uint8_t)(CSD_STATUS_NITER | flags);
+      } else {
+        P.status[v] = flags ? (uint8_t)(0x0F | flags) : (uint8_t)0xFF;
+        P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
+      }
+    }
+  }
+}
+
+template <int N>
+__global__ void csd_state_fod_kernel(const float* F, const uint8_t* status, const uint16_t* iters, const uint32_t* old,
+                                     int nw, long long n, float* fod, long long fod_stride, uint8_t* st_out,
+                                     uint8_t* it_out, uint32_t* neg_out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * N) return;
+  const long long v = i / N;
+  const int c = (int)(i - v * N);
+  fod[v * fod_stride + c] = F[v * Dims<N>::HS + c];
+  if (c == 0) {
+    uint8_t s = status[v];
+    if (s == 0xFF) s = CSD_STATUS_NITER;               // still iterating: not converged yet
+    else if ((s & 0x0F) == 0x0F) s = (uint8_t)(CSD_STATUS_NITER | (s & 0xF0));
+    if (st_out) st_out[v] = s;
+    if (it_out) it_out[v] = (uint8_t)(iters[v] > 255 ? 255 : iters[v]);
+    if (neg_out)
+      for (int p = 0; p < nw; ++p) neg_out[v * nw + p] = old[v * nw + p];
+  }
+}
+
+}  // namespace csdb200
+
+// ---------------------------------------------------------------------------
+// shared tables
+
+struct csd_shared {
+  HostShared h;
+  double cond_thr = 1e6;
+  int device = -1;               // device holding the tables (-1: not uploaded yet)
+  std::mutex upload_mu;
+  int HS = 0, WSZ = 0;
+  std::vector<float> H32_host;
+  std::vector<float> MtMp_host;
+  std::vector<double> rconvT_host;
+  float* H32 = nullptr;
+  double* H64 = nullptr;
+  float* MtMp = nullptr;
+  double* MtM64 = nullptr;
+  double* rconvT = nullptr;
+  double* M64 = nullptr;
+  int* dwis = nullptr;
+};
+
+static bool supported_nsh(int n) { return n == 6 || n == 15 || n == 28 || n == 45 || n == 66 || n == 91; }
+
+extern "C" void csd_params_init(csd_params* p) {
+  if (!p) return;
+  p->lmax = 0;
+  p->niter = 50;
+  p->neg_lambda = 1.0;
+  p->norm_lambda = 1.0;
+  p->threshold = 0.0;
+  p->filter = nullptr;
+  p->n_filter = 0;
+  p->bzero_threshold = 10.0;
+  p->bvalue_epsilon = 80.0;
+  p->fp64_condition = 1e6;
+}
+
+template <typename T>
+static int upload(T** dst, const std::vector<T>& src) {
+  CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), std::max<size_t>(src.size(), 1) * sizeof(T)));
+  if (!src.empty()) CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static std::vector<double> builtin_hr_dirs();
+
+extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_volumes, const double* response,
+                                 int n_response, const double* hr_dirs, int n_hr, csd_shared** out) {
+  if (!out) return fail(CSD_ERR_INVALID, "csd_shared_create: out is NULL");
+  *out = nullptr;
+  csd_params def;
+  csd_params_init(&def);
+  if (!p) p = &def;
+  SharedParams sp;
+  sp.lmax = p->lmax;
+  sp.niter = p->niter;
+  sp.neg_lambda = p->neg_lambda;
+  sp.norm_lambda = p->norm_lambda;
+  sp.threshold = p->threshold;
+  if (p->filter && p->n_filter > 0) sp.filter.assign(p->filter, p->filter + p->n_filter);
+  sp.bzero_threshold = p->bzero_threshold;
+  sp.bvalue_epsilon = p->bvalue_epsilon;
+  std::vector<double> hr;
+  if (hr_dirs) {
+    if (n_hr <= 0) return fail(CSD_ERR_INVALID, "n_hr must be positive");
+    hr.assign(hr_dirs, hr_dirs + 2 * (size_t)n_hr);
+  } else {
+    hr = builtin_hr_dirs();
+    n_hr = (int)(hr.size() / 2);
+  }
+  std::unique_ptr<csd_shared> s(new csd_shared);
+  try {
+    s->h = build_shared(sp, grad, n_volumes, response, n_response, hr.data(), n_hr);
+  } catch (const std::exception& e) {
+    return fail(CSD_ERR_INVALID, e.what());
+  }
+  const HostShared& h = s->h;
+  if (!supported_nsh(h.nsh)) return fail(CSD_ERR_UNSUPPORTED, "lmax above the compiled maximum (12)");
+  if (h.nhr > kMaxHR) return fail(CSD_ERR_UNSUPPORTED, "more than 512 constraint directions");
+  if (h.ndw > kMaxDW) return fail(CSD_ERR_UNSUPPORTED, "more than 512 DW volumes in the shell");
+  if (h.niter > 255 * 4) return fail(CSD_ERR_INVALID, "niter out of range [0,1000]");
+  s->cond_thr = p->fp64_condition > 0 ? p->fp64_condition : 1e6;
+  const int n = h.nsh;
+  s->HS = hr_stride(n);
+  s->WSZ = packoff(n);
+  // HR_trans fp32, rows padded to HS with zeros
+  s->H32_host.assign((size_t)h.nhr * s->HS, 0.f);
+  for (int d = 0; d < h.nhr; ++d)
+    for (int c = 0; c < n; ++c) s->H32_host[(size_t)d * s->HS + c] = (float)h.HR[(size_t)d * n + c];
+  s->MtMp_host.assign((size_t)s->WSZ, 0.f);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) s->MtMp_host[packoff(i) + j] = (float)h.MtM[(size_t)i * n + j];
+  s->rconvT_host.assign((size_t)h.ndw * h.ninit, 0.0);
+  for (int r = 0; r < h.ninit; ++r)
+    for (int t = 0; t < h.ndw; ++t) s->rconvT_host[(size_t)t * h.ninit + r] = h.rconv[(size_t)r * h.ndw + t];
+  *out = s.release();
+  return CSD_OK;
+}
+
+// The tables go to the device on first use (so the host precompute can be
+// created and inspected without a GPU); later calls must use the same device.
+static int ensure_device(const csd_shared* cs) {
+  csd_shared* s = const_cast<csd_shared*>(cs);
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(s->upload_mu);
+  if (s->device == dev) return 0;
+  if (s->device >= 0) return fail(CSD_ERR_INVALID, "shared tables live on another device");
+  int rc;
+  const HostShared& h = s->h;
+  if ((rc = upload(&s->H32, s->H32_host))) return rc;
+  if ((rc = upload(&s->H64, h.HR))) return rc;
+  if ((rc = upload(&s->MtMp, s->MtMp_host))) return rc;
+  if ((rc = upload(&s->MtM64, h.MtM))) return rc;
+  if ((rc = upload(&s->rconvT, s->rconvT_host))) return rc;
+  if ((rc = upload(&s->M64, h.M))) return rc;
+  if ((rc = upload(&s->dwis, h.dwis))) return rc;
+  s->device = dev;
+  return 0;
+}
+
+extern "C" void csd_shared_destroy(csd_shared* s) {
+  if (!s) return;
+  if (s->device >= 0) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(s->device);
+    cudaFree(s->H32);
+    cudaFree(s->H64);
+    cudaFree(s->MtMp);
+    cudaFree(s->MtM64);
+    cudaFree(s->rconvT);
+    cudaFree(s->M64);
+    cudaFree(s->dwis);
+    cudaSetDevice(cur);
+  }
+  delete s;
+}
+
+extern "C" int csd_shared_nsh(const csd_shared* s) { return s ? s->h.nsh : fail(CSD_ERR_INVALID, "NULL shared"); }
+
+extern "C" int csd_shared_info(const csd_shared* s, int* info) {
+  if (!s || !info) return fail(CSD_ERR_INVALID, "NULL argument");
+  const HostShared& h = s->h;
+  const int v[8] = {h.lmax, h.lmax_response, h.lmax_data, h.nsh, h.ninit, h.ndw, h.nhr, h.niter};
+  std::memcpy(info, v, sizeof(v));
+  return CSD_OK;
+}
+
+extern "C" int csd_shared_dwis(const csd_shared* s, int* out) {
+  if (!s || !out) return fail(CSD_ERR_INVALID, "NULL argument");
+  std::copy(s->h.dwis.begin(), s->h.dwis.end(), out);
+  return CSD_OK;
+}
+
+extern "C" int csd_shared_matrix(const csd_shared* s, int which, double* out) {
+  if (!s || !out) return fail(CSD_ERR_INVALID, "NULL argument");
+  const HostShared& h = s->h;
+  switch (which) {
+    case 0: std::copy(h.rconv.begin(), h.rconv.end(), out); break;
+    case 1: std::copy(h.M.begin(), h.M.end(), out); break;
+    case 2: std::copy(h.MtM.begin(), h.MtM.end(), out); break;
+    case 3: std::copy(h.HR.begin(), h.HR.end(), out); break;
+    case 4: out[0] = h.threshold; out[1] = h.norm_lambda; out[2] = h.neg_lambda; break;
+    default: return fail(CSD_ERR_INVALID, "unknown matrix id");
+  }
+  return CSD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-(device, stream) workspace: work counter and FP64 fallback slots
+
+namespace {
+struct Workspace {
+  unsigned long long* queue = nullptr;   // kMaxQueues counters
+  double* fp64 = nullptr;
+  size_t fp64_doubles = 0;
+  // device staging for the host-buffer entry point
+  float* d_dwi = nullptr;
+  size_t d_dwi_n = 0;
+  float* d_fod = nullptr;
+  size_t d_fod_n = 0;
+  uint8_t* d_small = nullptr;
+  size_t d_small_n = 0;
+  cudaStream_t streams[2] = {nullptr, nullptr};
+};
+std::mutex g_ws_mu;
+std::map<std::pair<int, void*>, Workspace> g_ws;
+
+int get_ws(void* stream, Workspace** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  Workspace& w = g_ws[{dev, stream}];
+  if (!w.queue) CUDA_TRY(cudaMalloc(&w.queue, 64 * sizeof(unsigned long long)));
+  *out = &w;
+  return 0;
+}
+
+template <typename T>
+int grow(T** p, size_t* have, size_t need) {
+  if (*have >= need) return 0;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  if (cudaMalloc(reinterpret_cast<void**>(p), need * sizeof(T)) != cudaSuccess)
+    return fail(CSD_ERR_NOMEM, "device allocation failed");
+  *have = need;
+  return 0;
+}
+
+struct LaunchShape {
+  int warps = 0, blocks = 0;
+  size_t smem = 0;
+};
+
+template <int N>
+int launch_persistent(const SolveParams& P, size_t smem, int warps, int blocks, cudaStream_t st) {
+  CUDA_TRY(cudaFuncSetAttribute(csd_persistent_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+  csd_persistent_kernel<N><<<blocks, warps * 32, smem, st>>>(P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+template <int N>
+int shape_for(int nhr, long long total, LaunchShape* ls) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  int smem_max = 0, nsm = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const size_t hbytes = ((size_t)nhr * Dims<N>::HS * 4 + 15) / 16 * 16;
+  const size_t wb = warp_ws_bytes<N>();
+  if (hbytes + wb > (size_t)smem_max) return fail(CSD_ERR_UNSUPPORTED, "constraint set too large for shared memory");
+  int warps = (int)std::min<size_t>(Dims<N>::THREADS / 32, ((size_t)smem_max - hbytes) / wb);
+  ls->warps = warps;
+  ls->smem = hbytes + wb * warps;
+  long long need_blocks = (total + warps - 1) / warps;
+  ls->blocks = (int)std::max<long long>(1, std::min<long long>(nsm, need_blocks));
+  return 0;
+}
+
+int dispatch(int nsh, const SolveParams& P, cudaStream_t st, Workspace* ws) {
+  LaunchShape ls;
+  int rc = 0;
+  size_t wsz = 0;
+  switch (nsh) {
+#define CSD_CASE(NN)                                                    \
+  case NN:                                                              \
+    if ((rc = shape_for<NN>(P.nhr, P.total, &ls))) return rc;          \
+    wsz = Dims<NN>::WSZ;                                                \
+    break;
+    CSD_CASE(6) CSD_CASE(15) CSD_CASE(28) CSD_CASE(45) CSD_CASE(66) CSD_CASE(91)
+#undef CSD_CASE
+    default:
+      return fail(CSD_ERR_UNSUPPORTED, "unsupported nSH");
+  }
+  if ((rc = grow(&ws->fp64, &ws->fp64_doubles, (size_t)ls.blocks * ls.warps * wsz))) return rc;
+  SolveParams Q = P;
+  Q.fp64_scratch = ws->fp64;
+  switch (nsh) {
+#define CSD_CASE(NN) \
+  case NN: return launch_persistent<NN>(Q, ls.smem, ls.warps, ls.blocks, st);
+    CSD_CASE(6) CSD_CASE(15) CSD_CASE(28) CSD_CASE(45) CSD_CASE(66) CSD_CASE(91)
+#undef CSD_CASE
+  }
+  return 0;
+}
+
+}  // namespace
+
+static Scheme scheme_of(const csd_shared* s) {
+  Scheme sc;
+  sc.H32 = s->H32;
+  sc.H64 = s->H64;
+  sc.MtMp = s->MtMp;
+  sc.MtM64 = s->MtM64;
+  sc.rconvT = s->rconvT;
+  sc.M64 = s->M64;
+  sc.dwis = s->dwis;
+  sc.ndw = s->h.ndw;
+  sc.ninit = s->h.ninit;
+  sc.niter = s->h.niter;
+  sc.threshold = (float)s->h.threshold;
+  return sc;
+}
+
+static int g_refine = 1;  // one FP64-residual refinement step per solve
+
+extern "C" int csd_solve(const csd_shared* const* shared, const csd_volume* volumes, int n_volumes, void* stream) {
+  if (n_volumes < 0 || (n_volumes > 0 && (!shared || !volumes)))
+    return fail(CSD_ERR_INVALID, "csd_solve: invalid volume list");
+  if (n_volumes == 0) return CSD_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nsh = shared[0] ? shared[0]->h.nsh : 0;
+  const int nhr = shared[0] ? shared[0]->h.nhr : 0;
+  for (int i = 0; i < n_volumes; ++i) {
+    const csd_shared* s = shared[i];
+    const csd_volume& v = volumes[i];
+    if (!s) return fail(CSD_ERR_INVALID, "csd_solve: NULL shared");
+    if (s->h.nsh != nsh || s->h.nhr != nhr)
+      return fail(CSD_ERR_INVALID, "csd_solve: all volumes of one call must share nSH and the constraint set size");
+    if (v.n_voxels < 0) return fail(CSD_ERR_INVALID, "csd_solve: negative voxel count");
+    if (v.n_voxels > 0 && (!v.dwi || !v.fod)) return fail(CSD_ERR_INVALID, "csd_solve: NULL dwi or fod");
+    if (v.fod_stride < nsh) return fail(CSD_ERR_INVALID, "csd_solve: fod_stride smaller than nSH");
+    if (v.voxel_stride < 0 || v.volume_stride < 0) return fail(CSD_ERR_INVALID, "csd_solve: negative stride");
+  }
+  Workspace* ws = nullptr;
+  int rc = get_ws(stream, &ws);
+  if (rc) return rc;
+  for (int i = 0; i < n_volumes; ++i)
+    if ((rc = ensure_device(shared[i]))) return rc;
+  // group volumes by identical constraint tables; each group is one launch
+  std::vector<int> order(n_volumes);
+  std::vector<char> done(n_volumes, 0);
+  for (int i = 0; i < n_volumes; ++i) {
+    if (done[i]) continue;
+    std::vector<int> group;
+    for (int j = i; j < n_volumes; ++j)
+      if (!done[j] && (shared[j] == shared[i] || shared[j]->H32_host == shared[i]->H32_host)) {
+        group.push_back(j);
+        done[j] = 1;
+      }
+    for (size_t g0 = 0; g0 < group.size(); g0 += kMaxVolumesPerLaunch) {
+      const size_t g1 = std::min(group.size(), g0 + kMaxVolumesPerLaunch);
+      SolveParams P;
+      std::memset(&P, 0, sizeof(P));
+      P.nhr = nhr;
+      P.nw = (nhr + 31) / 32;
+      P.refine = g_refine;
+      P.cond_thr = (float)shared[group[g0]]->cond_thr;
+      long long total = 0;
+      int nv = 0;
+      for (size_t q = g0; q < g1; ++q) {
+        const int j = group[q];
+        const csd_volume& v = volumes[j];
+        if (v.n_voxels == 0) continue;
+        VolumeDesc& d = P.vol[nv++];
+        d.sc = scheme_of(shared[j]);
+        d.dwi = v.dwi;
+        d.n_voxels = v.n_voxels;
+        d.vox_stride = v.voxel_stride;
+        d.vol_stride = v.volume_stride;
+        d.first = total;
+        d.mask = v.mask;
+        d.warm = v.warm_negmask;
+        d.fod = v.fod;
+        d.fod_stride = v.fod_stride;
+        d.status = v.status;
+        d.iters = v.iterations;
+        d.negmask = v.negmask;
+        total += v.n_voxels;
+      }
+      if (nv == 0) continue;
+      P.n_vol = nv;
+      P.total = total;
+      P.queue = ws->queue;
+      CUDA_TRY(cudaMemsetAsync(ws->queue, 0, sizeof(unsigned long long), st));
+      if ((rc = dispatch(nsh, P, st, ws))) return rc;
+    }
+  }
+  return CSD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host-buffer entry point: slabs of voxels staged host -> device -> host with
+// copies on two streams overlapping the solve of the neighbouring slab.
+
+extern "C" int csd_dwi2fod_host(const csd_shared* s, const float* dwi, int64_t n_voxels, const uint8_t* mask,
+                                float* fod, uint8_t* status, uint8_t* iterations) {
+  if (!s || n_voxels < 0 || (n_voxels > 0 && (!dwi || !fod)))
+    return fail(CSD_ERR_INVALID, "csd_dwi2fod_host: invalid argument");
+  if (n_voxels == 0) return CSD_OK;
+  const int nvol = s->h.nvol, nsh = s->h.nsh;
+  Workspace* ws = nullptr;
+  int rc = get_ws(reinterpret_cast<void*>(1), &ws);  // private key for this entry point
+  if (rc) return rc;
+  if (!ws->streams[0]) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&ws->streams[0], cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&ws->streams[1], cudaStreamNonBlocking));
+  }
+  cudaStream_t* streams = ws->streams;
+  if ((rc = grow(&ws->d_dwi, &ws->d_dwi_n, (size_t)n_voxels * nvol))) return rc;
+  if ((rc = grow(&ws->d_fod, &ws->d_fod_n, (size_t)n_voxels * nsh))) return rc;
+  if ((rc = grow(&ws->d_small, &ws->d_small_n, (size_t)n_voxels * 3))) return rc;
+  uint8_t* d_mask = ws->d_small;
+  uint8_t* d_status = ws->d_small + n_voxels;
+  uint8_t* d_iters = ws->d_small + 2 * n_voxels;
+  const int64_t nslab = std::min<int64_t>(8, std::max<int64_t>(1, n_voxels / 65536));
+  const int64_t per = (n_voxels + nslab - 1) / nslab;
+  const csd_shared* sh[1] = {s};
+  for (int64_t k = 0; k < nslab; ++k) {
+    const int64_t a = k * per, n = std::min(per, n_voxels - a);
+    if (n <= 0) break;
+    cudaStream_t st = streams[k & 1];
+    CUDA_TRY(cudaMemcpyAsync(ws->d_dwi + a * nvol, dwi + a * nvol, (size_t)n * nvol * sizeof(float),
+                             cudaMemcpyHostToDevice, st));
+    if (mask) CUDA_TRY(cudaMemcpyAsync(d_mask + a, mask + a, (size_t)n, cudaMemcpyHostToDevice, st));
+    csd_volume v;
+    std::memset(&v, 0, sizeof(v));
+    v.dwi = ws->d_dwi + a * nvol;
+    v.n_voxels = n;
+    v.voxel_stride = nvol;
+    v.volume_stride = 1;
+    v.mask = mask ? d_mask + a : nullptr;
+    v.fod = ws->d_fod + a * nsh;
+    v.fod_stride = nsh;
+    v.status = status ? d_status + a : nullptr;
+    v.iterations = iterations ? d_iters + a : nullptr;
+    if ((rc = csd_solve(sh, &v, 1, st))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(fod + a * nsh, ws->d_fod + a * nsh, (size_t)n * nsh * sizeof(float),
+                             cudaMemcpyDeviceToHost, st));
+    if (status) CUDA_TRY(cudaMemcpyAsync(status + a, d_status + a, (size_t)n, cudaMemcpyDeviceToHost, st));
+    if (iterations) CUDA_TRY(cudaMemcpyAsync(iterations + a, d_iters + a, (size_t)n, cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(streams[0]));
+  CUDA_TRY(cudaStreamSynchronize(streams[1]));
+  return CSD_OK;
+}
+
+// test hook: enable/disable the refinement step (default on)
+extern "C" int csd_debug_set_refine(int on) {
+  g_refine = on ? 1 : 0;
+  return CSD_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// csd_state_*: per-step surface (CSD::set / iterate / FOD over a batch)
+
+struct csd_state {
+  const csd_shared* sh = nullptr;
+  int64_t cap = 0, n = 0, n_active = 0;
+  int use_warm = 0;
+  float* F = nullptr;
+  double* b = nullptr;
+  uint32_t* old = nullptr;
+  uint32_t* warm = nullptr;
+  uint8_t* status = nullptr;
+  uint16_t* iters = nullptr;
+  int* act[2] = {nullptr, nullptr};
+  int* counter = nullptr;
+  int cur = 0;
+  double* fp64 = nullptr;
+  int blocks = 0, warps = 0;
+  size_t smem = 0;
+};
+
+namespace {
+template <int N>
+int state_shape(csd_state* st) {
+  LaunchShape ls;
+  int rc = shape_for<N>(st->sh->h.nhr, 1LL << 40, &ls);
+  if (rc) return rc;
+  st->blocks = ls.blocks;
+  st->warps = ls.warps;
+  st->smem = ls.smem;
+  CUDA_TRY(cudaMalloc(&st->fp64, (size_t)ls.blocks * ls.warps * Dims<N>::WSZ * sizeof(double)));
+  CUDA_TRY(cudaFuncSetAttribute(csd_state_iterate_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem));
+  CUDA_TRY(cudaFuncSetAttribute(csd_state_set_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(8 * warp_ws_bytes<N>())));
+  return 0;
+}
+
+StateParams state_params(const csd_state* st) {
+  StateParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.sc = scheme_of(st->sh);
+  P.nhr = st->sh->h.nhr;
+  P.nw = (P.nhr + 31) / 32;
+  P.refine = g_refine;
+  P.cond_thr = (float)st->sh->cond_thr;
+  P.F = st->F;
+  P.b = st->b;
+  P.old = st->old;
+  P.warm = st->warm;
+  P.use_warm = st->use_warm;
+  P.status = st->status;
+  P.iters = st->iters;
+  P.n_out = st->counter;
+  P.fp64_scratch = st->fp64;
+  return P;
+}
+
+template <int N>
+int state_set_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  const int blocks = (int)std::min<long long>(4096, (P.n_in + 7) / 8);
+  csd_state_set_kernel<N><<<std::max(blocks, 1), 256, 8 * warp_ws_bytes<N>(), s>>>(P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+template <int N>
+int state_iter_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  const int need = (int)std::min<long long>(st->blocks, (P.n_in + st->warps - 1) / st->warps);
+  csd_state_iterate_kernel<N><<<std::max(need, 1), st->warps * 32, st->smem, s>>>(P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+template <int N>
+int state_fod_launch(const csd_state* st, float* fod, int64_t fs, uint8_t* so, uint8_t* io, uint32_t* no,
+                     cudaStream_t s) {
+  const long long tot = st->n * N;
+  if (tot == 0) return 0;
+  csd_state_fod_kernel<N><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(st->F, st->status, st->iters, st->old,
+                                                                        (st->sh->h.nhr + 31) / 32, st->n, fod, fs,
+                                                                        so, io, no);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+}  // namespace
+
+#define CSD_DISPATCH(nsh, CALL)                                                          \
+  switch (nsh) {                                                                         \
+    case 6: { constexpr int NN = 6; CALL; } break;                                       \
+    case 15: { constexpr int NN = 15; CALL; } break;                                     \
+    case 28: { constexpr int NN = 28; CALL; } break;                                     \
+    case 45: { constexpr int NN = 45; CALL; } break;                                     \
+    case 66: { constexpr int NN = 66; CALL; } break;                                     \
+    case 91: { constexpr int NN = 91; CALL; } break;                                     \
+    default: return fail(CSD_ERR_UNSUPPORTED, "unsupported nSH");                        \
+  }
+
+extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state** out) {
+  if (!s || !out || capacity <= 0 || capacity > (1LL << 31) - 1)
+    return fail(CSD_ERR_INVALID, "csd_state_create: invalid argument");
+  *out = nullptr;
+  int rc0 = ensure_device(s);
+  if (rc0) return rc0;
+  std::unique_ptr<csd_state> st(new csd_state);
+  st->sh = s;
+  st->cap = capacity;
+  const int n = s->h.nsh, nw = (s->h.nhr + 31) / 32, HS = s->HS;
+  CUDA_TRY(cudaMalloc(&st->F, (size_t)capacity * HS * sizeof(float)));
+  CUDA_TRY(cudaMalloc(&st->b, (size_t)capacity * n * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&st->old, (size_t)capacity * nw * sizeof(uint32_t)));
+  CUDA_TRY(cudaMalloc(&st->warm, (size_t)capacity * nw * sizeof(uint32_t)));
+  CUDA_TRY(cudaMalloc(&st->status, (size_t)capacity));
+  CUDA_TRY(cudaMalloc(&st->iters, (size_t)capacity * sizeof(uint16_t)));
+  CUDA_TRY(cudaMalloc(&st->act[0], (size_t)capacity * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&st->act[1], (size_t)capacity * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&st->counter, 2 * sizeof(int)));
+  int rc = 0;
+  CSD_DISPATCH(n, rc = state_shape<NN>(st.get()));
+  if (rc) return rc;
+  *out = st.release();
+  return CSD_OK;
+}
+
+extern "C" void csd_state_destroy(csd_state* st) {
+  if (!st) return;
+  cudaFree(st->F);
+  cudaFree(st->b);
+  cudaFree(st->old);
+  cudaFree(st->warm);
+  cudaFree(st->status);
+  cudaFree(st->iters);
+  cudaFree(st->act[0]);
+  cudaFree(st->act[1]);
+  cudaFree(st->counter);
+  cudaFree(st->fp64);
+  delete st;
+}
+
+extern "C" int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, int64_t voxel_stride,
+                             int64_t volume_stride, const uint8_t* mask, void* stream) {
+  if (!st || n_voxels < 0 || n_voxels > st->cap || (n_voxels > 0 && !dwi))
+    return fail(CSD_ERR_INVALID, "csd_state_set: invalid argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  st->n = n_voxels;
+  st->use_warm = 0;
+  st->cur = 0;
+  CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
+  if (n_voxels == 0) {
+    st->n_active = 0;
+    return CSD_OK;
+  }
+  StateParams P = state_params(st);
+  P.n_in = (int)n_voxels;
+  P.dwi = dwi;
+  P.vox_stride = voxel_stride;
+  P.vol_stride = volume_stride;
+  P.mask = mask;
+  P.act_out = st->act[0];
+  int rc = 0;
+  CSD_DISPATCH(st->sh->h.nsh, rc = state_set_launch<NN>(st, P, s));
+  if (rc) return rc;
+  int na = 0;
+  CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  st->n_active = na;
+  return CSD_OK;
+}
+
+extern "C" int csd_state_warm(csd_state* st, const uint32_t* negmask, void* stream) {
+  if (!st || !negmask) return fail(CSD_ERR_INVALID, "csd_state_warm: invalid argument");
+  const int nw = (st->sh->h.nhr + 31) / 32;
+  if (st->n > 0)
+    CUDA_TRY(cudaMemcpyAsync(st->warm, negmask, (size_t)st->n * nw * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                             static_cast<cudaStream_t>(stream)));
+  st->use_warm = 1;
+  return CSD_OK;
+}
+
+extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream) {
+  if (!st) return fail(CSD_ERR_INVALID, "csd_state_iterate: NULL state");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (st->n_active > 0) {
+    StateParams P = state_params(st);
+    P.n_in = (int)st->n_active;
+    P.act_in = st->act[st->cur];
+    P.act_out = st->act[st->cur ^ 1];
+    CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
+    int rc = 0;
+    CSD_DISPATCH(st->sh->h.nsh, rc = state_iter_launch<NN>(st, P, s));
+    if (rc) return rc;
+    int na = 0;
+    CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    st->n_active = na;
+    st->cur ^= 1;
+  }
+  if (n_active) *n_active = st->n_active;
+  return CSD_OK;
+}
+
+extern "C" int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride, uint8_t* status,
+                             uint8_t* iterations, uint32_t* negmask, void* stream) {
+  if (!st || !fod || fod_stride < st->sh->h.nsh) return fail(CSD_ERR_INVALID, "csd_state_fod: invalid argument");
+  int rc = 0;
+  CSD_DISPATCH(st->sh->h.nsh,
+               rc = state_fod_launch<NN>(st, fod, fod_stride, status, iterations, negmask,
+                                         static_cast<cudaStream_t>(stream)));
+  return rc;
+}
+
+#include "hr_dirs_builtin.inc"

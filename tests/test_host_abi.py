@@ -1,0 +1,108 @@
+"""CPU tests of the C ABI library: it loads, exports every declared symbol, and
+its host FP64 precompute (CSD::Shared::init, csd.h:117-198) equals the oracle.
+No device compute runs here."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from mrtrix3_b200 import csd, synth
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    syms = []
+    for f in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if f.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", f)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            syms += re.findall(r"^\s*(?:[\w\s\*]+?)\b(csd_\w+)\s*\(", txt, flags=re.M)
+    return sorted(set(syms))
+
+
+def test_library_exports_every_declared_symbol():
+    L = csd.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 16
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(csd.EXPORTED) <= set(syms)
+
+
+@pytest.mark.parametrize("lmax,ndw", [(0, 60), (8, 64), (10, 90), (6, 45), (12, 90), (2, 12)])
+def test_host_precompute_equals_oracle(hr_dirs, lmax, ndw):
+    v = synth.make_volume((2, 1, 1), 6, ndw, 30.0, 8, None, 5)
+    s = csd.make_shared(v.grad, synth.RESPONSE, lmax=lmax or None)
+    o = O.OracleShared(v.grad, synth.RESPONSE, hr_dirs, lmax=lmax)
+    assert (s.lmax, s.nSH(), s.n_init, s.n_dw, s.n_hr) == (o.lmax, o.n, o.nr, o.ndw, o.nhr)
+    assert np.array_equal(s.dwis, o.dwis)
+    for k in ("rconv", "M", "HR_trans", "Mt_M"):
+        a, b = getattr(s, k), getattr(o, k)
+        assert np.abs(a - b).max() <= 1e-14 * max(np.abs(b).max(), 1.0), k
+
+
+def test_options_pass_through(hr_dirs):
+    v = synth.make_volume((2, 1, 1), 6, 60, 30.0, 8, None, 5)
+    s = csd.Shared(v.grad)
+    s.parse_cmdline_options(lmax=[6], neg_lambda=0.5, norm_lambda=2.0, threshold=0.1, niter=7,
+                            filter=[1, 1, 0.5, 0.25])
+    s.set_response(synth.RESPONSE)
+    s.init()
+    o = O.OracleShared(v.grad, synth.RESPONSE, hr_dirs, lmax=6, neg_lambda=0.5, norm_lambda=2.0, threshold=0.1,
+                       niter=7, filter=np.array([1, 1, 0.5, 0.25]))
+    assert s.niter == 7 and s.lmax == 6
+    for k in ("rconv", "HR_trans", "Mt_M"):
+        assert np.abs(getattr(s, k) - getattr(o, k)).max() <= 1e-13 * np.abs(getattr(o, k)).max()
+
+
+def test_custom_directions(hr_dirs):
+    v = synth.make_volume((2, 1, 1), 6, 60, 30.0, 8, None, 5)
+    dirs = hr_dirs[:129].copy()
+    s = csd.make_shared(v.grad, synth.RESPONSE, directions=dirs)
+    o = O.OracleShared(v.grad, synth.RESPONSE, dirs)
+    assert s.n_hr == 129
+    assert np.abs(s.HR_trans - o.HR_trans).max() <= 1e-13 * np.abs(o.HR_trans).max()
+
+
+def test_response_file(tmp_path):
+    v = synth.make_volume((2, 1, 1), 6, 60, 30.0, 8, None, 5)
+    p = tmp_path / "response.txt"
+    p.write_text(" ".join(str(x) for x in synth.RESPONSE) + "\n")
+    s = csd.Shared(v.grad)
+    s.set_response(str(p))
+    s.init()
+    assert s.nSH() == 45
+
+
+def test_errors_follow_reference_messages():
+    g = synth.grad_table(2, synth.fibonacci_hemisphere(5))
+    with pytest.raises(csd.CSDError, match="too few directions"):
+        csd.make_shared(g, synth.RESPONSE)
+    g = synth.grad_table(2, synth.fibonacci_hemisphere(30))
+    with pytest.raises(csd.CSDError, match="anisotropic"):
+        csd.make_shared(g, synth.RESPONSE[:1])
+    with pytest.raises(csd.CSDError, match="positive even"):
+        csd.make_shared(g, synth.RESPONSE, lmax=5)
+    with pytest.raises(csd.CSDError, match="compiled maximum"):
+        csd.make_shared(g, synth.RESPONSE, lmax=14)
+    with pytest.raises(csd.CSDError, match="single lmax"):
+        s = csd.Shared(g)
+        s.parse_cmdline_options(lmax=[6, 8])
+    L = csd.lib()
+    assert L.csd_shared_nsh(None) == csd.lib().csd_shared_nsh(None) < 0
+
+
+def test_cpp_shim_compiles():
+    """The C++ drop-in header (CSD::Shared / CSD, csd.h:46-271) and the
+    dwi2fod-style example compile against the C ABI."""
+    ex = os.path.join(ROOT, "mrtrix3_b200", "csrc", "dwi2fod_csd_example.cpp")
+    if not os.path.exists(ex):
+        pytest.skip("C++ shim example not present")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I",
+                        os.path.join(ROOT, "mrtrix3_b200", "csrc"), ex], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -269,7 +269,9 @@ def main():
             "vs_baseline": None, "dtype": "fp32 (fp64 refinement residual)", "data": "synthetic",
             "config": workload_config(vol, args.method), "roofline": roofline, "e2e": e2e,
             "gpu_launches": args.steps, "clocks": clk.summary(),
-            "mean_iterations": float(iters[(status & 0x0F) == 1].mean())}
+            "mean_iterations": float(iters[(status & 0x0F) == 1].mean()),
+            "status_counts": {"converged": int(((status & 0x0F) == 1).sum()), "niter": int(((status & 0x0F) == 2).sum()),
+                              "fp64": int(((status & 0x10) != 0).sum()), "cholfail": int(((status & 0x20) != 0).sum())}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(vol)
     if rank == 0:

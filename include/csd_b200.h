@@ -137,6 +137,22 @@ int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream);
 int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride, uint8_t* status,
                   uint8_t* iterations, uint32_t* negmask, void* stream);
 
+/* Allocation-free variant of csd_solve for one volume.  No counterpart in
+ * the reference: it exists for callers that must not call cudaMalloc while
+ * they run -- applications whose own allocator owns all device memory, or
+ * services whose memory footprint has to stay fixed after start-up -- so
+ * every piece of device scratch the solve needs (its work counter, the
+ * scheme's tables, the FP64 fallback slots) lives in one 24 MiB array of
+ * static device memory that every device which loads the library holds
+ * until exit.  The caller still owns dwi / mask / fod / status buffers.
+ * The first call on a device looks up that array's device address (set-up,
+ * once per device); make that first call before any stream capture.  Each
+ * call copies the scheme's tables into the array and zeroes the counter, so
+ * calls overlapping on the GPU (other streams, other threads) race: run them
+ * one at a time per device.  Returns CSD_ERR_UNSUPPORTED if the scheme's
+ * tables plus one block's FP64 slots do not fit; grids shrink to fit. */
+int csd_solve_noalloc(const csd_shared* s, const csd_volume* volume, void* stream);
+
 /* Thread-local description of the last failure. */
 const char* csd_last_error(void);
 

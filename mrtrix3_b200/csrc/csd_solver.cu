@@ -932,4 +932,120 @@ extern "C" int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride
   return rc;
 }
 
+
+// ---------------------------------------------------------------------------
+// csd_solve_noalloc: the persistent solve with every piece of device scratch
+// (work counter, the scheme's tables, the FP64 fallback slots) carved from
+// one file-scope device array instead of cudaMalloc'd workspace.
+
+static constexpr size_t kNoAllocBytes = size_t(24) << 20;  // 24 MiB, held by every device that loads the library
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+static std::mutex g_noalloc_mu;
+static std::map<int, unsigned char*> g_noalloc_base;  // device -> device address of g_noalloc_scratch
+
+// Set-up, once per device with that device current: host code may not use
+// g_noalloc_scratch's name as an address, so ask the runtime for it.
+static int noalloc_base(unsigned char** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  auto it = g_noalloc_base.find(dev);
+  if (it == g_noalloc_base.end()) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(CSD_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") +
+                                    cudaGetErrorString(e));
+    it = g_noalloc_base.emplace(dev, static_cast<unsigned char*>(p)).first;
+  }
+  *out = it->second;
+  return 0;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <int N>
+static int noalloc_launch(const csd_shared* s, const csd_volume* v, cudaStream_t st, unsigned char* base) {
+  const HostShared& h = s->h;
+  // layout: [counter | H32 | H64 | MtMp | MtM64 | rconvT | M64 | dwis | FP64 slots]
+  size_t off = 256;
+  const size_t oH32 = off; off = align256(off + s->H32_host.size() * sizeof(float));
+  const size_t oH64 = off; off = align256(off + h.HR.size() * sizeof(double));
+  const size_t oMtMp = off; off = align256(off + s->MtMp_host.size() * sizeof(float));
+  const size_t oMtM64 = off; off = align256(off + h.MtM.size() * sizeof(double));
+  const size_t oRc = off; off = align256(off + s->rconvT_host.size() * sizeof(double));
+  const size_t oM = off; off = align256(off + h.M.size() * sizeof(double));
+  const size_t oDw = off; off = align256(off + h.dwis.size() * sizeof(int));
+  const size_t oSlots = off;
+  if (oSlots >= kNoAllocBytes)
+    return fail(CSD_ERR_UNSUPPORTED, "csd_solve_noalloc: the scheme's tables exceed the 24 MiB scratch");
+  LaunchShape ls;
+  int rc = shape_for<N>(h.nhr, v->n_voxels, &ls);
+  if (rc) return rc;
+  const size_t per_block = (size_t)ls.warps * Dims<N>::WSZ * sizeof(double);
+  const long long fit = (long long)((kNoAllocBytes - oSlots) / per_block);
+  if (fit < 1)
+    return fail(CSD_ERR_UNSUPPORTED, "csd_solve_noalloc: no room for one block's FP64 slots in the 24 MiB scratch");
+  const int blocks = (int)std::min<long long>(ls.blocks, fit);
+  CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemcpyAsync(base + oH32, s->H32_host.data(), s->H32_host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oH64, h.HR.data(), h.HR.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oMtMp, s->MtMp_host.data(), s->MtMp_host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oMtM64, h.MtM.data(), h.MtM.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oRc, s->rconvT_host.data(), s->rconvT_host.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oM, h.M.data(), h.M.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oDw, h.dwis.data(), h.dwis.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  SolveParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.n_vol = 1;
+  P.nhr = h.nhr;
+  P.nw = (h.nhr + 31) / 32;
+  P.refine = g_refine;
+  P.cond_thr = (float)s->cond_thr;
+  P.total = v->n_voxels;
+  P.queue = reinterpret_cast<unsigned long long*>(base);
+  P.fp64_scratch = reinterpret_cast<double*>(base + oSlots);
+  VolumeDesc& d = P.vol[0];
+  d.sc.H32 = reinterpret_cast<const float*>(base + oH32);
+  d.sc.H64 = reinterpret_cast<const double*>(base + oH64);
+  d.sc.MtMp = reinterpret_cast<const float*>(base + oMtMp);
+  d.sc.MtM64 = reinterpret_cast<const double*>(base + oMtM64);
+  d.sc.rconvT = reinterpret_cast<const double*>(base + oRc);
+  d.sc.M64 = reinterpret_cast<const double*>(base + oM);
+  d.sc.dwis = reinterpret_cast<const int*>(base + oDw);
+  d.sc.ndw = h.ndw;
+  d.sc.ninit = h.ninit;
+  d.sc.niter = h.niter;
+  d.sc.threshold = (float)h.threshold;
+  d.dwi = v->dwi;
+  d.n_voxels = v->n_voxels;
+  d.vox_stride = v->voxel_stride;
+  d.vol_stride = v->volume_stride;
+  d.first = 0;
+  d.mask = v->mask;
+  d.warm = v->warm_negmask;
+  d.fod = v->fod;
+  d.fod_stride = v->fod_stride;
+  d.status = v->status;
+  d.iters = v->iterations;
+  d.negmask = v->negmask;
+  return launch_persistent<N>(P, ls.smem, ls.warps, blocks, st);
+}
+
+extern "C" int csd_solve_noalloc(const csd_shared* s, const csd_volume* v, void* stream) {
+  if (!s || !v) return fail(CSD_ERR_INVALID, "csd_solve_noalloc: NULL argument");
+  if (v->n_voxels < 0) return fail(CSD_ERR_INVALID, "csd_solve_noalloc: negative voxel count");
+  if (v->n_voxels == 0) return CSD_OK;
+  if (!v->dwi || !v->fod) return fail(CSD_ERR_INVALID, "csd_solve_noalloc: NULL dwi or fod");
+  if (v->fod_stride < s->h.nsh) return fail(CSD_ERR_INVALID, "csd_solve_noalloc: fod_stride smaller than nSH");
+  if (v->voxel_stride < 0 || v->volume_stride < 0) return fail(CSD_ERR_INVALID, "csd_solve_noalloc: negative stride");
+  unsigned char* base = nullptr;
+  int rc = noalloc_base(&base);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CSD_DISPATCH(s->h.nsh, rc = noalloc_launch<NN>(s, v, st, base));
+  return rc;
+}
+
 #include "hr_dirs_builtin.inc"

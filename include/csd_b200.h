@@ -57,6 +57,10 @@ typedef struct csd_params {
   double bvalue_epsilon;    /* config BValueEpsilon, default 80 (dwi/shells.cpp:43-46) */
   double fp64_condition;    /* GPU only: condition estimate above which a voxel's
                                factorisation is redone in FP64 (default 1e6) */
+  int refine;               /* GPU only: one FP64-residual refinement step of the FP32
+                               solution -- 0 never, 1 after every solve, 2 once at the
+                               fixed point (then re-checked), 3 (default) only for voxels
+                               whose negative set cycles in FP32, after every solve */
 } csd_params;
 
 typedef struct csd_shared csd_shared;  /* immutable after creation, like CSD::Shared after init() */

@@ -15,12 +15,12 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
-LIB = os.path.join(HERE, "libcsd_b200.so")
+BUILD = os.environ.get("CSD_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("CSD_LIB_OUT", os.path.join(HERE, "libcsd_b200.so"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-           "-Xptxas", "-warn-spills"]
+           "-Xptxas", "-warn-spills"] + os.environ.get("CSD_EXTRA_NVFLAGS", "").split()
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall"]
 
 

@@ -43,7 +43,7 @@ class csd_params(ctypes.Structure):
                 ("norm_lambda", ctypes.c_double), ("threshold", ctypes.c_double),
                 ("filter", ctypes.POINTER(ctypes.c_double)), ("n_filter", ctypes.c_int),
                 ("bzero_threshold", ctypes.c_double), ("bvalue_epsilon", ctypes.c_double),
-                ("fp64_condition", ctypes.c_double)]
+                ("fp64_condition", ctypes.c_double), ("refine", ctypes.c_int)]
 
 
 class csd_volume(ctypes.Structure):
@@ -131,6 +131,7 @@ class Shared:
         self.bzero_threshold = 10.0
         self.bvalue_epsilon = 80.0
         self.fp64_condition = 1e6
+        self.refine = 3
         self._h = None
 
     def parse_cmdline_options(self, lmax=None, filter=None, directions=None, neg_lambda=None,
@@ -176,6 +177,7 @@ class Shared:
         p.bzero_threshold = self.bzero_threshold
         p.bvalue_epsilon = self.bvalue_epsilon
         p.fp64_condition = self.fp64_condition
+        p.refine = self.refine
         h = ctypes.c_void_p()
         hr = self.HR_dirs
         check(lib().csd_shared_create(ctypes.byref(p), _dp(self.grad), self.grad.shape[0], _dp(self.response),

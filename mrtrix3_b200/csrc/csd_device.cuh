@@ -7,16 +7,41 @@
 //   compare  stop when neg equals the previous set              (csd.h:252-253)
 //   assemble W = Mt_M + HR_trans[neg]^T HR_trans[neg]           (csd.h:255-262)
 //   solve    F = W^-1 b by Cholesky                             (csd.h:264)
-// Numerics: projection, assembly, factorisation and substitutions in FP32;
-// one refinement step whose residual b - W F is accumulated in FP64; a
-// factorisation is redone in FP64 when its pivots fail or the condition
-// estimate (max L_ii / min L_ii)^2 exceeds a threshold.
+// Numerics:
+//   * projection in FP32 (FP32 HR_trans, or its FP16 hi+lo pair re-summed);
+//   * the rank-k assembly on the tensor cores with mma.sync m16n8k16: HR_trans
+//     is split into FP16 hi + lo (22 significant bits) and W accumulates
+//     hi*hi + hi*lo + lo*hi in FP32; the gathered rows are read straight from
+//     the shared-memory table by ldmatrix row addresses (no gather copy);
+//   * Cholesky and substitutions in FP32;
+//   * one refinement step whose residual b - W F is accumulated in FP64
+//     against the FP32 operator -- applied once the negative set repeats
+//     (the fixed-point check is then repeated on the refined F), or after
+//     every solve, or never, or (the default) after every solve of a voxel
+//     whose negative set has come back after one step, i.e. cycles in FP32
+//     (SolveParams::refine = 2 / 1 / 0 / 3);
+//   * a factorisation is redone in FP64 when a pivot fails or the condition
+//     estimate (max L_ii / min L_ii)^2 exceeds a threshold.
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace csdb200 {
+
+// Optional per-phase cycle counters (build with -DCSD_PHASE_TIMERS): each
+// warp accumulates clock64() deltas per phase and adds them to
+// g_phase_cycles at the end of the launch.  Off in the normal build.
+#ifdef CSD_PHASE_TIMERS
+__device__ unsigned long long g_phase_cycles[16];
+#define CSD_T0(var) long long var = clock64()
+#define CSD_T1(acc, idx, var) acc[idx] += clock64() - var
+#else
+#define CSD_T0(var)
+#define CSD_T1(acc, idx, var)
+#endif
+enum Phase { kPhSet = 0, kPhProject, kPhAssemble, kPhChol, kPhSubst, kPhRefine, kPhFp64, kPhList, kPhTotal };
 
 constexpr int kMaxHR = 512;          // constraint directions supported
 constexpr int kMaxDW = 512;          // DW volumes in the selected shell supported
@@ -28,22 +53,27 @@ constexpr int kMaxVolumesPerLaunch = 48;
 __host__ __device__ constexpr int packoff(int i) {
   return 4 * (i + 2 * (i >> 2) * ((i >> 2) - 1) + (i & 3) * (i >> 2));
 }
-// Row stride of the constraint matrix in shared memory: a multiple of 4 whose
-// float4 count is odd, so lanes reading different rows hit distinct banks.
+// Row stride of the FP32 constraint matrix in shared memory: a multiple of 4
+// whose float4 count is odd, so lanes reading different rows hit distinct banks.
 __host__ __device__ constexpr int hr_stride(int n) {
   return (((n + 3) / 4) % 2 == 1) ? ((n + 3) / 4) * 4 : ((n + 3) / 4 + 1) * 4;
+}
+// Row stride (halves) of the FP16 hi/lo tables: covers 16-column blocks and
+// has an odd number of 16-byte chunks (spreads ldmatrix rows over banks).
+__host__ __device__ constexpr int hr_stride16(int n) {
+  return ((((n + 15) / 16) * 16 / 8) % 2 == 1) ? ((n + 15) / 16) * 16 : ((n + 15) / 16) * 16 + 8;
 }
 
 template <int N>
 struct Dims {
   static constexpr int CQ = (N + 31) / 32;        // coefficient slots per lane
-  static constexpr int HS = hr_stride(N);         // HR row stride (floats)
+  static constexpr int HS = hr_stride(N);         // FP32 HR row stride (floats)
+  static constexpr int HS16 = hr_stride16(N);     // FP16 HR row stride (halves)
+  static constexpr int NQ = (N + 3) / 4;          // float4 quads per row
   static constexpr int WSZ = packoff(N);          // packed W size (floats)
-  static constexpr int NB = (N + 3) / 4;          // 4-row blocks
-  static constexpr int NBLK = NB * (NB + 1) / 2;  // lower-triangle blocks
-  static constexpr int BPL = (NBLK + 31) / 32;    // blocks per lane
-  static constexpr int GROUP = 3;                 // blocks accumulated per pass
-  static constexpr int PASSES = (BPL + GROUP - 1) / GROUP;
+  static constexpr int NRB = (N + 15) / 16;       // 16-row blocks of W
+  static constexpr int NJB = (N + 7) / 8;         // 8-column blocks of W
+  static constexpr bool KEEP32 = N <= 45;         // FP32 HR table kept in shared memory
   // threads per block of the persistent kernel (bounds the register budget)
   static constexpr int THREADS = N <= 45 ? 512 : (N <= 66 ? 384 : 192);
 };
@@ -51,11 +81,12 @@ struct Dims {
 // Everything a voxel of one image needs, by device pointer.
 struct Scheme {
   const float* H32;       // [nhr][HS] HR_trans, fp32, zero padded
+  const __half* H16;      // [2][nhr+1][HS16] HR_trans hi then lo, fp16, row nhr = 0
   const double* H64;      // [nhr][nsh] HR_trans, fp64 (FP64 fallback)
   const float* MtMp;      // packed-padded lower Mt_M, fp32
   const double* MtM64;    // [nsh][nsh] full Mt_M, fp64 (refinement residual)
-  const double* rconvT;   // [ndw][ninit] rconv^T, fp64
-  const double* M64;      // [ndw][nsh] M, fp64
+  const float* rconvT;    // [ndw][ninit] rconv^T, fp32
+  const float* M32;       // [ndw][nsh] M, fp32
   const int* dwis;        // [ndw]
   int ndw, ninit, niter;
   float threshold;
@@ -83,23 +114,95 @@ struct SolveParams {
   VolumeDesc vol[kMaxVolumesPerLaunch];
 };
 
+// Bytes of the constraint tables a block keeps in shared memory.
+template <int N>
+__host__ __device__ constexpr int htab_bytes_32(int nhr) {
+  return Dims<N>::KEEP32 ? ((nhr * Dims<N>::HS * 4 + 15) / 16) * 16 : 0;
+}
+template <int N>
+__host__ __device__ constexpr int htab_bytes(int nhr) {
+  return htab_bytes_32<N>(nhr) + 2 * (nhr + 1) * Dims<N>::HS16 * 2;
+}
+
+// Shared-memory view of the constraint tables.
+template <int N>
+struct HTab {
+  const float* h32;   // [nhr][HS] (KEEP32 only)
+  const __half* hh;   // [nhr+1][HS16]
+  const __half* hl;   // [nhr+1][HS16]
+  int nhr;
+
+  // FP32 values of row d, columns 4j..4j+3
+  __device__ __forceinline__ float4 quad(int d, int j) const {
+    if constexpr (Dims<N>::KEEP32) {
+      return reinterpret_cast<const float4*>(h32 + d * Dims<N>::HS)[j];
+    } else {
+      const uint2 a = *reinterpret_cast<const uint2*>(hh + d * Dims<N>::HS16 + 4 * j);
+      const uint2 b = *reinterpret_cast<const uint2*>(hl + d * Dims<N>::HS16 + 4 * j);
+      const float2 a0 = __half22float2(*reinterpret_cast<const __half2*>(&a.x));
+      const float2 a1 = __half22float2(*reinterpret_cast<const __half2*>(&a.y));
+      const float2 b0 = __half22float2(*reinterpret_cast<const __half2*>(&b.x));
+      const float2 b1 = __half22float2(*reinterpret_cast<const __half2*>(&b.y));
+      return make_float4(a0.x + b0.x, a0.y + b0.y, a1.x + b1.x, a1.y + b1.y);
+    }
+  }
+  __device__ __forceinline__ float val(int d, int i) const {
+    if constexpr (Dims<N>::KEEP32) {
+      return h32[d * Dims<N>::HS + i];
+    } else {
+      return __half2float(hh[d * Dims<N>::HS16 + i]) + __half2float(hl[d * Dims<N>::HS16 + i]);
+    }
+  }
+};
+
+// Copy a scheme's constraint tables into shared memory (whole block).
+template <int N>
+__device__ HTab<N> load_htab(unsigned char* smem, const Scheme& sc, int nhr) {
+  HTab<N> t;
+  t.nhr = nhr;
+  const int b32 = htab_bytes_32<N>(nhr);
+  t.h32 = reinterpret_cast<const float*>(smem);
+  if constexpr (Dims<N>::KEEP32) {
+    const float4* src = reinterpret_cast<const float4*>(sc.H32);
+    float4* dst = reinterpret_cast<float4*>(smem);
+    for (int i = threadIdx.x; i < nhr * Dims<N>::HS / 4; i += blockDim.x) dst[i] = __ldg(src + i);
+  }
+  const int n16 = 2 * (nhr + 1) * Dims<N>::HS16;  // halves, a multiple of 8
+  const uint4* src = reinterpret_cast<const uint4*>(sc.H16);
+  uint4* dst = reinterpret_cast<uint4*>(smem + b32);
+  for (int i = threadIdx.x; i < n16 / 8; i += blockDim.x) dst[i] = __ldg(src + i);
+  t.hh = reinterpret_cast<const __half*>(smem + b32);
+  t.hl = t.hh + (nhr + 1) * Dims<N>::HS16;
+  return t;
+}
+
 // Per-warp shared-memory workspace (carved from dynamic shared memory).
 template <int N>
 __host__ __device__ constexpr int wbuf_floats() {
-  return Dims<N>::WSZ > kMaxDW ? Dims<N>::WSZ : kMaxDW;
+  // packed W plus one appended row (the right-hand side during factorisation)
+  return packoff(N + 1) > kMaxDW ? packoff(N + 1) : kMaxDW;
 }
 
 template <int N>
 struct WarpWS {
-  float* W;        // [WSZ] packed W / L (also holds S during set)
+  float* W;        // packed W / L (also holds S during set)
   float* F;        // [HS] current F (fp32)
+  float* rdiag;    // [N] 1 / L_ii
   double* b;       // [N] M^T S (fp64)
   uint16_t* neg;   // [kMaxHR] negative-set index list
+  uint32_t* old;   // [kMaxWords] negative set of the last solve (bitmask)
+  uint32_t* old2;  // [kMaxWords] negative set of the solve before
 };
 
 template <int N>
+__host__ __device__ constexpr int rdiag_bytes() {
+  return ((N * 4 + 15) / 16) * 16;
+}
+
+template <int N>
 __host__ __device__ constexpr int warp_ws_bytes() {
-  return wbuf_floats<N>() * 4 + Dims<N>::HS * 4 + ((N * 8 + 15) / 16) * 16 + kMaxHR * 2;
+  return wbuf_floats<N>() * 4 + Dims<N>::HS * 4 + rdiag_bytes<N>() + ((N * 8 + 15) / 16) * 16 + kMaxHR * 2 +
+         2 * kMaxWords * 4;
 }
 
 template <int N>
@@ -107,8 +210,11 @@ __device__ __forceinline__ WarpWS<N> carve_ws(unsigned char* base) {
   WarpWS<N> w;
   w.W = reinterpret_cast<float*>(base);
   w.F = w.W + wbuf_floats<N>();
-  w.b = reinterpret_cast<double*>(w.F + Dims<N>::HS);
+  w.rdiag = w.F + Dims<N>::HS;
+  w.b = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(w.rdiag) + rdiag_bytes<N>());
   w.neg = reinterpret_cast<uint16_t*>(reinterpret_cast<unsigned char*>(w.b) + ((N * 8 + 15) / 16) * 16);
+  w.old = reinterpret_cast<uint32_t*>(w.neg + kMaxHR);
+  w.old2 = w.old + kMaxWords;
   return w;
 }
 
@@ -118,8 +224,9 @@ __device__ __forceinline__ double shfl_d(double v, int src) {
 
 // ---------------------------------------------------------------------------
 // set(): load + clamp the voxel's DW samples (dwi2fod.cpp:156-173), then
-// F = [rconv S; 0] and b = M^T S (csd.h:237-243), both accumulated in FP64.
-// Returns 0 = ok, 1 = masked out, 3 = non-finite sample.
+// F = [rconv S; 0] and b = M^T S (csd.h:237-243) in FP32 (b kept as double
+// for the refinement residual).  Returns 0 = ok, 1 = masked out, 3 =
+// non-finite sample.
 template <int N>
 __device__ int voxel_set(const Scheme& sc, const float* dwi, long long vol_stride, bool masked,
                          const WarpWS<N>& w, int lane) {
@@ -132,20 +239,37 @@ __device__ int voxel_set(const Scheme& sc, const float* dwi, long long vol_strid
     S[t] = v < 0.f ? 0.f : v;
   }
   if (__any_sync(0xffffffffu, bad)) return 3;
+  const int nd4 = sc.ndw & ~3;
   __syncwarp();
 #pragma unroll
   for (int q = 0; q < Dims<N>::CQ; ++q) {
     const int c = lane + 32 * q;
-    double f = 0.0, bb = 0.0;
+    float f0 = 0.f, f1 = 0.f, b0 = 0.f, b1 = 0.f;
     if (c < N) {
-      for (int t = 0; t < sc.ndw; ++t) {
-        const double s = (double)S[t];
-        if (c < sc.ninit) f = fma(__ldg(sc.rconvT + (long long)t * sc.ninit + c), s, f);
-        bb = fma(__ldg(sc.M64 + (long long)t * N + c), s, bb);
+      const bool hasf = c < sc.ninit;
+      const float* rc = sc.rconvT + c;
+      const float* mc = sc.M32 + c;
+      int t = 0;
+      for (; t < nd4; t += 4) {
+        const float4 s4 = *reinterpret_cast<const float4*>(S + t);
+        if (hasf) {
+          f0 = fmaf(__ldg(rc + (long long)t * sc.ninit), s4.x, f0);
+          f1 = fmaf(__ldg(rc + (long long)(t + 1) * sc.ninit), s4.y, f1);
+          f0 = fmaf(__ldg(rc + (long long)(t + 2) * sc.ninit), s4.z, f0);
+          f1 = fmaf(__ldg(rc + (long long)(t + 3) * sc.ninit), s4.w, f1);
+        }
+        b0 = fmaf(__ldg(mc + (long long)t * N), s4.x, b0);
+        b1 = fmaf(__ldg(mc + (long long)(t + 1) * N), s4.y, b1);
+        b0 = fmaf(__ldg(mc + (long long)(t + 2) * N), s4.z, b0);
+        b1 = fmaf(__ldg(mc + (long long)(t + 3) * N), s4.w, b1);
       }
-      w.b[c] = bb;
+      for (; t < sc.ndw; ++t) {
+        if (hasf) f0 = fmaf(__ldg(rc + (long long)t * sc.ninit), S[t], f0);
+        b0 = fmaf(__ldg(mc + (long long)t * N), S[t], b0);
+      }
+      w.b[c] = (double)(b0 + b1);
     }
-    if (c < Dims<N>::HS) w.F[c] = (c < N) ? (float)f : 0.f;
+    if (c < Dims<N>::HS) w.F[c] = (c < N) ? (f0 + f1) : 0.f;
   }
   for (int c = lane + 32 * Dims<N>::CQ; c < Dims<N>::HS; c += 32) w.F[c] = 0.f;
   __syncwarp();
@@ -154,24 +278,24 @@ __device__ int voxel_set(const Scheme& sc, const float* dwi, long long vol_strid
 
 // ---------------------------------------------------------------------------
 // Projection onto the constraint directions and the negative-set bitmask
-// (csd.h:246-250).  Lane l evaluates directions l, l+32, ...; the F vector is
-// read as broadcast float4s, HR rows as float4s (conflict-free stride).
+// (csd.h:246-250).  Lane l evaluates directions l, l+32, ...; F is read as
+// broadcast float4s.
 template <int N>
-__device__ __forceinline__ void project_mask(const float* Hs, int nhr, int nw, float thr,
-                                             const WarpWS<N>& w, int lane, uint32_t* bits) {
-  constexpr int HS = Dims<N>::HS;
+__device__ __forceinline__ void project_mask(const HTab<N>& H, int nw, float thr, const WarpWS<N>& w, int lane,
+                                             uint32_t* bits) {
+  const int nhr = H.nhr;
   float acc[kMaxWords];
 #pragma unroll
   for (int p = 0; p < kMaxWords; ++p) acc[p] = 0.f;
 #pragma unroll 4
-  for (int j = 0; j < HS / 4; ++j) {
+  for (int j = 0; j < Dims<N>::NQ; ++j) {
     const float4 f4 = reinterpret_cast<const float4*>(w.F)[j];
 #pragma unroll
     for (int p = 0; p < kMaxWords; ++p) {
       if (p < nw) {
         const int d = lane + 32 * p;
         if (d < nhr) {
-          const float4 h4 = reinterpret_cast<const float4*>(Hs + d * HS)[j];
+          const float4 h4 = H.quad(d, j);
           acc[p] = fmaf(h4.x, f4.x, acc[p]);
           acc[p] = fmaf(h4.y, f4.y, acc[p]);
           acc[p] = fmaf(h4.z, f4.z, acc[p]);
@@ -206,78 +330,113 @@ __device__ __forceinline__ int mask_to_list(const uint32_t* bits, int nw, uint16
 }
 
 // ---------------------------------------------------------------------------
-// W = Mt_M + sum_{d in neg} h_d h_d^T, lower triangle (csd.h:255-262).
-// Each lane owns up to 3 4x4 blocks of the lower triangle per pass and keeps
-// them in registers while streaming over the gathered rows.
-template <int N>
-__device__ void assemble(const float* Hs, const float* MtMp, int k, const WarpWS<N>& w, int lane) {
+// Tensor-core rank-k assembly: W = Mt_M + G^T G, G = HR_trans rows in neg
+// (csd.h:255-262).  As a GEMM, A = G^T (N x k) and B = G (k x N); both
+// fragments of m16n8k16 come from ldmatrix.trans on 8x8 blocks of G, whose
+// rows are the table rows neg[q] -- each lane hands ldmatrix one row
+// address, so the gather costs nothing.  Only the lower triangle's tiles
+// are computed: row block ib (16 rows) x column block jb (8 columns),
+// jb <= 2 ib + 1.  Row blocks [IB0, IB1) are accumulated in this pass.
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const __half* p) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
+__device__ __forceinline__ void mma_f16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int N, int IB0, int IB1>
+__device__ __forceinline__ void assemble_pass(const HTab<N>& H, const float* MtMp, int k, const WarpWS<N>& w,
+                                              int lane) {
   using D = Dims<N>;
+  constexpr int NJ = 2 * IB1 < D::NJB ? 2 * IB1 : D::NJB;  // column blocks touched
+  float acc[IB1 - IB0][NJ][4];
+#pragma unroll
+  for (int a = 0; a < IB1 - IB0; ++a)
+#pragma unroll
+    for (int c = 0; c < NJ; ++c)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[a][c][e] = 0.f;
+  const int qsel = (lane & 7) + 8 * (lane >> 4);
+  const int csel = 8 * ((lane >> 3) & 1);
 #pragma unroll 1
-  for (int pass = 0; pass < D::PASSES; ++pass) {
-    int bi[D::GROUP], bj[D::GROUP];
-    bool valid[D::GROUP];
-    float acc[D::GROUP][16];
+  for (int k0 = 0; k0 < k; k0 += 16) {
+    const int q = k0 + qsel;
+    const int d = q < k ? (int)w.neg[q] : H.nhr;  // row nhr of the tables is zero
+    const __half* ph = H.hh + d * D::HS16 + csel;
+    const __half* pl = H.hl + d * D::HS16 + csel;
+    uint32_t ah[IB1][4], al[IB1][4];
 #pragma unroll
-    for (int g = 0; g < D::GROUP; ++g) {
-      const int b = lane + 32 * (pass * D::GROUP + g);
-      valid[g] = b < D::NBLK;
-      // invert b = bi (bi + 1) / 2 + bj
-      int r = (int)((sqrtf(8.f * (float)b + 1.f) - 1.f) * 0.5f);
-      while ((r + 1) * (r + 2) / 2 <= b) ++r;
-      while (r * (r + 1) / 2 > b) --r;
-      bi[g] = valid[g] ? r : 0;
-      bj[g] = valid[g] ? b - r * (r + 1) / 2 : 0;
-#pragma unroll
-      for (int e = 0; e < 16; ++e) acc[g][e] = 0.f;
+    for (int b = 0; b < IB1; ++b) {
+      ldsm_x4_trans(ah[b], ph + 16 * b);
+      ldsm_x4_trans(al[b], pl + 16 * b);
     }
-#pragma unroll 2
-    for (int q = 0; q < k; ++q) {
-      const float4* h = reinterpret_cast<const float4*>(Hs + (int)w.neg[q] * D::HS);
 #pragma unroll
-      for (int g = 0; g < D::GROUP; ++g) {
-        if (valid[g]) {
-          const float4 a = h[bi[g]];
-          const float4 c = h[bj[g]];
-          const float av[4] = {a.x, a.y, a.z, a.w};
-          const float cv[4] = {c.x, c.y, c.z, c.w};
+    for (int ib = IB0; ib < IB1; ++ib) {
 #pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int s = 0; s < 4; ++s) acc[g][r * 4 + s] = fmaf(av[r], cv[s], acc[g][r * 4 + s]);
+      for (int jb = 0; jb < NJ; ++jb) {
+        if (jb <= 2 * ib + 1) {
+          const int bb = jb >> 1, hs = jb & 1;
+          mma_f16(acc[ib - IB0][jb], ah[ib], ah[bb][hs], ah[bb][2 + hs]);
+          mma_f16(acc[ib - IB0][jb], ah[ib], al[bb][hs], al[bb][2 + hs]);
+          mma_f16(acc[ib - IB0][jb], al[ib], ah[bb][hs], ah[bb][2 + hs]);
         }
       }
     }
+  }
+  const int gid = lane >> 2, tig = lane & 3;
 #pragma unroll
-    for (int g = 0; g < D::GROUP; ++g) {
-      if (valid[g]) {
+  for (int ib = IB0; ib < IB1; ++ib) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int i = 4 * bi[g] + r;
+    for (int jb = 0; jb < NJ; ++jb) {
+      if (jb <= 2 * ib + 1) {
 #pragma unroll
-          for (int s = 0; s < 4; ++s) {
-            const int j = 4 * bj[g] + s;
+        for (int r = 0; r < 2; ++r) {
+          const int i = 16 * ib + gid + 8 * r;
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const int j = 8 * jb + 2 * tig + c;
             if (i < N && j <= i) {
               const int o = packoff(i) + j;
-              w.W[o] = __ldg(MtMp + o) + acc[g][r * 4 + s];
+              w.W[o] = __ldg(MtMp + o) + acc[ib - IB0][jb][2 * r + c];
             }
           }
         }
       }
     }
   }
+}
+
+template <int N>
+__device__ void assemble(const HTab<N>& H, const float* MtMp, int k, const WarpWS<N>& w, int lane) {
+  constexpr int R = Dims<N>::NRB;
+  if constexpr (R <= 3) {
+    assemble_pass<N, 0, R>(H, MtMp, k, w, lane);
+  } else if constexpr (R <= 5) {
+    assemble_pass<N, 0, 3>(H, MtMp, k, w, lane);
+    assemble_pass<N, 3, R>(H, MtMp, k, w, lane);
+  } else {
+    assemble_pass<N, 0, 3>(H, MtMp, k, w, lane);
+    assemble_pass<N, 3, 5>(H, MtMp, k, w, lane);
+    assemble_pass<N, 5, R>(H, MtMp, k, w, lane);
+  }
   __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
 // In-place left-looking Cholesky of the packed-padded lower matrix A (shared
-// or global memory).  Lane l computes rows j+l, j+l+32, ... of column j.
-// Returns false if a pivot is not positive; dmin/dmax receive the range of
-// the diagonal of L.
+// or global memory), FP64 version for the fallback.  Lane l computes rows
+// j+l, j+l+32, ... of column j.  Returns false if a pivot is not positive.
 template <int N, typename T>
-__device__ bool cholesky_packed(T* A, int lane, T& dmin, T& dmax) {
-  dmin = (T)1.0e300;
-  dmax = (T)0;
-  bool ok = true;
+__device__ bool cholesky_packed(T* A, int lane) {
 #pragma unroll 1
   for (int j = 0; j < N; ++j) {
     const T* Lj = A + packoff(j);
@@ -294,59 +453,8 @@ __device__ bool cholesky_packed(T* A, int lane, T& dmin, T& dmax) {
       }
     }
     const T djj = __shfl_sync(0xffffffffu, s[0], 0);
-    if (!(djj > (T)0)) {
-      ok = false;
-      break;
-    }
+    if (!(djj > (T)0)) return false;
     const T d = sqrt(djj);
-    dmin = d < dmin ? d : dmin;
-    dmax = d > dmax ? d : dmax;
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < Dims<N>::CQ; ++q) {
-      const int i = j + lane + 32 * q;
-      if (i < N) A[packoff(i) + j] = (i == j) ? d : s[q] / d;
-    }
-    __syncwarp();
-  }
-  __syncwarp();
-  return ok;
-}
-
-// float specialisation with float4 row reads for the dot products
-template <int N>
-__device__ bool cholesky_packed_f32(float* A, int lane, float& dmin, float& dmax) {
-  dmin = 3.0e38f;
-  dmax = 0.f;
-#pragma unroll 1
-  for (int j = 0; j < N; ++j) {
-    const float* Lj = A + packoff(j);
-    const int j4 = j & ~3;
-    float s[Dims<N>::CQ];
-#pragma unroll
-    for (int q = 0; q < Dims<N>::CQ; ++q) {
-      const int i = j + lane + 32 * q;
-      s[q] = 0.f;
-      if (i < N) {
-        const float* Li = A + packoff(i);
-        float a0 = 0.f, a1 = 0.f;
-        for (int kk = 0; kk < j4; kk += 4) {
-          const float4 x = *reinterpret_cast<const float4*>(Li + kk);
-          const float4 y = *reinterpret_cast<const float4*>(Lj + kk);
-          a0 = fmaf(x.x, y.x, a0);
-          a1 = fmaf(x.y, y.y, a1);
-          a0 = fmaf(x.z, y.z, a0);
-          a1 = fmaf(x.w, y.w, a1);
-        }
-        for (int kk = j4; kk < j; ++kk) a0 = fmaf(Li[kk], Lj[kk], a0);
-        s[q] = Li[j] - (a0 + a1);
-      }
-    }
-    const float djj = __shfl_sync(0xffffffffu, s[0], 0);
-    if (!(djj > 0.f) || !isfinite(djj)) return false;
-    const float d = sqrtf(djj);
-    dmin = fminf(dmin, d);
-    dmax = fmaxf(dmax, d);
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < Dims<N>::CQ; ++q) {
@@ -358,50 +466,301 @@ __device__ bool cholesky_packed_f32(float* A, int lane, float& dmin, float& dmax
   return true;
 }
 
-// x := L^-T L^-1 x with x distributed as x[q] = element lane + 32 q.
-template <int N, typename T, typename LT>
-__device__ __forceinline__ void chol_subst(const LT* L, T* x, int lane) {
-  // forward: column sweep
+// FP32 version, blocked by 4 columns: for column block [j0, j0+4) every
+// active row i >= j0 (lane i - j0 + 32 q) forms s_c = A[i][j0+c] -
+// L[i][0:j0] . L[j0+c][0:j0] with one float4 of its own row against four
+// broadcast float4s per step; the 4x4 diagonal block is then factored by
+// every lane from shuffled values, and the rows below divide through it.
+// Stores 1/L_jj in rdiag; dmin/dmax receive the range of diag(L).
+template <int N>
+__device__ bool cholesky_packed_f32(float* A, float* rdiag, int lane, float& dmin, float& dmax) {
+  dmin = 3.0e38f;
+  dmax = 0.f;
+  constexpr int NB = (N + 3) / 4;
+#pragma unroll 1
+  for (int cb = 0; cb < NB; ++cb) {
+    const int j0 = 4 * cb;
+    const float* Lj0 = A + packoff(j0);
+    const float* Lj1 = A + packoff(j0 + 1);
+    const float* Lj2 = A + packoff(j0 + 2);
+    const float* Lj3 = A + packoff(j0 + 3);
+    float s[Dims<N>::CQ][4];
+#pragma unroll
+    for (int q = 0; q < Dims<N>::CQ; ++q) {
+      const int i = j0 + lane + 32 * q;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s[q][c] = 0.f;
+      if (i <= N) {  // row N is the appended right-hand side
+        const float* Li = A + packoff(i);
+        const float4 w4 = *reinterpret_cast<const float4*>(Li + j0);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
+        for (int kk = 0; kk < j0; kk += 4) {
+          const float4 x = *reinterpret_cast<const float4*>(Li + kk);
+          const float4 y0 = *reinterpret_cast<const float4*>(Lj0 + kk);
+          const float4 y1 = *reinterpret_cast<const float4*>(Lj1 + kk);
+          const float4 y2 = *reinterpret_cast<const float4*>(Lj2 + kk);
+          const float4 y3 = *reinterpret_cast<const float4*>(Lj3 + kk);
+          a0 = fmaf(x.x, y0.x, a0); b0 = fmaf(x.y, y0.y, b0); a0 = fmaf(x.z, y0.z, a0); b0 = fmaf(x.w, y0.w, b0);
+          a1 = fmaf(x.x, y1.x, a1); b1 = fmaf(x.y, y1.y, b1); a1 = fmaf(x.z, y1.z, a1); b1 = fmaf(x.w, y1.w, b1);
+          a2 = fmaf(x.x, y2.x, a2); b2 = fmaf(x.y, y2.y, b2); a2 = fmaf(x.z, y2.z, a2); b2 = fmaf(x.w, y2.w, b2);
+          a3 = fmaf(x.x, y3.x, a3); b3 = fmaf(x.y, y3.y, b3); a3 = fmaf(x.z, y3.z, a3); b3 = fmaf(x.w, y3.w, b3);
+        }
+        s[q][0] = w4.x - (a0 + b0);
+        s[q][1] = w4.y - (a1 + b1);
+        s[q][2] = w4.z - (a2 + b2);
+        s[q][3] = w4.w - (a3 + b3);
+      }
+    }
+    // the diagonal block rows j0..j0+3 sit in lanes 0..3 of slot 0
+    float d[4][4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+      for (int c = 0; c <= t; ++c) d[t][c] = __shfl_sync(0xffffffffu, s[0][c], t);
+    // rows t < nb of the block are matrix rows; row t == nb, if it is N, is
+    // the right-hand side (off-diagonal part only); rows beyond are unused
+    const int nb = N - j0 < 4 ? N - j0 : 4;
+    float L[4][4], rd[4];
+    bool ok = true;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+#pragma unroll
+      for (int c = 0; c < t; ++c) {
+        float v = d[t][c];
+#pragma unroll
+        for (int e = 0; e < c; ++e) v = fmaf(-L[t][e], L[c][e], v);
+        L[t][c] = (t <= nb && c < nb) ? v * rd[c] : 0.f;
+      }
+      float v = d[t][t];
+#pragma unroll
+      for (int e = 0; e < t; ++e) v = fmaf(-L[t][e], L[t][e], v);
+      if (t >= nb) v = 1.f;  // the right-hand-side row and rows past it: identity
+      ok = ok && (v > 0.f) && isfinite(v);
+      const float dd = sqrtf(v);
+      L[t][t] = dd;
+      rd[t] = 1.0f / dd;
+      if (t < nb) {
+        dmin = fminf(dmin, dd);
+        dmax = fmaxf(dmax, dd);
+      }
+    }
+    if (!ok) return false;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < Dims<N>::CQ; ++q) {
+      const int i = j0 + lane + 32 * q;
+      if (i <= N) {
+        float o[4];
+        if (q == 0 && lane < 4) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            float v = 0.f;
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+              if (t == lane && c <= t) v = L[t][c];
+            o[c] = v;
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            float v = s[q][c];
+#pragma unroll
+            for (int e = 0; e < c; ++e) v = fmaf(-o[e], L[c][e], v);
+            o[c] = v * rd[c];
+          }
+        }
+        *reinterpret_cast<float4*>(A + packoff(i) + j0) = make_float4(o[0], o[1], o[2], o[3]);
+      }
+    }
+    if (lane < 4) rdiag[j0 + lane] = lane == 0 ? rd[0] : lane == 1 ? rd[1] : lane == 2 ? rd[2] : rd[3];
+    __syncwarp();
+  }
+  return true;
+}
+
+// x := L^-T L^-1 x with x distributed as x[q] = element lane + 32 q, blocked
+// by 4: each block's four unknowns are gathered by shuffles, solved against
+// the 4x4 diagonal block, and pushed into the remaining rows with one float4
+// (forward) or four scalars (backward) of L per row.
+template <int N>
+__device__ __forceinline__ void chol_subst_f32(const float* L, const float* rdiag, float* x, int lane) {
+  constexpr int NB = (N + 3) / 4;
+#pragma unroll 1
+  for (int cb = 0; cb < NB; ++cb) {
+    const int j0 = 4 * cb;
+    float y[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int r = j0 + c;
+      float xv = 0.f;
+#pragma unroll
+      for (int q = 0; q < Dims<N>::CQ; ++q)
+        if (q == (r >> 5)) xv = x[q];
+      y[c] = __shfl_sync(0xffffffffu, xv, r & 31);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (j0 + c < N) {
+        const float* Lc = L + packoff(j0 + c) + j0;
+        float v = y[c];
+#pragma unroll
+        for (int e = 0; e < c; ++e) v = fmaf(-Lc[e], y[e], v);
+        y[c] = v * rdiag[j0 + c];
+      } else {
+        y[c] = 0.f;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < Dims<N>::CQ; ++q) {
+      const int i = lane + 32 * q;
+      if (i >= j0 + 4 && i < N) {
+        const float4 l4 = *reinterpret_cast<const float4*>(L + packoff(i) + j0);
+        x[q] = fmaf(-l4.x, y[0], x[q]);
+        x[q] = fmaf(-l4.y, y[1], x[q]);
+        x[q] = fmaf(-l4.z, y[2], x[q]);
+        x[q] = fmaf(-l4.w, y[3], x[q]);
+      } else if (i >= j0 && i < j0 + 4 && i < N) {
+        x[q] = (i == j0) ? y[0] : (i == j0 + 1) ? y[1] : (i == j0 + 2) ? y[2] : y[3];
+      }
+    }
+  }
+#pragma unroll 1
+  for (int cb = NB - 1; cb >= 0; --cb) {
+    const int j0 = 4 * cb;
+    float y[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int r = j0 + c;
+      float xv = 0.f;
+#pragma unroll
+      for (int q = 0; q < Dims<N>::CQ; ++q)
+        if (q == (r >> 5)) xv = x[q];
+      y[c] = __shfl_sync(0xffffffffu, xv, r & 31);
+    }
+#pragma unroll
+    for (int c = 3; c >= 0; --c) {
+      if (j0 + c < N) {
+        float v = y[c];
+#pragma unroll
+        for (int e = c + 1; e < 4; ++e)
+          if (j0 + e < N) v = fmaf(-L[packoff(j0 + e) + j0 + c], y[e], v);
+        y[c] = v * rdiag[j0 + c];
+      } else {
+        y[c] = 0.f;
+      }
+    }
+    const float* L0 = L + packoff(j0);
+    const float* L1 = L + packoff(j0 + 1);
+    const float* L2 = L + packoff(j0 + 2);
+    const float* L3 = L + packoff(j0 + 3);
+#pragma unroll
+    for (int q = 0; q < Dims<N>::CQ; ++q) {
+      const int i = lane + 32 * q;
+      if (i < j0) {
+        float v = x[q];
+        v = fmaf(-L0[i], y[0], v);
+        if (j0 + 1 < N) v = fmaf(-L1[i], y[1], v);
+        if (j0 + 2 < N) v = fmaf(-L2[i], y[2], v);
+        if (j0 + 3 < N) v = fmaf(-L3[i], y[3], v);
+        x[q] = v;
+      } else if (i < j0 + 4 && i < N) {
+        x[q] = (i == j0) ? y[0] : (i == j0 + 1) ? y[1] : (i == j0 + 2) ? y[2] : y[3];
+      }
+    }
+  }
+}
+
+// x := L^-T x (the backward half of chol_subst_f32), x distributed as above.
+template <int N>
+__device__ __forceinline__ void chol_back_f32(const float* L, const float* rdiag, float* x, int lane) {
+  constexpr int NB = (N + 3) / 4;
+#pragma unroll 1
+  for (int cb = NB - 1; cb >= 0; --cb) {
+    const int j0 = 4 * cb;
+    float y[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int r = j0 + c;
+      float xv = 0.f;
+#pragma unroll
+      for (int q = 0; q < Dims<N>::CQ; ++q)
+        if (q == (r >> 5)) xv = x[q];
+      y[c] = __shfl_sync(0xffffffffu, xv, r & 31);
+    }
+#pragma unroll
+    for (int c = 3; c >= 0; --c) {
+      if (j0 + c < N) {
+        float v = y[c];
+#pragma unroll
+        for (int e = c + 1; e < 4; ++e)
+          if (j0 + e < N) v = fmaf(-L[packoff(j0 + e) + j0 + c], y[e], v);
+        y[c] = v * rdiag[j0 + c];
+      } else {
+        y[c] = 0.f;
+      }
+    }
+    const float* L0 = L + packoff(j0);
+    const float* L1 = L + packoff(j0 + 1);
+    const float* L2 = L + packoff(j0 + 2);
+    const float* L3 = L + packoff(j0 + 3);
+#pragma unroll
+    for (int q = 0; q < Dims<N>::CQ; ++q) {
+      const int i = lane + 32 * q;
+      if (i < j0) {
+        float v = x[q];
+        v = fmaf(-L0[i], y[0], v);
+        if (j0 + 1 < N) v = fmaf(-L1[i], y[1], v);
+        if (j0 + 2 < N) v = fmaf(-L2[i], y[2], v);
+        if (j0 + 3 < N) v = fmaf(-L3[i], y[3], v);
+        x[q] = v;
+      } else if (i < j0 + 4 && i < N) {
+        x[q] = (i == j0) ? y[0] : (i == j0 + 1) ? y[1] : (i == j0 + 2) ? y[2] : y[3];
+      }
+    }
+  }
+}
+
+// FP64 version (fallback path, L in FP64 global scratch).
+template <int N>
+__device__ __forceinline__ void chol_subst_f64(const double* L, double* x, int lane) {
 #pragma unroll 1
   for (int kk = 0; kk < N; ++kk) {
     const int src = kk & 31, slot = kk >> 5;
-    T xv = 0;
+    double xv = 0.0;
 #pragma unroll
     for (int q = 0; q < Dims<N>::CQ; ++q)
       if (q == slot) xv = x[q];
-    const T xk = __shfl_sync(0xffffffffu, xv, src) / (T)L[packoff(kk) + kk];
+    const double xk = shfl_d(xv, src) / L[packoff(kk) + kk];
 #pragma unroll
     for (int q = 0; q < Dims<N>::CQ; ++q) {
       const int i = lane + 32 * q;
-      if (i > kk && i < N) x[q] -= (T)L[packoff(i) + kk] * xk;
+      if (i > kk && i < N) x[q] -= L[packoff(i) + kk] * xk;
       if (i == kk) x[q] = xk;
     }
   }
-  // backward with L^T: row kk of L holds column kk of L^T
 #pragma unroll 1
   for (int kk = N - 1; kk >= 0; --kk) {
     const int src = kk & 31, slot = kk >> 5;
-    T xv = 0;
+    double xv = 0.0;
 #pragma unroll
     for (int q = 0; q < Dims<N>::CQ; ++q)
       if (q == slot) xv = x[q];
-    const T xk = __shfl_sync(0xffffffffu, xv, src) / (T)L[packoff(kk) + kk];
-    const LT* Lk = L + packoff(kk);
+    const double xk = shfl_d(xv, src) / L[packoff(kk) + kk];
+    const double* Lk = L + packoff(kk);
 #pragma unroll
     for (int q = 0; q < Dims<N>::CQ; ++q) {
       const int i = lane + 32 * q;
-      if (i < kk) x[q] -= (T)Lk[i] * xk;
+      if (i < kk) x[q] -= Lk[i] * xk;
       if (i == kk) x[q] = xk;
     }
   }
 }
 
 // r = b - (Mt_M F + sum_{d in neg} h_d (h_d . F)), accumulated in FP64 with
-// the FP32 operators the solve used.  F is read from w.F.
+// the FP32 operators.  F is read from w.F.
 template <int N>
-__device__ void residual_fp64(const Scheme& sc, const float* Hs, int k, const WarpWS<N>& w, int lane,
+__device__ void residual_fp64(const Scheme& sc, const HTab<N>& H, int k, const WarpWS<N>& w, int lane,
                               double* r) {
-  constexpr int HS = Dims<N>::HS;
   double u[Dims<N>::CQ];
 #pragma unroll
   for (int q = 0; q < Dims<N>::CQ; ++q) u[q] = 0.0;
@@ -409,11 +768,11 @@ __device__ void residual_fp64(const Scheme& sc, const float* Hs, int k, const Wa
     const int qq = q0 + lane;
     double t = 0.0;
     if (qq < k) {
-      const float4* h = reinterpret_cast<const float4*>(Hs + (int)w.neg[qq] * HS);
+      const int d = (int)w.neg[qq];
       const float4* f = reinterpret_cast<const float4*>(w.F);
 #pragma unroll 4
-      for (int j = 0; j < HS / 4; ++j) {
-        const float4 a = h[j], c = f[j];
+      for (int j = 0; j < Dims<N>::NQ; ++j) {
+        const float4 a = H.quad(d, j), c = f[j];
         t = fma((double)a.x, (double)c.x, t);
         t = fma((double)a.y, (double)c.y, t);
         t = fma((double)a.z, (double)c.z, t);
@@ -423,11 +782,11 @@ __device__ void residual_fp64(const Scheme& sc, const float* Hs, int k, const Wa
     const int cnt = min(32, k - q0);
     for (int s = 0; s < cnt; ++s) {
       const double ts = shfl_d(t, s);
-      const float* h = Hs + (int)w.neg[q0 + s] * HS;
+      const int d = (int)w.neg[q0 + s];
 #pragma unroll
       for (int q = 0; q < Dims<N>::CQ; ++q) {
         const int i = lane + 32 * q;
-        if (i < N) u[q] = fma(ts, (double)h[i], u[q]);
+        if (i < N) u[q] = fma(ts, (double)H.val(d, i), u[q]);
       }
     }
   }
@@ -443,6 +802,25 @@ __device__ void residual_fp64(const Scheme& sc, const float* Hs, int k, const Wa
       r[q] = 0.0;
     }
   }
+}
+
+// One refinement step of the current solution in w.F, with the FP32 factor
+// still in w.W / w.rdiag and the set in w.neg[0..k).
+template <int N>
+__device__ void refine_step(const Scheme& sc, const HTab<N>& H, int k, const WarpWS<N>& w, int lane) {
+  double r[Dims<N>::CQ];
+  residual_fp64<N>(sc, H, k, w, lane, r);
+  float d[Dims<N>::CQ];
+#pragma unroll
+  for (int q = 0; q < Dims<N>::CQ; ++q) d[q] = (float)r[q];
+  chol_subst_f32<N>(w.W, w.rdiag, d, lane);
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < Dims<N>::CQ; ++q) {
+    const int i = lane + 32 * q;
+    if (i < N) w.F[i] += d[q];
+  }
+  __syncwarp();
 }
 
 // FP64 rebuild + factorisation + solve of the current system into w.F,
@@ -463,15 +841,14 @@ __device__ bool solve_fp64(const Scheme& sc, int k, const WarpWS<N>& w, double* 
   }
   __syncwarp();
   __threadfence_block();
-  double dmin, dmax;
-  const bool ok = cholesky_packed<N, double>(A, lane, dmin, dmax);
+  const bool ok = cholesky_packed<N, double>(A, lane);
   double x[Dims<N>::CQ];
 #pragma unroll
   for (int q = 0; q < Dims<N>::CQ; ++q) {
     const int i = lane + 32 * q;
     x[q] = i < N ? w.b[i] : 0.0;
   }
-  if (ok) chol_subst<N, double, double>(A, x, lane);
+  if (ok) chol_subst_f64<N>(A, x, lane);
   __syncwarp();
 #pragma unroll
   for (int q = 0; q < Dims<N>::CQ; ++q) {
@@ -482,46 +859,52 @@ __device__ bool solve_fp64(const Scheme& sc, int k, const WarpWS<N>& w, double* 
   return ok;
 }
 
-// One assemble + factorise + solve (+ refinement) for the set in w.neg[0..k).
-// Returns status flags (CSD_STATUS_FP64 / CSD_STATUS_CHOLFAIL bits).
+// One assemble + factorise + solve for the set in w.neg[0..k); refines the
+// result when refine == 1.  Returns status flags (0x10 FP64 used, 0x20 the
+// FP64 factorisation failed too); bit 0x100 marks that w.W holds no usable
+// FP32 factor (the FP64 path ran).
 template <int N>
-__device__ int assemble_solve(const Scheme& sc, const float* Hs, int k, const WarpWS<N>& w, int lane,
-                              float cond_thr, int refine, double* fp64_slot) {
-  assemble<N>(Hs, sc.MtMp, k, w, lane);
+__device__ int assemble_solve(const Scheme& sc, const HTab<N>& H, int k, const WarpWS<N>& w, int lane,
+                              float cond_thr, int refine, double* fp64_slot, long long* tacc = nullptr) {
+  CSD_T0(t0);
+  assemble<N>(H, sc.MtMp, k, w, lane);
+  // append b as row N: the factorisation then leaves y = L^-1 b in that row
+  {
+    float* bN = w.W + packoff(N);
+    for (int c = lane; c < packoff(N + 1) - packoff(N); c += 32) bN[c] = c < N ? (float)w.b[c] : 0.f;
+    __syncwarp();
+  }
+  CSD_T1(tacc, kPhAssemble, t0);
+  CSD_T0(t1);
   float dmin, dmax;
-  const bool ok = cholesky_packed_f32<N>(w.W, lane, dmin, dmax);
+  const bool ok = cholesky_packed_f32<N>(w.W, w.rdiag, lane, dmin, dmax);
+  CSD_T1(tacc, kPhChol, t1);
   const float cond = ok ? (dmax / dmin) * (dmax / dmin) : 3.0e38f;
   if (!ok || !(cond <= cond_thr)) {
+    CSD_T0(t2);
     const bool ok64 = solve_fp64<N>(sc, k, w, fp64_slot, lane);
-    return 0x10 | (ok64 ? 0 : 0x20);
+    CSD_T1(tacc, kPhFp64, t2);
+    return 0x110 | (ok64 ? 0 : 0x20);
   }
+  CSD_T0(t3);
   float x[Dims<N>::CQ];
 #pragma unroll
   for (int q = 0; q < Dims<N>::CQ; ++q) {
     const int i = lane + 32 * q;
-    x[q] = i < N ? (float)w.b[i] : 0.f;
+    x[q] = i < N ? w.W[packoff(N) + i] : 0.f;
   }
-  chol_subst<N, float, float>(w.W, x, lane);
+  chol_back_f32<N>(w.W, w.rdiag, x, lane);
 #pragma unroll
   for (int q = 0; q < Dims<N>::CQ; ++q) {
     const int i = lane + 32 * q;
     if (i < N) w.F[i] = x[q];
   }
   __syncwarp();
-  if (refine) {
-    double r[Dims<N>::CQ];
-    residual_fp64<N>(sc, Hs, k, w, lane, r);
-    float d[Dims<N>::CQ];
-#pragma unroll
-    for (int q = 0; q < Dims<N>::CQ; ++q) d[q] = (float)r[q];
-    chol_subst<N, float, float>(w.W, d, lane);
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < Dims<N>::CQ; ++q) {
-      const int i = lane + 32 * q;
-      if (i < N) w.F[i] = x[q] + d[q];
-    }
-    __syncwarp();
+  CSD_T1(tacc, kPhSubst, t3);
+  if (refine == 1) {
+    CSD_T0(t4);
+    refine_step<N>(sc, H, k, w, lane);
+    CSD_T1(tacc, kPhRefine, t4);
   }
   return 0;
 }

@@ -47,16 +47,28 @@ extern "C" const char* csd_last_error(void) { return g_err.c_str(); }
 
 namespace csdb200 {
 
+template <int N>
+__device__ __forceinline__ bool same_set(const uint32_t* a, const uint32_t* b, int nw) {
+  bool same = true;
+#pragma unroll
+  for (int p = 0; p < kMaxWords; ++p)
+    if (p < nw) same = same && (a[p] == b[p]);
+  return same;
+}
+
 // Solve voxel v of volume V with one warp (CSD_Processor::operator(),
 // cmd/dwi2fod.cpp:128-147, with CSD::set/iterate, csd.h:237-269).
 template <int N>
-__device__ void solve_voxel(const VolumeDesc& V, long long v, const float* Hs, int nhr, int nw,
-                            float cond_thr, int refine, const WarpWS<N>& w, int lane, double* slot) {
+__device__ void solve_voxel(const VolumeDesc& V, long long v, const HTab<N>& H, int nw, float cond_thr,
+                            int refine, const WarpWS<N>& w, int lane, double* slot, long long* tacc = nullptr) {
   const Scheme& sc = V.sc;
+  const int nhr = H.nhr;
   const bool masked = V.mask && !V.mask[v];
   const float* dwi = V.dwi + v * V.vox_stride;
   float* out = V.fod + v * V.fod_stride;
+  CSD_T0(tset);
   int st = voxel_set<N>(sc, dwi, V.vol_stride, masked, w, lane);
+  CSD_T1(tacc, kPhSet, tset);
   if (st != 0) {
     for (int c = lane; c < N; c += 32) out[c] = 0.f;
     if (lane == 0) {
@@ -67,13 +79,16 @@ __device__ void solve_voxel(const VolumeDesc& V, long long v, const float* Hs, i
       for (int p = lane; p < nw; p += 32) V.negmask[v * nw + p] = 0u;
     return;
   }
-  uint32_t bits[kMaxWords], old[kMaxWords];
-#pragma unroll
-  for (int p = 0; p < kMaxWords; ++p) old[p] = 0u;
+  uint32_t bits[kMaxWords];
+  uint32_t* old = w.old;  // warp-uniform, kept in shared memory
+  uint32_t* old2 = w.old2;
+  if (lane < kMaxWords) old[lane] = 0u;
+  __syncwarp();
   int flags = 0, it = 0;
   bool conv = false, use_warm = V.warm != nullptr;
   for (int attempt = 0; attempt < 2; ++attempt) {
-    bool have_old = false;
+    bool have_old = false, fp32_factor = false, refined = false;
+    int k = 0, rmode = refine;
     conv = false;
 #pragma unroll 1
     for (it = 0; it < sc.niter; ++it) {
@@ -83,32 +98,65 @@ __device__ void solve_voxel(const VolumeDesc& V, long long v, const float* Hs, i
         for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < nw) ? __ldg(V.warm + v * nw + p) : 0u;
         if (nhr & 31) bits[nw - 1] &= (1u << (nhr & 31)) - 1u;
       } else {
-        project_mask<N>(Hs, nhr, nw, sc.threshold, w, lane, bits);
-        if (have_old) {
-          bool same = true;
-#pragma unroll
-          for (int p = 0; p < kMaxWords; ++p)
-            if (p < nw) same = same && (bits[p] == old[p]);
-          if (same) {  // csd.h:252-253
+        CSD_T0(tp);
+        project_mask<N>(H, nw, sc.threshold, w, lane, bits);
+        CSD_T1(tacc, kPhProject, tp);
+        // a set that returns after one step is an FP32 two-cycle around a
+        // sign change: refine every remaining solve of this voxel
+        if ((rmode == 2 || rmode == 3) && it >= 2 && same_set<N>(bits, old2, nw)) rmode = 1;
+        if (have_old && same_set<N>(bits, old, nw)) {  // csd.h:252-253
+          if (rmode == 2 && fp32_factor && !refined) {
+            // refine the fixed point once, then check that it still is one
+            CSD_T0(tr);
+            refine_step<N>(sc, H, k, w, lane);
+            CSD_T1(tacc, kPhRefine, tr);
+            refined = true;
+            CSD_T0(tp2);
+            project_mask<N>(H, nw, sc.threshold, w, lane, bits);
+            CSD_T1(tacc, kPhProject, tp2);
+            if (same_set<N>(bits, old, nw)) {
+              conv = true;
+              ++it;
+              break;
+            }
+            // refinement moved the set: this voxel sits close to a sign
+            // change, so refine after every remaining solve
+            rmode = 1;
+          } else {
             conv = true;
             ++it;
             break;
           }
         }
       }
-      const int k = mask_to_list(bits, nw, w.neg, lane);
-      flags |= assemble_solve<N>(sc, Hs, k, w, lane, cond_thr, refine, slot);
+      CSD_T0(tl);
+      k = mask_to_list(bits, nw, w.neg, lane);
+      CSD_T1(tacc, kPhList, tl);
+      const int fl = assemble_solve<N>(sc, H, k, w, lane, cond_thr, rmode, slot, tacc);
+      flags |= fl & 0xF0;
+      fp32_factor = !(fl & 0x100);
+      refined = rmode == 1 && fp32_factor;
+      __syncwarp();
+      if (lane == 0) {
 #pragma unroll
-      for (int p = 0; p < kMaxWords; ++p) old[p] = bits[p];
+        for (int p = 0; p < kMaxWords; ++p)
+          if (p < nw) {
+            old2[p] = old[p];
+            old[p] = bits[p];
+          }
+      }
+      __syncwarp();
       have_old = true;
     }
+    // niter exhausted: still refine the last solution
+    if (!conv && rmode == 2 && fp32_factor && !refined && it > 0) refine_step<N>(sc, H, k, w, lane);
     if (conv || !use_warm || sc.niter == 0) break;
     // the warm-started iteration did not reach a fixed point: restart the
     // voxel from the plain start
     flags |= CSD_STATUS_WARM_RESTART;
     use_warm = false;
-#pragma unroll
-    for (int p = 0; p < kMaxWords; ++p) old[p] = 0u;
+    if (lane < kMaxWords) old[lane] = 0u;
+    __syncwarp();
     voxel_set<N>(sc, dwi, V.vol_stride, false, w, lane);
   }
   for (int c = lane; c < N; c += 32) out[c] = w.F[c];
@@ -117,30 +165,26 @@ __device__ void solve_voxel(const VolumeDesc& V, long long v, const float* Hs, i
     if (V.status) V.status[v] = (uint8_t)(outcome | flags);
     if (V.iters) V.iters[v] = (uint8_t)(it > 255 ? 255 : it);
   }
-  if (V.negmask) {
-#pragma unroll
-    for (int p = 0; p < kMaxWords; ++p)
-      if (p < nw && p == lane) V.negmask[v * nw + p] = old[p];
-  }
+  if (V.negmask && lane < nw) V.negmask[v * nw + lane] = old[lane];
+  __syncwarp();
 }
 
 template <int N>
 __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_persistent_kernel(const __grid_constant__ SolveParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int HS = Dims<N>::HS;
-  float* Hs = reinterpret_cast<float*>(smem);
   const int nhr = P.nhr;
-  {
-    const float4* src = reinterpret_cast<const float4*>(P.vol[0].sc.H32);
-    float4* dst = reinterpret_cast<float4*>(Hs);
-    for (int i = threadIdx.x; i < nhr * HS / 4; i += blockDim.x) dst[i] = __ldg(src + i);
-  }
+  const HTab<N> H = load_htab<N>(smem, P.vol[0].sc, nhr);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  const int hbytes = ((nhr * HS * 4 + 15) / 16) * 16;
-  WarpWS<N> w = carve_ws<N>(smem + hbytes + warp * warp_ws_bytes<N>());
+  WarpWS<N> w = carve_ws<N>(smem + htab_bytes<N>(nhr) + warp * warp_ws_bytes<N>());
   double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
+#ifdef CSD_PHASE_TIMERS
+  long long tacc[kPhTotal + 1] = {};
+  const long long tstart = clock64();
+#else
+  long long* tacc = nullptr;
+#endif
   for (;;) {
     unsigned long long g = 0;
     if (lane == 0) g = atomicAdd(P.queue, 1ULL);
@@ -149,10 +193,18 @@ __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_persistent_kernel(con
     int vi = 0;
     while (vi + 1 < P.n_vol && (long long)g >= P.vol[vi + 1].first) ++vi;
     const VolumeDesc& V = P.vol[vi];
-    solve_voxel<N>(V, (long long)g - V.first, Hs, nhr, P.nw, P.cond_thr, P.refine, w, lane, slot);
+    solve_voxel<N>(V, (long long)g - V.first, H, P.nw, P.cond_thr, P.refine, w, lane, slot, tacc);
   }
+#ifdef CSD_PHASE_TIMERS
+  tacc[kPhTotal] = clock64() - tstart;
+  if (lane == 0)
+    for (int p = 0; p <= kPhTotal; ++p) atomicAdd(&g_phase_cycles[p], (unsigned long long)tacc[p]);
+#endif
 }
 
+}  // namespace csdb200
+
+namespace csdb200 {
 
 // ---- phased kernels behind the csd_state_* surface ------------------------
 
@@ -212,17 +264,11 @@ template <int N>
 __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_state_iterate_kernel(const __grid_constant__ StateParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int HS = Dims<N>::HS;
-  float* Hs = reinterpret_cast<float*>(smem);
-  {
-    const float4* src = reinterpret_cast<const float4*>(P.sc.H32);
-    float4* dst = reinterpret_cast<float4*>(Hs);
-    for (int i = threadIdx.x; i < P.nhr * HS / 4; i += blockDim.x) dst[i] = __ldg(src + i);
-  }
+  const HTab<N> H = load_htab<N>(smem, P.sc, P.nhr);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  const int hbytes = ((P.nhr * HS * 4 + 15) / 16) * 16;
-  WarpWS<N> w = carve_ws<N>(smem + hbytes + warp * warp_ws_bytes<N>());
+  WarpWS<N> w = carve_ws<N>(smem + htab_bytes<N>(P.nhr) + warp * warp_ws_bytes<N>());
   double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
   const int gw = blockIdx.x * nwarps + warp, nwt = gridDim.x * nwarps;
   for (int e = gw; e < P.n_in; e += nwt) {
@@ -237,7 +283,7 @@ __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_state_iterate_kernel(
       for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.warm[v * P.nw + p] : 0u;
       if (P.nhr & 31) bits[P.nw - 1] &= (1u << (P.nhr & 31)) - 1u;
     } else {
-      project_mask<N>(Hs, P.nhr, P.nw, P.sc.threshold, w, lane, bits);
+      project_mask<N>(H, P.nw, P.sc.threshold, w, lane, bits);
       if (it > 0) {
         bool same = true;
 #pragma unroll
@@ -253,7 +299,7 @@ __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_state_iterate_kernel(
       }
     }
     const int k = mask_to_list(bits, P.nw, w.neg, lane);
-    const int fl = assemble_solve<N>(P.sc, Hs, k, w, lane, P.cond_thr, P.refine, slot);
+    const int fl = assemble_solve<N>(P.sc, H, k, w, lane, P.cond_thr, P.refine ? 1 : 0, slot) & 0xF0;
     for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
 #pragma unroll
     for (int p = 0; p < kMaxWords; ++p)
@@ -302,18 +348,22 @@ __global__ void csd_state_fod_kernel(const float* F, const uint8_t* status, cons
 struct csd_shared {
   HostShared h;
   double cond_thr = 1e6;
+  int refine = 3;
   int device = -1;               // device holding the tables (-1: not uploaded yet)
   std::mutex upload_mu;
   int HS = 0, WSZ = 0;
   std::vector<float> H32_host;
+  std::vector<__half> H16_host;    // [2][nhr+1][HS16]: hi then lo
   std::vector<float> MtMp_host;
-  std::vector<double> rconvT_host;
+  std::vector<float> rconvT_host;
+  std::vector<float> M32_host;
   float* H32 = nullptr;
+  __half* H16 = nullptr;
   double* H64 = nullptr;
   float* MtMp = nullptr;
   double* MtM64 = nullptr;
-  double* rconvT = nullptr;
-  double* M64 = nullptr;
+  float* rconvT = nullptr;
+  float* M32 = nullptr;
   int* dwis = nullptr;
 };
 
@@ -331,6 +381,7 @@ extern "C" void csd_params_init(csd_params* p) {
   p->bzero_threshold = 10.0;
   p->bvalue_epsilon = 80.0;
   p->fp64_condition = 1e6;
+  p->refine = 3;
 }
 
 template <typename T>
@@ -378,6 +429,8 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
   if (h.ndw > kMaxDW) return fail(CSD_ERR_UNSUPPORTED, "more than 512 DW volumes in the shell");
   if (h.niter > 255 * 4) return fail(CSD_ERR_INVALID, "niter out of range [0,1000]");
   s->cond_thr = p->fp64_condition > 0 ? p->fp64_condition : 1e6;
+  if (p->refine < 0 || p->refine > 3) return fail(CSD_ERR_INVALID, "refine must be 0, 1, 2 or 3");
+  s->refine = p->refine;
   const int n = h.nsh;
   s->HS = hr_stride(n);
   s->WSZ = packoff(n);
@@ -385,12 +438,25 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
   s->H32_host.assign((size_t)h.nhr * s->HS, 0.f);
   for (int d = 0; d < h.nhr; ++d)
     for (int c = 0; c < n; ++c) s->H32_host[(size_t)d * s->HS + c] = (float)h.HR[(size_t)d * n + c];
+  // FP16 hi/lo split of HR_trans for the tensor-core assembly, plus a zero row
+  const int HS16 = hr_stride16(n);
+  s->H16_host.assign((size_t)2 * (h.nhr + 1) * HS16, __float2half_rn(0.f));
+  for (int d = 0; d < h.nhr; ++d)
+    for (int c = 0; c < n; ++c) {
+      const double x = h.HR[(size_t)d * n + c];
+      const __half hi = __float2half_rn((float)x);
+      const __half lo = __float2half_rn((float)(x - (double)__half2float(hi)));
+      s->H16_host[(size_t)d * HS16 + c] = hi;
+      s->H16_host[(size_t)(h.nhr + 1 + d) * HS16 + c] = lo;
+    }
   s->MtMp_host.assign((size_t)s->WSZ, 0.f);
   for (int i = 0; i < n; ++i)
     for (int j = 0; j <= i; ++j) s->MtMp_host[packoff(i) + j] = (float)h.MtM[(size_t)i * n + j];
-  s->rconvT_host.assign((size_t)h.ndw * h.ninit, 0.0);
+  s->rconvT_host.assign((size_t)h.ndw * h.ninit, 0.f);
   for (int r = 0; r < h.ninit; ++r)
-    for (int t = 0; t < h.ndw; ++t) s->rconvT_host[(size_t)t * h.ninit + r] = h.rconv[(size_t)r * h.ndw + t];
+    for (int t = 0; t < h.ndw; ++t) s->rconvT_host[(size_t)t * h.ninit + r] = (float)h.rconv[(size_t)r * h.ndw + t];
+  s->M32_host.assign(h.M.size(), 0.f);
+  for (size_t i = 0; i < h.M.size(); ++i) s->M32_host[i] = (float)h.M[i];
   *out = s.release();
   return CSD_OK;
 }
@@ -407,11 +473,12 @@ static int ensure_device(const csd_shared* cs) {
   int rc;
   const HostShared& h = s->h;
   if ((rc = upload(&s->H32, s->H32_host))) return rc;
+  if ((rc = upload(&s->H16, s->H16_host))) return rc;
   if ((rc = upload(&s->H64, h.HR))) return rc;
   if ((rc = upload(&s->MtMp, s->MtMp_host))) return rc;
   if ((rc = upload(&s->MtM64, h.MtM))) return rc;
   if ((rc = upload(&s->rconvT, s->rconvT_host))) return rc;
-  if ((rc = upload(&s->M64, h.M))) return rc;
+  if ((rc = upload(&s->M32, s->M32_host))) return rc;
   if ((rc = upload(&s->dwis, h.dwis))) return rc;
   s->device = dev;
   return 0;
@@ -424,11 +491,12 @@ extern "C" void csd_shared_destroy(csd_shared* s) {
     cudaGetDevice(&cur);
     cudaSetDevice(s->device);
     cudaFree(s->H32);
+    cudaFree(s->H16);
     cudaFree(s->H64);
     cudaFree(s->MtMp);
     cudaFree(s->MtM64);
     cudaFree(s->rconvT);
-    cudaFree(s->M64);
+    cudaFree(s->M32);
     cudaFree(s->dwis);
     cudaSetDevice(cur);
   }
@@ -528,7 +596,7 @@ int shape_for(int nhr, long long total, LaunchShape* ls) {
   int smem_max = 0, nsm = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const size_t hbytes = ((size_t)nhr * Dims<N>::HS * 4 + 15) / 16 * 16;
+  const size_t hbytes = (size_t)htab_bytes<N>(nhr);
   const size_t wb = warp_ws_bytes<N>();
   if (hbytes + wb > (size_t)smem_max) return fail(CSD_ERR_UNSUPPORTED, "constraint set too large for shared memory");
   int warps = (int)std::min<size_t>(Dims<N>::THREADS / 32, ((size_t)smem_max - hbytes) / wb);
@@ -571,11 +639,12 @@ int dispatch(int nsh, const SolveParams& P, cudaStream_t st, Workspace* ws) {
 static Scheme scheme_of(const csd_shared* s) {
   Scheme sc;
   sc.H32 = s->H32;
+  sc.H16 = s->H16;
   sc.H64 = s->H64;
   sc.MtMp = s->MtMp;
   sc.MtM64 = s->MtM64;
   sc.rconvT = s->rconvT;
-  sc.M64 = s->M64;
+  sc.M32 = s->M32;
   sc.dwis = s->dwis;
   sc.ndw = s->h.ndw;
   sc.ninit = s->h.ninit;
@@ -584,7 +653,8 @@ static Scheme scheme_of(const csd_shared* s) {
   return sc;
 }
 
-static int g_refine = 1;  // one FP64-residual refinement step per solve
+static int g_refine = -1;  // test override of csd_params::refine (-1 = none)
+static int refine_of(const csd_shared* s) { return g_refine >= 0 ? g_refine : s->refine; }
 
 extern "C" int csd_solve(const csd_shared* const* shared, const csd_volume* volumes, int n_volumes, void* stream) {
   if (n_volumes < 0 || (n_volumes > 0 && (!shared || !volumes)))
@@ -626,7 +696,7 @@ extern "C" int csd_solve(const csd_shared* const* shared, const csd_volume* volu
       std::memset(&P, 0, sizeof(P));
       P.nhr = nhr;
       P.nw = (nhr + 31) / 32;
-      P.refine = g_refine;
+      P.refine = refine_of(shared[group[g0]]);
       P.cond_thr = (float)shared[group[g0]]->cond_thr;
       long long total = 0;
       int nv = 0;
@@ -717,9 +787,26 @@ extern "C" int csd_dwi2fod_host(const csd_shared* s, const float* dwi, int64_t n
   return CSD_OK;
 }
 
-// test hook: enable/disable the refinement step (default on)
-extern "C" int csd_debug_set_refine(int on) {
-  g_refine = on ? 1 : 0;
+// Profiling hook: per-phase cycle totals of the persistent kernel since the
+// last reset (only in a build with -DCSD_PHASE_TIMERS; returns -5 otherwise).
+extern "C" int csd_debug_phase_cycles(unsigned long long* out, int reset) {
+#ifdef CSD_PHASE_TIMERS
+  CUDA_TRY(cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(unsigned long long) * 16));
+  if (reset) {
+    unsigned long long z[16] = {};
+    CUDA_TRY(cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z)));
+  }
+  return CSD_OK;
+#else
+  (void)out;
+  (void)reset;
+  return fail(CSD_ERR_UNSUPPORTED, "built without CSD_PHASE_TIMERS");
+#endif
+}
+
+// test hook: refinement mode
+extern "C" int csd_debug_set_refine(int mode) {
+  g_refine = mode < 0 ? -1 : (mode > 3 ? 3 : mode);
   return CSD_OK;
 }
 
@@ -767,7 +854,7 @@ StateParams state_params(const csd_state* st) {
   P.sc = scheme_of(st->sh);
   P.nhr = st->sh->h.nhr;
   P.nw = (P.nhr + 31) / 32;
-  P.refine = g_refine;
+  P.refine = refine_of(st->sh);
   P.cond_thr = (float)st->sh->cond_thr;
   P.F = st->F;
   P.b = st->b;
@@ -968,14 +1055,15 @@ static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 template <int N>
 static int noalloc_launch(const csd_shared* s, const csd_volume* v, cudaStream_t st, unsigned char* base) {
   const HostShared& h = s->h;
-  // layout: [counter | H32 | H64 | MtMp | MtM64 | rconvT | M64 | dwis | FP64 slots]
+  // layout: [counter | H32 | H16 | H64 | MtMp | MtM64 | rconvT | M32 | dwis | FP64 slots]
   size_t off = 256;
   const size_t oH32 = off; off = align256(off + s->H32_host.size() * sizeof(float));
+  const size_t oH16 = off; off = align256(off + s->H16_host.size() * sizeof(__half));
   const size_t oH64 = off; off = align256(off + h.HR.size() * sizeof(double));
   const size_t oMtMp = off; off = align256(off + s->MtMp_host.size() * sizeof(float));
   const size_t oMtM64 = off; off = align256(off + h.MtM.size() * sizeof(double));
-  const size_t oRc = off; off = align256(off + s->rconvT_host.size() * sizeof(double));
-  const size_t oM = off; off = align256(off + h.M.size() * sizeof(double));
+  const size_t oRc = off; off = align256(off + s->rconvT_host.size() * sizeof(float));
+  const size_t oM = off; off = align256(off + s->M32_host.size() * sizeof(float));
   const size_t oDw = off; off = align256(off + h.dwis.size() * sizeof(int));
   const size_t oSlots = off;
   if (oSlots >= kNoAllocBytes)
@@ -990,29 +1078,31 @@ static int noalloc_launch(const csd_shared* s, const csd_volume* v, cudaStream_t
   const int blocks = (int)std::min<long long>(ls.blocks, fit);
   CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(unsigned long long), st));
   CUDA_TRY(cudaMemcpyAsync(base + oH32, s->H32_host.data(), s->H32_host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oH16, s->H16_host.data(), s->H16_host.size() * sizeof(__half), cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(base + oH64, h.HR.data(), h.HR.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(base + oMtMp, s->MtMp_host.data(), s->MtMp_host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(base + oMtM64, h.MtM.data(), h.MtM.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(base + oRc, s->rconvT_host.data(), s->rconvT_host.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(base + oM, h.M.data(), h.M.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oRc, s->rconvT_host.data(), s->rconvT_host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(base + oM, s->M32_host.data(), s->M32_host.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(base + oDw, h.dwis.data(), h.dwis.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   SolveParams P;
   std::memset(&P, 0, sizeof(P));
   P.n_vol = 1;
   P.nhr = h.nhr;
   P.nw = (h.nhr + 31) / 32;
-  P.refine = g_refine;
+  P.refine = refine_of(s);
   P.cond_thr = (float)s->cond_thr;
   P.total = v->n_voxels;
   P.queue = reinterpret_cast<unsigned long long*>(base);
   P.fp64_scratch = reinterpret_cast<double*>(base + oSlots);
   VolumeDesc& d = P.vol[0];
   d.sc.H32 = reinterpret_cast<const float*>(base + oH32);
+  d.sc.H16 = reinterpret_cast<const __half*>(base + oH16);
   d.sc.H64 = reinterpret_cast<const double*>(base + oH64);
   d.sc.MtMp = reinterpret_cast<const float*>(base + oMtMp);
   d.sc.MtM64 = reinterpret_cast<const double*>(base + oMtM64);
-  d.sc.rconvT = reinterpret_cast<const double*>(base + oRc);
-  d.sc.M64 = reinterpret_cast<const double*>(base + oM);
+  d.sc.rconvT = reinterpret_cast<const float*>(base + oRc);
+  d.sc.M32 = reinterpret_cast<const float*>(base + oM);
   d.sc.dwis = reinterpret_cast<const int*>(base + oDw);
   d.sc.ndw = h.ndw;
   d.sc.ninit = h.ninit;

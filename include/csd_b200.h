@@ -157,6 +157,38 @@ int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride, uint8_t* 
  * tables plus one block's FP64 slots do not fit; grids shrink to fit. */
 int csd_solve_noalloc(const csd_shared* s, const csd_volume* volume, void* stream);
 
+/* ---- warm-start network.  No counterpart in the reference: a 66 -> 256 ->
+ *      256 -> 300 MLP (GELU, sigmoid head; BF16 weights and activations, FP32
+ *      accumulation and Adam) that predicts each voxel's converged negative
+ *      set from its normalised signal.  The prediction only replaces the
+ *      first negative set (csd_volume.warm_negmask); the iteration then runs
+ *      to its own stopping rule, and a voxel that does not reach a fixed
+ *      point is re-solved from the plain start. */
+typedef struct csd_mlp csd_mlp;
+int csd_mlp_create(int n_in, int n_hidden, int n_out, uint64_t seed, csd_mlp** out);
+void csd_mlp_destroy(csd_mlp* m);
+int64_t csd_mlp_param_count(const csd_mlp* m);
+/* flat FP32 parameters [W1 b1 W2 b2 W3 b3], weights [out][in padded to 16 / 8] */
+int csd_mlp_get_params(const csd_mlp* m, float* out, int64_t n);
+int csd_mlp_set_params(csd_mlp* m, const float* in, int64_t n);
+/* input = (S_t / mean over b0_index of S - mean_t) / stdev_t for every volume t */
+int csd_mlp_set_inputs(csd_mlp* m, const int* b0_index, int n_b0, const float* mean, const float* stdev);
+/* normalised BF16 inputs [n][n_in padded to 16] for training (device) */
+int csd_mlp_inputs(const csd_mlp* m, const float* dwi, int64_t n_voxels, int64_t voxel_stride,
+                   int64_t volume_stride, uint16_t* x, void* stream);
+/* one epoch of Adam over n rows in batches (a multiple of 128) of shuffled order */
+int csd_mlp_train_epoch(csd_mlp* m, const uint16_t* x, const uint32_t* negmask, int64_t n, int batch, float lr,
+                        float weight_decay, uint64_t seed, float* mean_loss, void* stream);
+/* predicted first negative sets [n][ceil(n_out/32)] (device): direction d is in
+ * the set when its logit exceeds logit_threshold (0 = probability 1/2);
+ * masked-out voxels get none */
+int csd_mlp_predict(csd_mlp* m, const float* dwi, int64_t n_voxels, int64_t voxel_stride, int64_t volume_stride,
+                    const uint8_t* mask, float logit_threshold, uint32_t* negmask, void* stream);
+/* checks: BCE gradients (host copy of the flat gradient) and raw logits [n][n_out padded to 8] */
+int csd_mlp_gradients(csd_mlp* m, const uint16_t* x, const uint32_t* negmask, int64_t n, float* grad_out,
+                      float* loss_out);
+int csd_mlp_logits(csd_mlp* m, const uint16_t* x, int64_t n, float* z_out);
+
 /* Thread-local description of the last failure. */
 const char* csd_last_error(void);
 

@@ -32,6 +32,9 @@ static int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
+namespace csdb200 {
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace csdb200
 
 #define CUDA_TRY(expr)                                                                  \
   do {                                                                                  \

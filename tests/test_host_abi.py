@@ -100,9 +100,10 @@ def test_errors_follow_reference_messages():
 def test_cpp_shim_compiles():
     """The C++ drop-in header (CSD::Shared / CSD, csd.h:46-271) and the
     dwi2fod-style example compile against the C ABI."""
-    ex = os.path.join(ROOT, "mrtrix3_b200", "csrc", "dwi2fod_csd_example.cpp")
+    ex = os.path.join(ROOT, "mrtrix3_b200", "csrc", "examples", "dwi2fod_csd_example.cpp")
     if not os.path.exists(ex):
         pytest.skip("C++ shim example not present")
-    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I",
-                        os.path.join(ROOT, "mrtrix3_b200", "csrc"), ex], capture_output=True, text=True)
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-I", os.path.join(ROOT, "include"), "-I",
+                        os.path.join(ROOT, "mrtrix3_b200", "csrc"), "-I", "/usr/local/cuda/include", ex],
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

@@ -338,6 +338,13 @@ __device__ __forceinline__ int mask_to_list(const uint32_t* bits, int nw, uint16
 // are computed: row block ib (16 rows) x column block jb (8 columns),
 // jb <= 2 ib + 1.  Row blocks [IB0, IB1) are accumulated in this pass.
 
+__device__ __forceinline__ void ldsm4(uint32_t (&r)[4], const __half* p) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
 __device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const __half* p) {
   const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
   asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"

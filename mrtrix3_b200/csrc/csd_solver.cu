@@ -210,19 +210,38 @@ __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_persistent_kernel(con
 namespace csdb200 {
 
 // ---- phased kernels behind the csd_state_* surface ------------------------
+//
+// The plain GPU method: one pass per CSD::iterate() over every still-active
+// voxel.  csd_project_kernel evaluates HR_trans F for all active voxels as
+// one dense tensor-core contraction ([voxels x nSH] x [nSH x directions],
+// FP16 hi/lo split, three products, FP32 accumulation) with the sign test,
+// the comparison with the previous set and the compaction fused into its
+// epilogue; csd_solve_kernel then assembles and factorises (warp per voxel)
+// only the voxels whose set changed.
+
+constexpr int kProjRows = 64;       // voxels per projection tile
+constexpr float kProjFScale = 256.f;  // F is scaled by 2^8 before the FP16 split
+
+// status byte while iterating: low nibble 0xF, high bits = flags; 0x80 marks
+// a voxel whose set cycles in FP32 (its solves are refined)
+constexpr uint8_t kActive = 0x0F;
+constexpr uint8_t kCycling = 0x80;
 
 struct StateParams {
   Scheme sc;
-  int nhr, nw, refine, n_in, use_warm;
-  float cond_thr;
+  int nhr, nw, n_in, use_warm, npd;
+  float cond_thr, thr_scaled;
+  const __half* Hp16;   // [2][npd][HS16] projection table (hi, lo), zero rows past nhr
   float* F;             // [cap][HS]
   double* b;            // [cap][N]
-  uint32_t* old;        // [cap][nw]
+  uint32_t* old;        // [cap][nw] set of the last solve
+  uint32_t* old2;       // [cap][nw] set of the solve before
+  uint32_t* newm;       // [cap][nw] set found by the projection
   const uint32_t* warm; // [cap][nw] or NULL
   uint8_t* status;      // [cap]
   uint16_t* iters;      // [cap] iterate() calls made
-  const int* act_in;    // [n_in] active voxel ids
-  int* act_out;         // compacted survivors
+  const int* act_in;    // [n_in] voxel ids
+  int* act_out;         // compacted output list
   int* n_out;
   double* fp64_scratch;
   // set() inputs
@@ -246,7 +265,10 @@ __global__ void __launch_bounds__(256) csd_state_set_kernel(const __grid_constan
     float* F = P.F + v * Dims<N>::HS;
     for (int c = lane; c < Dims<N>::HS; c += 32) F[c] = st ? 0.f : w.F[c];
     for (int c = lane; c < N; c += 32) P.b[v * N + c] = st ? 0.0 : w.b[c];
-    for (int p = lane; p < P.nw; p += 32) P.old[v * P.nw + p] = 0u;
+    for (int p = lane; p < P.nw; p += 32) {
+      P.old[v * P.nw + p] = 0u;
+      P.old2[v * P.nw + p] = 0u;
+    }
     if (lane == 0) {
       P.iters[v] = 0;
       if (st) {
@@ -254,17 +276,130 @@ __global__ void __launch_bounds__(256) csd_state_set_kernel(const __grid_constan
       } else if (P.sc.niter == 0) {
         P.status[v] = CSD_STATUS_CONVERGED;
       } else {
-        P.status[v] = 0xFF;  // active
+        P.status[v] = kActive;
         P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
       }
     }
   }
 }
 
-// One CSD::iterate() (csd.h:245-269) on each listed voxel; voxels that
-// converge or exhaust niter drop out, the others are appended to act_out.
+// Projection pass: tiles of 64 active voxels.  Warp w computes rows
+// 16 (w & 3) .. +15 against half (w >> 2) of the directions with mma.sync
+// m16n8k16 (F hi/lo from shared memory as A, the direction table as B, both
+// K-major, loaded by ldmatrix); the epilogue sets one bit per negative
+// amplitude in a shared bitmap, then each voxel's bitmap is compared with
+// its previous set (csd.h:246-253): converged voxels finish, the others go
+// to the solve list.
 template <int N>
-__global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_state_iterate_kernel(const __grid_constant__ StateParams P) {
+__global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant__ StateParams P) {
+  using D = Dims<N>;
+  constexpr int KS = D::NRB;                 // k16 steps over the coefficients
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int npd = P.npd;                     // directions padded to a multiple of 32
+  __half* Hh = reinterpret_cast<__half*>(smem);
+  __half* Hl = Hh + npd * D::HS16;
+  __half* Fh = Hl + npd * D::HS16;
+  __half* Fl = Fh + kProjRows * D::HS16;
+  uint32_t* bm = reinterpret_cast<uint32_t*>(Fl + kProjRows * D::HS16);  // [64][kMaxWords]
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(P.Hp16);
+    uint4* dst = reinterpret_cast<uint4*>(Hh);
+    for (int i = threadIdx.x; i < 2 * npd * D::HS16 / 8; i += blockDim.x) dst[i] = __ldg(src + i);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mrow = 16 * (warp & 3);
+  const int half = warp >> 2;
+  constexpr int tpw = 20;                    // n8 tiles per warp: half of a 320-direction chunk
+  const int ntiles = (P.n_in + kProjRows - 1) / kProjRows;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int e0 = tile * kProjRows;
+    __syncthreads();
+    // F rows -> scaled FP16 hi / lo
+    for (int i = threadIdx.x; i < kProjRows * D::HS16; i += blockDim.x) {
+      const int r = i / D::HS16, c = i - r * D::HS16;
+      float f = 0.f;
+      if (e0 + r < P.n_in && c < N) f = P.F[(long long)P.act_in[e0 + r] * D::HS + c] * kProjFScale;
+      const __half h = __float2half_rn(f);
+      Fh[i] = h;
+      Fl[i] = __float2half_rn(f - __half2float(h));
+    }
+    for (int i = threadIdx.x; i < kProjRows * kMaxWords; i += blockDim.x) bm[i] = 0u;
+    __syncthreads();
+    for (int c0 = 0; c0 < npd; c0 += 320) {
+    float acc[20][4];
+#pragma unroll
+    for (int t = 0; t < 20; ++t)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[t][e] = 0.f;
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+      uint32_t ah[4], al[4];
+      ldsm4(ah, Fh + (mrow + (lane & 15)) * D::HS16 + 16 * ks + (lane >> 4) * 8);
+      ldsm4(al, Fl + (mrow + (lane & 15)) * D::HS16 + 16 * ks + (lane >> 4) * 8);
+#pragma unroll
+      for (int t = 0; t < 20; t += 2) {
+        {
+          const int nb = c0 + 8 * (half * tpw + t);
+          const int noff = (lane & 7) + ((lane >> 4) << 3), koff = ((lane >> 3) & 1) * 8;
+          uint32_t bh[4], bl[4];
+          ldsm4(bh, Hh + (nb + noff) * D::HS16 + 16 * ks + koff);
+          ldsm4(bl, Hl + (nb + noff) * D::HS16 + 16 * ks + koff);
+          mma_f16(acc[t], ah, bh[0], bh[1]);
+          mma_f16(acc[t], ah, bl[0], bl[1]);
+          mma_f16(acc[t], al, bh[0], bh[1]);
+          mma_f16(acc[t + 1], ah, bh[2], bh[3]);
+          mma_f16(acc[t + 1], ah, bl[2], bl[3]);
+          mma_f16(acc[t + 1], al, bh[2], bh[3]);
+        }
+      }
+    }
+    const int gid = lane >> 2, tig = lane & 3;
+#pragma unroll
+    for (int t = 0; t < 20; ++t) {
+      {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int r = mrow + gid + 8 * (e >> 1);
+          const int c = c0 + 8 * (half * tpw + t) + 2 * tig + (e & 1);
+          if (c < P.nhr && acc[t][e] < P.thr_scaled) atomicOr(&bm[r * kMaxWords + (c >> 5)], 1u << (c & 31));
+        }
+      }
+    }
+    }
+    __syncthreads();
+    // per-voxel decision: warp w handles rows w, w + 8, ...
+    for (int r = warp; r < kProjRows; r += 8) {
+      if (e0 + r >= P.n_in) break;
+      const long long v = P.act_in[e0 + r];
+      const int it = P.iters[v];
+      const bool warm = it == 0 && P.use_warm && P.warm;
+      uint32_t bits = 0u;
+      if (lane < P.nw) {
+        bits = warm ? P.warm[v * P.nw + lane] : bm[r * kMaxWords + lane];
+        if (warm && lane == P.nw - 1 && (P.nhr & 31)) bits &= (1u << (P.nhr & 31)) - 1u;
+      }
+      const bool same = __all_sync(0xffffffffu, lane >= P.nw || bits == P.old[v * P.nw + lane]);
+      const bool back = __all_sync(0xffffffffu, lane >= P.nw || bits == P.old2[v * P.nw + lane]);
+      const bool conv = !warm && it > 0 && same;
+      if (!conv && lane < P.nw) P.newm[v * P.nw + lane] = bits;
+      if (lane == 0) {
+        P.iters[v] = (uint16_t)(it + 1);
+        uint8_t st = P.status[v];
+        if (conv) {
+          P.status[v] = (uint8_t)(CSD_STATUS_CONVERGED | (st & 0x70));
+        } else {
+          if (!warm && it >= 2 && back) st |= kCycling;
+          P.status[v] = st;
+          P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
+        }
+      }
+    }
+  }
+}
+
+// Solve pass: warp per voxel of the solve list (csd.h:255-266).
+template <int N>
+__global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_solve_kernel(const __grid_constant__ StateParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int HS = Dims<N>::HS;
   const HTab<N> H = load_htab<N>(smem, P.sc, P.nhr);
@@ -276,47 +411,26 @@ __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_state_iterate_kernel(
   const int gw = blockIdx.x * nwarps + warp, nwt = gridDim.x * nwarps;
   for (int e = gw; e < P.n_in; e += nwt) {
     const long long v = P.act_in[e];
-    for (int c = lane; c < HS; c += 32) w.F[c] = P.F[v * HS + c];
     for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
-    __syncwarp();
-    const int it = P.iters[v];
+    for (int c = lane; c < HS; c += 32) w.F[c] = 0.f;
     uint32_t bits[kMaxWords];
-    if (it == 0 && P.use_warm && P.warm) {
 #pragma unroll
-      for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.warm[v * P.nw + p] : 0u;
-      if (P.nhr & 31) bits[P.nw - 1] &= (1u << (P.nhr & 31)) - 1u;
-    } else {
-      project_mask<N>(H, P.nw, P.sc.threshold, w, lane, bits);
-      if (it > 0) {
-        bool same = true;
-#pragma unroll
-        for (int p = 0; p < kMaxWords; ++p)
-          if (p < P.nw) same = same && (bits[p] == P.old[v * P.nw + p]);
-        if (same) {
-          if (lane == 0) {
-            P.iters[v] = (uint16_t)(it + 1);
-            P.status[v] = (uint8_t)(CSD_STATUS_CONVERGED | (P.status[v] == 0xFF ? 0 : (P.status[v] & 0xF0)));
-          }
-          continue;
-        }
-      }
-    }
+    for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.newm[v * P.nw + p] : 0u;
+    __syncwarp();
+    const uint8_t st = P.status[v];
     const int k = mask_to_list(bits, P.nw, w.neg, lane);
-    const int fl = assemble_solve<N>(P.sc, H, k, w, lane, P.cond_thr, P.refine ? 1 : 0, slot) & 0xF0;
+    const int fl = assemble_solve<N>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot) & 0x70;
     for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
-#pragma unroll
-    for (int p = 0; p < kMaxWords; ++p)
-      if (p < P.nw && p == lane) P.old[v * P.nw + p] = bits[p];
+    if (lane < P.nw) {
+      P.old2[v * P.nw + lane] = P.old[v * P.nw + lane];
+      P.old[v * P.nw + lane] = P.newm[v * P.nw + lane];
+    }
     if (lane == 0) {
-      const int nit = it + 1;
-      P.iters[v] = (uint16_t)nit;
-      // status holds 0xFF while active with no flags; flags accumulate in the high nibble
-      uint8_t stv = P.status[v];
-      uint8_t flags = (uint8_t)((stv == 0xFF ? 0 : (stv & 0xF0)) | fl);
-      if (nit >= P.sc.niter) {
-        P.status[v] = (uint8_t)(CSD_STATUS_NITER | flags);
+      const uint8_t flags = (uint8_t)((st & 0xF0) | fl);
+      if (P.iters[v] >= P.sc.niter) {
+        P.status[v] = (uint8_t)(CSD_STATUS_NITER | (flags & 0x70));
       } else {
-        P.status[v] = flags ? (uint8_t)(0x0F | flags) : (uint8_t)0xFF;
+        P.status[v] = (uint8_t)(kActive | flags);
         P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
       }
     }
@@ -334,8 +448,8 @@ __global__ void csd_state_fod_kernel(const float* F, const uint8_t* status, cons
   fod[v * fod_stride + c] = F[v * Dims<N>::HS + c];
   if (c == 0) {
     uint8_t s = status[v];
-    if (s == 0xFF) s = CSD_STATUS_NITER;               // still iterating: not converged yet
-    else if ((s & 0x0F) == 0x0F) s = (uint8_t)(CSD_STATUS_NITER | (s & 0xF0));
+    if ((s & 0x0F) == 0x0F) s = (uint8_t)(CSD_STATUS_NITER | (s & 0x70));  // still iterating
+    else s = (uint8_t)(s & 0x7F);
     if (st_out) st_out[v] = s;
     if (it_out) it_out[v] = (uint8_t)(iters[v] > 255 ? 255 : iters[v]);
     if (neg_out)
@@ -357,11 +471,14 @@ struct csd_shared {
   int HS = 0, WSZ = 0;
   std::vector<float> H32_host;
   std::vector<__half> H16_host;    // [2][nhr+1][HS16]: hi then lo
+  std::vector<__half> Hp16_host;   // [2][npd][HS16]: projection table, hi then lo
+  int npd = 0;                     // directions padded to a multiple of 320
   std::vector<float> MtMp_host;
   std::vector<float> rconvT_host;
   std::vector<float> M32_host;
   float* H32 = nullptr;
   __half* H16 = nullptr;
+  __half* Hp16 = nullptr;
   double* H64 = nullptr;
   float* MtMp = nullptr;
   double* MtM64 = nullptr;
@@ -452,6 +569,13 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
       s->H16_host[(size_t)d * HS16 + c] = hi;
       s->H16_host[(size_t)(h.nhr + 1 + d) * HS16 + c] = lo;
     }
+  s->npd = (h.nhr + 319) / 320 * 320;
+  s->Hp16_host.assign((size_t)2 * s->npd * HS16, __float2half_rn(0.f));
+  for (int d = 0; d < h.nhr; ++d)
+    for (int c = 0; c < n; ++c) {
+      s->Hp16_host[(size_t)d * HS16 + c] = s->H16_host[(size_t)d * HS16 + c];
+      s->Hp16_host[(size_t)(s->npd + d) * HS16 + c] = s->H16_host[(size_t)(h.nhr + 1 + d) * HS16 + c];
+    }
   s->MtMp_host.assign((size_t)s->WSZ, 0.f);
   for (int i = 0; i < n; ++i)
     for (int j = 0; j <= i; ++j) s->MtMp_host[packoff(i) + j] = (float)h.MtM[(size_t)i * n + j];
@@ -477,6 +601,7 @@ static int ensure_device(const csd_shared* cs) {
   const HostShared& h = s->h;
   if ((rc = upload(&s->H32, s->H32_host))) return rc;
   if ((rc = upload(&s->H16, s->H16_host))) return rc;
+  if ((rc = upload(&s->Hp16, s->Hp16_host))) return rc;
   if ((rc = upload(&s->H64, h.HR))) return rc;
   if ((rc = upload(&s->MtMp, s->MtMp_host))) return rc;
   if ((rc = upload(&s->MtM64, h.MtM))) return rc;
@@ -495,6 +620,7 @@ extern "C" void csd_shared_destroy(csd_shared* s) {
     cudaSetDevice(s->device);
     cudaFree(s->H32);
     cudaFree(s->H16);
+    cudaFree(s->Hp16);
     cudaFree(s->H64);
     cudaFree(s->MtMp);
     cudaFree(s->MtM64);
@@ -824,15 +950,21 @@ struct csd_state {
   float* F = nullptr;
   double* b = nullptr;
   uint32_t* old = nullptr;
+  uint32_t* old2 = nullptr;
+  uint32_t* newm = nullptr;
   uint32_t* warm = nullptr;
   uint8_t* status = nullptr;
   uint16_t* iters = nullptr;
   int* act[2] = {nullptr, nullptr};
+  int* slist = nullptr;
   int* counter = nullptr;
   int cur = 0;
   double* fp64 = nullptr;
   int blocks = 0, warps = 0;
   size_t smem = 0;
+  int proj_blocks = 0;
+  size_t proj_smem = 0;
+  long long passes = 0, projected = 0, solved = 0;  // work counters since the last set()
 };
 
 namespace {
@@ -845,7 +977,17 @@ int state_shape(csd_state* st) {
   st->warps = ls.warps;
   st->smem = ls.smem;
   CUDA_TRY(cudaMalloc(&st->fp64, (size_t)ls.blocks * ls.warps * Dims<N>::WSZ * sizeof(double)));
-  CUDA_TRY(cudaFuncSetAttribute(csd_state_iterate_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem));
+  CUDA_TRY(cudaFuncSetAttribute(csd_solve_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem));
+  int dev = 0, smem_max = 0, nsm = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const size_t psm = (size_t)2 * st->sh->npd * Dims<N>::HS16 * 2 + (size_t)2 * kProjRows * Dims<N>::HS16 * 2 +
+                     (size_t)kProjRows * kMaxWords * 4;
+  if (psm > (size_t)smem_max) return fail(CSD_ERR_UNSUPPORTED, "projection tables too large for shared memory");
+  st->proj_smem = psm;
+  st->proj_blocks = nsm * std::max(1, (int)(smem_max / psm));
+  CUDA_TRY(cudaFuncSetAttribute(csd_project_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
   CUDA_TRY(cudaFuncSetAttribute(csd_state_set_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(8 * warp_ws_bytes<N>())));
   return 0;
@@ -857,11 +999,15 @@ StateParams state_params(const csd_state* st) {
   P.sc = scheme_of(st->sh);
   P.nhr = st->sh->h.nhr;
   P.nw = (P.nhr + 31) / 32;
-  P.refine = refine_of(st->sh);
+  P.npd = st->sh->npd;
+  P.Hp16 = st->sh->Hp16;
+  P.thr_scaled = (float)(st->sh->h.threshold * kProjFScale);
   P.cond_thr = (float)st->sh->cond_thr;
   P.F = st->F;
   P.b = st->b;
   P.old = st->old;
+  P.old2 = st->old2;
+  P.newm = st->newm;
   P.warm = st->warm;
   P.use_warm = st->use_warm;
   P.status = st->status;
@@ -879,9 +1025,16 @@ int state_set_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
   return 0;
 }
 template <int N>
-int state_iter_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+int state_project_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  const int tiles = (P.n_in + kProjRows - 1) / kProjRows;
+  csd_project_kernel<N><<<std::max(1, std::min(tiles, st->proj_blocks)), 256, st->proj_smem, s>>>(P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+template <int N>
+int state_solve_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
   const int need = (int)std::min<long long>(st->blocks, (P.n_in + st->warps - 1) / st->warps);
-  csd_state_iterate_kernel<N><<<std::max(need, 1), st->warps * 32, st->smem, s>>>(P);
+  csd_solve_kernel<N><<<std::max(need, 1), st->warps * 32, st->smem, s>>>(P);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -922,7 +1075,10 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->F, (size_t)capacity * HS * sizeof(float)));
   CUDA_TRY(cudaMalloc(&st->b, (size_t)capacity * n * sizeof(double)));
   CUDA_TRY(cudaMalloc(&st->old, (size_t)capacity * nw * sizeof(uint32_t)));
+  CUDA_TRY(cudaMalloc(&st->old2, (size_t)capacity * nw * sizeof(uint32_t)));
+  CUDA_TRY(cudaMalloc(&st->newm, (size_t)capacity * nw * sizeof(uint32_t)));
   CUDA_TRY(cudaMalloc(&st->warm, (size_t)capacity * nw * sizeof(uint32_t)));
+  CUDA_TRY(cudaMalloc(&st->slist, (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->status, (size_t)capacity));
   CUDA_TRY(cudaMalloc(&st->iters, (size_t)capacity * sizeof(uint16_t)));
   CUDA_TRY(cudaMalloc(&st->act[0], (size_t)capacity * sizeof(int)));
@@ -940,7 +1096,10 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->F);
   cudaFree(st->b);
   cudaFree(st->old);
+  cudaFree(st->old2);
+  cudaFree(st->newm);
   cudaFree(st->warm);
+  cudaFree(st->slist);
   cudaFree(st->status);
   cudaFree(st->iters);
   cudaFree(st->act[0]);
@@ -958,6 +1117,7 @@ extern "C" int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, 
   st->n = n_voxels;
   st->use_warm = 0;
   st->cur = 0;
+  st->passes = st->projected = st->solved = 0;
   CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
   if (n_voxels == 0) {
     st->n_active = 0;
@@ -994,19 +1154,36 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
   if (!st) return fail(CSD_ERR_INVALID, "csd_state_iterate: NULL state");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (st->n_active > 0) {
+    int rc = 0;
+    // pass 1: dense projection of every active voxel -> solve list
     StateParams P = state_params(st);
     P.n_in = (int)st->n_active;
     P.act_in = st->act[st->cur];
-    P.act_out = st->act[st->cur ^ 1];
+    P.act_out = st->slist;
     CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
-    int rc = 0;
-    CSD_DISPATCH(st->sh->h.nsh, rc = state_iter_launch<NN>(st, P, s));
+    CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
     if (rc) return rc;
-    int na = 0;
-    CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int ns = 0;
+    CUDA_TRY(cudaMemcpyAsync(&ns, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    st->projected += st->n_active;
+    // pass 2: assemble + factorise the voxels whose set changed -> next active list
+    int na = 0;
+    if (ns > 0) {
+      StateParams Q = state_params(st);
+      Q.n_in = ns;
+      Q.act_in = st->slist;
+      Q.act_out = st->act[st->cur ^ 1];
+      CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Q, s));
+      if (rc) return rc;
+      CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaStreamSynchronize(s));
+      st->solved += ns;
+    }
     st->n_active = na;
     st->cur ^= 1;
+    st->passes += 1;
   }
   if (n_active) *n_active = st->n_active;
   return CSD_OK;

@@ -76,6 +76,8 @@ struct Dims {
   static constexpr bool KEEP32 = N <= 45;         // FP32 HR table kept in shared memory
   // threads per block of the persistent kernel (bounds the register budget)
   static constexpr int THREADS = N <= 45 ? 512 : (N <= 66 ? 384 : 192);
+  // threads per block of the phased solve kernel (no FP32 table, split assembly)
+  static constexpr int SOLVE_THREADS = N <= 45 ? 640 : THREADS;
 };
 
 // Everything a voxel of one image needs, by device pointer.
@@ -116,12 +118,12 @@ struct SolveParams {
 
 // Bytes of the constraint tables a block keeps in shared memory.
 template <int N>
-__host__ __device__ constexpr int htab_bytes_32(int nhr) {
-  return Dims<N>::KEEP32 ? ((nhr * Dims<N>::HS * 4 + 15) / 16) * 16 : 0;
+__host__ __device__ constexpr int htab_bytes_32(int nhr, bool use32 = true) {
+  return (Dims<N>::KEEP32 && use32) ? ((nhr * Dims<N>::HS * 4 + 15) / 16) * 16 : 0;
 }
 template <int N>
-__host__ __device__ constexpr int htab_bytes(int nhr) {
-  return htab_bytes_32<N>(nhr) + 2 * (nhr + 1) * Dims<N>::HS16 * 2;
+__host__ __device__ constexpr int htab_bytes(int nhr, bool use32 = true) {
+  return htab_bytes_32<N>(nhr, use32) + 2 * (nhr + 1) * Dims<N>::HS16 * 2;
 }
 
 // Shared-memory view of the constraint tables.
@@ -131,10 +133,11 @@ struct HTab {
   const __half* hh;   // [nhr+1][HS16]
   const __half* hl;   // [nhr+1][HS16]
   int nhr;
+  bool use32;         // read FP32 values from h32 (else re-sum the FP16 pair)
 
   // FP32 values of row d, columns 4j..4j+3
   __device__ __forceinline__ float4 quad(int d, int j) const {
-    if constexpr (Dims<N>::KEEP32) {
+    if (Dims<N>::KEEP32 && use32) {
       return reinterpret_cast<const float4*>(h32 + d * Dims<N>::HS)[j];
     } else {
       const uint2 a = *reinterpret_cast<const uint2*>(hh + d * Dims<N>::HS16 + 4 * j);
@@ -147,7 +150,7 @@ struct HTab {
     }
   }
   __device__ __forceinline__ float val(int d, int i) const {
-    if constexpr (Dims<N>::KEEP32) {
+    if (Dims<N>::KEEP32 && use32) {
       return h32[d * Dims<N>::HS + i];
     } else {
       return __half2float(hh[d * Dims<N>::HS16 + i]) + __half2float(hl[d * Dims<N>::HS16 + i]);
@@ -157,12 +160,13 @@ struct HTab {
 
 // Copy a scheme's constraint tables into shared memory (whole block).
 template <int N>
-__device__ HTab<N> load_htab(unsigned char* smem, const Scheme& sc, int nhr) {
+__device__ HTab<N> load_htab(unsigned char* smem, const Scheme& sc, int nhr, bool use32 = true) {
   HTab<N> t;
   t.nhr = nhr;
-  const int b32 = htab_bytes_32<N>(nhr);
+  t.use32 = Dims<N>::KEEP32 && use32;
+  const int b32 = htab_bytes_32<N>(nhr, use32);
   t.h32 = reinterpret_cast<const float*>(smem);
-  if constexpr (Dims<N>::KEEP32) {
+  if (t.use32) {
     const float4* src = reinterpret_cast<const float4*>(sc.H32);
     float4* dst = reinterpret_cast<float4*>(smem);
     for (int i = threadIdx.x; i < nhr * Dims<N>::HS / 4; i += blockDim.x) dst[i] = __ldg(src + i);
@@ -422,10 +426,15 @@ __device__ __forceinline__ void assemble_pass(const HTab<N>& H, const float* MtM
   }
 }
 
-template <int N>
+template <int N, bool SPLIT = false>
 __device__ void assemble(const HTab<N>& H, const float* MtMp, int k, const WarpWS<N>& w, int lane) {
   constexpr int R = Dims<N>::NRB;
-  if constexpr (R <= 3) {
+  if constexpr (SPLIT && R == 3) {
+    // one 16-row block per pass: fewer live accumulators for high occupancy
+    assemble_pass<N, 0, 1>(H, MtMp, k, w, lane);
+    assemble_pass<N, 1, 2>(H, MtMp, k, w, lane);
+    assemble_pass<N, 2, 3>(H, MtMp, k, w, lane);
+  } else if constexpr (R <= 3) {
     assemble_pass<N, 0, R>(H, MtMp, k, w, lane);
   } else if constexpr (R <= 5) {
     assemble_pass<N, 0, 3>(H, MtMp, k, w, lane);
@@ -870,11 +879,11 @@ __device__ bool solve_fp64(const Scheme& sc, int k, const WarpWS<N>& w, double* 
 // result when refine == 1.  Returns status flags (0x10 FP64 used, 0x20 the
 // FP64 factorisation failed too); bit 0x100 marks that w.W holds no usable
 // FP32 factor (the FP64 path ran).
-template <int N>
+template <int N, bool SPLIT = false>
 __device__ int assemble_solve(const Scheme& sc, const HTab<N>& H, int k, const WarpWS<N>& w, int lane,
                               float cond_thr, int refine, double* fp64_slot, long long* tacc = nullptr) {
   CSD_T0(t0);
-  assemble<N>(H, sc.MtMp, k, w, lane);
+  assemble<N, SPLIT>(H, sc.MtMp, k, w, lane);
   // append b as row N: the factorisation then leaves y = L^-1 b in that row
   {
     float* bN = w.W + packoff(N);

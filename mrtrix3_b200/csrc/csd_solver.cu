@@ -399,14 +399,14 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
 
 // Solve pass: warp per voxel of the solve list (csd.h:255-266).
 template <int N>
-__global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_solve_kernel(const __grid_constant__ StateParams P) {
+__global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(const __grid_constant__ StateParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int HS = Dims<N>::HS;
-  const HTab<N> H = load_htab<N>(smem, P.sc, P.nhr);
+  const HTab<N> H = load_htab<N>(smem, P.sc, P.nhr, false);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  WarpWS<N> w = carve_ws<N>(smem + htab_bytes<N>(P.nhr) + warp * warp_ws_bytes<N>());
+  WarpWS<N> w = carve_ws<N>(smem + htab_bytes<N>(P.nhr, false) + warp * warp_ws_bytes<N>());
   double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
   const int gw = blockIdx.x * nwarps + warp, nwt = gridDim.x * nwarps;
   for (int e = gw; e < P.n_in; e += nwt) {
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_solve_kernel(const __
     __syncwarp();
     const uint8_t st = P.status[v];
     const int k = mask_to_list(bits, P.nw, w.neg, lane);
-    const int fl = assemble_solve<N>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot) & 0x70;
+    const int fl = assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot) & 0x70;
     for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
     if (lane < P.nw) {
       P.old2[v * P.nw + lane] = P.old[v * P.nw + lane];
@@ -971,8 +971,18 @@ namespace {
 template <int N>
 int state_shape(csd_state* st) {
   LaunchShape ls;
-  int rc = shape_for<N>(st->sh->h.nhr, 1LL << 40, &ls);
-  if (rc) return rc;
+  {
+    int dev = 0, smem_max = 0, nsm = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const size_t hbytes = (size_t)htab_bytes<N>(st->sh->h.nhr, false);
+    const size_t wb = warp_ws_bytes<N>();
+    if (hbytes + wb > (size_t)smem_max) return fail(CSD_ERR_UNSUPPORTED, "constraint set too large for shared memory");
+    ls.warps = (int)std::min<size_t>(Dims<N>::SOLVE_THREADS / 32, ((size_t)smem_max - hbytes) / wb);
+    ls.smem = hbytes + wb * ls.warps;
+    ls.blocks = nsm;
+  }
   st->blocks = ls.blocks;
   st->warps = ls.warps;
   st->smem = ls.smem;

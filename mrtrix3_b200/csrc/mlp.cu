@@ -246,11 +246,12 @@ int gemm(const GemmArgs& a0, int splits, cudaStream_t st) {
 
 // x[v][t] = (S_t / mean_b0 - mu_t) * inv_sd_t for t < n_in, zero up to ld.
 __global__ void mlp_inputs_kernel(const float* dwi, long long n, long long vs, long long ts, int n_in, int ld,
-                                  const int* b0, int n_b0, const float* mu, const float* isd, bf16* x) {
+                                  const int* b0, int n_b0, const float* mu, const float* isd, const int* index,
+                                  bf16* x) {
   const long long v = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x & 31;
   if (v >= n) return;
-  const float* d = dwi + v * vs;
+  const float* d = dwi + (index ? (long long)index[v] : v) * vs;
   float s0 = 0.f;
   for (int i = lane; i < n_b0; i += 32) {
     const float x0 = d[(long long)b0[i] * ts];
@@ -327,17 +328,28 @@ __global__ void mlp_to_bf16_kernel(const float* w, long long n, bf16* w16) {
 
 // negmask[v][w] bit b = logit[v][32 w + b] > thr (thr = 0: sigmoid > 1/2);
 // masked-out voxels get an empty set.
-__global__ void mlp_pack_kernel(const float* z, long long rows, int n_out, int ld, int nw, const uint8_t* mask,
+__global__ void mlp_pack_kernel(const float* z, long long rows, int n_out, int ld, int nw, const int* index,
                                 float thr, uint32_t* out) {
-  const long long wid = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const long long r = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x & 31;
-  if (wid >= rows * nw) return;
-  const long long r = wid / nw;
-  const int w = (int)(wid - r * nw);
-  const int c = 32 * w + lane;
-  const bool neg = c < n_out && z[r * ld + c] > thr && (!mask || mask[r]);
-  const uint32_t bits = __ballot_sync(0xffffffffu, neg);
-  if (lane == 0) out[r * nw + w] = bits;
+  if (r >= rows) return;
+  const long long o = (index ? (long long)index[r] : r) * nw;
+  for (int w = 0; w < nw; ++w) {
+    const int c = 32 * w + lane;
+    const uint32_t bits = __ballot_sync(0xffffffffu, c < n_out && z[r * ld + c] > thr);
+    if (lane == 0) out[o + w] = bits;
+  }
+}
+
+// index[] = positions of the voxels with mask != 0 (order not preserved)
+__global__ void mlp_compact_kernel(const uint8_t* mask, long long n, int* index, int* count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool on = i < n && mask[i];
+  const unsigned b = __ballot_sync(0xffffffffu, on);
+  int base = 0;
+  if ((threadIdx.x & 31) == 0 && b) base = atomicAdd(count, __popc(b));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (on) index[base + __popc(b & ((1u << (threadIdx.x & 31)) - 1u))] = (int)i;
 }
 
 }  // namespace
@@ -370,6 +382,8 @@ struct csd_mlp {
        *da1 = nullptr;
   float* z = nullptr;
   float* loss = nullptr;
+  int* idx = nullptr;          // compacted voxel index list for masked prediction
+  long long idx_cap = 0;
 };
 
 static int mlp_reserve(csd_mlp* m, long long rows) {
@@ -453,7 +467,7 @@ extern "C" int csd_mlp_create(int n_in, int n_hidden, int n_out, uint64_t seed, 
 extern "C" void csd_mlp_destroy(csd_mlp* m) {
   if (!m) return;
   void* ps[] = {m->w, m->g, m->am, m->av, m->w16, m->b0, m->mu, m->isd, m->x, m->a1, m->h1, m->a2, m->h2,
-                m->dz, m->da2, m->da1, m->z, m->loss};
+                m->dz, m->da2, m->da1, m->z, m->loss, m->idx};
   for (void* p : ps) cudaFree(p);
   delete m;
 }
@@ -494,10 +508,10 @@ extern "C" int csd_mlp_set_inputs(csd_mlp* m, const int* b0_index, int n_b0, con
 }
 
 static int mlp_inputs(const csd_mlp* m, const float* dwi, long long n, long long vs, long long ts, bf16* x,
-                      cudaStream_t st) {
+                      cudaStream_t st, const int* index = nullptr) {
   if (n <= 0) return 0;
   mlp_inputs_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(dwi, n, vs, ts, m->n_in, m->ld_in, m->b0,
-                                                            (int)m->b0_host.size(), m->mu, m->isd, x);
+                                                            (int)m->b0_host.size(), m->mu, m->isd, index, x);
   MLP_TRY(cudaGetLastError());
   return 0;
 }
@@ -631,24 +645,50 @@ extern "C" int csd_mlp_train_epoch(csd_mlp* m, const uint16_t* x, const uint32_t
   return CSD_OK;
 }
 
-// Predicted first negative sets for n voxels of a DWI volume (device).
+// Predicted first negative sets for n voxels of a DWI volume (device).  With
+// a mask, only the voxels inside it go through the network (the others get
+// an empty set).
 extern "C" int csd_mlp_predict(csd_mlp* m, const float* dwi, int64_t n_voxels, int64_t voxel_stride,
                                int64_t volume_stride, const uint8_t* mask, float logit_threshold, uint32_t* negmask,
                                void* stream) {
   if (!m || n_voxels < 0 || (n_voxels > 0 && (!dwi || !negmask)) || !m->b0)
     return mfail(CSD_ERR_INVALID, "csd_mlp_predict: invalid argument (inputs not configured?)");
+  if (n_voxels == 0) return CSD_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const long long chunk = 1 << 18;
-  int rc = mlp_reserve(m, std::min<long long>(chunk, std::max<long long>(n_voxels, 1)));
+  int rc = mlp_reserve(m, std::min<long long>(chunk, n_voxels));
   if (rc) return rc;
-  for (long long a = 0; a < n_voxels; a += chunk) {
-    const long long n = std::min<long long>(chunk, n_voxels - a);
-    if ((rc = mlp_inputs(m, dwi + a * voxel_stride, n, voxel_stride, volume_stride, m->x, st))) return rc;
-    if ((rc = mlp_forward(m, m->x, n, st))) return rc;
-    const long long words = n * m->nw;
-    mlp_pack_kernel<<<(unsigned)((words + 7) / 8), 256, 0, st>>>(m->z, n, m->n_out, m->ld_out, m->nw,
-                                                                mask ? mask + a : nullptr, logit_threshold,
-                                                                negmask + a * m->nw);
+  const int* index = nullptr;
+  long long n = n_voxels;
+  if (mask) {
+    if (m->idx_cap < n_voxels) {
+      cudaFree(m->idx);
+      m->idx = nullptr;
+      m->idx_cap = 0;
+      MLP_TRY(cudaMalloc(&m->idx, (n_voxels + 1) * sizeof(int)));
+      m->idx_cap = n_voxels;
+    }
+    MLP_TRY(cudaMemsetAsync(m->idx + n_voxels, 0, sizeof(int), st));
+    mlp_compact_kernel<<<(unsigned)((n_voxels + 255) / 256), 256, 0, st>>>(mask, n_voxels, m->idx, m->idx + n_voxels);
+    MLP_TRY(cudaGetLastError());
+    int cnt = 0;
+    MLP_TRY(cudaMemcpyAsync(&cnt, m->idx + n_voxels, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MLP_TRY(cudaMemsetAsync(negmask, 0, (size_t)n_voxels * m->nw * sizeof(uint32_t), st));
+    MLP_TRY(cudaStreamSynchronize(st));
+    index = m->idx;
+    n = cnt;
+  }
+  for (long long a = 0; a < n; a += chunk) {
+    const long long c = std::min<long long>(chunk, n - a);
+    if (index) {
+      if ((rc = mlp_inputs(m, dwi, c, voxel_stride, volume_stride, m->x, st, index + a))) return rc;
+    } else {
+      if ((rc = mlp_inputs(m, dwi + a * voxel_stride, c, voxel_stride, volume_stride, m->x, st))) return rc;
+    }
+    if ((rc = mlp_forward(m, m->x, c, st))) return rc;
+    mlp_pack_kernel<<<(unsigned)((c + 7) / 8), 256, 0, st>>>(m->z, c, m->n_out, m->ld_out, m->nw,
+                                                             index ? index + a : nullptr, logit_threshold,
+                                                             index ? negmask : negmask + a * m->nw);
     MLP_TRY(cudaGetLastError());
   }
   return CSD_OK;

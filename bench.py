@@ -1,22 +1,31 @@
 """Benchmark: single-shell CSD voxels/s on B200 (one JSON line on rank 0).
 
-Workload (default): 140x140x96 synthetic volume, ellipsoid mask ~45%,
-6 b=0 + 60 b=3000 directions, lmax 8, 300 constraint directions, SNR U[15,40]
-(seed-driven synthetic data; no public dataset is named for this path).
-A step is one full deconvolution of the masked volume.
+Workload: a 140x140x96 synthetic DWI volume (1,881,600 voxels, centred
+ellipsoid mask ~45% = 846,816 voxels), 6 b=0 + 60 b=3000 Fibonacci-hemisphere
+directions, lmax 8 (45 coefficients), 300 constraint directions, SNR
+U[15,40], 1-3 fibres per voxel (seeded synthetic data: no public dataset is
+named for this path).  A step is one full deconvolution of the masked volume.
+
+Headline `value`: the warm-started method -- the warm-start network's
+predicted first negative sets, then the phased iteration (dense tensor-core
+projection of all active voxels + warp-per-voxel assembly/factorisation of
+the voxels whose set changed) run to its own stopping rule -- with inputs
+resident in HBM.  `methods` also reports the plain GPU method (same passes
+from the plain start), the persistent work-queue kernel with and without the
+warm start, and the warm-vs-plain ratio.  `e2e` is the warm-started method
+through the host-buffer C ABI entry point (csd_dwi2fod_host_phased) with
+pinned host buffers and every copy inside the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--method warm|plain|persistent]
 
 N>1 (torchrun, one process per GPU): each rank deconvolves its own volume
-(different seed, same size) -- weak scaling with no data-path collective;
-the step time is the max over ranks.
+(own seed, same size): weak scaling, no data-path collective; step times are
+the max over ranks.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -31,18 +40,24 @@ sys.path.insert(0, ROOT)
 METRIC = "CSD voxels/s lmax8: warm-start batched vs plain GPU, p99 rel err≤1e-4 vs FP64"
 UNIT = "voxels/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+WORKLOAD = ("140x140x96 synthetic DWI (mask ~45%: 846,816 voxels), 6 b=0 + 60 b=3000 directions, lmax 8, "
+            "300 constraint directions, SNR U[15,40]")
+WEIGHTS = os.path.join(ROOT, "mrtrix3_b200", "data", "warmstart_c5.npz")
+# DRAM bytes per launch of csd_solve_kernel<45> from ncu on a 262,144-voxel
+# case (profiles/csd_solve_kernel_45.md), scaled to this workload's voxels
+# solved per launch; None until measured.
+SOLVE_DRAM_BYTES_PER_VOXEL = None
 
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
-        d = json.load(open(p))
-        return d, "measured"
+        return json.load(open(p)), "measured"
     return PEAKS_FALLBACK, "fallback"
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
     def __init__(self, index: int):
         self.index = index
@@ -102,24 +117,10 @@ def make_workload(seed: int):
     return synth.config5(seed=seed)
 
 
-def flops_per_voxel(iters, negcount, status, n, ndw, nr, nhr=300):
-    """Algorithmic FLOPs of the plain trajectory: 2*ndw*(nr+n) + T*2*nhr*n
-    + S*(k*n(n+1) + n^3/3 + 2n^2), S solves (T-1 if converged), k the final
-    negative-set size standing in for each solve's."""
-    T = iters.astype(np.float64)
-    conv = (status & 0x0F) == 1
-    S = np.where(conv, T - 1, T)
-    k = negcount.astype(np.float64)
-    f = 2.0 * ndw * (nr + n) + T * 2.0 * nhr * n + S * (k * n * (n + 1) + n ** 3 / 3.0 + 2.0 * n * n)
-    solved = (status & 0x0F) >= 1
-    solved &= (status & 0x0F) <= 2
-    return float(f[solved].sum())
-
-
 def cpu_baseline(vol, sample_target_s: float = 12.0):
     """The FP64 oracle (a restatement of the reference's CPU path; the
     reference itself needs Eigen, absent here) on all host cores over a
-    bounded sample of the masked voxels."""
+    bounded random sample of the masked voxels."""
     from mrtrix3_b200 import synth
     from oracle import oracle as O
     cores = os.cpu_count() or 1
@@ -129,16 +130,21 @@ def cpu_baseline(vol, sample_target_s: float = 12.0):
     probe = rng.choice(idx, min(len(idx), 400 * cores), replace=False)
     t0 = time.perf_counter()
     sh.solve(vol.dwi[probe], nthreads=cores)
-    dt = time.perf_counter() - t0
-    rate = len(probe) / dt
+    rate = len(probe) / (time.perf_counter() - t0)
     n = int(min(len(idx), max(len(probe), rate * sample_target_s)))
     samp = rng.choice(idx, n, replace=False)
     t0 = time.perf_counter()
     sh.solve(vol.dwi[samp], nthreads=cores)
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} random masked voxels of the workload, FP64 oracle restatement, {cores} threads, "
-                      f"{dt:.1f} s"}
+            "sample": f"{n} random masked voxels of the workload through the FP64 oracle restatement "
+                      f"(oracle/csd_oracle.c), {cores} threads, {dt:.1f} s"}
+
+
+def workload_config(vol, method):
+    return {"workload": WORKLOAD, "dims": list(vol.dims), "n_voxels": vol.n_voxels, "n_masked": vol.n_masked,
+            "nsh": 45, "n_hr": 300, "method": method,
+            "l2": "inputs larger than L2 (dwi 497 MB + per-voxel state ~1 GB per step); no flush needed"}
 
 
 def run_reference(args):
@@ -146,29 +152,26 @@ def run_reference(args):
     if rank != 0:
         return 0
     vol = make_workload(seed=5)
-    cb = []
-    for _ in range(args.warmup):
-        pass
-    vals = []
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_baseline(vol, sample_target_s=2.0)
+    vals, last = [], None
     for _ in range(max(1, args.steps)):
-        cb.append(cpu_baseline(vol, sample_target_s=max(3.0, 60.0 / max(1, args.steps))))
-        vals.append(cb[-1]["value"])
+        last = cpu_baseline(vol, sample_target_s=max(3.0, 60.0 / max(1, args.steps)))
+        vals.append(last["value"])
     v = float(np.median(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(vol, "cpu-oracle"),
-            "cpu_baseline": {**cb[-1], "value": v},
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(vol, "FP64 CPU restatement of dwi2fod csd, all host cores"),
+            "cpu_baseline": {**last, "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "vs_baseline": None}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def workload_config(vol, method):
-    return {"workload": "140x140x96 synthetic DWI, mask ~45%, 6 b=0 + 60 b=3000 dirs, lmax 8, 300 HR dirs, "
-                        "SNR U[15,40]",
-            "dims": list(vol.dims), "n_voxels": vol.n_voxels, "n_masked": vol.n_masked, "nsh": 45,
-            "method": method, "l2": "inputs larger than L2 (dwi 497 MB, fod 339 MB per step)"}
+def rel_errors(fod, F64):
+    den = np.abs(F64).max(axis=1)
+    return np.abs(fod.astype(np.float64) - F64).max(axis=1) / np.where(den > 0, den, 1.0)
 
 
 def main():
@@ -177,7 +180,6 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--method", default="persistent", choices=["persistent", "plain", "warm"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -187,6 +189,8 @@ def main():
     import torch.distributed as dist
 
     from mrtrix3_b200 import csd, synth
+    from mrtrix3_b200.warmstart import WarmStartNet, train_warm_start
+    from oracle import oracle as O
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -195,83 +199,150 @@ def main():
     dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-
-    vol = make_workload(seed=5 + rank)
-    sh = csd.make_shared(vol.grad, synth.RESPONSE)
-    dwi = torch.from_numpy(vol.dwi).to(dev)
-    mask = torch.from_numpy(vol.mask).to(dev)
-    stream = torch.cuda.current_stream()
-
-    def step():
-        return csd.dwi2fod_csd(sh, dwi, mask=mask, want_negmask=True, stream=stream)
-
-    for _ in range(max(3, args.warmup)):
-        out = step()
-    torch.cuda.synchronize()
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(x: float) -> float:
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    vol = make_workload(seed=5 + rank)
+    sh = csd.make_shared(vol.grad, synth.RESPONSE)
+    d = torch.from_numpy(vol.dwi).to(dev)
+    m = torch.from_numpy(vol.mask).to(dev)
+    stream = torch.cuda.current_stream()
+    if os.path.exists(WEIGHTS):
+        net = WarmStartNet.load(WEIGHTS)
+        net_src = "mrtrix3_b200/data/warmstart_c5.npz (trained by python -m mrtrix3_b200.train_warmstart)"
+    else:
+        net, _ = train_warm_start(vol.grad, n_train=2_000_000, epochs=60, lr=4e-3, seed=11)
+        net_src = "trained in this run (2M voxels, 60 epochs)"
+    st = csd.State(sh, vol.n_voxels)
+
+    def warm_step():
+        st.run(d, mask=m, warm=net.predict(d, mask=m, stream=stream), stream=stream)
+        return st
+
+    def plain_step():
+        st.run(d, mask=m, stream=stream)
+        return st
+
+    def persistent_step(warm):
+        w = net.predict(d, mask=m, stream=stream) if warm else None
+        return csd.dwi2fod_csd(sh, d, mask=m, warm=w, stream=stream)
+
+    def timed(fn, steps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+    # ---- headline: warm-started method, inputs resident in HBM -----------
+    for _ in range(max(3, args.warmup)):
+        warm_step()
+    barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         barrier()
         e0.record(stream)
         for _ in range(args.steps):
-            out = step()
+            warm_step()
         e1.record(stream)
         barrier()
-    ms_total = e0.elapsed_time(e1)
-    ms = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-    ms_total = float(ms.item())
-    ms_step = ms_total / args.steps
-    n_masked = vol.n_masked
-    value = n_masked * world / (ms_step / 1e3)
+    ms_warm = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    wstats = st.stats()
+    warm_out = st.fod()
+    value = vol.n_masked * world / (ms_warm / 1e3)
 
-    # algorithmic work of this step
-    iters = out["iterations"].cpu().numpy()
-    status = out["status"].cpu().numpy()
-    negc = np.unpackbits(out["negmask"].cpu().numpy().view(np.uint8), axis=1).sum(axis=1)
-    flops = flops_per_voxel(iters, negc, status, sh.nSH(), sh.n_dw, sh.n_init)
+    # ---- the other methods (same timing rules) -----------------------------
+    ms_plain = timed(plain_step, args.steps)
+    pstats = st.stats()
+    plain_out = st.fod()
+    ms_pers_plain = timed(lambda: persistent_step(False), max(2, args.steps // 2))
+    ms_pers_warm = timed(lambda: persistent_step(True), max(2, args.steps // 2))
+
+    def rate(ms):
+        return vol.n_masked * world / (ms / 1e3)
+
+    methods = {
+        "warm_phased": {"voxels_per_s": value, "ms": ms_warm, "passes": wstats["passes"],
+                        "solves_per_voxel": wstats["solved"] / vol.n_masked},
+        "plain_phased": {"voxels_per_s": rate(ms_plain), "ms": ms_plain, "passes": pstats["passes"],
+                         "solves_per_voxel": pstats["solved"] / vol.n_masked},
+        "persistent_plain": {"voxels_per_s": rate(ms_pers_plain), "ms": ms_pers_plain},
+        "persistent_warm": {"voxels_per_s": rate(ms_pers_warm), "ms": ms_pers_warm},
+        "warm_vs_plain": ms_plain / ms_warm,
+    }
+
+    # ---- parity of the warm and plain outputs on a sample ------------------
+    inside = np.nonzero(vol.mask)[0]
+    idx = np.random.default_rng(1).choice(inside, 4000, replace=False)
+    ref = O.OracleShared(vol.grad, synth.RESPONSE, synth.load_hr_dirs()).solve(vol.dwi[idx])
+    parity = {}
+    for name, out in (("warm", warm_out), ("plain", plain_out)):
+        r = rel_errors(out["fod"][idx], ref["F"])
+        parity[name] = {"p99_rel_err": float(np.percentile(r, 99)), "max_rel_err": float(r.max()),
+                        "negset_match": float(np.mean(np.all(out["negmask"][idx].view(np.uint32) == ref["negmask"],
+                                                             axis=1))),
+                        "sample_voxels": len(idx)}
+
+    # ---- roofline of the dominant kernel (csd_solve_kernel<45>) ------------
+    n = 45
+    flops = wstats["sum_neg"] * n * (n + 1) + wstats["solved"] * (n ** 3 / 3.0 + 2 * n * n)
+    solve_s = wstats["ms_solve"] / 1e3
     peaks, peak_kind = load_peaks()
-    achieved_tflops = flops / (ms_step / 1e3) / 1e12
-    roofline = {"bound": "tensor", "achieved": achieved_tflops, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                "frac": achieved_tflops / peaks["bf16_tflops"], "traffic": None,
-                "peak_source": f"bf16 dense burst, {peak_kind}",
-                "kernel": "csd_persistent_kernel<45>", "flops_per_launch": flops,
-                "hbm_gbs": (vol.n_voxels * (66 * 4 + 45 * 4 + 3)) / (ms_step / 1e3) / 1e9}
+    achieved = flops / solve_s / 1e12
+    solve_launches = max(1.0, wstats["passes"])
+    traffic = None
+    if SOLVE_DRAM_BYTES_PER_VOXEL is not None:
+        traffic = SOLVE_DRAM_BYTES_PER_VOXEL * wstats["solved"] / solve_launches
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
+                "kernel": "csd_solve_kernel<45>",
+                "peak_source": f"dense bf16 tensor peak, burst ({peak_kind})",
+                "algorithmic_flops_per_launch": flops / solve_launches,
+                "avg_launch_ms": wstats["ms_solve"] / solve_launches,
+                "flops_counted": "sum over solves of k*n(n+1) + n^3/3 + 2n^2 (n=45, k=|negative set|)",
+                "kernel_share_of_step": wstats["ms_solve"] / ms_warm}
 
-    # end to end through the host-buffer C ABI entry point (pinned inputs)
+    # ---- end to end through the host-buffer C ABI (pinned buffers) ---------
     pinned = torch.from_numpy(vol.dwi).pin_memory()
     pmask = torch.from_numpy(vol.mask).pin_memory()
-    csd.dwi2fod_csd_host(sh, pinned, pmask.numpy())
+    pfod = torch.empty((vol.n_voxels, 45), dtype=torch.float32).pin_memory()
+    csd.dwi2fod_csd_host_phased(sh, pinned, pmask, net=net, fod=pfod)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        r = csd.dwi2fod_csd_host(sh, pinned, pmask.numpy())
+        csd.dwi2fod_csd_host_phased(sh, pinned, pmask, net=net, fod=pfod)
     barrier()
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_s = float(t.item())
-    e2e = {"value": n_masked * world / e2e_s, "unit": UNIT,
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    e2e = {"value": vol.n_masked * world / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": int(vol.dwi.nbytes + vol.mask.nbytes),
            "d2h_bytes_per_step": int(vol.n_voxels * (45 * 4 + 2)),
-           "api": "csd_dwi2fod_host (pinned host buffers, copies inside the timed region)"}
+           "api": "csd_dwi2fod_host_phased (warm start, pinned host buffers, copies inside the timed region)"}
 
+    mlp_launches = 1 + 5 * ((vol.n_masked + 262143) // 262144)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp32 (fp64 refinement residual)", "data": "synthetic",
-            "config": workload_config(vol, args.method), "roofline": roofline, "e2e": e2e,
-            "gpu_launches": args.steps, "clocks": clk.summary(),
-            "mean_iterations": float(iters[(status & 0x0F) == 1].mean()),
-            "status_counts": {"converged": int(((status & 0x0F) == 1).sum()), "niter": int(((status & 0x0F) == 2).sum()),
-                              "fp64": int(((status & 0x10) != 0).sum()), "cholfail": int(((status & 0x20) != 0).sum())}}
+            "warmup": args.warmup, "ms_per_step": ms_warm, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "fp32 (tensor-core projection/assembly on fp16 hi+lo splits, fp64 fallback/refinement)",
+            "data": "synthetic",
+            "config": workload_config(vol, "warm-started phased CSD (network first sets + plain iteration)"),
+            "methods": methods, "parity": parity, "roofline": roofline, "e2e": e2e,
+            "gpu_launches": int(wstats["launches"] + 1 + mlp_launches) * args.steps,
+            "clocks": clk.summary(), "warm_start_net": net_src}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(vol)
     if rank == 0:

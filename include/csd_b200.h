@@ -120,6 +120,16 @@ int csd_solve(const csd_shared* const* shared, const csd_volume* volumes, int n_
 int csd_dwi2fod_host(const csd_shared* s, const float* dwi, int64_t n_voxels, const uint8_t* mask,
                      float* fod, uint8_t* status, uint8_t* iterations);
 
+typedef struct csd_mlp csd_mlp;  /* the warm-start network, below */
+
+/* The phased method on HOST buffers (same layout as csd_dwi2fod_host):
+ * per slab of voxels, csd_state_set, then -- when `net` is not NULL -- the
+ * network's predicted first negative sets (csd_mlp_predict + csd_state_warm),
+ * then csd_state_iterate until no voxel is active, then csd_state_fod.  Slab
+ * uploads / downloads overlap the passes of the other slab.  Synchronous. */
+int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const float* dwi, int64_t n_voxels,
+                            const uint8_t* mask, float* fod, uint8_t* status, uint8_t* iterations);
+
 /* ---- per-step surface: CSD::set / iterate / FOD (csd.h:237-271) over a
  *      batch of voxels (the reference object is one voxel: a batch of 1).
  *      The plain GPU method drives these phases from the host, one pass per
@@ -137,6 +147,11 @@ int csd_state_warm(csd_state* st, const uint32_t* negmask, void* stream);
 /* One CSD::iterate() on every active voxel.  *n_active receives how many
  * voxels are still iterating afterwards (synchronises the stream). */
 int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream);
+/* Work and device time since the last csd_state_set: out[8] = passes, voxels
+ * projected, voxels solved, sum of |negative set| over the solves, then the
+ * device milliseconds of the set / projection / solve kernels, and the
+ * number of kernel launches. */
+int csd_state_stats(const csd_state* st, double* out);
 /* CSD::FOD(): copy F (float) out, plus optional status/iterations/negmask. */
 int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride, uint8_t* status,
                   uint8_t* iterations, uint32_t* negmask, void* stream);
@@ -164,7 +179,6 @@ int csd_solve_noalloc(const csd_shared* s, const csd_volume* volume, void* strea
  *      first negative set (csd_volume.warm_negmask); the iteration then runs
  *      to its own stopping rule, and a voxel that does not reach a fixed
  *      point is re-solved from the plain start. */
-typedef struct csd_mlp csd_mlp;
 int csd_mlp_create(int n_in, int n_hidden, int n_out, uint64_t seed, csd_mlp** out);
 void csd_mlp_destroy(csd_mlp* m);
 int64_t csd_mlp_param_count(const csd_mlp* m);

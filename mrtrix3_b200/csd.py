@@ -30,7 +30,7 @@ EXPORTED = [
     "csd_params_init", "csd_shared_create", "csd_shared_destroy", "csd_shared_nsh", "csd_shared_info",
     "csd_shared_dwis", "csd_shared_matrix", "csd_solve", "csd_dwi2fod_host", "csd_state_create",
     "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_fod",
-    "csd_last_error",
+    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_last_error",
 ]
 
 
@@ -83,6 +83,8 @@ def lib():
         L.csd_state_warm.argtypes = [vp, vp, vp]
         L.csd_state_iterate.argtypes = [vp, ctypes.POINTER(i64), vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]
+        L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.csd_dwi2fod_host_phased.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
         L.csd_last_error.restype = ctypes.c_char_p
         _LIB = L
     return _LIB
@@ -311,6 +313,21 @@ def dwi2fod_csd_host(shared: Shared, dwi: np.ndarray, mask: np.ndarray | None = 
     return {"fod": fod, "status": status, "iterations": iters}
 
 
+def dwi2fod_csd_host_phased(shared: Shared, dwi, mask=None, net=None, fod=None):
+    """The phased method (optionally warm-started by a WarmStartNet) on host
+    arrays or pinned torch CPU tensors; copies are inside the call."""
+    nvox = dwi.shape[0]
+    if fod is None:
+        fod = np.zeros((nvox, shared.nSH()), np.float32)
+    status = np.zeros(nvox, np.uint8)
+    iters = np.zeros(nvox, np.uint8)
+    check(lib().csd_dwi2fod_host_phased(shared.handle, None if net is None else net._h, ctypes.c_void_p(_ptr(dwi)),
+                                        nvox, ctypes.c_void_p(_ptr(mask)) if mask is not None else None,
+                                        ctypes.c_void_p(_ptr(fod)), ctypes.c_void_p(status.ctypes.data),
+                                        ctypes.c_void_p(iters.ctypes.data)))
+    return {"fod": fod, "status": status, "iterations": iters}
+
+
 def negmask_to_bool(negmask, n_hr: int) -> np.ndarray:
     """[n][nwords] uint32/int32 words -> [n][n_hr] bool."""
     a = np.ascontiguousarray(np.asarray(negmask).astype(np.uint32))
@@ -344,6 +361,24 @@ class State:
         n = ctypes.c_int64()
         check(lib().csd_state_iterate(self._h, ctypes.byref(n), ctypes.c_void_p(_stream_ptr(stream))))
         return n.value
+
+    def stats(self) -> dict:
+        """Work and device time since the last set() (csd_state_stats)."""
+        out = (ctypes.c_double * 8)()
+        check(lib().csd_state_stats(self._h, out))
+        keys = ("passes", "projected", "solved", "sum_neg", "ms_set", "ms_project", "ms_solve", "launches")
+        return dict(zip(keys, list(out)))
+
+    def run(self, dwi, mask=None, warm=None, stream=None):
+        """The phased method over one volume: set (+ warm sets), then iterate
+        until no voxel is active.  Returns the number of passes."""
+        self.set(dwi, mask=mask, stream=stream)
+        if warm is not None:
+            self.warm(warm, stream=stream)
+        passes = 0
+        while self.iterate(stream=stream) > 0:
+            passes += 1
+        return passes + 1
 
     def fod(self, stream=None, as_numpy=True):
         import torch

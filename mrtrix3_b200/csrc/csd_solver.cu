@@ -243,6 +243,7 @@ struct StateParams {
   const int* act_in;    // [n_in] voxel ids
   int* act_out;         // compacted output list
   int* n_out;
+  unsigned long long* stats;  // [0] sum of |neg| over solves, [1] solves
   double* fp64_scratch;
   // set() inputs
   const float* dwi;
@@ -419,6 +420,10 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
     __syncwarp();
     const uint8_t st = P.status[v];
     const int k = mask_to_list(bits, P.nw, w.neg, lane);
+    if (lane == 0 && P.stats) {
+      atomicAdd(P.stats, (unsigned long long)k);
+      atomicAdd(P.stats + 1, 1ULL);
+    }
     const int fl = assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot) & 0x70;
     for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
     if (lane < P.nw) {
@@ -965,6 +970,10 @@ struct csd_state {
   int proj_blocks = 0;
   size_t proj_smem = 0;
   long long passes = 0, projected = 0, solved = 0;  // work counters since the last set()
+  unsigned long long* stats = nullptr;              // device: sum |neg|, solves
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double ms_set = 0, ms_project = 0, ms_solve = 0;  // device time of the kernels since the last set()
+  long long launches = 0;
 };
 
 namespace {
@@ -1023,6 +1032,7 @@ StateParams state_params(const csd_state* st) {
   P.status = st->status;
   P.iters = st->iters;
   P.n_out = st->counter;
+  P.stats = st->stats;
   P.fp64_scratch = st->fp64;
   return P;
 }
@@ -1094,6 +1104,8 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->act[0], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->act[1], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->counter, 2 * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&st->stats, 2 * sizeof(unsigned long long)));
+  for (auto& e : st->ev) CUDA_TRY(cudaEventCreate(&e));
   int rc = 0;
   CSD_DISPATCH(n, rc = state_shape<NN>(st.get()));
   if (rc) return rc;
@@ -1115,7 +1127,10 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->act[0]);
   cudaFree(st->act[1]);
   cudaFree(st->counter);
+  cudaFree(st->stats);
   cudaFree(st->fp64);
+  for (auto& e : st->ev)
+    if (e) cudaEventDestroy(e);
   delete st;
 }
 
@@ -1128,7 +1143,10 @@ extern "C" int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, 
   st->use_warm = 0;
   st->cur = 0;
   st->passes = st->projected = st->solved = 0;
+  st->ms_set = st->ms_project = st->ms_solve = 0;
+  st->launches = 0;
   CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(st->stats, 0, 2 * sizeof(unsigned long long), s));
   if (n_voxels == 0) {
     st->n_active = 0;
     return CSD_OK;
@@ -1141,11 +1159,17 @@ extern "C" int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, 
   P.mask = mask;
   P.act_out = st->act[0];
   int rc = 0;
+  CUDA_TRY(cudaEventRecord(st->ev[0], s));
   CSD_DISPATCH(st->sh->h.nsh, rc = state_set_launch<NN>(st, P, s));
   if (rc) return rc;
+  CUDA_TRY(cudaEventRecord(st->ev[1], s));
   int na = 0;
   CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&ms, st->ev[0], st->ev[1]));
+  st->ms_set += ms;
+  st->launches += 1;
   st->n_active = na;
   return CSD_OK;
 }
@@ -1171,11 +1195,17 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
     P.act_in = st->act[st->cur];
     P.act_out = st->slist;
     CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
+    CUDA_TRY(cudaEventRecord(st->ev[0], s));
     CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
     if (rc) return rc;
+    CUDA_TRY(cudaEventRecord(st->ev[1], s));
     int ns = 0;
     CUDA_TRY(cudaMemcpyAsync(&ns, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, st->ev[0], st->ev[1]));
+    st->ms_project += ms;
+    st->launches += 1;
     st->projected += st->n_active;
     // pass 2: assemble + factorise the voxels whose set changed -> next active list
     int na = 0;
@@ -1185,10 +1215,16 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
       Q.act_in = st->slist;
       Q.act_out = st->act[st->cur ^ 1];
       CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
+      CUDA_TRY(cudaEventRecord(st->ev[2], s));
       CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Q, s));
       if (rc) return rc;
+      CUDA_TRY(cudaEventRecord(st->ev[3], s));
       CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
       CUDA_TRY(cudaStreamSynchronize(s));
+      float ms2 = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&ms2, st->ev[2], st->ev[3]));
+      st->ms_solve += ms2;
+      st->launches += 1;
       st->solved += ns;
     }
     st->n_active = na;
@@ -1196,6 +1232,21 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
     st->passes += 1;
   }
   if (n_active) *n_active = st->n_active;
+  return CSD_OK;
+}
+
+extern "C" int csd_state_stats(const csd_state* st, double* out) {
+  if (!st || !out) return fail(CSD_ERR_INVALID, "csd_state_stats: invalid argument");
+  unsigned long long d[2] = {0, 0};
+  CUDA_TRY(cudaMemcpy(d, st->stats, sizeof(d), cudaMemcpyDeviceToHost));
+  out[0] = (double)st->passes;
+  out[1] = (double)st->projected;
+  out[2] = (double)st->solved;
+  out[3] = (double)d[0];
+  out[4] = st->ms_set;
+  out[5] = st->ms_project;
+  out[6] = st->ms_solve;
+  out[7] = (double)st->launches;
   return CSD_OK;
 }
 
@@ -1326,6 +1377,114 @@ extern "C" int csd_solve_noalloc(const csd_shared* s, const csd_volume* v, void*
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   CSD_DISPATCH(s->h.nsh, rc = noalloc_launch<NN>(s, v, st, base));
   return rc;
+}
+
+
+// ---------------------------------------------------------------------------
+// csd_dwi2fod_host_phased: the phased method (optionally warm-started by the
+// network) on HOST buffers.  The volume is cut into slabs; each slab's
+// host->device copy, solve and device->host copy run on one of two streams,
+// so the copies of one slab overlap the passes of the other.
+
+namespace {
+struct PhasedHostWS {
+  const csd_shared* sh = nullptr;
+  int64_t cap = 0;
+  csd_state* st[2] = {nullptr, nullptr};
+  float* dwi[2] = {nullptr, nullptr};
+  float* fod[2] = {nullptr, nullptr};
+  uint8_t* small[2] = {nullptr, nullptr};   // mask | status | iterations
+  uint32_t* warm[2] = {nullptr, nullptr};
+  cudaStream_t stream[2] = {nullptr, nullptr};
+};
+std::mutex g_phws_mu;
+std::map<int, PhasedHostWS> g_phws;
+
+void release(PhasedHostWS& w) {
+  for (int i = 0; i < 2; ++i) {
+    csd_state_destroy(w.st[i]);
+    cudaFree(w.dwi[i]);
+    cudaFree(w.fod[i]);
+    cudaFree(w.small[i]);
+    cudaFree(w.warm[i]);
+    w.st[i] = nullptr;
+    w.dwi[i] = w.fod[i] = nullptr;
+    w.small[i] = nullptr;
+    w.warm[i] = nullptr;
+  }
+  w.cap = 0;
+  w.sh = nullptr;
+}
+}  // namespace
+
+extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const float* dwi, int64_t n_voxels,
+                                       const uint8_t* mask, float* fod, uint8_t* status, uint8_t* iterations) {
+  if (!s || n_voxels < 0 || (n_voxels > 0 && (!dwi || !fod)))
+    return fail(CSD_ERR_INVALID, "csd_dwi2fod_host_phased: invalid argument");
+  if (n_voxels == 0) return CSD_OK;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_phws_mu);
+  PhasedHostWS& w = g_phws[dev];
+  const int nvol = s->h.nvol, nsh = s->h.nsh, nw = (s->h.nhr + 31) / 32;
+  const int64_t nslab = std::min<int64_t>(4, std::max<int64_t>(1, n_voxels / 131072));
+  const int64_t per = (n_voxels + nslab - 1) / nslab;
+  if (w.sh != s || w.cap < per) {
+    release(w);
+    for (int i = 0; i < 2; ++i) {
+      int rc = csd_state_create(s, per, &w.st[i]);
+      if (rc) return rc;
+      CUDA_TRY(cudaMalloc(&w.dwi[i], (size_t)per * nvol * sizeof(float)));
+      CUDA_TRY(cudaMalloc(&w.fod[i], (size_t)per * nsh * sizeof(float)));
+      CUDA_TRY(cudaMalloc(&w.small[i], (size_t)per * 3));
+      CUDA_TRY(cudaMalloc(&w.warm[i], (size_t)per * nw * sizeof(uint32_t)));
+      if (!w.stream[i]) CUDA_TRY(cudaStreamCreateWithFlags(&w.stream[i], cudaStreamNonBlocking));
+    }
+    w.sh = s;
+    w.cap = per;
+  }
+  // enqueue the first slab's upload, then per slab: enqueue the next upload
+  // on the other stream, solve this slab, enqueue its download
+  auto upload = [&](int64_t k) -> int {
+    const int64_t a = k * per, n = std::min(per, n_voxels - a);
+    const int b = (int)(k & 1);
+    CUDA_TRY(cudaMemcpyAsync(w.dwi[b], dwi + a * nvol, (size_t)n * nvol * sizeof(float), cudaMemcpyHostToDevice,
+                             w.stream[b]));
+    if (mask) CUDA_TRY(cudaMemcpyAsync(w.small[b], mask + a, (size_t)n, cudaMemcpyHostToDevice, w.stream[b]));
+    return 0;
+  };
+  int rc = upload(0);
+  if (rc) return rc;
+  for (int64_t k = 0; k < nslab; ++k) {
+    const int64_t a = k * per, n = std::min(per, n_voxels - a);
+    if (n <= 0) break;
+    const int b = (int)(k & 1);
+    cudaStream_t st = w.stream[b];
+    if (k + 1 < nslab && (k + 1) * per < n_voxels) {
+      // the other buffer's previous download must finish before reuse
+      CUDA_TRY(cudaStreamSynchronize(w.stream[b ^ 1]));
+      if ((rc = upload(k + 1))) return rc;
+    }
+    const uint8_t* dmask = mask ? w.small[b] : nullptr;
+    if ((rc = csd_state_set(w.st[b], w.dwi[b], n, nvol, 1, dmask, st))) return rc;
+    if (net) {
+      if ((rc = csd_mlp_predict(net, w.dwi[b], n, nvol, 1, dmask, 0.f, w.warm[b], st))) return rc;
+      if ((rc = csd_state_warm(w.st[b], w.warm[b], st))) return rc;
+    }
+    int64_t active = 1;
+    while (active > 0)
+      if ((rc = csd_state_iterate(w.st[b], &active, st))) return rc;
+    uint8_t* dst = w.small[b] + per;
+    uint8_t* dit = w.small[b] + 2 * per;
+    if ((rc = csd_state_fod(w.st[b], w.fod[b], nsh, status ? dst : nullptr, iterations ? dit : nullptr, nullptr, st)))
+      return rc;
+    CUDA_TRY(cudaMemcpyAsync(fod + a * nsh, w.fod[b], (size_t)n * nsh * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (status) CUDA_TRY(cudaMemcpyAsync(status + a, dst, (size_t)n, cudaMemcpyDeviceToHost, st));
+    if (iterations) CUDA_TRY(cudaMemcpyAsync(iterations + a, dit, (size_t)n, cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(w.stream[0]));
+  CUDA_TRY(cudaStreamSynchronize(w.stream[1]));
+  return CSD_OK;
 }
 
 #include "hr_dirs_builtin.inc"

@@ -1,0 +1,47 @@
+"""Run one CSD method on a synthetic case, for profilers (ncu) and timing.
+
+    python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
+        [--method warm|plain|persistent|persistent_warm] [--reps 2]
+
+Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
+(lmax 8) or 8 b=0 + 90 DW (lmax 10).  Prints the state's work / time
+counters of the last repetition.
+"""
+import argparse
+import os
+import time
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dims", type=int, nargs=3, default=[64, 64, 64])
+    ap.add_argument("--lmax", type=int, default=8)
+    ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm"])
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args()
+    import torch
+
+    from . import csd, synth
+    from .warmstart import WarmStartNet
+    ndw, nb0 = (60, 6) if a.lmax <= 8 else (90, 8)
+    v = synth.make_volume(tuple(a.dims), nb0, ndw, (15.0, 40.0), a.lmax, None, 5)
+    s = csd.make_shared(v.grad, synth.RESPONSE, lmax=a.lmax)
+    d = torch.from_numpy(v.dwi).cuda()
+    net = None
+    if a.method in ("warm", "persistent_warm"):
+        net = WarmStartNet.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_c5.npz"))
+    st = csd.State(s, d.shape[0]) if a.method in ("warm", "plain") else None
+    t0 = time.perf_counter()
+    for _ in range(a.reps):
+        if st is not None:
+            st.run(d, warm=net.predict(d) if net is not None else None)
+        else:
+            csd.dwi2fod_csd(s, d, warm=net.predict(d) if net is not None else None)
+    torch.cuda.synchronize()
+    print(f"{a.method}: {d.shape[0]} voxels x {a.reps} reps in {time.perf_counter() - t0:.3f} s")
+    if st is not None:
+        print(st.stats())
+
+
+if __name__ == "__main__":
+    main()

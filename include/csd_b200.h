@@ -203,6 +203,14 @@ int csd_mlp_gradients(csd_mlp* m, const uint16_t* x, const uint32_t* negmask, in
                       float* loss_out);
 int csd_mlp_logits(csd_mlp* m, const uint16_t* x, int64_t n, float* z_out);
 
+/* Launch-shape knobs (process-wide), chosen by the project's autotuner
+ * (mrtrix3_b200/autotune.py): which = 0 warps per block of the persistent
+ * kernel, 1 warps per block of the phased solve kernel, 2 projection blocks
+ * per SM, 3 projection kernel of the phased method (1 mma.sync, 2 tcgen05
+ * with the accumulators in tensor memory; up to 320 constraint directions);
+ * value 0 = built-in default.  Outputs do not depend on them. */
+int csd_set_launch_config(int which, int value);
+
 /* Thread-local description of the last failure. */
 const char* csd_last_error(void);
 

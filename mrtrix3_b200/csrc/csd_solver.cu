@@ -45,6 +45,14 @@ int set_error(int code, const std::string& msg) { return fail(code, msg); }
 
 extern "C" const char* csd_last_error(void) { return g_err.c_str(); }
 
+// launch-shape knobs chosen by the autotuner (0 = the built-in default)
+static int g_tune_persistent_warps = 0;  // warps per block of csd_persistent_kernel
+static int g_tune_solve_warps = 0;       // warps per block of csd_solve_kernel
+static int g_tune_proj_blocks_per_sm = 0;
+static int g_proj_kind = 0;  // projection kernel: 0 default, 1 mma.sync, 2 tcgen05 (nhr <= 320)
+static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
+
+
 // ---------------------------------------------------------------------------
 // kernels
 
@@ -232,6 +240,7 @@ struct StateParams {
   int nhr, nw, n_in, use_warm, npd;
   float cond_thr, thr_scaled;
   const __half* Hp16;   // [2][npd][HS16] projection table (hi, lo), zero rows past nhr
+  const __half* Htc16;  // [2][K chunks][320 rows][8] tcgen05 projection table (hi, lo), core-matrix layout
   float* F;             // [cap][HS]
   double* b;            // [cap][N]
   uint32_t* old;        // [cap][nw] set of the last solve
@@ -398,6 +407,226 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
   }
 }
 
+// ---- tcgen05 projection (sm_100a): the same pass as csd_project_kernel on
+// the 5th-generation tensor cores.  A tile of 128 active voxels is the
+// M=128 operand (F, split into FP16 hi/lo, scaled by 2^8), the 320-row
+// direction table the N operand (two N=160 instructions), K = 16 per
+// instruction; D accumulates hi*hi + hi*lo + lo*hi in FP32 in tensor memory
+// (320 of 512 allocated columns).  Operands sit in shared memory in the
+// canonical K-major, non-swizzled layout: 8-row x 16-byte core matrices,
+// row groups SBO = 128 B apart, K chunks LBO apart.  One elected thread
+// issues the instructions and commits them to an mbarrier; every thread
+// then reads its own voxel's row of D (tcgen05.ld 32x32b), packs the sign
+// bits, and makes the convergence decision itself.  Waits are bounded: on
+// time-out the kernel raises an error flag, frees its tensor memory and
+// returns.
+
+constexpr int kTcRows = 128;          // voxels per tile (M)
+constexpr int kTcDirs = 320;          // directions (N, two instructions of 160)
+constexpr unsigned kTcWaitLimit = 1u << 26;
+
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);             // start address, bits [0,14)
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;         // leading (K-chunk) byte offset, bits [16,30)
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;         // stride (row-group) byte offset, bits [32,46)
+  d |= (uint64_t)1 << 46;                             // descriptor version 1 (sm_100)
+  return d;                                           // base offset 0, no swizzle (layout type 0)
+}
+
+// kind::f16 instruction descriptor: F16 A and B, F32 D, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (unsigned i = 0; i < kTcWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity));
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_constant__ StateParams P) {
+  using D = Dims<N>;
+  constexpr int KC = 2 * D::NRB;                     // 8-half K chunks
+  constexpr int A_BYTES = KC * (kTcRows / 8) * 128;  // one of hi / lo
+  constexpr int B_BYTES = KC * (kTcDirs / 8) * 128;
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned char* sBh = smem;
+  unsigned char* sBl = sBh + B_BYTES;
+  unsigned char* sAh = sBl + B_BYTES;
+  unsigned char* sAl = sAh + A_BYTES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sAl + A_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  // direction table (host-prepared in the core-matrix layout), once per block
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(P.Htc16);
+    uint4* dst = reinterpret_cast<uint4*>(sBh);
+    for (int i = tid; i < 2 * B_BYTES / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+  }
+  const uint32_t mbar_a = static_cast<uint32_t>(__cvta_generic_to_shared(mbar));
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar_a));
+  }
+  if (warp == 0) {
+    const uint32_t slot = static_cast<uint32_t>(__cvta_generic_to_shared(tmem_slot));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(slot));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc_f16(kTcRows, kTcDirs / 2);
+  const uint32_t aH = static_cast<uint32_t>(__cvta_generic_to_shared(sAh));
+  const uint32_t aL = static_cast<uint32_t>(__cvta_generic_to_shared(sAl));
+  const uint32_t bH = static_cast<uint32_t>(__cvta_generic_to_shared(sBh));
+  const uint32_t bL = static_cast<uint32_t>(__cvta_generic_to_shared(sBl));
+  constexpr uint32_t A_LBO = (kTcRows / 8) * 128, B_LBO = (kTcDirs / 8) * 128;
+  const int ntiles = (P.n_in + kTcRows - 1) / kTcRows;
+  uint32_t phase = 0;
+  bool failed = false;
+  for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+    const int e0 = tile * kTcRows;
+    // this thread's voxel row -> scaled FP16 hi / lo chunks in the core-matrix layout
+    {
+      const int r = tid;
+      float f[KC * 8];
+#pragma unroll
+      for (int c = 0; c < KC * 8; ++c) f[c] = 0.f;
+      if (e0 + r < P.n_in) {
+        const float4* src = reinterpret_cast<const float4*>(P.F + (long long)P.act_in[e0 + r] * D::HS);
+#pragma unroll
+        for (int q = 0; q < (KC * 8) / 4; ++q) {
+          if (4 * q < D::HS) {
+            const float4 x = src[q];
+            f[4 * q] = 4 * q < N ? x.x : 0.f;
+            f[4 * q + 1] = 4 * q + 1 < N ? x.y : 0.f;
+            f[4 * q + 2] = 4 * q + 2 < N ? x.z : 0.f;
+            f[4 * q + 3] = 4 * q + 3 < N ? x.w : 0.f;
+          }
+        }
+      }
+#pragma unroll
+      for (int kc = 0; kc < KC; ++kc) {
+        __align__(16) __half hi[8], lo[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const float v = f[8 * kc + e] * kProjFScale;
+          hi[e] = __float2half_rn(v);
+          lo[e] = __float2half_rn(v - __half2float(hi[e]));
+        }
+        const int off = kc * A_LBO + (r >> 3) * 128 + (r & 7) * 16;
+        *reinterpret_cast<uint4*>(sAh + off) = *reinterpret_cast<const uint4*>(hi);
+        *reinterpret_cast<uint4*>(sAl + off) = *reinterpret_cast<const uint4*>(lo);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    if (tid == 0) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t dcol = tmem + (uint32_t)(h * (kTcDirs / 2));
+        const uint32_t boff = (uint32_t)(h * (kTcDirs / 16)) * 128;  // 20 row groups per half
+#pragma unroll
+        for (int ks = 0; ks < D::NRB; ++ks) {
+          const uint32_t ak = (uint32_t)(2 * ks) * A_LBO, bk = (uint32_t)(2 * ks) * B_LBO + boff;
+          const uint64_t dAh = umma_smem_desc(aH + ak, A_LBO, 128), dAl = umma_smem_desc(aL + ak, A_LBO, 128);
+          const uint64_t dBh = umma_smem_desc(bH + bk, B_LBO, 128), dBl = umma_smem_desc(bL + bk, B_LBO, 128);
+          const uint64_t pa[3] = {dAh, dAh, dAl}, pb[3] = {dBh, dBl, dBh};
+#pragma unroll
+          for (int p = 0; p < 3; ++p) {
+            const uint32_t acc = (ks > 0 || p > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred q;\n\t"
+                "setp.ne.b32 q, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, q;\n\t}\n"
+                :
+                : "r"(dcol), "l"(pa[p]), "l"(pb[p]), "r"(idesc), "r"(acc), "r"(0u));
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_a));
+    }
+    const int ok = mbar_wait(mbar_a, phase) ? 1 : 0;
+    phase ^= 1u;
+    if (!__syncthreads_and(ok)) {
+      // give the tensor core a second bounded chance to drain before the
+      // tensor memory is freed, then report the time-out
+      mbar_wait(mbar_a, phase ^ 1u);
+      if (tid == 0) atomicExch(P.n_out + 1, 1);
+      failed = true;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    // this thread's row of D: sign bits of its 300 amplitudes
+    uint32_t words[kTcDirs / 32];
+#pragma unroll
+    for (int w = 0; w < kTcDirs / 32; ++w) words[w] = 0u;
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+#pragma unroll
+    for (int j = 0; j < kTcDirs / 16; ++j) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(lane_addr + (uint32_t)(16 * j)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int c = 16 * j + e;
+        if (c < P.nhr && __uint_as_float(v[e]) < P.thr_scaled) words[c >> 5] |= 1u << (c & 31);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    // per-voxel decision (csd.h:246-253), one thread per voxel
+    const int r = tid;
+    if (e0 + r < P.n_in) {
+      const long long v = P.act_in[e0 + r];
+      const int it = P.iters[v];
+      const bool warm = it == 0 && P.use_warm && P.warm;
+      bool same = true, back = true;
+      for (int w = 0; w < P.nw; ++w) {
+        uint32_t b = words[w < kTcDirs / 32 ? w : 0];
+        if (warm) {
+          b = P.warm[v * P.nw + w];
+          if (w == P.nw - 1 && (P.nhr & 31)) b &= (1u << (P.nhr & 31)) - 1u;
+        }
+        words[w < kTcDirs / 32 ? w : 0] = b;
+        same = same && b == P.old[v * P.nw + w];
+        back = back && b == P.old2[v * P.nw + w];
+      }
+      const bool conv = !warm && it > 0 && same;
+      P.iters[v] = (uint16_t)(it + 1);
+      uint8_t st = P.status[v];
+      if (conv) {
+        P.status[v] = (uint8_t)(CSD_STATUS_CONVERGED | (st & 0x70));
+      } else {
+        for (int w = 0; w < P.nw; ++w) P.newm[v * P.nw + w] = words[w < kTcDirs / 32 ? w : 0];
+        if (!warm && it >= 2 && back) st |= kCycling;
+        P.status[v] = st;
+        P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
+      }
+    }
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
+}
+
 // Solve pass: warp per voxel of the solve list (csd.h:255-266).
 template <int N>
 __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(const __grid_constant__ StateParams P) {
@@ -477,6 +706,7 @@ struct csd_shared {
   std::vector<float> H32_host;
   std::vector<__half> H16_host;    // [2][nhr+1][HS16]: hi then lo
   std::vector<__half> Hp16_host;   // [2][npd][HS16]: projection table, hi then lo
+  std::vector<__half> Htc16_host;  // tcgen05 projection table (core-matrix layout), hi then lo
   int npd = 0;                     // directions padded to a multiple of 320
   std::vector<float> MtMp_host;
   std::vector<float> rconvT_host;
@@ -484,6 +714,7 @@ struct csd_shared {
   float* H32 = nullptr;
   __half* H16 = nullptr;
   __half* Hp16 = nullptr;
+  __half* Htc16 = nullptr;
   double* H64 = nullptr;
   float* MtMp = nullptr;
   double* MtM64 = nullptr;
@@ -581,6 +812,21 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
       s->Hp16_host[(size_t)d * HS16 + c] = s->H16_host[(size_t)d * HS16 + c];
       s->Hp16_host[(size_t)(s->npd + d) * HS16 + c] = s->H16_host[(size_t)(h.nhr + 1 + d) * HS16 + c];
     }
+  if (h.nhr <= 320) {
+    // canonical K-major core matrices: [K chunk][row group of 8][row][8 halves]
+    const int KC = 2 * ((n + 15) / 16);
+    const size_t per = (size_t)KC * 320 * 8;
+    s->Htc16_host.assign(2 * per, __float2half_rn(0.f));
+    for (int kc = 0; kc < KC; ++kc)
+      for (int d = 0; d < h.nhr; ++d)
+        for (int e = 0; e < 8; ++e) {
+          const int c = 8 * kc + e;
+          if (c >= n) continue;
+          const size_t o = ((size_t)(kc * 40 + d / 8) * 8 + (d % 8)) * 8 + e;
+          s->Htc16_host[o] = s->H16_host[(size_t)d * HS16 + c];
+          s->Htc16_host[per + o] = s->H16_host[(size_t)(h.nhr + 1 + d) * HS16 + c];
+        }
+  }
   s->MtMp_host.assign((size_t)s->WSZ, 0.f);
   for (int i = 0; i < n; ++i)
     for (int j = 0; j <= i; ++j) s->MtMp_host[packoff(i) + j] = (float)h.MtM[(size_t)i * n + j];
@@ -607,6 +853,7 @@ static int ensure_device(const csd_shared* cs) {
   if ((rc = upload(&s->H32, s->H32_host))) return rc;
   if ((rc = upload(&s->H16, s->H16_host))) return rc;
   if ((rc = upload(&s->Hp16, s->Hp16_host))) return rc;
+  if (!s->Htc16_host.empty() && (rc = upload(&s->Htc16, s->Htc16_host))) return rc;
   if ((rc = upload(&s->H64, h.HR))) return rc;
   if ((rc = upload(&s->MtMp, s->MtMp_host))) return rc;
   if ((rc = upload(&s->MtM64, h.MtM))) return rc;
@@ -626,6 +873,7 @@ extern "C" void csd_shared_destroy(csd_shared* s) {
     cudaFree(s->H32);
     cudaFree(s->H16);
     cudaFree(s->Hp16);
+    cudaFree(s->Htc16);
     cudaFree(s->H64);
     cudaFree(s->MtMp);
     cudaFree(s->MtM64);
@@ -734,6 +982,7 @@ int shape_for(int nhr, long long total, LaunchShape* ls) {
   const size_t wb = warp_ws_bytes<N>();
   if (hbytes + wb > (size_t)smem_max) return fail(CSD_ERR_UNSUPPORTED, "constraint set too large for shared memory");
   int warps = (int)std::min<size_t>(Dims<N>::THREADS / 32, ((size_t)smem_max - hbytes) / wb);
+  if (g_tune_persistent_warps > 0) warps = std::min(warps, g_tune_persistent_warps);
   ls->warps = warps;
   ls->smem = hbytes + wb * warps;
   long long need_blocks = (total + warps - 1) / warps;
@@ -921,6 +1170,25 @@ extern "C" int csd_dwi2fod_host(const csd_shared* s, const float* dwi, int64_t n
   return CSD_OK;
 }
 
+// Launch-shape knobs (set by the autotuner): which = 0 persistent-kernel
+// warps per block, 1 phased solve-kernel warps per block, 2 projection
+// blocks per SM; value 0 restores the default.  Results do not depend on
+// them (each voxel's arithmetic is the same whatever warp runs it).
+extern "C" int csd_set_launch_config(int which, int value) {
+  if (value < 0 || value > 64) return fail(CSD_ERR_INVALID, "csd_set_launch_config: value out of range");
+  switch (which) {
+    case 0: g_tune_persistent_warps = value; break;
+    case 1: g_tune_solve_warps = value; break;
+    case 2: g_tune_proj_blocks_per_sm = value; break;
+    case 3:
+      if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: projection kind is 0, 1 or 2");
+      g_proj_kind = value;
+      break;
+    default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
+  }
+  return CSD_OK;
+}
+
 // Profiling hook: per-phase cycle totals of the persistent kernel since the
 // last reset (only in a build with -DCSD_PHASE_TIMERS; returns -5 otherwise).
 extern "C" int csd_debug_phase_cycles(unsigned long long* out, int reset) {
@@ -1020,6 +1288,7 @@ StateParams state_params(const csd_state* st) {
   P.nw = (P.nhr + 31) / 32;
   P.npd = st->sh->npd;
   P.Hp16 = st->sh->Hp16;
+  P.Htc16 = st->sh->Htc16;
   P.thr_scaled = (float)(st->sh->h.threshold * kProjFScale);
   P.cond_thr = (float)st->sh->cond_thr;
   P.F = st->F;
@@ -1045,16 +1314,39 @@ int state_set_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
   return 0;
 }
 template <int N>
+int state_project_tc_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  constexpr int KC = 2 * Dims<N>::NRB;
+  const size_t need = (size_t)2 * KC * (kTcDirs / 8) * 128 + (size_t)2 * KC * (kTcRows / 8) * 128 + 16;
+  const size_t smem = std::max<size_t>(need, 120 * 1024);  // > half an SM: one block (and one TMEM owner) per SM
+  CUDA_TRY(cudaFuncSetAttribute(csd_project_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, nsm = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int tiles = (P.n_in + kTcRows - 1) / kTcRows;
+  csd_project_tc_kernel<N><<<std::max(1, std::min(tiles, nsm)), 128, smem, s>>>(P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+template <int N>
 int state_project_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  if ((g_proj_kind ? g_proj_kind : kProjDefault) == 2 && P.Htc16) return state_project_tc_launch<N>(st, P, s);
   const int tiles = (P.n_in + kProjRows - 1) / kProjRows;
-  csd_project_kernel<N><<<std::max(1, std::min(tiles, st->proj_blocks)), 256, st->proj_smem, s>>>(P);
+  int pb = st->proj_blocks;
+  if (g_tune_proj_blocks_per_sm > 0) {
+    int dev = 0, nsm = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    pb = std::min(pb, nsm * g_tune_proj_blocks_per_sm);
+  }
+  csd_project_kernel<N><<<std::max(1, std::min(tiles, pb)), 256, st->proj_smem, s>>>(P);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
 template <int N>
 int state_solve_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
-  const int need = (int)std::min<long long>(st->blocks, (P.n_in + st->warps - 1) / st->warps);
-  csd_solve_kernel<N><<<std::max(need, 1), st->warps * 32, st->smem, s>>>(P);
+  const int warps = g_tune_solve_warps > 0 ? std::min(st->warps, g_tune_solve_warps) : st->warps;
+  const int need = (int)std::min<long long>(st->blocks, (P.n_in + warps - 1) / warps);
+  csd_solve_kernel<N><<<std::max(need, 1), warps * 32, st->smem, s>>>(P);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -1194,14 +1486,16 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
     P.n_in = (int)st->n_active;
     P.act_in = st->act[st->cur];
     P.act_out = st->slist;
-    CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
+    CUDA_TRY(cudaMemsetAsync(st->counter, 0, 2 * sizeof(int), s));
     CUDA_TRY(cudaEventRecord(st->ev[0], s));
     CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(st->ev[1], s));
-    int ns = 0;
-    CUDA_TRY(cudaMemcpyAsync(&ns, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int cnt[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(cnt, st->counter, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    if (cnt[1]) return fail(CSD_ERR_TIMEOUT, "projection: a bounded wait on the tensor cores timed out");
+    const int ns = cnt[0];
     float ms = 0.f;
     CUDA_TRY(cudaEventElapsedTime(&ms, st->ev[0], st->ev[1]));
     st->ms_project += ms;

@@ -2,6 +2,7 @@
 
     python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
         [--method warm|plain|persistent|persistent_warm] [--reps 2]
+        [--projection mma|tcgen05]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
 (lmax 8) or 8 b=0 + 90 DW (lmax 10).  Prints the state's work / time
@@ -18,10 +19,12 @@ def main():
     ap.add_argument("--lmax", type=int, default=8)
     ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm"])
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--projection", default="mma", choices=["mma", "tcgen05"])
     a = ap.parse_args()
     import torch
 
-    from . import csd, synth
+    from . import autotune, csd, synth
+    autotune.set_knob(autotune.KNOB_TC_PROJECTION, 2 if a.projection == "tcgen05" else 1)
     from .warmstart import WarmStartNet
     ndw, nb0 = (60, 6) if a.lmax <= 8 else (90, 8)
     v = synth.make_volume(tuple(a.dims), nb0, ndw, (15.0, 40.0), a.lmax, None, 5)

@@ -71,3 +71,64 @@ def test_uneven_volumes_one_graph_launch(cuda, hr_dirs):
         assert torch.equal(a["status"], b["status"])
     for i, (v, sh, o) in enumerate(zip(vols, shs, outs)):
         _check({k: t.cpu().numpy() for k, t in o.items()}, v, sh, hr_dirs, 8, n_sample=300, seed=i)
+
+
+def test_autotuner_picks_valid_shapes_and_results_do_not_change(cuda, tmp_path, monkeypatch):
+    import torch
+
+    from mrtrix3_b200 import autotune
+    monkeypatch.setenv("CSD_TUNE_CACHE", str(tmp_path / "launch.json"))
+    v = synth.make_volume((48, 48, 24), 6, 60, (15.0, 40.0), 8, 0.5, 55)
+    s = csd.make_shared(v.grad, synth.RESPONSE)
+    d = torch.from_numpy(v.dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    before = csd.dwi2fod_csd(s, d, mask=m)["fod"].clone()
+    st = csd.State(s, v.n_voxels)
+    st.run(d, mask=m)
+    before_phased = st.fod()["fod"]
+    entry = autotune.tune(s, d, mask=m)
+    for k, vals in autotune.CANDIDATES.items():
+        assert entry["config"][str(k)] in vals
+    after = csd.dwi2fod_csd(s, d, mask=m)["fod"]
+    st.run(d, mask=m)
+    assert torch.equal(before, after)
+    assert np.array_equal(before_phased, st.fod()["fod"])
+    again = autotune.tune(s, d, mask=m)          # served from the cache
+    assert again["config"] == entry["config"]
+    autotune.apply({str(k): 0 for k in autotune.CANDIDATES})
+
+
+@pytest.mark.parametrize("lmax", [8, 10])
+def test_tcgen05_projection_equals_mma_projection(cuda, hr_dirs, lmax):
+    """The phased method's tcgen05 projection (accumulators in tensor memory)
+    and its mma.sync projection compute the same products in the same FP16
+    hi/lo split with FP32 accumulation, so the sets and FODs agree exactly
+    on every voxel (plain and warm starts), and both stay on the oracle."""
+    import torch
+
+    from mrtrix3_b200 import autotune
+    ndw, nb0 = (60, 6) if lmax == 8 else (90, 8)
+    v = synth.make_volume((40, 36, 20), nb0, ndw, (15.0, 40.0), lmax, 0.5, 77 + lmax)
+    s = csd.make_shared(v.grad, synth.RESPONSE, lmax=lmax)
+    d = torch.from_numpy(v.dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    plain = csd.dwi2fod_csd(s, d, mask=m, want_negmask=True)
+    warm = plain["negmask"].clone()
+    warm[:, 0] ^= 0x5  # a near-miss first set for every voxel
+    outs = {}
+    try:
+        for kind in (1, 2):
+            autotune.set_knob(autotune.KNOB_TC_PROJECTION, kind)
+            st = csd.State(s, v.n_voxels)
+            st.run(d, mask=m)
+            a = st.fod()
+            st.run(d, mask=m, warm=warm)
+            outs[kind] = (a, st.fod(), st.stats())
+            st.close()
+    finally:
+        autotune.set_knob(autotune.KNOB_TC_PROJECTION, 0)
+    for i in range(2):
+        for k in ("fod", "negmask", "status", "iterations"):
+            assert np.array_equal(outs[1][i][k], outs[2][i][k]), k
+    assert outs[1][2]["projected"] == outs[2][2]["projected"]
+    _check(outs[2][0], v, s, hr_dirs, lmax, n_sample=800)

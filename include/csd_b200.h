@@ -125,7 +125,7 @@ typedef struct csd_mlp csd_mlp;  /* the warm-start network, below */
 /* The phased method on HOST buffers (same layout as csd_dwi2fod_host):
  * per slab of voxels, csd_state_set, then -- when `net` is not NULL -- the
  * network's predicted first negative sets (csd_mlp_predict + csd_state_warm),
- * then csd_state_iterate until no voxel is active, then csd_state_fod.  Slab
+ * then csd_state_run until no voxel is active, then csd_state_fod.  Slab
  * uploads / downloads overlap the passes of the other slab.  Synchronous. */
 int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const float* dwi, int64_t n_voxels,
                             const uint8_t* mask, float* fod, uint8_t* status, uint8_t* iterations);
@@ -147,6 +147,13 @@ int csd_state_warm(csd_state* st, const uint32_t* negmask, void* stream);
 /* One CSD::iterate() on every active voxel.  *n_active receives how many
  * voxels are still iterating afterwards (synchronises the stream). */
 int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream);
+/* CSD::iterate() until every voxel is done (the `for (n < niter) if
+ * (iterate()) break;` loop of dwi2fod.cpp:137-139 over the batch), or for at most max_passes passes when
+ * max_passes > 0.  Passes are enqueued in batches that read their voxel
+ * counts on the device, with one host round trip per batch; the results are
+ * identical to calling csd_state_iterate until it reports 0.  *n_active (may
+ * be NULL) receives how many voxels are still iterating (synchronises). */
+int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, void* stream);
 /* Work and device time since the last csd_state_set: out[8] = passes, voxels
  * projected, voxels solved, sum of |negative set| over the solves, then the
  * device milliseconds of the set / projection / solve kernels, and the

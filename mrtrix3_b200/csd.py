@@ -29,7 +29,8 @@ STATUS_FP64, STATUS_CHOLFAIL, STATUS_WARM_RESTART = 0x10, 0x20, 0x40
 EXPORTED = [
     "csd_params_init", "csd_shared_create", "csd_shared_destroy", "csd_shared_nsh", "csd_shared_info",
     "csd_shared_dwis", "csd_shared_matrix", "csd_solve", "csd_dwi2fod_host", "csd_state_create",
-    "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_fod",
+    "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_run",
+    "csd_state_fod",
     "csd_state_stats", "csd_dwi2fod_host_phased", "csd_last_error",
 ]
 
@@ -82,6 +83,7 @@ def lib():
         L.csd_state_set.argtypes = [vp, vp, i64, i64, i64, vp, vp]
         L.csd_state_warm.argtypes = [vp, vp, vp]
         L.csd_state_iterate.argtypes = [vp, ctypes.POINTER(i64), vp]
+        L.csd_state_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(i64), vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]
         L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_dwi2fod_host_phased.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
@@ -369,16 +371,21 @@ class State:
         keys = ("passes", "projected", "solved", "sum_neg", "ms_set", "ms_project", "ms_solve", "launches")
         return dict(zip(keys, list(out)))
 
+    def iterate_all(self, max_passes: int = 0, stream=None) -> int:
+        """iterate() until no voxel is active (csd_state_run: passes batched on
+        the device, same results); returns how many remain active."""
+        n = ctypes.c_int64()
+        check(lib().csd_state_run(self._h, int(max_passes), ctypes.byref(n), ctypes.c_void_p(_stream_ptr(stream))))
+        return n.value
+
     def run(self, dwi, mask=None, warm=None, stream=None):
         """The phased method over one volume: set (+ warm sets), then iterate
         until no voxel is active.  Returns the number of passes."""
         self.set(dwi, mask=mask, stream=stream)
         if warm is not None:
             self.warm(warm, stream=stream)
-        passes = 0
-        while self.iterate(stream=stream) > 0:
-            passes += 1
-        return passes + 1
+        self.iterate_all(stream=stream)
+        return int(self.stats()["passes"])
 
     def fod(self, stream=None, as_numpy=True):
         import torch

@@ -250,8 +250,10 @@ struct StateParams {
   uint8_t* status;      // [cap]
   uint16_t* iters;      // [cap] iterate() calls made
   const int* act_in;    // [n_in] voxel ids
+  const int* n_in_dev;  // device count of act_in (overrides n_in when set)
   int* act_out;         // compacted output list
   int* n_out;
+  int* err;             // set to 1 when a bounded wait times out
   unsigned long long* stats;  // [0] sum of |neg| over solves, [1] solves
   double* fp64_scratch;
   // set() inputs
@@ -311,6 +313,8 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
   __half* Fh = Hl + npd * D::HS16;
   __half* Fl = Fh + kProjRows * D::HS16;
   uint32_t* bm = reinterpret_cast<uint32_t*>(Fl + kProjRows * D::HS16);  // [64][kMaxWords]
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
+  if ((long long)blockIdx.x * kProjRows >= n_in) return;  // the grid is an upper bound
   {
     const uint4* src = reinterpret_cast<const uint4*>(P.Hp16);
     uint4* dst = reinterpret_cast<uint4*>(Hh);
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
   const int mrow = 16 * (warp & 3);
   const int half = warp >> 2;
   constexpr int tpw = 20;                    // n8 tiles per warp: half of a 320-direction chunk
-  const int ntiles = (P.n_in + kProjRows - 1) / kProjRows;
+  const int ntiles = (n_in + kProjRows - 1) / kProjRows;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * kProjRows;
     __syncthreads();
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
     for (int i = threadIdx.x; i < kProjRows * D::HS16; i += blockDim.x) {
       const int r = i / D::HS16, c = i - r * D::HS16;
       float f = 0.f;
-      if (e0 + r < P.n_in && c < N) f = P.F[(long long)P.act_in[e0 + r] * D::HS + c] * kProjFScale;
+      if (e0 + r < n_in && c < N) f = P.F[(long long)P.act_in[e0 + r] * D::HS + c] * kProjFScale;
       const __half h = __float2half_rn(f);
       Fh[i] = h;
       Fl[i] = __float2half_rn(f - __half2float(h));
@@ -379,7 +383,7 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
     __syncthreads();
     // per-voxel decision: warp w handles rows w, w + 8, ...
     for (int r = warp; r < kProjRows; r += 8) {
-      if (e0 + r >= P.n_in) break;
+      if (e0 + r >= n_in) break;
       const long long v = P.act_in[e0 + r];
       const int it = P.iters[v];
       const bool warm = it == 0 && P.use_warm && P.warm;
@@ -467,6 +471,9 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sAl + A_BYTES);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
+  const int ntiles = (n_in + kTcRows - 1) / kTcRows;
+  if ((int)blockIdx.x >= ntiles) return;  // the grid is an upper bound; before any allocation
   // direction table (host-prepared in the core-matrix layout), once per block
   {
     const uint4* src = reinterpret_cast<const uint4*>(P.Htc16);
@@ -492,7 +499,6 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
   const uint32_t bH = static_cast<uint32_t>(__cvta_generic_to_shared(sBh));
   const uint32_t bL = static_cast<uint32_t>(__cvta_generic_to_shared(sBl));
   constexpr uint32_t A_LBO = (kTcRows / 8) * 128, B_LBO = (kTcDirs / 8) * 128;
-  const int ntiles = (P.n_in + kTcRows - 1) / kTcRows;
   uint32_t phase = 0;
   bool failed = false;
   for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
@@ -503,7 +509,7 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
       float f[KC * 8];
 #pragma unroll
       for (int c = 0; c < KC * 8; ++c) f[c] = 0.f;
-      if (e0 + r < P.n_in) {
+      if (e0 + r < n_in) {
         const float4* src = reinterpret_cast<const float4*>(P.F + (long long)P.act_in[e0 + r] * D::HS);
 #pragma unroll
         for (int q = 0; q < (KC * 8) / 4; ++q) {
@@ -565,7 +571,7 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
       // give the tensor core a second bounded chance to drain before the
       // tensor memory is freed, then report the time-out
       mbar_wait(mbar_a, phase ^ 1u);
-      if (tid == 0) atomicExch(P.n_out + 1, 1);
+      if (tid == 0) atomicExch(P.err, 1);
       failed = true;
       break;
     }
@@ -593,7 +599,7 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     // per-voxel decision (csd.h:246-253), one thread per voxel
     const int r = tid;
-    if (e0 + r < P.n_in) {
+    if (e0 + r < n_in) {
       const long long v = P.act_in[e0 + r];
       const int it = P.iters[v];
       const bool warm = it == 0 && P.use_warm && P.warm;
@@ -632,14 +638,16 @@ template <int N>
 __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(const __grid_constant__ StateParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int HS = Dims<N>::HS;
+  const int nwarps = blockDim.x >> 5;
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
+  if ((long long)blockIdx.x * nwarps >= n_in) return;  // the grid is an upper bound
   const HTab<N> H = load_htab<N>(smem, P.sc, P.nhr, false);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
   WarpWS<N> w = carve_ws<N>(smem + htab_bytes<N>(P.nhr, false) + warp * warp_ws_bytes<N>());
   double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
   const int gw = blockIdx.x * nwarps + warp, nwt = gridDim.x * nwarps;
-  for (int e = gw; e < P.n_in; e += nwt) {
+  for (int e = gw; e < n_in; e += nwt) {
     const long long v = P.act_in[e];
     for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
     for (int c = lane; c < HS; c += 32) w.F[c] = 0.f;
@@ -1216,6 +1224,9 @@ extern "C" int csd_debug_set_refine(int mode) {
 // ---------------------------------------------------------------------------
 // csd_state_*: per-step surface (CSD::set / iterate / FOD over a batch)
 
+// passes enqueued by csd_state_run between two reads of the active count
+static constexpr int kRunBatch = 16;
+
 struct csd_state {
   const csd_shared* sh = nullptr;
   int64_t cap = 0, n = 0, n_active = 0;
@@ -1240,6 +1251,8 @@ struct csd_state {
   long long passes = 0, projected = 0, solved = 0;  // work counters since the last set()
   unsigned long long* stats = nullptr;              // device: sum |neg|, solves
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int* pcount = nullptr;                            // device: per-pass counts of csd_state_run
+  cudaEvent_t bev[2 * kRunBatch + 1] = {};          // pass boundaries of one csd_state_run batch
   double ms_set = 0, ms_project = 0, ms_solve = 0;  // device time of the kernels since the last set()
   long long launches = 0;
 };
@@ -1301,6 +1314,7 @@ StateParams state_params(const csd_state* st) {
   P.status = st->status;
   P.iters = st->iters;
   P.n_out = st->counter;
+  P.err = st->counter + 1;
   P.stats = st->stats;
   P.fp64_scratch = st->fp64;
   return P;
@@ -1397,7 +1411,9 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->act[1], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->counter, 2 * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->stats, 2 * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMalloc(&st->pcount, (2 * kRunBatch + 2) * sizeof(int)));
   for (auto& e : st->ev) CUDA_TRY(cudaEventCreate(&e));
+  for (auto& e : st->bev) CUDA_TRY(cudaEventCreate(&e));
   int rc = 0;
   CSD_DISPATCH(n, rc = state_shape<NN>(st.get()));
   if (rc) return rc;
@@ -1421,7 +1437,10 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->counter);
   cudaFree(st->stats);
   cudaFree(st->fp64);
+  cudaFree(st->pcount);
   for (auto& e : st->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : st->bev)
     if (e) cudaEventDestroy(e);
   delete st;
 }
@@ -1524,6 +1543,74 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
     st->n_active = na;
     st->cur ^= 1;
     st->passes += 1;
+  }
+  if (n_active) *n_active = st->n_active;
+  return CSD_OK;
+}
+
+// Iterate until no voxel is active (or max_passes passes, when > 0).  The
+// passes are enqueued in batches of up to kRunBatch without a host round
+// trip between them: each kernel reads its input count from the device
+// (the count the previous kernel produced) and the launch grids are sized
+// for the active count at the start of the batch, an upper bound for every
+// later pass since a voxel never becomes active again.  The kernels and
+// their per-voxel arithmetic are the ones csd_state_iterate launches, so the
+// results are identical to calling csd_state_iterate until it reports 0.
+extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, void* stream) {
+  if (!st) return fail(CSD_ERR_INVALID, "csd_state_run: NULL state");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int done = 0, batch = 4;
+  while (st->n_active > 0 && (max_passes <= 0 || done < max_passes)) {
+    int K = std::min(batch, kRunBatch);
+    if (max_passes > 0) K = std::min(K, max_passes - done);
+    batch *= 2;
+    const int U = (int)st->n_active;
+    CUDA_TRY(cudaMemsetAsync(st->pcount, 0, (2 * K + 1) * sizeof(int), s));
+    CUDA_TRY(cudaMemsetAsync(st->counter + 1, 0, sizeof(int), s));
+    CUDA_TRY(cudaEventRecord(st->bev[0], s));
+    int rc = 0;
+    for (int p = 0; p < K; ++p) {
+      StateParams P = state_params(st);
+      P.n_in = U;  // grid size; the count itself comes from the device after the first pass
+      P.n_in_dev = p == 0 ? nullptr : st->pcount + 2 * p;
+      P.act_in = st->act[st->cur];
+      P.act_out = st->slist;
+      P.n_out = st->pcount + 2 * p + 1;
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+      if (rc) return rc;
+      CUDA_TRY(cudaEventRecord(st->bev[2 * p + 1], s));
+      StateParams Q = state_params(st);
+      Q.n_in = U;
+      Q.n_in_dev = st->pcount + 2 * p + 1;
+      Q.act_in = st->slist;
+      Q.act_out = st->act[st->cur ^ 1];
+      Q.n_out = st->pcount + 2 * p + 2;
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Q, s));
+      if (rc) return rc;
+      CUDA_TRY(cudaEventRecord(st->bev[2 * p + 2], s));
+      st->cur ^= 1;
+    }
+    int cnt[2 * kRunBatch + 1];
+    int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(cnt, st->pcount, (2 * K + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(&err, st->counter + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) return fail(CSD_ERR_TIMEOUT, "projection: a bounded wait on the tensor cores timed out");
+    cnt[0] = U;
+    st->launches += 2 * K;  // every enqueued pass launches both kernels (empty ones return at once)
+    for (int p = 0; p < K; ++p) {
+      if (cnt[2 * p] == 0) break;
+      float a = 0.f, b = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&a, st->bev[2 * p], st->bev[2 * p + 1]));
+      CUDA_TRY(cudaEventElapsedTime(&b, st->bev[2 * p + 1], st->bev[2 * p + 2]));
+      st->ms_project += a;
+      st->ms_solve += b;
+      st->projected += cnt[2 * p];
+      st->solved += cnt[2 * p + 1];
+      st->passes += 1;
+      ++done;
+    }
+    st->n_active = cnt[2 * K];
   }
   if (n_active) *n_active = st->n_active;
   return CSD_OK;
@@ -1765,9 +1852,7 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
       if ((rc = csd_mlp_predict(net, w.dwi[b], n, nvol, 1, dmask, 0.f, w.warm[b], st))) return rc;
       if ((rc = csd_state_warm(w.st[b], w.warm[b], st))) return rc;
     }
-    int64_t active = 1;
-    while (active > 0)
-      if ((rc = csd_state_iterate(w.st[b], &active, st))) return rc;
+    if ((rc = csd_state_run(w.st[b], 0, nullptr, st))) return rc;
     uint8_t* dst = w.small[b] + per;
     uint8_t* dit = w.small[b] + 2 * per;
     if ((rc = csd_state_fod(w.st[b], w.fod[b], nsh, status ? dst : nullptr, iterations ? dit : nullptr, nullptr, st)))

@@ -203,6 +203,44 @@ def test_state_api_matches_oracle(cuda, hr_dirs):
     check_parity(out, ref)
 
 
+def test_state_run_equals_iterate_loop(cuda):
+    """csd_state_run (passes batched on the device, counts read back once per
+    batch) gives the same FODs, sets, statuses and iteration counts as
+    calling csd_state_iterate until it reports 0, plain and warm-started,
+    and max_passes stops it after that many passes."""
+    import torch
+    v = synth.make_volume((48, 40, 12), 6, 60, (15.0, 40.0), 8, 0.5, 82)
+    s = csd.make_shared(v.grad, synth.RESPONSE)
+    d = torch.from_numpy(v.dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    plain = csd.dwi2fod_csd(s, d, mask=m, want_negmask=True)
+    warm = plain["negmask"].clone()
+    warm[:, 1] ^= 0x30
+    st = csd.State(s, v.n_voxels)
+    for w in (None, warm):
+        st.set(d, mask=m)
+        if w is not None:
+            st.warm(w)
+        loop = 0
+        while st.iterate() > 0:
+            loop += 1
+        a = st.fod()
+        stats_loop = st.stats()
+        st.set(d, mask=m)
+        if w is not None:
+            st.warm(w)
+        assert st.iterate_all(max_passes=2) > 0
+        assert st.stats()["passes"] == 2
+        assert st.iterate_all() == 0
+        b = st.fod()
+        for k in ("fod", "negmask", "status", "iterations"):
+            assert np.array_equal(a[k], b[k]), k
+        sb = st.stats()
+        for k in ("passes", "projected", "solved", "sum_neg"):
+            assert sb[k] == stats_loop[k], k
+    st.close()
+
+
 def test_per_voxel_surface(cuda, hr_dirs):
     """CSD(shared).set(S); while not iterate(); FOD() -- the reference's per-voxel object."""
     v = synth.make_volume((4, 1, 1), 6, 60, 30.0, 8, None, 81)

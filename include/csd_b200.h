@@ -214,8 +214,10 @@ int csd_mlp_logits(csd_mlp* m, const uint16_t* x, int64_t n, float* z_out);
  * (mrtrix3_b200/autotune.py): which = 0 warps per block of the persistent
  * kernel, 1 warps per block of the phased solve kernel, 2 projection blocks
  * per SM, 3 projection kernel of the phased method (1 mma.sync, 2 tcgen05
- * with the accumulators in tensor memory; up to 320 constraint directions);
- * value 0 = built-in default.  Outputs do not depend on them. */
+ * with the accumulators in tensor memory; up to 320 constraint directions),
+ * 4 phased solve kernel (1 a warp per voxel, 2 / 3 groups of 16 / 8 lanes
+ * per voxel, lmax <= 8); value 0 = built-in default.  Outputs do not depend
+ * on them (bit for bit). */
 int csd_set_launch_config(int which, int value);
 
 /* Thread-local description of the last failure. */

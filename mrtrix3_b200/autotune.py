@@ -2,8 +2,8 @@
 
 Times candidate values of the launch knobs of csd_set_launch_config (warps
 per block of the persistent kernel and of the phased solve kernel, the
-projection kernel -- mma.sync or tcgen05 -- and its blocks per SM) on a
-probe volume, keeps the fastest, and caches
+phased solve kernel's lanes per voxel, the projection kernel -- mma.sync or
+tcgen05 -- and its blocks per SM) on a probe volume, keeps the fastest, and caches
 the choice per (GPU name, nSH, constraint directions, DW directions) in a
 JSON file (default ~/.cache/mrtrix3_b200/launch.json, or $CSD_TUNE_CACHE).
 Outputs do not depend on the knobs, so tuning never changes results.
@@ -18,10 +18,11 @@ import numpy as np
 
 from . import csd
 
-KNOB_PERSISTENT, KNOB_SOLVE, KNOB_PROJ, KNOB_TC_PROJECTION = 0, 1, 2, 3
+KNOB_PERSISTENT, KNOB_SOLVE, KNOB_PROJ, KNOB_TC_PROJECTION, KNOB_SOLVE_KIND = 0, 1, 2, 3, 4
 # the projection kernel is chosen before its blocks per SM (which only the
 # mma.sync kernel uses)
-CANDIDATES = {KNOB_PERSISTENT: [8, 12, 16], KNOB_SOLVE: [12, 16, 20], KNOB_TC_PROJECTION: [1, 2], KNOB_PROJ: [1, 2]}
+CANDIDATES = {KNOB_PERSISTENT: [8, 12, 16], KNOB_SOLVE: [12, 16, 20], KNOB_SOLVE_KIND: [1, 2], KNOB_TC_PROJECTION: [1, 2],
+              KNOB_PROJ: [1, 2]}
 
 
 def cache_path() -> str:

@@ -736,6 +736,226 @@ __device__ __forceinline__ void chol_back_f32(const float* L, const float* rdiag
   }
 }
 
+// ---- grouped variants: G lanes per system, 32 / G systems per warp.  Each
+// group runs the exact operation sequence of cholesky_packed_f32 /
+// chol_back_f32 on its own matrix (sublane s in place of the lane, G in
+// place of 32, shuffles of width G), so the results are bit-identical to
+// the warp-per-system versions while one warp instruction serves 32 / G
+// systems and fewer lanes idle on the short rows of late column blocks.
+template <int N, int G>
+struct GroupDims {
+  static constexpr int V = 32 / G;               // systems per warp
+  static constexpr int CQG = (N + 1 + G - 1) / G;  // row slots per lane (rows 0..N)
+};
+
+// Factorisation of the group's packed matrix A (rows 0..N, row N the
+// right-hand side).  Never returns early: the shuffles need every lane of
+// the warp, so a failed pivot only clears the returned flag (group-uniform).
+template <int N, int G>
+__device__ bool cholesky_group_f32(float* A, float* rdiag, int s, float& dmin, float& dmax) {
+  constexpr int CQG = GroupDims<N, G>::CQG;
+  dmin = 3.0e38f;
+  dmax = 0.f;
+  bool okall = true;
+  constexpr int NB = (N + 3) / 4;
+#pragma unroll 1
+  for (int cb = 0; cb < NB; ++cb) {
+    const int j0 = 4 * cb;
+    const float* Lj0 = A + packoff(j0);
+    const float* Lj1 = A + packoff(j0 + 1);
+    const float* Lj2 = A + packoff(j0 + 2);
+    const float* Lj3 = A + packoff(j0 + 3);
+    // every row slot of this lane in one pass over k: the four pivot-row
+    // quads are loaded once per step and shared by the slots, whose chains
+    // are independent (the same fmaf sequence per element as the warp form)
+    const float* Li[CQG];
+    bool act[CQG];
+    float acc[CQG][8];
+#pragma unroll
+    for (int q = 0; q < CQG; ++q) {
+      const int i = j0 + s + G * q;
+      act[q] = i <= N;
+      Li[q] = A + packoff(act[q] ? i : j0);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[q][c] = 0.f;
+    }
+    for (int kk = 0; kk < j0; kk += 4) {
+      const float4 y0 = *reinterpret_cast<const float4*>(Lj0 + kk);
+      const float4 y1 = *reinterpret_cast<const float4*>(Lj1 + kk);
+      const float4 y2 = *reinterpret_cast<const float4*>(Lj2 + kk);
+      const float4 y3 = *reinterpret_cast<const float4*>(Lj3 + kk);
+#pragma unroll
+      for (int q = 0; q < CQG; ++q) {
+        if (act[q]) {
+          const float4 x = *reinterpret_cast<const float4*>(Li[q] + kk);
+          float* a = acc[q];
+          a[0] = fmaf(x.x, y0.x, a[0]); a[4] = fmaf(x.y, y0.y, a[4]); a[0] = fmaf(x.z, y0.z, a[0]); a[4] = fmaf(x.w, y0.w, a[4]);
+          a[1] = fmaf(x.x, y1.x, a[1]); a[5] = fmaf(x.y, y1.y, a[5]); a[1] = fmaf(x.z, y1.z, a[1]); a[5] = fmaf(x.w, y1.w, a[5]);
+          a[2] = fmaf(x.x, y2.x, a[2]); a[6] = fmaf(x.y, y2.y, a[6]); a[2] = fmaf(x.z, y2.z, a[2]); a[6] = fmaf(x.w, y2.w, a[6]);
+          a[3] = fmaf(x.x, y3.x, a[3]); a[7] = fmaf(x.y, y3.y, a[7]); a[3] = fmaf(x.z, y3.z, a[3]); a[7] = fmaf(x.w, y3.w, a[7]);
+        }
+      }
+    }
+    float sv[CQG][4];
+#pragma unroll
+    for (int q = 0; q < CQG; ++q) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) sv[q][c] = 0.f;
+      if (act[q]) {
+        const float4 w4 = *reinterpret_cast<const float4*>(Li[q] + j0);
+        sv[q][0] = w4.x - (acc[q][0] + acc[q][4]);
+        sv[q][1] = w4.y - (acc[q][1] + acc[q][5]);
+        sv[q][2] = w4.z - (acc[q][2] + acc[q][6]);
+        sv[q][3] = w4.w - (acc[q][3] + acc[q][7]);
+      }
+    }
+    // the diagonal block rows j0..j0+3 sit in sublanes 0..3 of slot 0
+    float d[4][4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+      for (int c = 0; c <= t; ++c) d[t][c] = __shfl_sync(0xffffffffu, sv[0][c], t, G);
+    const int nb = N - j0 < 4 ? N - j0 : 4;
+    float L[4][4], rd[4];
+    bool ok = true;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+#pragma unroll
+      for (int c = 0; c < t; ++c) {
+        float v = d[t][c];
+#pragma unroll
+        for (int e = 0; e < c; ++e) v = fmaf(-L[t][e], L[c][e], v);
+        L[t][c] = (t <= nb && c < nb) ? v * rd[c] : 0.f;
+      }
+      float v = d[t][t];
+#pragma unroll
+      for (int e = 0; e < t; ++e) v = fmaf(-L[t][e], L[t][e], v);
+      if (t >= nb) v = 1.f;
+      ok = ok && (v > 0.f) && isfinite(v);
+      const float dd = sqrtf(v);
+      L[t][t] = dd;
+      rd[t] = 1.0f / dd;
+      if (t < nb) {
+        dmin = fminf(dmin, dd);
+        dmax = fmaxf(dmax, dd);
+      }
+    }
+    okall = okall && ok;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < CQG; ++q) {
+      const int i = j0 + s + G * q;
+      if (i <= N) {
+        float o[4];
+        if (q == 0 && s < 4) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            float v = 0.f;
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+              if (t == s && c <= t) v = L[t][c];
+            o[c] = v;
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            float v = sv[q][c];
+#pragma unroll
+            for (int e = 0; e < c; ++e) v = fmaf(-o[e], L[c][e], v);
+            o[c] = v * rd[c];
+          }
+        }
+        *reinterpret_cast<float4*>(A + packoff(i) + j0) = make_float4(o[0], o[1], o[2], o[3]);
+      }
+    }
+    if (s < 4) rdiag[j0 + s] = s == 0 ? rd[0] : s == 1 ? rd[1] : s == 2 ? rd[2] : rd[3];
+    __syncwarp();
+  }
+  return okall;
+}
+
+// x := L^-T x for the group's factor, x distributed as x[q] = element s + G q.
+template <int N, int G>
+__device__ __forceinline__ void chol_back_group_f32(const float* L, const float* rdiag, float* x, int s) {
+  constexpr int CQG = GroupDims<N, G>::CQG;
+  constexpr int NB = (N + 3) / 4;
+#pragma unroll 1
+  for (int cb = NB - 1; cb >= 0; --cb) {
+    const int j0 = 4 * cb;
+    float y[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int r = j0 + c;
+      float xv = 0.f;
+#pragma unroll
+      for (int q = 0; q < CQG; ++q)
+        if (q == r / G) xv = x[q];
+      y[c] = __shfl_sync(0xffffffffu, xv, r % G, G);
+    }
+#pragma unroll
+    for (int c = 3; c >= 0; --c) {
+      if (j0 + c < N) {
+        float v = y[c];
+#pragma unroll
+        for (int e = c + 1; e < 4; ++e)
+          if (j0 + e < N) v = fmaf(-L[packoff(j0 + e) + j0 + c], y[e], v);
+        y[c] = v * rdiag[j0 + c];
+      } else {
+        y[c] = 0.f;
+      }
+    }
+    const float* L0 = L + packoff(j0);
+    const float* L1 = L + packoff(j0 + 1);
+    const float* L2 = L + packoff(j0 + 2);
+    const float* L3 = L + packoff(j0 + 3);
+#pragma unroll
+    for (int q = 0; q < CQG; ++q) {
+      const int i = s + G * q;
+      if (i < j0) {
+        float v = x[q];
+        v = fmaf(-L0[i], y[0], v);
+        if (j0 + 1 < N) v = fmaf(-L1[i], y[1], v);
+        if (j0 + 2 < N) v = fmaf(-L2[i], y[2], v);
+        if (j0 + 3 < N) v = fmaf(-L3[i], y[3], v);
+        x[q] = v;
+      } else if (i < j0 + 4 && i < N) {
+        x[q] = (i == j0) ? y[0] : (i == j0 + 1) ? y[1] : (i == j0 + 2) ? y[2] : y[3];
+      }
+    }
+  }
+}
+
+// Per-warp workspace of the grouped solve: V slots, each [packed W + the
+// right-hand-side row][F][1/L_ii][b (fp64)], then one negative-set list
+// shared by the slots (the assembly uses it one slot at a time).  The slot
+// stride is padded to 128/V bytes past a multiple of 128 so the groups'
+// scalar accesses at equal offsets fall in different banks.
+template <int N, int V>
+struct GroupWSLayout {
+  static constexpr int W_BYTES = ((packoff(N + 1) * 4 + 15) / 16) * 16;
+  static constexpr int F_BYTES = Dims<N>::HS * 4;
+  static constexpr int B_BYTES = ((N * 8 + 15) / 16) * 16;
+  static constexpr int RAW = W_BYTES + F_BYTES + rdiag_bytes<N>() + B_BYTES;
+  static constexpr int PAD = 128 / V;
+  static constexpr int SLOT = ((RAW - PAD + 127) / 128) * 128 + PAD;
+  static constexpr int WARP = V * SLOT + ((kMaxHR * 2 + 15) / 16) * 16;
+};
+
+template <int N, int V>
+__device__ __forceinline__ WarpWS<N> group_slot_ws(unsigned char* base, int g) {
+  using Lw = GroupWSLayout<N, V>;
+  WarpWS<N> w;
+  unsigned char* p = base + g * Lw::SLOT;
+  w.W = reinterpret_cast<float*>(p);
+  w.F = reinterpret_cast<float*>(p + Lw::W_BYTES);
+  w.rdiag = reinterpret_cast<float*>(p + Lw::W_BYTES + Lw::F_BYTES);
+  w.b = reinterpret_cast<double*>(p + Lw::W_BYTES + Lw::F_BYTES + rdiag_bytes<N>());
+  w.neg = reinterpret_cast<uint16_t*>(base + V * Lw::SLOT);
+  w.old = nullptr;
+  w.old2 = nullptr;
+  return w;
+}
+
 // FP64 version (fallback path, L in FP64 global scratch).
 template <int N>
 __device__ __forceinline__ void chol_subst_f64(const double* L, double* x, int lane) {

@@ -50,6 +50,8 @@ static int g_tune_persistent_warps = 0;  // warps per block of csd_persistent_ke
 static int g_tune_solve_warps = 0;       // warps per block of csd_solve_kernel
 static int g_tune_proj_blocks_per_sm = 0;
 static int g_proj_kind = 0;  // projection kernel: 0 default, 1 mma.sync, 2 tcgen05 (nhr <= 320)
+static int g_solve_kind = 0;  // phased solve kernel: 0 default, 1 warp per voxel, 2 / 3 groups of 16 / 8 lanes
+static constexpr int kSolveDefault = 1;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
 
 
@@ -647,7 +649,14 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
   WarpWS<N> w = carve_ws<N>(smem + htab_bytes<N>(P.nhr, false) + warp * warp_ws_bytes<N>());
   double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
   const int gw = blockIdx.x * nwarps + warp, nwt = gridDim.x * nwarps;
+#ifdef CSD_PHASE_TIMERS
+  long long tacc[kPhTotal + 1] = {};
+  const long long tstart = clock64();
+#else
+  long long* tacc = nullptr;
+#endif
   for (int e = gw; e < n_in; e += nwt) {
+    CSD_T0(tl);
     const long long v = P.act_in[e];
     for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
     for (int c = lane; c < HS; c += 32) w.F[c] = 0.f;
@@ -661,7 +670,10 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
       atomicAdd(P.stats, (unsigned long long)k);
       atomicAdd(P.stats + 1, 1ULL);
     }
-    const int fl = assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot) & 0x70;
+    CSD_T1(tacc, kPhList, tl);
+    const int fl =
+        assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot, tacc) & 0x70;
+    CSD_T0(tw);
     for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
     if (lane < P.nw) {
       P.old2[v * P.nw + lane] = P.old[v * P.nw + lane];
@@ -675,6 +687,128 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
         P.status[v] = (uint8_t)(kActive | flags);
         P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
       }
+    }
+    CSD_T1(tacc, kPhSet, tw);
+  }
+#ifdef CSD_PHASE_TIMERS
+  tacc[kPhTotal] = clock64() - tstart;
+  if (lane == 0)
+    for (int p = 0; p <= kPhTotal; ++p) atomicAdd(&g_phase_cycles[p], (unsigned long long)tacc[p]);
+#endif
+}
+
+// Solve pass with G lanes per voxel: each warp takes 32 / G voxels of the
+// solve list, assembles them one after another (warp-wide tensor-core
+// rank-k, as csd_solve_kernel), factorises and back-substitutes all of them
+// at once (one group of G lanes per voxel), then finishes them one by one
+// (FP64 fallback, refinement of cycling voxels, stores).  The arithmetic of
+// every voxel is the sequence csd_solve_kernel performs, so the outputs are
+// bit-identical; the grouping cuts the instructions per voxel of the
+// factorisation and substitution, where a whole warp on one 45 x 45 system
+// leaves most lanes idle on the short rows of the late column blocks.
+template <int G>
+struct GroupSolveThreads {
+  static constexpr int value = G == 16 ? 416 : 224;  // 13 / 7 warps: what fits beside the tables
+};
+
+template <int N, int G>
+__global__ void __launch_bounds__(GroupSolveThreads<G>::value, 1)
+    csd_solve_group_kernel(const __grid_constant__ StateParams P) {
+  constexpr int V = 32 / G;
+  constexpr int CQG = GroupDims<N, G>::CQG;
+  using Lw = GroupWSLayout<N, V>;
+  constexpr int HS = Dims<N>::HS;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nwarps = blockDim.x >> 5;
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
+  if ((long long)blockIdx.x * nwarps * V >= n_in) return;  // the grid is an upper bound
+  const HTab<N> H = load_htab<N>(smem, P.sc, P.nhr, false);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = lane / G, sl = lane % G;
+  unsigned char* base = smem + htab_bytes<N>(P.nhr, false) + warp * Lw::WARP;
+  double* slot64 = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
+  const WarpWS<N> mine = group_slot_ws<N, V>(base, grp);
+  const long long stride = (long long)gridDim.x * nwarps * V;
+  for (long long e0 = ((long long)blockIdx.x * nwarps + warp) * V; e0 < n_in; e0 += stride) {
+    // 1. assembly of each voxel's system (+ its right-hand side as row N)
+#pragma unroll 1
+    for (int g = 0; g < V; ++g) {
+      if (e0 + g >= n_in) break;
+      const WarpWS<N> w = group_slot_ws<N, V>(base, g);
+      const long long v = P.act_in[e0 + g];
+      for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
+      for (int c = lane; c < HS; c += 32) w.F[c] = 0.f;
+      uint32_t bits[kMaxWords];
+#pragma unroll
+      for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.newm[v * P.nw + p] : 0u;
+      __syncwarp();
+      const int k = mask_to_list(bits, P.nw, w.neg, lane);
+      if (lane == 0 && P.stats) {
+        atomicAdd(P.stats, (unsigned long long)k);
+        atomicAdd(P.stats + 1, 1ULL);
+      }
+      assemble<N, true>(H, P.sc.MtMp, k, w, lane);
+      float* bN = w.W + packoff(N);
+      for (int c = lane; c < packoff(N + 1) - packoff(N); c += 32) bN[c] = c < N ? (float)w.b[c] : 0.f;
+      __syncwarp();
+    }
+    // 2. factorisation (forward solve fused) + back substitution, all voxels
+    float dmin, dmax;
+    const bool okl = cholesky_group_f32<N, G>(mine.W, mine.rdiag, sl, dmin, dmax);
+    const float cond = okl ? (dmax / dmin) * (dmax / dmin) : 3.0e38f;
+    const bool goodl = okl && (cond <= P.cond_thr);
+    const unsigned good = __ballot_sync(0xffffffffu, goodl);
+    float x[CQG];
+#pragma unroll
+    for (int q = 0; q < CQG; ++q) {
+      const int i = sl + G * q;
+      x[q] = i < N ? mine.W[packoff(N) + i] : 0.f;
+    }
+    chol_back_group_f32<N, G>(mine.W, mine.rdiag, x, sl);
+    if (goodl) {
+#pragma unroll
+      for (int q = 0; q < CQG; ++q) {
+        const int i = sl + G * q;
+        if (i < N) mine.F[i] = x[q];
+      }
+    }
+    __syncwarp();
+    // 3. per voxel: FP64 fallback / refinement, stores, next active list
+#pragma unroll 1
+    for (int g = 0; g < V; ++g) {
+      if (e0 + g >= n_in) break;
+      const WarpWS<N> w = group_slot_ws<N, V>(base, g);
+      const long long v = P.act_in[e0 + g];
+      const uint8_t st = P.status[v];
+      const bool ok = (good >> (g * G)) & 1u;
+      int fl = 0;
+      if (!ok || (st & kCycling)) {
+        // the shared list holds the last voxel's set: rebuild this one's
+        uint32_t bits[kMaxWords];
+#pragma unroll
+        for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.newm[v * P.nw + p] : 0u;
+        const int k = mask_to_list(bits, P.nw, w.neg, lane);
+        if (!ok)
+          fl = 0x10 | (solve_fp64<N>(P.sc, k, w, slot64, lane) ? 0 : 0x20);
+        else
+          refine_step<N>(P.sc, H, k, w, lane);
+      }
+      for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
+      if (lane < P.nw) {
+        P.old2[v * P.nw + lane] = P.old[v * P.nw + lane];
+        P.old[v * P.nw + lane] = P.newm[v * P.nw + lane];
+      }
+      if (lane == 0) {
+        const uint8_t flags = (uint8_t)((st & 0xF0) | fl);
+        if (P.iters[v] >= P.sc.niter) {
+          P.status[v] = (uint8_t)(CSD_STATUS_NITER | (flags & 0x70));
+        } else {
+          P.status[v] = (uint8_t)(kActive | flags);
+          P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
+        }
+      }
+      __syncwarp();
     }
   }
 }
@@ -1192,6 +1326,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: projection kind is 0, 1 or 2");
       g_proj_kind = value;
       break;
+    case 4:
+      if (value > 3) return fail(CSD_ERR_INVALID, "csd_set_launch_config: solve kind is 0, 1, 2 or 3");
+      g_solve_kind = value;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -1246,6 +1384,8 @@ struct csd_state {
   double* fp64 = nullptr;
   int blocks = 0, warps = 0;
   size_t smem = 0;
+  int gwarps[2] = {0, 0};     // grouped solve kernel, 16 / 8 lanes per voxel (0: unavailable)
+  size_t gsmem[2] = {0, 0};
   int proj_blocks = 0;
   size_t proj_smem = 0;
   long long passes = 0, projected = 0, solved = 0;  // work counters since the last set()
@@ -1276,7 +1416,28 @@ int state_shape(csd_state* st) {
   st->blocks = ls.blocks;
   st->warps = ls.warps;
   st->smem = ls.smem;
-  CUDA_TRY(cudaMalloc(&st->fp64, (size_t)ls.blocks * ls.warps * Dims<N>::WSZ * sizeof(double)));
+  int maxw = ls.warps;
+  if constexpr (N <= 45) {
+    int dev = 0, smem_max = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t hbytes = (size_t)htab_bytes<N>(st->sh->h.nhr, false);
+    const size_t wb[2] = {(size_t)GroupWSLayout<N, 2>::WARP, (size_t)GroupWSLayout<N, 4>::WARP};
+    const int cap[2] = {GroupSolveThreads<16>::value / 32, GroupSolveThreads<8>::value / 32};
+    for (int i = 0; i < 2; ++i) {
+      if (hbytes + wb[i] > (size_t)smem_max) continue;
+      st->gwarps[i] = (int)std::min<size_t>(cap[i], ((size_t)smem_max - hbytes) / wb[i]);
+      st->gsmem[i] = hbytes + wb[i] * st->gwarps[i];
+      maxw = std::max(maxw, st->gwarps[i]);
+    }
+    if (st->gwarps[0])
+      CUDA_TRY(cudaFuncSetAttribute(csd_solve_group_kernel<N, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)st->gsmem[0]));
+    if (st->gwarps[1])
+      CUDA_TRY(cudaFuncSetAttribute(csd_solve_group_kernel<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)st->gsmem[1]));
+  }
+  CUDA_TRY(cudaMalloc(&st->fp64, (size_t)ls.blocks * maxw * Dims<N>::WSZ * sizeof(double)));
   CUDA_TRY(cudaFuncSetAttribute(csd_solve_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem));
   int dev = 0, smem_max = 0, nsm = 0;
   CUDA_TRY(cudaGetDevice(&dev));
@@ -1358,6 +1519,21 @@ int state_project_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
 }
 template <int N>
 int state_solve_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  const int kind = g_solve_kind ? g_solve_kind : kSolveDefault;
+  if constexpr (N <= 45) {
+    const int gi = kind == 2 ? 0 : kind == 3 ? 1 : -1;
+    if (gi >= 0 && st->gwarps[gi] > 0) {
+      const int vpw = gi == 0 ? 2 : 4;  // voxels per warp
+      const int gw = st->gwarps[gi];
+      const int need = (int)std::min<long long>(st->blocks, (P.n_in + (long long)gw * vpw - 1) / ((long long)gw * vpw));
+      if (gi == 0)
+        csd_solve_group_kernel<N, 16><<<std::max(need, 1), gw * 32, st->gsmem[0], s>>>(P);
+      else
+        csd_solve_group_kernel<N, 8><<<std::max(need, 1), gw * 32, st->gsmem[1], s>>>(P);
+      CUDA_TRY(cudaGetLastError());
+      return 0;
+    }
+  }
   const int warps = g_tune_solve_warps > 0 ? std::min(st->warps, g_tune_solve_warps) : st->warps;
   const int need = (int)std::min<long long>(st->blocks, (P.n_in + warps - 1) / warps);
   csd_solve_kernel<N><<<std::max(need, 1), warps * 32, st->smem, s>>>(P);

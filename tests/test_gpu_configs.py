@@ -132,3 +132,45 @@ def test_tcgen05_projection_equals_mma_projection(cuda, hr_dirs, lmax):
             assert np.array_equal(outs[1][i][k], outs[2][i][k]), k
     assert outs[1][2]["projected"] == outs[2][2]["projected"]
     _check(outs[2][0], v, s, hr_dirs, lmax, n_sample=800)
+
+
+@pytest.mark.parametrize("lmax", [4, 6, 8])
+def test_grouped_solve_equals_warp_solve(cuda, lmax):
+    """The phased solve with 16 or 8 lanes per voxel (2 or 4 voxels per warp)
+    performs every voxel's arithmetic in the order of the warp-per-voxel
+    solve, so FODs, sets, statuses and iteration counts are identical --
+    plain and warm-started, and with every factorisation forced into the
+    FP64 fallback."""
+    import torch
+
+    from mrtrix3_b200 import autotune
+    v = synth.make_volume((40, 36, 20), 6, 60, (15.0, 40.0), lmax, 0.5, 90 + lmax)
+    d = torch.from_numpy(v.dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    s = csd.make_shared(v.grad, synth.RESPONSE, lmax=lmax)
+    s64 = csd.Shared(v.grad)
+    s64.parse_cmdline_options(lmax=lmax)
+    s64.fp64_condition = 1.0
+    s64.set_response(synth.RESPONSE)
+    s64.init()
+    plain = csd.dwi2fod_csd(s, d, mask=m, want_negmask=True)
+    warm = plain["negmask"].clone()
+    warm[:, 0] ^= 0x9
+    outs = {}
+    try:
+        for kind in (1, 2, 3):
+            autotune.set_knob(autotune.KNOB_SOLVE_KIND, kind)
+            res = []
+            for sh, w in ((s, None), (s, warm), (s64, None)):
+                st = csd.State(sh, v.n_voxels)
+                st.run(d, mask=m, warm=w)
+                res.append(st.fod())
+                st.close()
+            outs[kind] = res
+    finally:
+        autotune.set_knob(autotune.KNOB_SOLVE_KIND, 0)
+    assert np.all(outs[1][2]["status"][v.mask.astype(bool)] & csd.STATUS_FP64)
+    for kind in (2, 3):
+        for a, b in zip(outs[1], outs[kind]):
+            for k in ("fod", "negmask", "status", "iterations"):
+                assert np.array_equal(a[k], b[k]), (kind, k)

@@ -216,8 +216,11 @@ int csd_mlp_logits(csd_mlp* m, const uint16_t* x, int64_t n, float* z_out);
  * per SM, 3 projection kernel of the phased method (1 mma.sync, 2 tcgen05
  * with the accumulators in tensor memory; up to 320 constraint directions),
  * 4 phased solve kernel (1 a warp per voxel, 2 / 3 groups of 16 / 8 lanes
- * per voxel, lmax <= 8); value 0 = built-in default.  Outputs do not depend
- * on them (bit for bit). */
+ * per voxel, lmax <= 8), 5 phased set kernel (1 a warp per voxel, 2 tiles
+ * of 64 voxels), 6 csd_mlp_predict kernels (1 one GEMM per layer, 2 the
+ * fused tcgen05 kernel; 66..80 -> 256 -> 256 -> <=320 networks); value 0 =
+ * built-in default.  Knobs 0-5 leave the outputs unchanged bit for bit;
+ * knob 6 changes the FP32 summation order of the logits. */
 int csd_set_launch_config(int which, int value);
 
 /* Thread-local description of the last failure. */

@@ -19,6 +19,7 @@
 
 #include "../../include/csd_b200.h"
 #include "csd_device.cuh"
+#include "umma.cuh"
 #include "shared_init.hpp"
 
 using namespace csdb200;
@@ -33,6 +34,7 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 namespace csdb200 {
+extern int g_mlp_infer_kind;  // mlp.cu
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace csdb200
 
@@ -52,6 +54,8 @@ static int g_tune_proj_blocks_per_sm = 0;
 static int g_proj_kind = 0;  // projection kernel: 0 default, 1 mma.sync, 2 tcgen05 (nhr <= 320)
 static int g_solve_kind = 0;  // phased solve kernel: 0 default, 1 warp per voxel, 2 / 3 groups of 16 / 8 lanes
 static constexpr int kSolveDefault = 1;
+static int g_set_kind = 0;    // phased set kernel: 0 default, 1 warp per voxel, 2 tiles of 64 voxels
+static constexpr int kSetDefault = 2;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
 
 
@@ -297,6 +301,163 @@ __global__ void __launch_bounds__(256) csd_state_set_kernel(const __grid_constan
   }
 }
 
+// set() over tiles of 64 voxels (csd.h:237-243 with dwi2fod.cpp:156-173):
+// the block stages the tile's selected, clamped DW samples and the scheme's
+// rconv^T / M tables in shared memory, then each thread forms F = rconv S
+// and b = M^T S for 4 voxels x ceil(N/16) coefficients in registers, with
+// the summation order of voxel_set (two accumulators over the samples in
+// steps of 4, the remainder on the first), so the results are the same bit
+// for bit.  Status, iteration counters and the active list follow
+// csd_state_set_kernel; the list is compacted with one atomic per warp.
+constexpr int kSetTile = 64;
+
+__host__ __device__ constexpr int set_tile_lds(int ndw) { return ((ndw + 3) & ~3) + 1; }
+
+__host__ __device__ constexpr size_t set_tile_smem(int ndw, int ninit, int n) {
+  return (size_t)ndw * (ninit + n) * 4 + (size_t)kSetTile * set_tile_lds(ndw) * 4 + kSetTile * 4;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) csd_state_set_tile_kernel(const __grid_constant__ StateParams P) {
+  constexpr int JC = (N + 15) / 16;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int ndw = P.sc.ndw, ninit = P.sc.ninit;
+  const int lds = set_tile_lds(ndw);
+  float* rT = reinterpret_cast<float*>(smem);  // [ndw][ninit]
+  float* Mt = rT + ndw * ninit;                 // [ndw][N]
+  float* S = Mt + ndw * N;                      // [kSetTile][lds]
+  int* flag = reinterpret_cast<int*>(S + kSetTile * lds);  // 0 ok, 1 masked, 3 non-finite
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < ndw * ninit; i += blockDim.x) rT[i] = __ldg(P.sc.rconvT + i);
+  for (int i = tid; i < ndw * N; i += blockDim.x) Mt[i] = __ldg(P.sc.M32 + i);
+  const int vg = tid >> 4, cg = tid & 15;
+  const int nd4 = ndw & ~3;
+  const long long ntiles = (P.n_in + kSetTile - 1) / kSetTile;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long v0 = tile * kSetTile;
+    __syncthreads();
+    // 1. samples: warp w stages voxels w, w + 8, ...
+    for (int r = warp; r < kSetTile; r += 8) {
+      const long long v = v0 + r;
+      int f = 1;
+      if (v < P.n_in && !(P.mask && !P.mask[v])) {
+        const float* d = P.dwi + v * P.vox_stride;
+        bool bad = false;
+        for (int t = lane; t < ndw; t += 32) {
+          const float x = __ldg(d + (long long)__ldg(P.sc.dwis + t) * P.vol_stride);
+          if (!isfinite(x)) bad = true;
+          S[r * lds + t] = x < 0.f ? 0.f : x;
+        }
+        f = __any_sync(0xffffffffu, bad) ? 3 : 0;
+      }
+      if (lane == 0) flag[r] = f;
+    }
+    __syncthreads();  // the flags are complete before anyone reads them (the vote's
+                      // predicate is evaluated before its own barrier)
+    // a tile with no voxel to solve (outside the mask) only writes zeros
+    const bool any = __syncthreads_or(tid < kSetTile && flag[tid] == 0);
+    // 2. F and b for voxels 4 vg .. 4 vg + 3, coefficients cg + 16 j
+    float f0[4][JC], f1[4][JC], b0[4][JC], b1[4][JC];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int j = 0; j < JC; ++j) f0[a][j] = f1[a][j] = b0[a][j] = b1[a][j] = 0.f;
+    const float* S0 = S + (4 * vg) * lds;
+    int t = any ? 0 : ndw;
+    for (; t < nd4; t += 4) {
+#pragma unroll
+      for (int tt = 0; tt < 4; ++tt) {
+        float sv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) sv[a] = S0[a * lds + t + tt];
+#pragma unroll
+        for (int j = 0; j < JC; ++j) {
+          const int c = cg + 16 * j;
+          if (c < N) {
+            const float m = Mt[(t + tt) * N + c];
+            const float r = c < ninit ? rT[(t + tt) * ninit + c] : 0.f;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+              if (tt & 1) {
+                if (c < ninit) f1[a][j] = fmaf(r, sv[a], f1[a][j]);
+                b1[a][j] = fmaf(m, sv[a], b1[a][j]);
+              } else {
+                if (c < ninit) f0[a][j] = fmaf(r, sv[a], f0[a][j]);
+                b0[a][j] = fmaf(m, sv[a], b0[a][j]);
+              }
+            }
+          }
+        }
+      }
+    }
+    for (; t < ndw; ++t) {
+      float sv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) sv[a] = S0[a * lds + t];
+#pragma unroll
+      for (int j = 0; j < JC; ++j) {
+        const int c = cg + 16 * j;
+        if (c < N) {
+          const float m = Mt[t * N + c];
+          const float r = c < ninit ? rT[t * ninit + c] : 0.f;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            if (c < ninit) f0[a][j] = fmaf(r, sv[a], f0[a][j]);
+            b0[a][j] = fmaf(m, sv[a], b0[a][j]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = 4 * vg + a;
+      const long long v = v0 + r;
+      if (v >= P.n_in) continue;
+      const bool ok = flag[r] == 0;
+      float* F = P.F + v * Dims<N>::HS;
+#pragma unroll
+      for (int j = 0; j < JC; ++j) {
+        const int c = cg + 16 * j;
+        if (c < N) {
+          F[c] = ok ? f0[a][j] + f1[a][j] : 0.f;
+          P.b[v * N + c] = ok ? (double)(b0[a][j] + b1[a][j]) : 0.0;
+        }
+      }
+      for (int c = N + cg; c < Dims<N>::HS; c += 16) F[c] = 0.f;
+    }
+    // 3. counters, sets and the active list
+    for (int i = tid; i < kSetTile * P.nw; i += blockDim.x) {
+      const long long v = v0 + i / P.nw;
+      if (v < P.n_in) {
+        P.old[v0 * P.nw + i] = 0u;
+        P.old2[v0 * P.nw + i] = 0u;
+      }
+    }
+    if (warp < kSetTile / 32) {
+      const int r = 32 * warp + lane;
+      const long long v = v0 + r;
+      bool act = false;
+      if (v < P.n_in) {
+        const int f = flag[r];
+        P.iters[v] = 0;
+        if (f) {
+          P.status[v] = (uint8_t)(f == 1 ? CSD_STATUS_MASKED : CSD_STATUS_NONFINITE);
+        } else if (P.sc.niter == 0) {
+          P.status[v] = CSD_STATUS_CONVERGED;
+        } else {
+          P.status[v] = kActive;
+          act = true;
+        }
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, act);
+      int base = 0;
+      if (lane == 0 && bal) base = atomicAdd(P.n_out, __popc(bal));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (act) P.act_out[base + __popc(bal & ((1u << lane) - 1u))] = (int)v;
+    }
+  }
+}
+
 // Projection pass: tiles of 64 active voxels.  Warp w computes rows
 // 16 (w & 3) .. +15 against half (w >> 2) of the directions with mma.sync
 // m16n8k16 (F hi/lo from shared memory as A, the direction table as B, both
@@ -429,35 +590,6 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
 
 constexpr int kTcRows = 128;          // voxels per tile (M)
 constexpr int kTcDirs = 320;          // directions (N, two instructions of 160)
-constexpr unsigned kTcWaitLimit = 1u << 26;
-
-__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);             // start address, bits [0,14)
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;         // leading (K-chunk) byte offset, bits [16,30)
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;         // stride (row-group) byte offset, bits [32,46)
-  d |= (uint64_t)1 << 46;                             // descriptor version 1 (sm_100)
-  return d;                                           // base offset 0, no swizzle (layout type 0)
-}
-
-// kind::f16 instruction descriptor: F16 A and B, F32 D, both K-major.
-__host__ __device__ constexpr uint32_t umma_idesc_f16(int M, int N) {
-  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (unsigned i = 0; i < kTcWaitLimit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity));
-    if (done) return true;
-  }
-  return false;
-}
 
 template <int N>
 __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_constant__ StateParams P) {
@@ -1330,6 +1462,14 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 3) return fail(CSD_ERR_INVALID, "csd_set_launch_config: solve kind is 0, 1, 2 or 3");
       g_solve_kind = value;
       break;
+    case 5:
+      if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: set kind is 0, 1 or 2");
+      g_set_kind = value;
+      break;
+    case 6:
+      if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: inference kind is 0, 1 or 2");
+      csdb200::g_mlp_infer_kind = value;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -1385,6 +1525,7 @@ struct csd_state {
   int blocks = 0, warps = 0;
   size_t smem = 0;
   int gwarps[2] = {0, 0};     // grouped solve kernel, 16 / 8 lanes per voxel (0: unavailable)
+  size_t set_smem = 0;        // tiled set kernel's shared memory (0: tables too large for it)
   size_t gsmem[2] = {0, 0};
   int proj_blocks = 0;
   size_t proj_smem = 0;
@@ -1451,6 +1592,13 @@ int state_shape(csd_state* st) {
   CUDA_TRY(cudaFuncSetAttribute(csd_project_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
   CUDA_TRY(cudaFuncSetAttribute(csd_state_set_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(8 * warp_ws_bytes<N>())));
+  {
+    const size_t ss = set_tile_smem(st->sh->h.ndw, st->sh->h.ninit, N);
+    if (ss <= (size_t)std::min(smem_max, 200 * 1024)) {
+      st->set_smem = ss;
+      CUDA_TRY(cudaFuncSetAttribute(csd_state_set_tile_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+    }
+  }
   return 0;
 }
 
@@ -1483,6 +1631,18 @@ StateParams state_params(const csd_state* st) {
 
 template <int N>
 int state_set_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  const int kind = g_set_kind ? g_set_kind : kSetDefault;
+  if (kind == 2 && st->set_smem > 0) {
+    int dev = 0, nsm = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const long long tiles = (P.n_in + kSetTile - 1) / kSetTile;
+    const int per_sm = std::max(1, (int)((228 * 1024) / (st->set_smem + 1024)));
+    const int blocks = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)nsm * std::min(per_sm, 8)));
+    csd_state_set_tile_kernel<N><<<blocks, 256, st->set_smem, s>>>(P);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+  }
   const int blocks = (int)std::min<long long>(4096, (P.n_in + 7) / 8);
   csd_state_set_kernel<N><<<std::max(blocks, 1), 256, 8 * warp_ws_bytes<N>(), s>>>(P);
   CUDA_TRY(cudaGetLastError());

@@ -23,9 +23,13 @@
 #include <vector>
 
 #include "../../include/csd_b200.h"
+#include "umma.cuh"
 
 namespace csdb200 {
 int set_error(int code, const std::string& msg);  // csd_solver.cu: feeds csd_last_error()
+// inference kernel of csd_mlp_predict: 0 default, 1 layer-by-layer GEMMs,
+// 2 fused tcgen05 (set through csd_set_launch_config)
+int g_mlp_infer_kind = 0;
 }
 
 namespace {
@@ -341,6 +345,360 @@ __global__ void mlp_pack_kernel(const float* z, long long rows, int n_out, int l
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused inference on the 5th-generation tensor cores (sm_100a): one CTA per
+// SM walks tiles of 128 voxels; per tile the normalised inputs are built in
+// shared memory, the three layers run as tcgen05.mma (M = 128, BF16 operands
+// from shared memory, FP32 accumulators in tensor memory: layer 1 in columns
+// [0,256), layer 2 in [256,512), the output layer in [0,320)), and 256
+// threads run the epilogues straight from tensor memory (bias + GELU back
+// into shared memory as the next layer's operand; bias + threshold into
+// negative-set bitmasks).  Nothing but the inputs and the bitmasks touches
+// HBM.  The weights stream through two shared-memory buffers as nine
+// pre-packed slabs (bulk copies completing on mbarriers), the next slab in
+// flight while the tensor core works on the current one.  Operands use the
+// canonical K-major, non-swizzled layout (8-row x 16-byte core matrices,
+// 8-row groups 128 B apart, K chunks of 8 a row-group count x 128 B apart).
+// Every wait is bounded; a time-out stops all threads together, drains the
+// copies and instructions in flight, frees the tensor memory and raises the
+// error flag.
+constexpr int kInfRows = 128;
+constexpr int kInfThreads = 512;
+constexpr int kInfIn = 80;     // padded input width
+constexpr int kInfHid = 256;
+constexpr int kInfOut = 320;   // padded output width (two N = 160 halves)
+constexpr uint32_t kSlabW1 = (kInfIn / 8) * (kInfHid / 8) * 128;  // K 80 x N 256
+constexpr uint32_t kSlabW2 = 8 * (kInfHid / 8) * 128;             // K 64 x N 256
+constexpr uint32_t kSlabW3 = 8 * (kInfOut / 8) * 128;             // K 64 x N 320
+constexpr int kSlabs = 9;                                          // W1, W2 x 4, W3 x 4
+constexpr uint32_t kPackedBytes = kSlabW1 + 4 * kSlabW2 + 4 * kSlabW3;
+__host__ __device__ constexpr uint32_t inf_slab_off(int j) {
+  return j == 0 ? 0u : j <= 4 ? kSlabW1 + (uint32_t)(j - 1) * kSlabW2 : kSlabW1 + 4 * kSlabW2 + (uint32_t)(j - 5) * kSlabW3;
+}
+__host__ __device__ constexpr uint32_t inf_slab_bytes(int j) { return j == 0 ? kSlabW1 : j <= 4 ? kSlabW2 : kSlabW3; }
+constexpr uint32_t kInfX = 0;                                   // [10 chunks][16 groups][8][8] bf16
+constexpr uint32_t kInfH = kInfX + (kInfIn / 8) * 2048;          // [32 chunks][16 groups][8][8] bf16
+constexpr int kInfBufs = 3;                                      // slab buffers (two copies ahead)
+constexpr uint32_t kInfW = kInfH + (kInfHid / 8) * 2048;         // slab buffers
+constexpr uint32_t kInfBar = kInfW + kInfBufs * kSlabW3;         // full[3], empty[3], layer, tmem slot
+constexpr uint32_t kInfVec = kInfBar + 64;                       // b1, b2, b3, mu, isd (fp32)
+constexpr uint32_t kInfSmem = kInfVec + (2 * kInfHid + kInfOut + 2 * kInfIn) * 4;
+
+// Rearranges the BF16 weights into the nine slabs in the core-matrix layout
+// (one thread per packed element); rows past n_out and columns past n_in
+// of the flat buffer become zero.
+__global__ void mlp_pack_tc_kernel(const bf16* w16, long long oW1, long long oW2, long long oW3, int ld_in, int H,
+                                   int n_out, bf16* packed) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kPackedBytes / 2) return;
+  const uint32_t byte = (uint32_t)i * 2;
+  int j = 0;
+  while (j + 1 < kSlabs && byte >= inf_slab_off(j + 1)) ++j;
+  const uint32_t local = (byte - inf_slab_off(j)) / 2;
+  const int nr = j == 0 ? kInfHid : j <= 4 ? kInfHid : kInfOut;  // rows (N) of the slab
+  const int e = local & 7, r = (local >> 3) & 7;
+  const int cg = local >> 6;                 // core-matrix index: kc * (nr / 8) + ng
+  const int kc = cg / (nr / 8), ng = cg - kc * (nr / 8);
+  const int n = ng * 8 + r;
+  const int k0 = j == 0 ? 0 : 64 * ((j - 1) & 3);
+  const int k = k0 + kc * 8 + e;
+  bf16 v = __float2bfloat16(0.f);
+  if (j == 0) {
+    if (k < ld_in) v = w16[oW1 + (long long)n * ld_in + k];
+  } else if (j <= 4) {
+    v = w16[oW2 + (long long)n * H + k];
+  } else if (n < n_out) {
+    v = w16[oW3 + (long long)n * H + k];
+  }
+  packed[i] = v;
+}
+
+struct InferArgs {
+  const float* dwi;
+  long long n, vs, ts;
+  const int* index;         // compacted voxel ids or NULL
+  const int* b0;
+  int n_b0, n_in, n_out, nw;
+  const float* mu;
+  const float* isd;
+  const bf16* packed;
+  const float* b1;
+  const float* b2;
+  const float* b3;
+  float thr;
+  uint32_t* out;
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_tc_kernel(const __grid_constant__ InferArgs a) {
+  using namespace csdb200;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row = 32 * (warp & 3) + lane;   // tensor-memory lane = tile row
+  const int qc = warp >> 2;                 // column quarter of the epilogues (4 warps per lane quarter)
+  // K chunks of the inputs and words of the output this thread builds: 10
+  // of each, split 2 / 3 / 2 / 3 over the quarters
+  const int ck0 = (10 * qc) >> 2, ck1 = (10 * (qc + 1)) >> 2;
+  const long long ntiles = (a.n + kInfRows - 1) / kInfRows;
+  if ((long long)blockIdx.x >= ntiles) return;
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const uint32_t sX = sbase + kInfX, sH = sbase + kInfH, sW = sbase + kInfW;
+  const uint32_t bar = sbase + kInfBar;
+  const uint32_t full0 = bar, empty0 = bar + 8 * kInfBufs, layer = bar + 16 * kInfBufs;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kInfBar + 16 * kInfBufs + 8);
+  if (tid == 0) {
+    for (int b = 0; b < 2 * kInfBufs + 1; ++b) mbar_init(bar + 8 * b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  if (warp == 0) tmem_alloc(sbase + kInfBar + 16 * kInfBufs + 8, 512);
+  // per-column vectors of the epilogues and the input normalisation
+  float* vb1 = reinterpret_cast<float*>(smem + kInfVec);
+  float* vb2 = vb1 + kInfHid;
+  float* vb3 = vb2 + kInfHid;
+  float* vmu = vb3 + kInfOut;
+  float* visd = vmu + kInfIn;
+  for (int i = tid; i < kInfHid; i += kInfThreads) {
+    vb1[i] = a.b1[i];
+    vb2[i] = a.b2[i];
+  }
+  for (int i = tid; i < kInfOut; i += kInfThreads) vb3[i] = i < a.n_out ? a.b3[i] : 0.f;
+  for (int i = tid; i < kInfIn; i += kInfThreads) {
+    vmu[i] = i < a.n_in ? a.mu[i] : 0.f;
+    visd[i] = i < a.n_in ? a.isd[i] : 0.f;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t id256 = umma_idesc_f16(128, 256, true), id160 = umma_idesc_f16(128, 160, true);
+  const long long my_tiles = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
+  const long long total_slabs = my_tiles * kSlabs;
+  // producer / issuer state (thread 0)
+  long long g_load = 0;   // slabs whose copy was issued
+  long long g_landed = 0; // slabs whose copy was waited for
+  bool ok0 = true;
+  // slab g lives in buffer g % kInfBufs; the k-th use of a buffer completes
+  // its barriers' phase k, of parity k & 1
+  auto issue_load = [&](long long g) {
+    const int j = (int)(g % kSlabs), b = (int)(g % kInfBufs);
+    mbar_arrive_expect_tx(full0 + 8 * b, inf_slab_bytes(j));
+    bulk_copy_g2s(sW + b * kSlabW3, reinterpret_cast<const unsigned char*>(a.packed) + inf_slab_off(j),
+                  inf_slab_bytes(j), full0 + 8 * b);
+    g_load = g + 1;
+  };
+  // consume slab g: wait for it, issue its instructions, free its buffer on
+  // completion, then refill the buffer of slab g - 1 with slab g + 2
+  auto consume = [&](long long g, auto&& issue) {
+    const int b = (int)(g % kInfBufs);
+    if (ok0 && !mbar_wait(full0 + 8 * b, (uint32_t)((g / kInfBufs) & 1))) ok0 = false;
+    if (ok0) {
+      g_landed = g + 1;
+      tc_fence_after();
+      issue(sW + b * kSlabW3);
+      umma_commit(empty0 + 8 * b);
+    }
+    if (ok0 && g + 2 < total_slabs) {
+      if (g >= 1 && !mbar_wait(empty0 + 8 * ((g - 1) % kInfBufs), (uint32_t)(((g - 1) / kInfBufs) & 1))) ok0 = false;
+      if (ok0) issue_load(g + 2);
+    }
+  };
+  if (tid == 0) {
+    issue_load(0);
+    if (total_slabs > 1) issue_load(1);
+  }
+  uint32_t lphase = 0;
+  long long g = 0;  // next slab to consume
+  bool failed = false;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long e0 = tile * kInfRows;
+    // ---- inputs: x = (S / mean(S_b0) - mu) * isd.  The tile's raw rows are
+    // staged (coalesced, one warp per row) in the H area, free until the
+    // first layer's epilogue; each thread then builds columns
+    // chunks [ck0, ck1) of its row.
+    {
+      constexpr int kLdS = kInfIn + 1;  // odd row stride: rows in distinct banks
+      float* Sraw = reinterpret_cast<float*>(smem + kInfH);
+      for (int rr = warp; rr < kInfRows; rr += kInfThreads / 32) {
+        const long long r = e0 + rr;
+        if (r < a.n) {
+          const float* d = a.dwi + (a.index ? (long long)a.index[r] : r) * a.vs;
+          for (int t = lane; t < a.n_in; t += 32) Sraw[rr * kLdS + t] = d[(long long)t * a.ts];
+        }
+      }
+      __syncthreads();
+      const long long r = e0 + row;
+      float xs[24];
+#pragma unroll
+      for (int c = 0; c < 24; ++c) xs[c] = 0.f;
+      if (r < a.n) {
+        const float* sr = Sraw + row * kLdS;
+        // mean of the b=0 samples, summed in the order of mlp_inputs_kernel
+        float part[32];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) part[l] = 0.f;
+        for (int i = 0; i < a.n_b0; ++i) {
+          const float x0 = sr[a.b0[i]];
+          part[i & 31] += isfinite(x0) ? x0 : 0.f;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1)
+#pragma unroll
+          for (int l = 0; l < o; ++l) part[l] = part[l] + part[l + o];
+        const float s0 = a.n_b0 ? part[0] / a.n_b0 : 1.f;
+        const float inv = s0 > 1e-6f ? 1.f / s0 : 0.f;
+#pragma unroll
+        for (int c = 0; c < 24; ++c) {
+          const int t = 8 * ck0 + c;
+          if (t < 8 * ck1 && t < a.n_in) {
+            float sv = sr[t];
+            sv = isfinite(sv) ? sv : 0.f;
+            xs[c] = (sv * inv - vmu[t]) * visd[t];
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int kc = ck0 + q;
+        if (kc >= ck1) break;
+        uint4 u;
+        u.x = pack_bf16x2(xs[8 * q], xs[8 * q + 1]);
+        u.y = pack_bf16x2(xs[8 * q + 2], xs[8 * q + 3]);
+        u.z = pack_bf16x2(xs[8 * q + 4], xs[8 * q + 5]);
+        u.w = pack_bf16x2(xs[8 * q + 6], xs[8 * q + 7]);
+        *reinterpret_cast<uint4*>(smem + kInfX + kc * 2048 + (row >> 3) * 128 + (row & 7) * 16) = u;
+      }
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    // ---- three layers: instructions (thread 0), then the epilogue (all)
+#pragma unroll 1
+    for (int L = 0; L < 3; ++L) {
+      if (tid == 0) {
+        tc_fence_after();
+        const int nsl = L == 0 ? 1 : 4;
+        for (int sl = 0; sl < nsl; ++sl, ++g) {
+          if (L == 0) {
+            consume(g, [&](uint32_t wb) {
+#pragma unroll
+              for (int ks = 0; ks < kInfIn / 16; ++ks)
+                umma_f16_ss(tmem, umma_smem_desc(sX + 2 * ks * 2048, 2048, 128),
+                            umma_smem_desc(wb + 2 * ks * (kInfHid / 8) * 128, (kInfHid / 8) * 128, 128), id256,
+                            ks > 0);
+            });
+          } else if (L == 1) {
+            consume(g, [&](uint32_t wb) {
+#pragma unroll
+              for (int ks = 0; ks < 4; ++ks)
+                umma_f16_ss(tmem + 256, umma_smem_desc(sH + (8 * sl + 2 * ks) * 2048, 2048, 128),
+                            umma_smem_desc(wb + 2 * ks * (kInfHid / 8) * 128, (kInfHid / 8) * 128, 128), id256,
+                            (sl | ks) != 0);
+            });
+          } else {
+            consume(g, [&](uint32_t wb) {
+#pragma unroll
+              for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                  umma_f16_ss(tmem + 160 * h, umma_smem_desc(sH + (8 * sl + 2 * ks) * 2048, 2048, 128),
+                              umma_smem_desc(wb + 2 * ks * (kInfOut / 8) * 128 + h * (160 / 8) * 128,
+                                             (kInfOut / 8) * 128, 128),
+                              id160, (sl | ks) != 0);
+            });
+          }
+        }
+        umma_commit(layer);  // also when stopping: lets the other threads reach the vote
+      }
+      bool okw = (tid != 0 || ok0) && mbar_wait(layer, lphase);
+      lphase ^= 1u;
+      if (!__syncthreads_and(okw)) {
+        failed = true;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t lane_base = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+      if (L < 2) {
+        // bias + GELU -> BF16 -> the next layer's A operand (columns [64 qc, 64 qc + 64))
+        const float* bias = L == 0 ? vb1 : vb2;
+#pragma unroll 1
+        for (int jj = 0; jj < 4; jj += 2) {
+          uint32_t v2[2][16];
+          tmem_ld16(lane_base + (uint32_t)(256 * L + 64 * qc + 16 * jj), v2[0]);
+          tmem_ld16(lane_base + (uint32_t)(256 * L + 64 * qc + 16 * jj + 16), v2[1]);
+          tmem_ld_wait();
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+          const int c0 = 64 * qc + 16 * (jj + u);
+          const uint32_t* v = v2[u];
+          float y[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) y[e] = gelu(__uint_as_float(v[e]) + bias[c0 + e]);
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            uint4 u;
+            u.x = pack_bf16x2(y[8 * q], y[8 * q + 1]);
+            u.y = pack_bf16x2(y[8 * q + 2], y[8 * q + 3]);
+            u.z = pack_bf16x2(y[8 * q + 4], y[8 * q + 5]);
+            u.w = pack_bf16x2(y[8 * q + 6], y[8 * q + 7]);
+            const int kc = c0 / 8 + q;
+            *reinterpret_cast<uint4*>(smem + kInfH + kc * 2048 + (row >> 3) * 128 + (row & 7) * 16) = u;
+          }
+          }
+        }
+        fence_async_smem();
+      } else {
+        // bias + threshold -> negative-set bits (words [ck0, ck1) of the 10)
+        const long long r = e0 + row;
+        uint32_t words[3] = {0u, 0u, 0u};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          if (ck0 + k >= ck1) break;  // uniform over the warp
+          const int c0 = 32 * (ck0 + k);
+          uint32_t v2[2][16];
+          tmem_ld16(lane_base + (uint32_t)c0, v2[0]);
+          tmem_ld16(lane_base + (uint32_t)(c0 + 16), v2[1]);
+          tmem_ld_wait();
+#pragma unroll
+          for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              const int c = c0 + 16 * u + e;
+              if (c < a.n_out && __uint_as_float(v2[u][e]) + vb3[c] > a.thr) words[k] |= 1u << (c & 31);
+            }
+        }
+        if (r < a.n) {
+          const long long o = (a.index ? (long long)a.index[r] : r) * a.nw;
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+            if (ck0 + k < ck1 && ck0 + k < a.nw) a.out[o + ck0 + k] = words[k];
+        }
+      }
+      tc_fence_before();
+      __syncthreads();
+    }
+    if (failed) break;
+  }
+  if (failed && tid == 0) {
+    // drain: the copies still in flight, the pending layer commit, then a
+    // fresh commit that completes once every issued instruction is done
+    for (long long q = g_landed; q < g_load; ++q)
+      mbar_wait(full0 + 8 * (q % kInfBufs), (uint32_t)((q / kInfBufs) & 1));
+    mbar_wait(layer, lphase ^ 1u);
+    umma_commit(layer);
+    mbar_wait(layer, lphase);
+    atomicExch(a.err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
 // index[] = positions of the voxels with mask != 0 (order not preserved)
 __global__ void mlp_compact_kernel(const uint8_t* mask, long long n, int* index, int* count) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -384,6 +742,10 @@ struct csd_mlp {
   float* loss = nullptr;
   int* idx = nullptr;          // compacted voxel index list for masked prediction
   long long idx_cap = 0;
+  // fused inference: weights packed into slabs, refreshed when they change
+  bf16* wpack = nullptr;
+  long long wver = 1, pver = 0;
+  int* err = nullptr;          // device time-out flag of the fused kernel
 };
 
 static int mlp_reserve(csd_mlp* m, long long rows) {
@@ -467,7 +829,7 @@ extern "C" int csd_mlp_create(int n_in, int n_hidden, int n_out, uint64_t seed, 
 extern "C" void csd_mlp_destroy(csd_mlp* m) {
   if (!m) return;
   void* ps[] = {m->w, m->g, m->am, m->av, m->w16, m->b0, m->mu, m->isd, m->x, m->a1, m->h1, m->a2, m->h2,
-                m->dz, m->da2, m->da1, m->z, m->loss, m->idx};
+                m->dz, m->da2, m->da1, m->z, m->loss, m->idx, m->wpack, m->err};
   for (void* p : ps) cudaFree(p);
   delete m;
 }
@@ -486,12 +848,16 @@ extern "C" int csd_mlp_set_params(csd_mlp* m, const float* in, int64_t n) {
   mlp_to_bf16_kernel<<<(unsigned)((n + 255) / 256), 256>>>(m->w, n, m->w16);
   MLP_TRY(cudaGetLastError());
   MLP_TRY(cudaDeviceSynchronize());
+  ++m->wver;
   return CSD_OK;
 }
 
 extern "C" int csd_mlp_set_inputs(csd_mlp* m, const int* b0_index, int n_b0, const float* mean, const float* stdev) {
   if (!m || n_b0 < 0 || (n_b0 && !b0_index) || !mean || !stdev)
     return mfail(CSD_ERR_INVALID, "csd_mlp_set_inputs: invalid argument");
+  for (int i = 0; i < n_b0; ++i)
+    if (b0_index[i] < 0 || b0_index[i] >= m->n_in)
+      return mfail(CSD_ERR_INVALID, "csd_mlp_set_inputs: b=0 volume index out of range");
   std::vector<float> mu(m->ld_in, 0.f), isd(m->ld_in, 0.f);
   for (int t = 0; t < m->n_in; ++t) {
     mu[t] = mean[t];
@@ -636,6 +1002,7 @@ extern "C" int csd_mlp_train_epoch(csd_mlp* m, const uint16_t* x, const uint32_t
                                                                            b1, b2, eps, c1, c2, weight_decay, m->w16);
     MLP_TRY(cudaGetLastError());
   }
+  ++m->wver;
   if (mean_loss) {
     float l = 0.f;
     MLP_TRY(cudaMemcpyAsync(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -648,6 +1015,54 @@ extern "C" int csd_mlp_train_epoch(csd_mlp* m, const uint16_t* x, const uint32_t
 // Predicted first negative sets for n voxels of a DWI volume (device).  With
 // a mask, only the voxels inside it go through the network (the others get
 // an empty set).
+// csd_mlp_predict's fused path over n rows (compacted through index when
+// it is not NULL); synchronises the stream to read the time-out flag.
+static int mlp_predict_fused(csd_mlp* m, const float* dwi, long long n, long long vs, long long ts, const int* index,
+                             float thr, uint32_t* negmask, cudaStream_t st) {
+  if (!m->wpack) MLP_TRY(cudaMalloc(&m->wpack, kPackedBytes));
+  if (!m->err) MLP_TRY(cudaMalloc(&m->err, sizeof(int)));
+  if (m->pver != m->wver) {
+    mlp_pack_tc_kernel<<<(kPackedBytes / 2 + 255) / 256, 256, 0, st>>>(m->w16, m->oW1, m->oW2, m->oW3, m->ld_in,
+                                                                       m->n_hid, m->n_out, m->wpack);
+    MLP_TRY(cudaGetLastError());
+    m->pver = m->wver;
+  }
+  if (n <= 0) return CSD_OK;
+  int dev = 0, nsm = 0;
+  MLP_TRY(cudaGetDevice(&dev));
+  MLP_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  MLP_TRY(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmem));
+  MLP_TRY(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+  InferArgs a{};
+  a.dwi = dwi;
+  a.n = n;
+  a.vs = vs;
+  a.ts = ts;
+  a.index = index;
+  a.b0 = m->b0;
+  a.n_b0 = (int)m->b0_host.size();
+  a.n_in = m->n_in;
+  a.n_out = m->n_out;
+  a.nw = m->nw;
+  a.mu = m->mu;
+  a.isd = m->isd;
+  a.packed = m->wpack;
+  a.b1 = m->w + m->ob1;
+  a.b2 = m->w + m->ob2;
+  a.b3 = m->w + m->ob3;
+  a.thr = thr;
+  a.out = negmask;
+  a.err = m->err;
+  const long long tiles = (n + kInfRows - 1) / kInfRows;
+  mlp_infer_tc_kernel<<<(unsigned)std::min<long long>(tiles, nsm), kInfThreads, kInfSmem, st>>>(a);
+  MLP_TRY(cudaGetLastError());
+  int err = 0;
+  MLP_TRY(cudaMemcpyAsync(&err, m->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MLP_TRY(cudaStreamSynchronize(st));
+  if (err) return mfail(CSD_ERR_TIMEOUT, "csd_mlp_predict: a bounded wait on the tensor cores timed out");
+  return CSD_OK;
+}
+
 extern "C" int csd_mlp_predict(csd_mlp* m, const float* dwi, int64_t n_voxels, int64_t voxel_stride,
                                int64_t volume_stride, const uint8_t* mask, float logit_threshold, uint32_t* negmask,
                                void* stream) {
@@ -655,8 +1070,10 @@ extern "C" int csd_mlp_predict(csd_mlp* m, const float* dwi, int64_t n_voxels, i
     return mfail(CSD_ERR_INVALID, "csd_mlp_predict: invalid argument (inputs not configured?)");
   if (n_voxels == 0) return CSD_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int kind = csdb200::g_mlp_infer_kind ? csdb200::g_mlp_infer_kind : 2;
+  const bool fused = kind == 2 && m->n_hid == kInfHid && m->ld_in <= kInfIn && m->ld_out <= kInfOut;
   const long long chunk = 1 << 18;
-  int rc = mlp_reserve(m, std::min<long long>(chunk, n_voxels));
+  int rc = fused ? 0 : mlp_reserve(m, std::min<long long>(chunk, n_voxels));
   if (rc) return rc;
   const int* index = nullptr;
   long long n = n_voxels;
@@ -678,6 +1095,7 @@ extern "C" int csd_mlp_predict(csd_mlp* m, const float* dwi, int64_t n_voxels, i
     index = m->idx;
     n = cnt;
   }
+  if (fused) return mlp_predict_fused(m, dwi, n, voxel_stride, volume_stride, index, logit_threshold, negmask, st);
   for (long long a = 0; a < n; a += chunk) {
     const long long c = std::min<long long>(chunk, n - a);
     if (index) {

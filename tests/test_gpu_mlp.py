@@ -92,3 +92,51 @@ def test_warm_start_gains_over_plain(cuda, hr_dirs):
     match = np.mean(np.all(warm["negmask"].cpu().numpy()[idx].view(np.uint32) == ref["negmask"], axis=1))
     assert np.percentile(rel, 99) <= 1e-4
     assert match >= 0.995
+
+
+def test_fused_inference_matches_layer_gemms(cuda):
+    """csd_mlp_predict's fused tcgen05 kernel (inputs, three layers and the
+    bit packing in one launch, accumulators in tensor memory) gives the sets
+    of the one-GEMM-per-layer path: the logits differ only in FP32 summation
+    order, so at most a few bits in 10^4 flip, masked-out voxels get empty
+    sets, ragged last tiles are handled, and new weights are re-packed."""
+    import os
+
+    import torch
+
+    from mrtrix3_b200 import autotune
+    from mrtrix3_b200.warmstart import WarmStartNet
+    here = os.path.dirname(os.path.abspath(__file__))
+    net = WarmStartNet.load(os.path.join(here, "..", "mrtrix3_b200", "data", "warmstart_c5.npz"))
+    grad = synth.config5_scheme()
+    rng = np.random.default_rng(12)
+    sig = synth.voxel_signals(rng, grad, 20_001, (15.0, 40.0))
+    d = torch.from_numpy(sig).cuda()
+    mask = torch.from_numpy((rng.random(len(sig)) < 0.5).astype(np.uint8)).cuda()
+
+    def both(mk):
+        out = {}
+        try:
+            for kind in (1, 2):
+                autotune.set_knob(autotune.KNOB_INFER, kind)
+                out[kind] = net.predict(d, mask=mk).cpu().numpy().view(np.uint32)
+        finally:
+            autotune.set_knob(autotune.KNOB_INFER, 0)
+        return out
+
+    for mk in (None, mask):
+        o = both(mk)
+        diff = np.unpackbits((o[1] ^ o[2]).view(np.uint8)).sum()
+        assert diff <= 2e-4 * o[1].size * 32, diff
+        if mk is not None:
+            off = mask.cpu().numpy() == 0
+            assert not o[2][off].any()
+        assert o[2][:, -1].max() < (1 << (300 - 288))  # no bits past the 300 directions
+        assert np.unpackbits(o[2].view(np.uint8)).mean() > 0.2  # the sets are not empty
+    # new weights must reach the fused kernel
+    p = net.get_params()
+    net.set_params(p * np.float32(0.5))
+    o = both(None)
+    diff = np.unpackbits((o[1] ^ o[2]).view(np.uint8)).sum()
+    assert diff <= 2e-4 * o[1].size * 32, diff
+    net.set_params(p)

@@ -302,3 +302,37 @@ def test_full_size_config2_properties(cuda, hr_dirs):
     ref = O.OracleShared(v.grad, synth.RESPONSE, hr_dirs).solve(v.dwi[idx])
     sub = {k: out[k][idx] for k in ("fod", "negmask", "iterations", "status")}
     check_parity(sub, ref)
+
+
+@pytest.mark.parametrize("lmax", [6, 8, 10])
+def test_tiled_set_equals_warp_set(cuda, lmax):
+    """The phased set() over tiles of 64 voxels sums in the order of the
+    warp-per-voxel set(), so a whole phased run -- with masked voxels,
+    non-finite samples, negative samples and a ragged last tile -- ends on
+    the same FODs, sets, statuses and iteration counts bit for bit."""
+    import torch
+
+    from mrtrix3_b200 import autotune
+    ndw, nb0 = (60, 6) if lmax <= 8 else (90, 8)
+    v = synth.make_volume((37, 29, 7), nb0, ndw, (15.0, 40.0), lmax, 0.6, 300 + lmax)
+    dwi = v.dwi.copy()
+    rng = np.random.default_rng(lmax)
+    dwi[rng.choice(len(dwi), 20, replace=False), 3] = np.nan
+    dwi[rng.choice(len(dwi), 20, replace=False), 7] = -50.0
+    s = csd.make_shared(v.grad, synth.RESPONSE, lmax=lmax)
+    d = torch.from_numpy(dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    outs = []
+    try:
+        for kind in (1, 2, 2, 2):  # the tiled kernel three times: its result may not depend on timing
+            autotune.set_knob(autotune.KNOB_SET_KIND, kind)
+            st = csd.State(s, v.n_voxels)
+            st.run(d, mask=m)
+            outs.append(st.fod())
+            st.close()
+    finally:
+        autotune.set_knob(autotune.KNOB_SET_KIND, 0)
+    for o in outs[1:]:
+        for k in ("fod", "negmask", "status", "iterations"):
+            assert np.array_equal(outs[0][k], o[k]), k
+    assert (outs[1]["status"] == csd.STATUS_NONFINITE).sum() > 0

@@ -50,6 +50,21 @@ constexpr int kMaxVolumesPerLaunch = 48;
 
 // Packed lower-triangular storage with every row padded to a multiple of 4
 // floats so rows can be read as float4: row i starts at packoff(i).
+// Loop shapes of the FP32 factorisation and back substitution: the column
+// blocks are unrolled, so every block's row offsets, trip counts and edge
+// tests are compile-time constants (the integer and branch instructions
+// around the arithmetic were half of the solve kernel's instructions); the
+// factorisation's inner dot-product loop stays rolled to bound code size
+// and registers.  Overridable for experiments.
+#ifndef CSD_CHOL_CB_PRAGMA
+#define CSD_CHOL_CB_PRAGMA _Pragma("unroll")
+#endif
+#ifndef CSD_CHOL_KK_PRAGMA
+#define CSD_CHOL_KK_PRAGMA _Pragma("unroll 1")
+#endif
+#ifndef CSD_BACK_CB_PRAGMA
+#define CSD_BACK_CB_PRAGMA _Pragma("unroll")
+#endif
 __host__ __device__ constexpr int packoff(int i) {
   return 4 * (i + 2 * (i >> 2) * ((i >> 2) - 1) + (i & 3) * (i >> 2));
 }
@@ -77,7 +92,13 @@ struct Dims {
   // threads per block of the persistent kernel (bounds the register budget)
   static constexpr int THREADS = N <= 45 ? 512 : (N <= 66 ? 384 : 192);
   // threads per block of the phased solve kernel (no FP32 table, split assembly)
+  // (its register budget is 65536 / SOLVE_THREADS; CSD_SOLVE_THREADS45
+  // overrides it for N <= 45)
+#ifdef CSD_SOLVE_THREADS45
+  static constexpr int SOLVE_THREADS = N <= 45 ? CSD_SOLVE_THREADS45 : THREADS;
+#else
   static constexpr int SOLVE_THREADS = N <= 45 ? 640 : THREADS;
+#endif
 };
 
 // Everything a voxel of one image needs, by device pointer.
@@ -493,7 +514,7 @@ __device__ bool cholesky_packed_f32(float* A, float* rdiag, int lane, float& dmi
   dmin = 3.0e38f;
   dmax = 0.f;
   constexpr int NB = (N + 3) / 4;
-#pragma unroll 1
+CSD_CHOL_CB_PRAGMA
   for (int cb = 0; cb < NB; ++cb) {
     const int j0 = 4 * cb;
     const float* Lj0 = A + packoff(j0);
@@ -510,6 +531,7 @@ __device__ bool cholesky_packed_f32(float* A, float* rdiag, int lane, float& dmi
         const float* Li = A + packoff(i);
         const float4 w4 = *reinterpret_cast<const float4*>(Li + j0);
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
+CSD_CHOL_KK_PRAGMA
         for (int kk = 0; kk < j0; kk += 4) {
           const float4 x = *reinterpret_cast<const float4*>(Li + kk);
           const float4 y0 = *reinterpret_cast<const float4*>(Lj0 + kk);
@@ -690,7 +712,7 @@ __device__ __forceinline__ void chol_subst_f32(const float* L, const float* rdia
 template <int N>
 __device__ __forceinline__ void chol_back_f32(const float* L, const float* rdiag, float* x, int lane) {
   constexpr int NB = (N + 3) / 4;
-#pragma unroll 1
+CSD_BACK_CB_PRAGMA
   for (int cb = NB - 1; cb >= 0; --cb) {
     const int j0 = 4 * cb;
     float y[4];
@@ -758,7 +780,7 @@ __device__ bool cholesky_group_f32(float* A, float* rdiag, int s, float& dmin, f
   dmax = 0.f;
   bool okall = true;
   constexpr int NB = (N + 3) / 4;
-#pragma unroll 1
+CSD_CHOL_CB_PRAGMA
   for (int cb = 0; cb < NB; ++cb) {
     const int j0 = 4 * cb;
     const float* Lj0 = A + packoff(j0);
@@ -779,6 +801,7 @@ __device__ bool cholesky_group_f32(float* A, float* rdiag, int s, float& dmin, f
 #pragma unroll
       for (int c = 0; c < 8; ++c) acc[q][c] = 0.f;
     }
+    CSD_CHOL_KK_PRAGMA
     for (int kk = 0; kk < j0; kk += 4) {
       const float4 y0 = *reinterpret_cast<const float4*>(Lj0 + kk);
       const float4 y1 = *reinterpret_cast<const float4*>(Lj1 + kk);
@@ -879,7 +902,7 @@ template <int N, int G>
 __device__ __forceinline__ void chol_back_group_f32(const float* L, const float* rdiag, float* x, int s) {
   constexpr int CQG = GroupDims<N, G>::CQG;
   constexpr int NB = (N + 3) / 4;
-#pragma unroll 1
+CSD_BACK_CB_PRAGMA
   for (int cb = NB - 1; cb >= 0; --cb) {
     const int j0 = 4 * cb;
     float y[4];

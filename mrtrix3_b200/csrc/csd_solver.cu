@@ -787,6 +787,7 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
 #else
   long long* tacc = nullptr;
 #endif
+  unsigned long long sum_k = 0, n_solved = 0;  // work counters, added once per warp
   for (int e = gw; e < n_in; e += nwt) {
     CSD_T0(tl);
     const long long v = P.act_in[e];
@@ -798,10 +799,8 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
     __syncwarp();
     const uint8_t st = P.status[v];
     const int k = mask_to_list(bits, P.nw, w.neg, lane);
-    if (lane == 0 && P.stats) {
-      atomicAdd(P.stats, (unsigned long long)k);
-      atomicAdd(P.stats + 1, 1ULL);
-    }
+    sum_k += (unsigned long long)k;
+    ++n_solved;
     CSD_T1(tacc, kPhList, tl);
     const int fl =
         assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot, tacc) & 0x70;
@@ -821,6 +820,10 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
       }
     }
     CSD_T1(tacc, kPhSet, tw);
+  }
+  if (lane == 0 && P.stats && n_solved) {
+    atomicAdd(P.stats, sum_k);
+    atomicAdd(P.stats + 1, n_solved);
   }
 #ifdef CSD_PHASE_TIMERS
   tacc[kPhTotal] = clock64() - tstart;
@@ -862,6 +865,7 @@ __global__ void __launch_bounds__(GroupSolveThreads<G>::value, 1)
   double* slot64 = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
   const WarpWS<N> mine = group_slot_ws<N, V>(base, grp);
   const long long stride = (long long)gridDim.x * nwarps * V;
+  unsigned long long sum_k = 0, n_solved = 0;  // work counters, added once per warp
   for (long long e0 = ((long long)blockIdx.x * nwarps + warp) * V; e0 < n_in; e0 += stride) {
     // 1. assembly of each voxel's system (+ its right-hand side as row N)
 #pragma unroll 1
@@ -876,10 +880,8 @@ __global__ void __launch_bounds__(GroupSolveThreads<G>::value, 1)
       for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.newm[v * P.nw + p] : 0u;
       __syncwarp();
       const int k = mask_to_list(bits, P.nw, w.neg, lane);
-      if (lane == 0 && P.stats) {
-        atomicAdd(P.stats, (unsigned long long)k);
-        atomicAdd(P.stats + 1, 1ULL);
-      }
+      sum_k += (unsigned long long)k;
+      ++n_solved;
       assemble<N, true>(H, P.sc.MtMp, k, w, lane);
       float* bN = w.W + packoff(N);
       for (int c = lane; c < packoff(N + 1) - packoff(N); c += 32) bN[c] = c < N ? (float)w.b[c] : 0.f;
@@ -942,6 +944,10 @@ __global__ void __launch_bounds__(GroupSolveThreads<G>::value, 1)
       }
       __syncwarp();
     }
+  }
+  if (lane == 0 && P.stats && n_solved) {
+    atomicAdd(P.stats, sum_k);
+    atomicAdd(P.stats + 1, n_solved);
   }
 }
 

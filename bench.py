@@ -46,7 +46,12 @@ WEIGHTS = os.path.join(ROOT, "mrtrix3_b200", "data", "warmstart_c5.npz")
 # DRAM bytes per launch of csd_solve_kernel<45> from ncu on a 262,144-voxel
 # case (profiles/csd_solve_kernel_45.md), scaled to this workload's voxels
 # solved per launch; None until measured.
-SOLVE_DRAM_BYTES_PER_VOXEL = None
+# DRAM bytes (read + write) per solved voxel of csd_solve_kernel<45>, from
+# one ncu capture of its first launch on a 64^3 warm-started volume (262,144
+# solves: 126.4 MB read + 47.1 MB written); see
+# profiles/csd_solve_kernel_45.md.  The per-launch traffic reported below
+# scales it by the voxels each launch solves.
+SOLVE_DRAM_BYTES_PER_VOXEL = (126.449152e6 + 47.146496e6) / 262144
 
 
 def load_peaks():

@@ -134,6 +134,29 @@ def voxel_signals(rng: np.random.Generator, grad: np.ndarray, nv: int, snr, s0: 
     return out
 
 
+def _signals_block(args):
+    grad, n, snr, seed, index = args
+    return voxel_signals(np.random.default_rng([seed, index]), grad, n, snr)
+
+
+def voxel_signals_parallel(grad: np.ndarray, nv: int, snr, seed: int, workers: int = 0,
+                           block: int = 1 << 20) -> np.ndarray:
+    """voxel_signals over blocks of ``block`` voxels, block i drawn from the
+    generator seeded [seed, i]: the result depends on (seed, nv, block) only,
+    not on the number of worker processes (``workers`` <= 1: this process).
+    Workers are spawned, so this is safe to call after CUDA is initialised."""
+    jobs = [(grad, min(block, nv - a), snr, seed, i) for i, a in enumerate(range(0, nv, block))]
+    if workers <= 1 or len(jobs) == 1:
+        parts = [_signals_block(j) for j in jobs]
+    else:
+        import concurrent.futures
+        import multiprocessing
+        with concurrent.futures.ProcessPoolExecutor(max_workers=workers,
+                                                    mp_context=multiprocessing.get_context("spawn")) as ex:
+            parts = list(ex.map(_signals_block, jobs))
+    return np.concatenate(parts) if parts else np.empty((0, grad.shape[0]), np.float32)
+
+
 def ellipsoid_mask(dims, fraction: float) -> np.ndarray:
     """uint8 [z][y][x] centred ellipsoid covering about ``fraction`` of the box."""
     nx, ny, nz = dims

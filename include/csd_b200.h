@@ -210,6 +210,22 @@ int csd_mlp_gradients(csd_mlp* m, const uint16_t* x, const uint32_t* negmask, in
                       float* loss_out);
 int csd_mlp_logits(csd_mlp* m, const uint16_t* x, int64_t n, float* z_out);
 
+/* ---- sh2peaks (cmd/sh2peaks.cpp:99-303, core/math/SH.h:515-650) on device
+ *      buffers: for each voxel's SH coefficients (float, [n][voxel_stride],
+ *      lmax even, 2..12) a Newton search from every seed direction (n_seeds
+ *      [azimuth elevation] pairs in radians, at most 256; the reference's 60
+ *      are mrtrix3_b200/data/sh2peaks_seeds_60.txt), duplicates within
+ *      |cos| > 0.99 of an earlier peak and peaks below `threshold` dropped;
+ *      output [n][3 npeaks] amplitude-scaled directions, NaN-padded (npeaks
+ *      at most 16).  With n_directions = npeaks unit vectors (-direction), or
+ *      a per-voxel [n][3 npeaks] peaks_in (-peaks), each output is the peak
+ *      of largest |cos| with its target; else the largest peaks.  Masked,
+ *      non-finite and all-isotropic voxels give NaN (check_input).  Returns
+ *      without synchronising. */
+int csd_sh2peaks(const float* sh, int64_t n_voxels, int64_t voxel_stride, int lmax, const uint8_t* mask,
+                 const float* seeds_azel, int n_seeds, int npeaks, float threshold, const float* directions,
+                 int n_directions, const float* peaks_in, float* peaks_out, void* stream);
+
 /* Launch-shape knobs (process-wide), chosen by the project's autotuner
  * (mrtrix3_b200/autotune.py): which = 0 warps per block of the persistent
  * kernel, 1 warps per block of the phased solve kernel, 2 projection blocks

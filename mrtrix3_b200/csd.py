@@ -14,6 +14,7 @@ if the library or a GPU is missing, these calls raise.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -31,7 +32,7 @@ EXPORTED = [
     "csd_shared_dwis", "csd_shared_matrix", "csd_solve", "csd_dwi2fod_host", "csd_state_create",
     "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_run",
     "csd_state_fod",
-    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_last_error",
+    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_last_error",
 ]
 
 
@@ -84,6 +85,8 @@ def lib():
         L.csd_state_warm.argtypes = [vp, vp, vp]
         L.csd_state_iterate.argtypes = [vp, ctypes.POINTER(i64), vp]
         L.csd_state_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(i64), vp]
+        L.csd_sh2peaks.argtypes = [vp, i64, i64, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                   vp, ctypes.c_int, vp, vp, vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]
         L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_dwi2fod_host_phased.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
@@ -328,6 +331,41 @@ def dwi2fod_csd_host_phased(shared: Shared, dwi, mask=None, net=None, fod=None):
                                         ctypes.c_void_p(_ptr(fod)), ctypes.c_void_p(status.ctypes.data),
                                         ctypes.c_void_p(iters.ctypes.data)))
     return {"fod": fod, "status": status, "iterations": iters}
+
+
+def default_peak_seeds() -> np.ndarray:
+    """sh2peaks' built-in 60 seed directions [azimuth elevation] (data/sh2peaks_seeds_60.txt)."""
+    return np.loadtxt(os.path.join(HERE, "data", "sh2peaks_seeds_60.txt"), dtype=np.float32, ndmin=2)
+
+
+def sh2peaks(sh, lmax: int | None = None, mask=None, seeds=None, npeaks: int = 3, threshold: float = -np.inf,
+             directions=None, peaks=None, stream=None):
+    """Peaks of each row of ``sh`` (float32 CUDA tensor [n][nSH]): a CUDA
+    tensor [n][3 npeaks] of amplitude-scaled directions, NaN-padded
+    (csd_sh2peaks; cmd/sh2peaks.cpp).  ``directions``: unit vectors
+    [npeaks][3] to match (-direction); ``peaks``: per-voxel [n][3 npeaks]
+    targets (-peaks)."""
+    import torch
+    n, nsh = sh.shape
+    if lmax is None:
+        lmax = int(round((math.sqrt(8 * nsh + 1) - 3) / 2))
+    if seeds is None:
+        seeds = default_peak_seeds()
+    seeds = np.ascontiguousarray(seeds, np.float32)
+    dirs = None if directions is None else np.ascontiguousarray(directions, np.float32)
+    if dirs is not None:
+        npeaks = len(dirs)
+    if peaks is not None:
+        npeaks = peaks.shape[1] // 3
+    out = torch.empty((n, 3 * npeaks), dtype=torch.float32, device=sh.device)
+    check(lib().csd_sh2peaks(ctypes.c_void_p(sh.data_ptr()), n, sh.stride(0), lmax,
+                             ctypes.c_void_p(_ptr(mask)) if mask is not None else None,
+                             ctypes.c_void_p(seeds.ctypes.data), len(seeds), npeaks, float(threshold),
+                             ctypes.c_void_p(dirs.ctypes.data) if dirs is not None else None,
+                             0 if dirs is None else len(dirs),
+                             ctypes.c_void_p(peaks.data_ptr()) if peaks is not None else None,
+                             ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(_stream_ptr(stream))))
+    return out
 
 
 def negmask_to_bool(negmask, n_hr: int) -> np.ndarray:

@@ -39,26 +39,36 @@ struct PeakArgs {
   float threshold;
   float seeds[kPkMaxSeeds][3];      // unit vectors (Direction(phi, theta) of sh2peaks.cpp:104)
   float targets[kPkMaxPeaks][3];    // global targets (-direction), normalised
+  float plm_k[13];                  // Legendre starting-value constants K_m, m <= 12
 };
 
+// Starting values of the Legendre recursion: P_mm = K_m sin^m(el), with
+// K_m = sqrt(1 / 4 pi) sqrt((2m+1) prod_{j<=m} (2j-1) / 2j), the closed form
+// of legendre.h:65-68's helper product (which the reference evaluates per
+// call); K_m is computed once on the host in double and passed in.
+static void plm_start_table(float* k, int lmax) {
+  for (int m = 0; m <= lmax; ++m) {
+    double h = 1.0;
+    for (int j = 1; j <= m; ++j) h *= (2.0 * j - 1.0) / (2.0 * j);
+    k[m] = (float)(0.282094791773878 * std::sqrt((2.0 * m + 1.0) * h));
+  }
+  k[0] = 0.282094791773878f;
+}
+
 // Normalised associated Legendre functions of order m at cos / sin of the
-// elevation (core/math/legendre.h:125-153): the m > 0 starting value in
-// double, as the reference's helper product is, the recursion in float.
+// elevation (core/math/legendre.h:125-153), in float.
 template <int L>
-__device__ __forceinline__ void plm_sph(float* a, int m, float x, float s) {
+__device__ __forceinline__ void plm_sph(float* a, int m, float x, float s, const float* kk) {
   const float s2 = s * s;
   if (m && s2 == 0.f) {
     for (int n = m; n <= L; ++n) a[n] = 0.f;
     return;
   }
-  float v = 0.282094791773878f;
+  float v = kk[0];
   if (m) {
-    double h = 1.0, mm = 2.0 * m;
-    while (mm >= 1.0) {
-      h *= (double)s2 * (mm - 1.0) / mm;
-      mm -= 2.0;
-    }
-    v = (float)((double)v * sqrt((double)(2 * m + 1) * h));
+    float sp = 1.f;
+    for (int j = 0; j < m; ++j) sp *= s;
+    v = kk[m] * fabsf(sp);
   }
   if (m & 1) v = -v;
   a[m] = v;
@@ -75,17 +85,19 @@ __device__ __forceinline__ void plm_sph(float* a, int m, float x, float s) {
 __device__ __forceinline__ int shi(int l, int m) { return l * (l + 1) / 2 + m; }
 __device__ __forceinline__ int mpos(int l, int m) { return l * l / 4 + m; }
 
-// SH::derivatives (SH.h:569-650)
+// SH::derivatives (SH.h:569-650), at the elevation / azimuth given by
+// their cosines and sines; cos(m az), sin(m az) by the angle-addition
+// recurrence instead of one sincos per order.
 template <int L>
-__device__ void sh_derivatives(const float* sh, float el, float az, float& amp, float& d_el, float& d_az,
-                               float& d2_el, float& d2_elaz, float& d2_az) {
-  const float sel = sinf(el), cel = cosf(el);
+__device__ void sh_derivatives(const float* sh, float cel, float sel, float caz1, float saz1, float& amp,
+                               float& d_el, float& d_az, float& d2_el, float& d2_elaz, float& d2_az,
+                               const float* kk) {
   const bool atpole = sel < 1e-4f;
   float AL[(L / 2 + 1) * (L / 2 + 1)];
   float buf[L + 1];
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
-    plm_sph<L>(buf, m, cel, sel);
+    plm_sph<L>(buf, m, cel, sel, kk);
 #pragma unroll
     for (int l = (m & 1) ? m + 1 : m; l <= L; l += 2) AL[mpos(l, m)] = buf[l];
   }
@@ -98,10 +110,12 @@ __device__ void sh_derivatives(const float* sh, float el, float az, float& amp, 
     d_el += v * sqrtf((float)(l * (l + 1))) * AL[mpos(l, 1)];
     d2_el += v * (sqrtf((float)(l * (l + 1) * (l - 1) * (l + 2))) * AL[mpos(l, 2)] - l * (l + 1) * AL[mpos(l, 0)]) / 2.f;
   }
+  float cm = 1.f, sm = 0.f;
 #pragma unroll
   for (int m = 1; m <= L; ++m) {
-    float sm, cm;
-    sincosf(m * az, &sm, &cm);
+    const float c2 = cm * caz1 - sm * saz1;
+    sm = sm * caz1 + cm * saz1;
+    cm = c2;
     const float caz = 1.41421356237309505f * cm, saz = 1.41421356237309505f * sm;
 #pragma unroll
     for (int l = (m & 1) ? m + 1 : m; l <= L; l += 2) {
@@ -139,12 +153,15 @@ __device__ void sh_derivatives(const float* sh, float el, float az, float& amp, 
 // SH::get_peak (SH.h:515-560): returns the amplitude (NaN if no convergence
 // in 50 steps) and leaves the peak direction in v.
 template <int L>
-__device__ float get_peak(const float* sh, float& v0, float& v1, float& v2) {
+__device__ float get_peak(const float* sh, float& v0, float& v1, float& v2, const float* kk) {
   for (int i = 0; i < 50; ++i) {
-    const float az = atan2f(v1, v0);
-    const float el = atan2f(hypotf(v0, v1), v2);
+    // az = atan2(v1, v0), el = atan2(hypot(v0, v1), v2) of the unit vector
+    // v, through their cosines and sines (atan2(0, 0) = 0 at the poles)
+    const float h = hypotf(v0, v1);
+    const float ce = v2, se = h;
+    const float ca = h > 0.f ? v0 / h : (v0 < 0.f ? -1.f : 1.f), sa = h > 0.f ? v1 / h : 0.f;
     float amp, dSH_del, dSH_daz, d2_del2, d2_deldaz, d2_daz2;
-    sh_derivatives<L>(sh, el, az, amp, dSH_del, dSH_daz, d2_del2, d2_deldaz, d2_daz2);
+    sh_derivatives<L>(sh, ce, se, ca, sa, amp, dSH_del, dSH_daz, d2_del2, d2_deldaz, d2_daz2, kk);
     float del = sqrtf(dSH_del * dSH_del + dSH_daz * dSH_daz);
     float daz = 0.f;
     if (del != 0.f) {
@@ -158,9 +175,6 @@ __device__ float get_peak(const float* sh, float& v0, float& v1, float& v2) {
     if (dt > 0.2f) dt = 0.2f;
     del *= dt;
     daz *= dt;
-    float sa, ca, se, ce;
-    sincosf(az, &sa, &ca);
-    sincosf(el, &se, &ce);
     v0 += del * ca * ce - daz * sa;
     v1 += del * sa * ce + daz * ca;
     v2 -= del * se;
@@ -172,6 +186,104 @@ __device__ float get_peak(const float* sh, float& v0, float& v1, float& v2) {
   }
   v0 = v1 = v2 = nanf("");
   return nanf("");
+}
+
+// Warp-parallel selection for up to 64 seeds, with the outcome of the
+// sequential walk below: every lane finds, for its seeds s, the earlier
+// seeds j whose peaks lie within |cos| > 0.99 (a 64-bit mask per seed);
+// the kept set is then built in seed order from those masks (a peak is
+// kept when it is finite, at or above the threshold and no kept earlier
+// peak is in its mask), and the outputs are picked by warp-wide arg-max
+// reductions (largest amplitude, or largest |cos| with each target; ties
+// go to the earlier seed, as the walk's strict comparisons do).
+__device__ __forceinline__ void warp_argmax(float& val, int& idx) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const float v2 = __shfl_xor_sync(0xffffffffu, val, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (v2 > val || (v2 == val && i2 < idx && i2 >= 0) || idx < 0) {
+      if (i2 >= 0) {
+        val = v2;
+        idx = i2;
+      }
+    }
+  }
+}
+
+__device__ void select_peaks_warp(const PeakArgs& a, const float* res, long long v, int lane, float* o) {
+  uint64_t dup[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int s = lane + 32 * q;
+    uint64_t d = 0;
+    if (s < a.n_seeds && isfinite(res[4 * s])) {
+      const float x = res[4 * s + 1], y = res[4 * s + 2], z = res[4 * s + 3];
+      for (int j = 0; j < s; ++j)
+        if (isfinite(res[4 * j]) && fabsf(x * res[4 * j + 1] + y * res[4 * j + 2] + z * res[4 * j + 3]) > 0.99f)
+          d |= 1ull << j;
+    }
+    dup[q] = d;
+  }
+  uint64_t K = 0;
+  for (int s = 0; s < a.n_seeds; ++s) {
+    const uint64_t mine = (s >> 5) ? dup[1] : dup[0];
+    const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)mine, s & 31);
+    const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(mine >> 32), s & 31);
+    const uint64_t d = ((uint64_t)hi << 32) | lo;
+    const float p = res[4 * s];
+    if (isfinite(p) && !(d & K) && p >= a.threshold) K |= 1ull << s;
+  }
+  const int nk = __popcll(K);
+  const int nout = nk < a.npeaks ? nk : a.npeaks;
+  const bool targets = a.n_targets || a.vtargets;
+  uint64_t used = 0;
+  int pick[kPkMaxPeaks];
+  for (int i = 0; i < nout; ++i) {
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    if (targets) {
+      if (a.vtargets) {
+        const float* t = a.vtargets + v * 3 * a.npeaks + 3 * i;
+        const float nrm = sqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        t0 = t[0] / nrm;
+        t1 = t[1] / nrm;
+        t2 = t[2] / nrm;
+      } else {
+        t0 = a.targets[i][0];
+        t1 = a.targets[i][1];
+        t2 = a.targets[i][2];
+      }
+    }
+    float best = -1.f;
+    int bi = -1;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int s = lane + 32 * q;
+      if (s < a.n_seeds && ((K >> s) & 1ull) && (targets || !((used >> s) & 1ull))) {
+        const float* r = res + 4 * s;
+        const float val = targets ? fabsf(t0 * r[1] + t1 * r[2] + t2 * r[3]) : r[0];
+        if (targets && !(val > 0.f)) continue;
+        if (bi < 0 || val > best) {
+          best = val;
+          bi = s;
+        }
+      }
+    }
+    warp_argmax(best, bi);
+    pick[i] = bi;
+    if (bi >= 0) used |= 1ull << bi;
+  }
+  if (lane == 0) {
+    for (int i = 0; i < a.npeaks; ++i) {
+      if (i < nout && pick[i] >= 0) {
+        const float* q = res + 4 * pick[i];
+        o[3 * i] = q[0] * q[1];
+        o[3 * i + 1] = q[0] * q[2];
+        o[3 * i + 2] = q[0] * q[3];
+      } else {
+        o[3 * i] = o[3 * i + 1] = o[3 * i + 2] = nanf("");
+      }
+    }
+  }
 }
 
 template <int L>
@@ -202,14 +314,16 @@ __global__ void __launch_bounds__(32 * kPkWarps) sh2peaks_kernel(const __grid_co
     __syncwarp();
     for (int s = lane; s < a.n_seeds; s += 32) {
       float v0 = a.seeds[s][0], v1 = a.seeds[s][1], v2 = a.seeds[s][2];
-      const float amp = get_peak<L>(sh, v0, v1, v2);
+      const float amp = get_peak<L>(sh, v0, v1, v2, a.plm_k);
       res[4 * s] = amp;
       res[4 * s + 1] = v0;
       res[4 * s + 2] = v1;
       res[4 * s + 3] = v2;
     }
     __syncwarp();
-    if (lane == 0) {
+    if (a.n_seeds <= 64) {
+      select_peaks_warp(a, res, v, lane, o);
+    } else if (lane == 0) {
       // peaks in seed order, duplicates (|cos| > 0.99 with a kept one) and
       // those below the threshold dropped; kept indices go back into res
       int kept[kPkMaxSeeds];
@@ -318,6 +432,7 @@ extern "C" int csd_sh2peaks(const float* sh, int64_t n_voxels, int64_t voxel_str
   a.npeaks = npeaks;
   a.n_targets = n_directions;
   a.threshold = threshold;
+  plm_start_table(a.plm_k, 12);
   for (int i = 0; i < n_seeds; ++i) {
     // Direction(phi, theta) (sh2peaks.cpp:104), in float as the reference
     const float phi = seeds_azel[2 * i], theta = seeds_azel[2 * i + 1];

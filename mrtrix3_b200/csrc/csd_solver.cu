@@ -55,6 +55,7 @@ static int g_proj_kind = 0;  // projection kernel: 0 default, 1 mma.sync, 2 tcge
 static int g_solve_kind = 0;  // phased solve kernel: 0 default, 1 warp per voxel, 2 / 3 groups of 16 / 8 lanes
 static constexpr int kSolveDefault = 1;
 static int g_set_kind = 0;    // phased set kernel: 0 default, 1 warp per voxel, 2 tiles of 64 voxels
+static int g_fast_cycles = 1; // phased method: jump periodic two-cycles to their last call (knob 7)
 static constexpr int kSetDefault = 2;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
 
@@ -255,6 +256,8 @@ struct StateParams {
   const uint32_t* warm; // [cap][nw] or NULL
   uint8_t* status;      // [cap]
   uint16_t* iters;      // [cap] iterate() calls made
+  uint16_t* cyc;        // [cap] calls made when the voxel was first seen cycling
+  int fast_cycles;      // jump periodic two-cycles to their last call
   const int* act_in;    // [n_in] voxel ids
   const int* n_in_dev;  // device count of act_in (overrides n_in when set)
   int* act_out;         // compacted output list
@@ -458,6 +461,29 @@ __global__ void __launch_bounds__(256) csd_state_set_tile_kernel(const __grid_co
   }
 }
 
+// Two-cycles (csd.h:246-253 iterated to niter).  A voxel whose new set
+// equals the one before last (`back`) is flagged cycling (st |= kCycling,
+// cyc = calls made) and from then on solves with one refinement step.  Once
+// both sets of the cycle have been solved with refinement (two calls after
+// the flag), the iteration is exactly periodic: a solve is a deterministic
+// function of its set, so F and the sets alternate until niter.  The voxel
+// then jumps to its last call: solve now with the set the niter-th call
+// would use (this one if niter - calls is even, else the last solved one,
+// in `old`) and finish with niter calls -- the same FOD, set and count as
+// running every call.  Returns 0 (no jump), 1 (jump, this set), 2 (jump,
+// the last solved set); updates st / cyc when the cycle is first seen.
+__device__ __forceinline__ int cycle_jump(const StateParams& P, long long v, int it, bool warm, bool back,
+                                          uint8_t& st) {
+  if (warm || it < 2 || !back) return 0;
+  if (!(st & kCycling)) {
+    st |= kCycling;
+    if (P.cyc) P.cyc[v] = (uint16_t)it;
+    return 0;
+  }
+  if (!P.fast_cycles || !P.cyc || it < (int)P.cyc[v] + 2 || it + 1 >= P.sc.niter) return 0;
+  return ((P.sc.niter - (it + 1)) & 1) ? 2 : 1;
+}
+
 // Projection pass: tiles of 64 active voxels.  Warp w computes rows
 // 16 (w & 3) .. +15 against half (w >> 2) of the directions with mma.sync
 // m16n8k16 (F hi/lo from shared memory as A, the direction table as B, both
@@ -558,14 +584,14 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
       const bool same = __all_sync(0xffffffffu, lane >= P.nw || bits == P.old[v * P.nw + lane]);
       const bool back = __all_sync(0xffffffffu, lane >= P.nw || bits == P.old2[v * P.nw + lane]);
       const bool conv = !warm && it > 0 && same;
-      if (!conv && lane < P.nw) P.newm[v * P.nw + lane] = bits;
+      uint8_t st = P.status[v];
+      const int ff = cycle_jump(P, v, it, warm, back, st);
+      if (!conv && lane < P.nw) P.newm[v * P.nw + lane] = ff == 2 ? P.old[v * P.nw + lane] : bits;
       if (lane == 0) {
-        P.iters[v] = (uint16_t)(it + 1);
-        uint8_t st = P.status[v];
+        P.iters[v] = (uint16_t)(ff ? P.sc.niter : it + 1);
         if (conv) {
           P.status[v] = (uint8_t)(CSD_STATUS_CONVERGED | (st & 0x70));
         } else {
-          if (!warm && it >= 2 && back) st |= kCycling;
           P.status[v] = st;
           P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
         }
@@ -749,13 +775,14 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
         back = back && b == P.old2[v * P.nw + w];
       }
       const bool conv = !warm && it > 0 && same;
-      P.iters[v] = (uint16_t)(it + 1);
       uint8_t st = P.status[v];
+      const int ff = cycle_jump(P, v, it, warm, back, st);
+      P.iters[v] = (uint16_t)(ff ? P.sc.niter : it + 1);
       if (conv) {
         P.status[v] = (uint8_t)(CSD_STATUS_CONVERGED | (st & 0x70));
       } else {
-        for (int w = 0; w < P.nw; ++w) P.newm[v * P.nw + w] = words[w < kTcDirs / 32 ? w : 0];
-        if (!warm && it >= 2 && back) st |= kCycling;
+        for (int w = 0; w < P.nw; ++w)
+          P.newm[v * P.nw + w] = ff == 2 ? P.old[v * P.nw + w] : words[w < kTcDirs / 32 ? w : 0];
         P.status[v] = st;
         P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
       }
@@ -1476,6 +1503,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: inference kind is 0, 1 or 2");
       csdb200::g_mlp_infer_kind = value;
       break;
+    case 7:
+      if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: cycle jumping is 0 (default), 1 on or 2 off");
+      g_fast_cycles = value == 2 ? 0 : 1;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -1523,6 +1554,7 @@ struct csd_state {
   uint32_t* warm = nullptr;
   uint8_t* status = nullptr;
   uint16_t* iters = nullptr;
+  uint16_t* cyc = nullptr;
   int* act[2] = {nullptr, nullptr};
   int* slist = nullptr;
   int* counter = nullptr;
@@ -1628,6 +1660,8 @@ StateParams state_params(const csd_state* st) {
   P.use_warm = st->use_warm;
   P.status = st->status;
   P.iters = st->iters;
+  P.cyc = st->cyc;
+  P.fast_cycles = g_fast_cycles;
   P.n_out = st->counter;
   P.err = st->counter + 1;
   P.stats = st->stats;
@@ -1749,6 +1783,7 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->slist, (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->status, (size_t)capacity));
   CUDA_TRY(cudaMalloc(&st->iters, (size_t)capacity * sizeof(uint16_t)));
+  CUDA_TRY(cudaMalloc(&st->cyc, (size_t)capacity * sizeof(uint16_t)));
   CUDA_TRY(cudaMalloc(&st->act[0], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->act[1], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->counter, 2 * sizeof(int)));
@@ -1774,6 +1809,7 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->slist);
   cudaFree(st->status);
   cudaFree(st->iters);
+  cudaFree(st->cyc);
   cudaFree(st->act[0]);
   cudaFree(st->act[1]);
   cudaFree(st->counter);

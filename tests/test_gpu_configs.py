@@ -174,3 +174,41 @@ def test_grouped_solve_equals_warp_solve(cuda, lmax):
         for a, b in zip(outs[1], outs[kind]):
             for k in ("fod", "negmask", "status", "iterations"):
                 assert np.array_equal(a[k], b[k]), (kind, k)
+
+
+def test_cycle_jump_equals_full_iteration(cuda):
+    """The 140x140x96 benchmark volume (6 b=0 + 60 DW, lmax 8) holds voxels
+    that two-cycle until niter.  Jumping such a cycle to its last call once
+    it is exactly periodic gives the FODs, sets, statuses and iteration
+    counts of running every call -- plain and warm-started -- while the
+    number of passes drops."""
+    import os
+
+    import torch
+
+    from mrtrix3_b200 import autotune
+    from mrtrix3_b200.warmstart import WarmStartNet
+    v = synth.config5(seed=5)
+    s = csd.make_shared(v.grad, synth.RESPONSE)
+    d = torch.from_numpy(v.dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    here = os.path.dirname(os.path.abspath(__file__))
+    net = WarmStartNet.load(os.path.join(here, "..", "mrtrix3_b200", "data", "warmstart_c5.npz"))
+    warm = net.predict(d, mask=m)
+    st = csd.State(s, v.n_voxels)
+    outs, passes = {}, {}
+    try:
+        for knob in (2, 1):
+            autotune.set_knob(autotune.KNOB_CYCLE_JUMP, knob)
+            for name, w in (("plain", None), ("warm", warm)):
+                st.run(d, mask=m, warm=w)
+                outs[(knob, name)] = st.fod()
+                passes[(knob, name)] = st.stats()["passes"]
+    finally:
+        autotune.set_knob(autotune.KNOB_CYCLE_JUMP, 0)
+    for name in ("plain", "warm"):
+        a, b = outs[(2, name)], outs[(1, name)]
+        for k in ("fod", "negmask", "status", "iterations"):
+            assert np.array_equal(a[k], b[k]), (name, k)
+        assert ((a["status"] & 0x0F) == csd.STATUS_NITER).sum() >= 1  # the case is exercised
+        assert passes[(1, name)] < passes[(2, name)]

@@ -235,8 +235,9 @@ int csd_sh2peaks(const float* sh, int64_t n_voxels, int64_t voxel_stride, int lm
  * per voxel, lmax <= 8), 5 phased set kernel (1 a warp per voxel, 2 tiles
  * of 64 voxels), 6 csd_mlp_predict kernels (1 one GEMM per layer, 2 the
  * fused tcgen05 kernel; 66..80 -> 256 -> 256 -> <=320 networks); value 0 =
- * built-in default, 7 the phased method's jump of exactly periodic
- * two-cycles to their last call (1 on, the default; 2 off).  Knobs 0-5 and 7
+ * built-in default, 7 the jump of exactly periodic two-cycles to their
+ * last call, in the phased method and the persistent kernel (1 on, the
+ * default; 2 off).  Knobs 0-5 and 7
  * leave the outputs unchanged bit for bit; knob 6 changes the FP32
  * summation order of the logits. */
 int csd_set_launch_config(int which, int value);

@@ -130,6 +130,7 @@ struct VolumeDesc {
 
 struct SolveParams {
   int n_vol, nhr, nw, refine;
+  int fast_cycles;               // jump exactly periodic two-cycles to their last call
   float cond_thr;
   long long total;
   unsigned long long* queue;     // work counter, zeroed before launch

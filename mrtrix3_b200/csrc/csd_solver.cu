@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -78,7 +79,8 @@ __device__ __forceinline__ bool same_set(const uint32_t* a, const uint32_t* b, i
 // cmd/dwi2fod.cpp:128-147, with CSD::set/iterate, csd.h:237-269).
 template <int N>
 __device__ void solve_voxel(const VolumeDesc& V, long long v, const HTab<N>& H, int nw, float cond_thr,
-                            int refine, const WarpWS<N>& w, int lane, double* slot, long long* tacc = nullptr) {
+                            int refine, bool fast_cycles, const WarpWS<N>& w, int lane, double* slot,
+                            long long* tacc = nullptr) {
   const Scheme& sc = V.sc;
   const int nhr = H.nhr;
   const bool masked = V.mask && !V.mask[v];
@@ -107,6 +109,7 @@ __device__ void solve_voxel(const VolumeDesc& V, long long v, const HTab<N>& H, 
   for (int attempt = 0; attempt < 2; ++attempt) {
     bool have_old = false, fp32_factor = false, refined = false;
     int k = 0, rmode = refine;
+    int mode_since = 0;  // every solve from this iteration on used the current rmode
     conv = false;
 #pragma unroll 1
     for (it = 0; it < sc.niter; ++it) {
@@ -121,7 +124,10 @@ __device__ void solve_voxel(const VolumeDesc& V, long long v, const HTab<N>& H, 
         CSD_T1(tacc, kPhProject, tp);
         // a set that returns after one step is an FP32 two-cycle around a
         // sign change: refine every remaining solve of this voxel
-        if ((rmode == 2 || rmode == 3) && it >= 2 && same_set<N>(bits, old2, nw)) rmode = 1;
+        if ((rmode == 2 || rmode == 3) && it >= 2 && same_set<N>(bits, old2, nw)) {
+          rmode = 1;
+          mode_since = it;
+        }
         if (have_old && same_set<N>(bits, old, nw)) {  // csd.h:252-253
           if (rmode == 2 && fp32_factor && !refined) {
             // refine the fixed point once, then check that it still is one
@@ -140,11 +146,24 @@ __device__ void solve_voxel(const VolumeDesc& V, long long v, const HTab<N>& H, 
             // refinement moved the set: this voxel sits close to a sign
             // change, so refine after every remaining solve
             rmode = 1;
+            mode_since = it;
           } else {
             conv = true;
             ++it;
             break;
           }
+        } else if (fast_cycles && it >= 2 && it >= mode_since + 2 && it + 1 < sc.niter &&
+                   same_set<N>(bits, old2, nw)) {
+          // a two-cycle whose both sets were last solved with the current
+          // refinement mode repeats exactly (a solve depends only on its
+          // set): go to the last call, whose set is this one if an even
+          // number of calls remain after it, else the last solved one
+          if ((sc.niter - (it + 1)) & 1) {
+#pragma unroll
+            for (int p = 0; p < kMaxWords; ++p)
+              if (p < nw) bits[p] = old[p];
+          }
+          it = sc.niter - 1;
         }
       }
       CSD_T0(tl);
@@ -211,7 +230,8 @@ __global__ void __launch_bounds__(Dims<N>::THREADS, 1) csd_persistent_kernel(con
     int vi = 0;
     while (vi + 1 < P.n_vol && (long long)g >= P.vol[vi + 1].first) ++vi;
     const VolumeDesc& V = P.vol[vi];
-    solve_voxel<N>(V, (long long)g - V.first, H, P.nw, P.cond_thr, P.refine, w, lane, slot, tacc);
+    solve_voxel<N>(V, (long long)g - V.first, H, P.nw, P.cond_thr, P.refine, P.fast_cycles != 0, w, lane, slot,
+                   tacc);
   }
 #ifdef CSD_PHASE_TIMERS
   tacc[kPhTotal] = clock64() - tstart;
@@ -1005,6 +1025,7 @@ __global__ void csd_state_fod_kernel(const float* F, const uint8_t* status, cons
 
 struct csd_shared {
   HostShared h;
+  uint64_t id = 0;               // unique per object: caches key on it, not on the address
   double cond_thr = 1e6;
   int refine = 3;
   int device = -1;               // device holding the tables (-1: not uploaded yet)
@@ -1081,6 +1102,8 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
     n_hr = (int)(hr.size() / 2);
   }
   std::unique_ptr<csd_shared> s(new csd_shared);
+  static std::atomic<uint64_t> next_id{1};
+  s->id = next_id++;
   try {
     s->h = build_shared(sp, grad, n_volumes, response, n_response, hr.data(), n_hr);
   } catch (const std::exception& e) {
@@ -1387,6 +1410,7 @@ extern "C" int csd_solve(const csd_shared* const* shared, const csd_volume* volu
       P.nhr = nhr;
       P.nw = (nhr + 31) / 32;
       P.refine = refine_of(shared[group[g0]]);
+      P.fast_cycles = g_fast_cycles;
       P.cond_thr = (float)shared[group[g0]]->cond_thr;
       long long total = 0;
       int nv = 0;
@@ -2091,6 +2115,7 @@ static int noalloc_launch(const csd_shared* s, const csd_volume* v, cudaStream_t
   P.nhr = h.nhr;
   P.nw = (h.nhr + 31) / 32;
   P.refine = refine_of(s);
+  P.fast_cycles = g_fast_cycles;
   P.cond_thr = (float)s->cond_thr;
   P.total = v->n_voxels;
   P.queue = reinterpret_cast<unsigned long long*>(base);
@@ -2147,7 +2172,7 @@ extern "C" int csd_solve_noalloc(const csd_shared* s, const csd_volume* v, void*
 
 namespace {
 struct PhasedHostWS {
-  const csd_shared* sh = nullptr;
+  uint64_t sh_id = 0;  // the csd_shared the states were made for (ids are never reused; addresses can be)
   int64_t cap = 0;
   csd_state* st[2] = {nullptr, nullptr};
   float* dwi[2] = {nullptr, nullptr};
@@ -2172,7 +2197,7 @@ void release(PhasedHostWS& w) {
     w.warm[i] = nullptr;
   }
   w.cap = 0;
-  w.sh = nullptr;
+  w.sh_id = 0;
 }
 }  // namespace
 
@@ -2183,12 +2208,14 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
   if (n_voxels == 0) return CSD_OK;
   int dev = 0;
   CUDA_TRY(cudaGetDevice(&dev));
+  int rc0 = ensure_device(s);
+  if (rc0) return rc0;
   std::lock_guard<std::mutex> lk(g_phws_mu);
   PhasedHostWS& w = g_phws[dev];
   const int nvol = s->h.nvol, nsh = s->h.nsh, nw = (s->h.nhr + 31) / 32;
   const int64_t nslab = std::min<int64_t>(4, std::max<int64_t>(1, n_voxels / 131072));
   const int64_t per = (n_voxels + nslab - 1) / nslab;
-  if (w.sh != s || w.cap < per) {
+  if (w.sh_id != s->id || w.cap < per) {
     release(w);
     for (int i = 0; i < 2; ++i) {
       int rc = csd_state_create(s, per, &w.st[i]);
@@ -2199,7 +2226,7 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
       CUDA_TRY(cudaMalloc(&w.warm[i], (size_t)per * nw * sizeof(uint32_t)));
       if (!w.stream[i]) CUDA_TRY(cudaStreamCreateWithFlags(&w.stream[i], cudaStreamNonBlocking));
     }
-    w.sh = s;
+    w.sh_id = s->id;
     w.cap = per;
   }
   // enqueue the first slab's upload, then per slab: enqueue the next upload

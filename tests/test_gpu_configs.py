@@ -212,3 +212,15 @@ def test_cycle_jump_equals_full_iteration(cuda):
             assert np.array_equal(a[k], b[k]), (name, k)
         assert ((a["status"] & 0x0F) == csd.STATUS_NITER).sum() >= 1  # the case is exercised
         assert passes[(1, name)] < passes[(2, name)]
+    # the persistent kernel's per-voxel loop jumps the same cycles
+    pers = {}
+    try:
+        for knob in (2, 1):
+            autotune.set_knob(autotune.KNOB_CYCLE_JUMP, knob)
+            o = csd.dwi2fod_csd(s, d, mask=m, want_negmask=True)
+            pers[knob] = {k: t.cpu().numpy() for k, t in o.items()}
+    finally:
+        autotune.set_knob(autotune.KNOB_CYCLE_JUMP, 0)
+    for k in ("fod", "negmask", "status", "iterations"):
+        assert np.array_equal(pers[2][k], pers[1][k]), ("persistent", k)
+    assert ((pers[1]["status"] & 0x0F) == csd.STATUS_NITER).sum() >= 1

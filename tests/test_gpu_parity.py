@@ -336,3 +336,27 @@ def test_tiled_set_equals_warp_set(cuda, lmax):
         for k in ("fod", "negmask", "status", "iterations"):
             assert np.array_equal(outs[0][k], o[k]), k
     assert (outs[1]["status"] == csd.STATUS_NONFINITE).sum() > 0
+
+
+def test_host_phased_after_shared_objects_are_replaced(cuda):
+    """The host-buffer entry point caches its device workspace between calls.
+    A scheme object destroyed and replaced by a new one (which may reuse the
+    address) must get a fresh workspace and uploaded tables: each call equals
+    the device-buffer result for its own scheme."""
+    import gc
+
+    import torch
+    v = synth.make_volume((31, 17, 3), 6, 60, (15.0, 40.0), 8, 0.7, 94)
+    d = torch.from_numpy(v.dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    for lmax in (8, 6, 8, 4, 8):
+        s = csd.make_shared(v.grad, synth.RESPONSE, lmax=lmax)
+        host = csd.dwi2fod_csd_host_phased(s, v.dwi, v.mask)
+        st = csd.State(s, v.n_voxels)
+        st.run(d, mask=m)
+        dev = st.fod()
+        st.close()
+        assert np.array_equal(host["fod"], dev["fod"]), lmax
+        assert np.array_equal(host["status"], dev["status"]), lmax
+        del s, st
+        gc.collect()

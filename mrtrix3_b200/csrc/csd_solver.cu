@@ -57,6 +57,7 @@ static int g_solve_kind = 0;  // phased solve kernel: 0 default, 1 warp per voxe
 static constexpr int kSolveDefault = 1;
 static int g_set_kind = 0;    // phased set kernel: 0 default, 1 warp per voxel, 2 tiles of 64 voxels
 static int g_fast_cycles = 1; // phased method: jump periodic two-cycles to their last call (knob 7)
+static int g_host_slabs = 0;  // host-buffer phased entry point: most slabs per call (knob 8; 0 = 4)
 static constexpr int kSetDefault = 2;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
 
@@ -1531,6 +1532,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: cycle jumping is 0 (default), 1 on or 2 off");
       g_fast_cycles = value == 2 ? 0 : 1;
       break;
+    case 8:
+      if (value > 16) return fail(CSD_ERR_INVALID, "csd_set_launch_config: at most 16 slabs");
+      g_host_slabs = value;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -2213,7 +2218,7 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
   std::lock_guard<std::mutex> lk(g_phws_mu);
   PhasedHostWS& w = g_phws[dev];
   const int nvol = s->h.nvol, nsh = s->h.nsh, nw = (s->h.nhr + 31) / 32;
-  const int64_t nslab = std::min<int64_t>(4, std::max<int64_t>(1, n_voxels / 131072));
+  const int64_t nslab = std::min<int64_t>(g_host_slabs > 0 ? g_host_slabs : 4, std::max<int64_t>(1, n_voxels / 131072));
   const int64_t per = (n_voxels + nslab - 1) / nslab;
   if (w.sh_id != s->id || w.cap < per) {
     release(w);

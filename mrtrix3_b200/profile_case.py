@@ -1,7 +1,7 @@
 """Run one CSD method on a synthetic case, for profilers (ncu) and timing.
 
     python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
-        [--method warm|plain|persistent|persistent_warm|predict] [--reps 2]
+        [--method warm|plain|persistent|persistent_warm|predict|peaks] [--reps 2]
         [--projection mma|tcgen05] [--solve warp|group16|group8]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
@@ -17,7 +17,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--dims", type=int, nargs=3, default=[64, 64, 64])
     ap.add_argument("--lmax", type=int, default=8)
-    ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm", "predict"])
+    ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm", "predict", "peaks"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--projection", default="tcgen05", choices=["mma", "tcgen05"])
     ap.add_argument("--solve", default="warp", choices=["warp", "group16", "group8"])
@@ -35,11 +35,17 @@ def main():
     net = None
     if a.method in ("warm", "persistent_warm", "predict"):
         net = WarmStartNet.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_c5.npz"))
-    st = csd.State(s, d.shape[0]) if a.method in ("warm", "plain") else None
+    st = csd.State(s, d.shape[0]) if a.method in ("warm", "plain", "peaks") else None
+    fod = None
+    if a.method == "peaks":  # sh2peaks on this volume's FODs
+        st.run(d)
+        fod = st.fod(as_numpy=False)["fod"]
     t0 = time.perf_counter()
     for _ in range(a.reps):
         if a.method == "predict":
             net.predict(d)
+        elif a.method == "peaks":
+            csd.sh2peaks(fod)
         elif st is not None:
             st.run(d, warm=net.predict(d) if net is not None else None)
         else:

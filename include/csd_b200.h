@@ -236,8 +236,8 @@ int csd_sh2peaks(const float* sh, int64_t n_voxels, int64_t voxel_stride, int lm
  * of 64 voxels), 6 csd_mlp_predict kernels (1 one GEMM per layer, 2 the
  * fused tcgen05 kernel; 66..80 -> 256 -> 256 -> <=320 networks); value 0 =
  * built-in default, 7 the jump of exactly periodic two-cycles to their
- * last call, in the phased method and the persistent kernel (1 on, the
- * default; 2 off), 8 the most slabs csd_dwi2fod_host_phased cuts a volume
+ * last call (1 on, 2 off; by default on in the phased method, off in the
+ * persistent kernel), 8 the most slabs csd_dwi2fod_host_phased cuts a volume
  * into (0 = 4).  Knobs 0-5, 7 and 8
  * leave the outputs unchanged bit for bit; knob 6 changes the FP32
  * summation order of the logits. */

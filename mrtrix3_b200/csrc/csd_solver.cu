@@ -56,7 +56,11 @@ static int g_proj_kind = 0;  // projection kernel: 0 default, 1 mma.sync, 2 tcge
 static int g_solve_kind = 0;  // phased solve kernel: 0 default, 1 warp per voxel, 2 / 3 groups of 16 / 8 lanes
 static constexpr int kSolveDefault = 1;
 static int g_set_kind = 0;    // phased set kernel: 0 default, 1 warp per voxel, 2 tiles of 64 voxels
-static int g_fast_cycles = 1; // phased method: jump periodic two-cycles to their last call (knob 7)
+// jump of exactly periodic two-cycles to their last call (knob 7: 0 default, 1 on, 2 off): on by default in
+// the phased method (it removes ~40 near-empty passes per volume); off by default in the persistent kernel,
+// where a cycling voxel only holds its own warp and the extra checks in every iteration cost more (83.8 vs
+// 87.9 ms per benchmark volume)
+static int g_fast_cycles = 0;
 static int g_host_slabs = 0;  // host-buffer phased entry point: most slabs per call (knob 8; 0 = 4)
 static constexpr int kSetDefault = 2;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
@@ -1411,7 +1415,7 @@ extern "C" int csd_solve(const csd_shared* const* shared, const csd_volume* volu
       P.nhr = nhr;
       P.nw = (nhr + 31) / 32;
       P.refine = refine_of(shared[group[g0]]);
-      P.fast_cycles = g_fast_cycles;
+      P.fast_cycles = g_fast_cycles == 1;
       P.cond_thr = (float)shared[group[g0]]->cond_thr;
       long long total = 0;
       int nv = 0;
@@ -1530,7 +1534,7 @@ extern "C" int csd_set_launch_config(int which, int value) {
       break;
     case 7:
       if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: cycle jumping is 0 (default), 1 on or 2 off");
-      g_fast_cycles = value == 2 ? 0 : 1;
+      g_fast_cycles = value;
       break;
     case 8:
       if (value > 16) return fail(CSD_ERR_INVALID, "csd_set_launch_config: at most 16 slabs");
@@ -1690,7 +1694,7 @@ StateParams state_params(const csd_state* st) {
   P.status = st->status;
   P.iters = st->iters;
   P.cyc = st->cyc;
-  P.fast_cycles = g_fast_cycles;
+  P.fast_cycles = g_fast_cycles != 2;
   P.n_out = st->counter;
   P.err = st->counter + 1;
   P.stats = st->stats;
@@ -2120,7 +2124,7 @@ static int noalloc_launch(const csd_shared* s, const csd_volume* v, cudaStream_t
   P.nhr = h.nhr;
   P.nw = (h.nhr + 31) / 32;
   P.refine = refine_of(s);
-  P.fast_cycles = g_fast_cycles;
+  P.fast_cycles = g_fast_cycles == 1;
   P.cond_thr = (float)s->cond_thr;
   P.total = v->n_voxels;
   P.queue = reinterpret_cast<unsigned long long*>(base);

@@ -1,10 +1,11 @@
 // sh2peaks on the GPU: the peaks of each voxel's spherical-harmonic function
 // (MRtrix3 cmd/sh2peaks.cpp:99-303 with core/math/SH.h:515-650).
 //
-// A warp takes a voxel: its coefficients go to shared memory, every lane
-// runs the Newton search of SH::get_peak from its seed directions (in FP32,
-// as the reference: at most 50 steps, steps capped at MAX_DIR_CHANGE = 0.2
-// rad, converged below ANGLE_TOLERANCE = 1e-4), then lane 0 walks the seeds
+// A warp takes a voxel: its coefficients go to shared memory, the lanes run
+// the Newton searches of SH::get_peak from the seed directions (in FP32, as
+// the reference: at most 50 steps, steps capped at MAX_DIR_CHANGE = 0.2 rad,
+// converged below ANGLE_TOLERANCE = 1e-4), one step per lane per round, a
+// lane taking the next seed as soon as its search ends; then the seeds are walked
 // in order, drops a peak within |cos| > 0.99 of an earlier kept one or below
 // the threshold, and either keeps the largest peaks or, per target
 // direction, the peak of largest |cos| with it.  Output: [voxel][3 npeaks]
@@ -150,42 +151,41 @@ __device__ void sh_derivatives(const float* sh, float cel, float sel, float caz1
   }
 }
 
-// SH::get_peak (SH.h:515-560): returns the amplitude (NaN if no convergence
-// in 50 steps) and leaves the peak direction in v.
+// One step of SH::get_peak's Newton search (SH.h:517-553) from the unit
+// vector v: amp receives the amplitude at v, v moves by the step; true when
+// the step is below ANGLE_TOLERANCE (1e-4 rad), i.e. the search has ended
+// with amp.  get_peak is at most 50 of these.
 template <int L>
-__device__ float get_peak(const float* sh, float& v0, float& v1, float& v2, const float* kk) {
-  for (int i = 0; i < 50; ++i) {
-    // az = atan2(v1, v0), el = atan2(hypot(v0, v1), v2) of the unit vector
-    // v, through their cosines and sines (atan2(0, 0) = 0 at the poles)
-    const float h = hypotf(v0, v1);
-    const float ce = v2, se = h;
-    const float ca = h > 0.f ? v0 / h : (v0 < 0.f ? -1.f : 1.f), sa = h > 0.f ? v1 / h : 0.f;
-    float amp, dSH_del, dSH_daz, d2_del2, d2_deldaz, d2_daz2;
-    sh_derivatives<L>(sh, ce, se, ca, sa, amp, dSH_del, dSH_daz, d2_del2, d2_deldaz, d2_daz2, kk);
-    float del = sqrtf(dSH_del * dSH_del + dSH_daz * dSH_daz);
-    float daz = 0.f;
-    if (del != 0.f) {
-      daz = dSH_daz / del;
-      del = dSH_del / del;
-    }
-    const float dSH_dt = daz * dSH_daz + del * dSH_del;
-    const float d2SH_dt2 = daz * daz * d2_daz2 + 2.f * daz * del * d2_deldaz + del * del * d2_del2;
-    float dt = d2SH_dt2 != 0.f ? (-dSH_dt / d2SH_dt2) : 0.2f;
-    if (dt < 0.f) dt = -dt;
-    if (dt > 0.2f) dt = 0.2f;
-    del *= dt;
-    daz *= dt;
-    v0 += del * ca * ce - daz * sa;
-    v1 += del * sa * ce + daz * ca;
-    v2 -= del * se;
-    const float inv = 1.f / sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
-    v0 *= inv;
-    v1 *= inv;
-    v2 *= inv;
-    if (dt < 1e-4f) return amp;
+__device__ __forceinline__ bool peak_step(const float* sh, float& v0, float& v1, float& v2, const float* kk,
+                                          float& amp) {
+  // az = atan2(v1, v0), el = atan2(hypot(v0, v1), v2) of the unit vector
+  // v, through their cosines and sines (atan2(0, 0) = 0 at the poles)
+  const float h = hypotf(v0, v1);
+  const float ce = v2, se = h;
+  const float ca = h > 0.f ? v0 / h : (v0 < 0.f ? -1.f : 1.f), sa = h > 0.f ? v1 / h : 0.f;
+  float dSH_del, dSH_daz, d2_del2, d2_deldaz, d2_daz2;
+  sh_derivatives<L>(sh, ce, se, ca, sa, amp, dSH_del, dSH_daz, d2_del2, d2_deldaz, d2_daz2, kk);
+  float del = sqrtf(dSH_del * dSH_del + dSH_daz * dSH_daz);
+  float daz = 0.f;
+  if (del != 0.f) {
+    daz = dSH_daz / del;
+    del = dSH_del / del;
   }
-  v0 = v1 = v2 = nanf("");
-  return nanf("");
+  const float dSH_dt = daz * dSH_daz + del * dSH_del;
+  const float d2SH_dt2 = daz * daz * d2_daz2 + 2.f * daz * del * d2_deldaz + del * del * d2_del2;
+  float dt = d2SH_dt2 != 0.f ? (-dSH_dt / d2SH_dt2) : 0.2f;
+  if (dt < 0.f) dt = -dt;
+  if (dt > 0.2f) dt = 0.2f;
+  del *= dt;
+  daz *= dt;
+  v0 += del * ca * ce - daz * sa;
+  v1 += del * sa * ce + daz * ca;
+  v2 -= del * se;
+  const float inv = 1.f / sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
+  v0 *= inv;
+  v1 *= inv;
+  v2 *= inv;
+  return dt < 1e-4f;
 }
 
 // Warp-parallel selection for up to 64 seeds, with the outcome of the
@@ -312,13 +312,45 @@ __global__ void __launch_bounds__(32 * kPkWarps) sh2peaks_kernel(const __grid_co
       continue;
     }
     __syncwarp();
-    for (int s = lane; s < a.n_seeds; s += 32) {
-      float v0 = a.seeds[s][0], v1 = a.seeds[s][1], v2 = a.seeds[s][2];
-      const float amp = get_peak<L>(sh, v0, v1, v2, a.plm_k);
-      res[4 * s] = amp;
-      res[4 * s + 1] = v0;
-      res[4 * s + 2] = v1;
-      res[4 * s + 3] = v2;
+    {
+      // the searches, one Newton step per lane per round: a lane whose seed's
+      // search ends (converged, or 50 steps without converging: NaN) stores
+      // it and takes the next unassigned seed, so the warp's lanes stay busy
+      // until the seeds run out instead of waiting, seed by seed, for the
+      // longest search of each group of 32
+      int s = lane, steps = 0, next = 32;
+      float v0 = 0.f, v1 = 0.f, v2 = 1.f;
+      if (s < a.n_seeds) {
+        v0 = a.seeds[s][0];
+        v1 = a.seeds[s][1];
+        v2 = a.seeds[s][2];
+      }
+      while (__any_sync(0xffffffffu, s < a.n_seeds)) {
+        bool fin = false;
+        if (s < a.n_seeds) {
+          float amp;
+          const bool done = peak_step<L>(sh, v0, v1, v2, a.plm_k, amp);
+          if (done || ++steps == 50) {
+            if (!done) amp = v0 = v1 = v2 = fnan;
+            res[4 * s] = amp;
+            res[4 * s + 1] = v0;
+            res[4 * s + 2] = v1;
+            res[4 * s + 3] = v2;
+            fin = true;
+          }
+        }
+        const unsigned f = __ballot_sync(0xffffffffu, fin);
+        if (fin) {
+          s = next + __popc(f & ((1u << lane) - 1u));
+          steps = 0;
+          if (s < a.n_seeds) {
+            v0 = a.seeds[s][0];
+            v1 = a.seeds[s][1];
+            v2 = a.seeds[s][2];
+          }
+        }
+        next += __popc(f);
+      }
     }
     __syncwarp();
     if (a.n_seeds <= 64) {

@@ -226,6 +226,20 @@ int csd_sh2peaks(const float* sh, int64_t n_voxels, int64_t voxel_stride, int lm
                  const float* seeds_azel, int n_seeds, int npeaks, float threshold, const float* directions,
                  int n_directions, const float* peaks_in, float* peaks_out, void* stream);
 
+/* ---- amp2sh (cmd/amp2sh.cpp:108-127, 153-171) on device buffers: per voxel
+ *      of `amp` ([n][voxel_stride], volumes volume_stride apart) the SH
+ *      coefficients fit * a in FP64, a = the amplitudes of the nd volumes
+ *      `dwis`, scaled by nb0 / (1 + their b=0 sum) when `normalise` (b=0
+ *      volumes `bzeros`); fit = pinv(SH2amp) [nsh][nd] (double), nd <= 800
+ *      (CSD_ERR_INVALID beyond).  All arrays
+ *      are device pointers; output float [n][out_stride].  The volume
+ *      indices in `dwis` and `bzeros` must address volumes of the voxel (the
+ *      kernel reads them unchecked; the Python binding checks them).  Returns
+ *      without synchronising.  The -rician correction is not provided. */
+int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t volume_stride, const double* fit,
+               int nsh, const int* dwis, int nd, const int* bzeros, int nb0, int normalise, float* sh_out,
+               int64_t out_stride, void* stream);
+
 /* Launch-shape knobs (process-wide), chosen by the project's autotuner
  * (mrtrix3_b200/autotune.py): which = 0 warps per block of the persistent
  * kernel, 1 warps per block of the phased solve kernel, 2 projection blocks

@@ -32,7 +32,7 @@ EXPORTED = [
     "csd_shared_dwis", "csd_shared_matrix", "csd_solve", "csd_dwi2fod_host", "csd_state_create",
     "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_run",
     "csd_state_fod",
-    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_last_error",
+    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_last_error",
 ]
 
 
@@ -85,6 +85,8 @@ def lib():
         L.csd_state_warm.argtypes = [vp, vp, vp]
         L.csd_state_iterate.argtypes = [vp, ctypes.POINTER(i64), vp]
         L.csd_state_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(i64), vp]
+        L.csd_amp2sh.argtypes = [vp, i64, i64, i64, vp, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
+                                 vp, i64, vp]
         L.csd_sh2peaks.argtypes = [vp, i64, i64, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                    vp, ctypes.c_int, vp, vp, vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]
@@ -366,6 +368,64 @@ def sh2peaks(sh, lmax: int | None = None, mask=None, seeds=None, npeaks: int = 3
                              ctypes.c_void_p(peaks.data_ptr()) if peaks is not None else None,
                              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(_stream_ptr(stream))))
     return out
+
+
+class Amp2SHCommon:
+    """The fit of amp2sh held on the device (Amp2SHCommon, cmd/amp2sh.cpp:86-104):
+    ``fit`` = pinv(SH2amp) [nSH][len(dwis)] (numpy, FP64), ``dwis`` the
+    volumes it applies to, ``bzeros`` the b=0 volumes for ``normalise``.
+    Calling it on amplitudes runs csd_amp2sh."""
+
+    def __init__(self, fit, dwis, bzeros=None, normalise: bool = False, device=None):
+        import torch
+        fit = np.asarray(fit, np.float64)
+        self.dwis = np.asarray(dwis, np.int64).reshape(-1)
+        self.bzeros = np.asarray([] if bzeros is None else bzeros, np.int64).reshape(-1)
+        if fit.ndim != 2 or fit.shape[1] != len(self.dwis):
+            raise ValueError("amp2sh: the fit matrix needs one column per selected volume")
+        if (self.dwis < 0).any() or (self.bzeros < 0).any():
+            raise ValueError("amp2sh: volume index out of range")
+        self.normalise = bool(normalise)
+        self.nsh, self.nd = fit.shape
+        # the highest volume index: the kernel reads the amplitude rows at
+        # these indices unchecked, so every call checks the rows are long enough
+        self.max_volume = int(max(self.dwis.max(initial=-1), self.bzeros.max(initial=-1)))
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.fit_d = torch.from_numpy(np.ascontiguousarray(fit)).to(dev)
+        self.dwis_d = torch.from_numpy(np.ascontiguousarray(self.dwis, np.int32)).to(dev)
+        self.b0_d = torch.from_numpy(np.ascontiguousarray(self.bzeros, np.int32)).to(dev) if len(self.bzeros) else None
+
+    def __call__(self, amp, out=None, stream=None):
+        """SH coefficients of each row of ``amp`` (float32 CUDA tensor
+        [n][volumes], any strides) into ``out`` (float32 [n][>= nSH], unit
+        column stride; allocated when None).  Returns ``out``."""
+        import torch
+        if amp.dim() != 2 or amp.dtype != torch.float32 or amp.device != self.fit_d.device:
+            raise ValueError("amp2sh: amplitudes must be a float32 tensor [n][volumes] on the fit's device")
+        if self.max_volume >= amp.shape[1]:
+            raise ValueError("amp2sh: volume index out of range")
+        if out is None:
+            out = torch.empty((amp.shape[0], self.nsh), dtype=torch.float32, device=amp.device)
+        if (out.dim() != 2 or out.dtype != torch.float32 or out.device != amp.device or out.shape[0] != amp.shape[0]
+                or out.shape[1] < self.nsh or out.stride(1) != 1):
+            raise ValueError("amp2sh: output must be float32 [n][>= nSH] with contiguous rows")
+        check(lib().csd_amp2sh(ctypes.c_void_p(amp.data_ptr()), amp.shape[0], amp.stride(0), amp.stride(1),
+                               ctypes.c_void_p(self.fit_d.data_ptr()), self.nsh,
+                               ctypes.c_void_p(self.dwis_d.data_ptr()), self.nd,
+                               ctypes.c_void_p(self.b0_d.data_ptr()) if self.b0_d is not None else None,
+                               len(self.bzeros), int(self.normalise), ctypes.c_void_p(out.data_ptr()),
+                               max(out.stride(0), self.nsh), ctypes.c_void_p(_stream_ptr(stream))))
+        return out
+
+
+def amp2sh(amp, fit, dwis, bzeros=None, normalise: bool = False, stream=None):
+    """SH coefficients of each row of ``amp`` (float32 CUDA tensor [n][nvol]):
+    one-off Amp2SHCommon(fit, dwis, bzeros, normalise)(amp).  Returns a
+    float32 CUDA tensor [n][nSH]."""
+    import torch
+    if not isinstance(amp, torch.Tensor) or not amp.is_cuda:
+        raise ValueError("amp2sh: amplitudes must be a float32 CUDA tensor [n][volumes]")
+    return Amp2SHCommon(fit, dwis, bzeros, normalise, device=amp.device)(amp, stream=stream)
 
 
 def negmask_to_bool(negmask, n_hr: int) -> np.ndarray:

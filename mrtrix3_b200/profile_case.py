@@ -1,7 +1,7 @@
 """Run one CSD method on a synthetic case, for profilers (ncu) and timing.
 
     python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
-        [--method warm|plain|persistent|persistent_warm|predict|peaks] [--reps 2]
+        [--method warm|plain|persistent|persistent_warm|predict|peaks|amp2sh] [--reps 2]
         [--projection mma|tcgen05] [--solve warp|group16|group8]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
@@ -12,12 +12,15 @@ import argparse
 import os
 import time
 
+import numpy as np
+
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--dims", type=int, nargs=3, default=[64, 64, 64])
     ap.add_argument("--lmax", type=int, default=8)
-    ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm", "predict", "peaks"])
+    ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm", "predict", "peaks",
+                                                          "amp2sh"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--projection", default="tcgen05", choices=["mma", "tcgen05"])
     ap.add_argument("--solve", default="warp", choices=["warp", "group16", "group8"])
@@ -37,6 +40,25 @@ def main():
         net = WarmStartNet.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_c5.npz"))
     st = csd.State(s, d.shape[0]) if a.method in ("warm", "plain", "peaks") else None
     fod = None
+    if a.method == "amp2sh":  # the SH fit of this volume's DW amplitudes (normalised by its b=0 volumes)
+        from . import sh
+        dwis = np.asarray(s.dwis)
+        bzeros = np.nonzero(v.grad[:, 3] <= 10.0)[0]
+        fit = sh.pinv(sh.init_transform(sh.cartesian_to_azel(v.grad[dwis, :3]), a.lmax))
+        plan = csd.Amp2SHCommon(fit, dwis, bzeros, normalise=True)
+        out = plan(d)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.reps):
+            plan(d, out)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+        nbytes = d.shape[0] * (len(dwis) + len(bzeros) + fit.shape[0]) * 4
+        print(f"amp2sh: {d.shape[0]} voxels in {ms:.3f} ms per call, {nbytes / ms / 1e6:.0f} GB/s "
+              f"({d.shape[0] / ms / 1e3:.1f}M voxels/s)")
+        return
     if a.method == "peaks":  # sh2peaks on this volume's FODs
         st.run(d)
         fod = st.fod(as_numpy=False)["fod"]

@@ -23,6 +23,9 @@
 
 namespace csdb200 {
 int set_error(int code, const std::string& msg);  // csd_solver.cu
+// amp2sh kernel: 0 the fastest that applies, 1 row, 2 tile (FP64 FMA),
+// 3 FP64 tensor cores (where they apply); set by csd_set_launch_config
+int g_amp2sh_kind = 0;
 }
 
 namespace {
@@ -38,6 +41,8 @@ struct Amp2ShArgs {
   const int* dwis;    // [nd]
   const int* b0;      // [nb0] or NULL
   int nd, nb0, nsh, normalise;
+  int contig;      // tensor-core kernel: volume stride 1 and 16-byte aligned rows
+  int row_floats;  // tensor-core kernel: staged floats a voxel
   float* out;
   long long os;
 };
@@ -57,11 +62,10 @@ __global__ void __launch_bounds__(kA2sThreads) amp2sh_kernel(const __grid_consta
       const float* p = a.amp + v * a.vs;
       double norm = 1.0;
       if (a.normalise) {
-        double s = 0.0;
-        for (int i = lane; i < a.nb0; i += 32) s += (double)p[(long long)a.b0[i] * a.ts];
-#pragma unroll
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        norm = (double)a.nb0 / (1.0 + s);
+        // get_amps' sum, in its order: 1 + the b=0 amplitudes one by one
+        double s = 1.0;
+        for (int i = 0; i < a.nb0; ++i) s += (double)p[(long long)a.b0[i] * a.ts];
+        norm = (double)a.nb0 / s;
       }
       for (int t = lane; t < a.nd; t += 32) A[r * lda + t] = (double)p[(long long)a.dwis[t] * a.ts] * norm;
     }
@@ -152,11 +156,9 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2) amp2sh_tile_kernel(const _
       }
       double norm = 1.0;
       if (a.normalise) {
-        double s = 0.0;
-        for (int i = lane; i < a.nb0; i += 32) s += (double)Bf[r * a.nb0 + i];
-#pragma unroll
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        norm = (double)a.nb0 / (1.0 + s);
+        double s = 1.0;  // get_amps' order, as above
+        for (int i = 0; i < a.nb0; ++i) s += (double)Bf[r * a.nb0 + i];
+        norm = (double)a.nb0 / s;
       }
       for (int t = lane; t < ndp; t += 32) row[t] = t < a.nd ? (double)Af[r * ndp + t] * norm : 0.0;
     }
@@ -191,6 +193,169 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2) amp2sh_tile_kernel(const _
       for (int j = 0; j < JC; ++j) {
         const int c = lane + 32 * j;
         if (c < a.nsh) a.out[v * a.os + c] = (float)acc[i][j];
+      }
+    }
+  }
+}
+
+// ---- FP64 tensor-core kernel (mma.sync m8n8k4 f64) for fits of nd <= 64
+// directions and nSH <= 48 columns (lmax <= 8).  D [voxels][columns] =
+// A [voxels][directions] x B [directions][columns], B = fit^T; the b=0
+// normalisation scales D's rows (norm (fit a) = fit (norm a)).  The block
+// has 2 x WN warps: warp (wm, wn) forms 4 m-tiles (32 voxels) x 1 n-tile (8
+// columns) of the block's 64 voxels, with its B fragments for all k-steps
+// held in registers for the life of the block; two blocks an SM, so that
+// one block's staging overlaps the other's products.  The next tile's
+// amplitudes arrive by cp.async while the current one computes: whole voxel
+// rows in 16-byte pieces when the volumes are contiguous (volume stride 1,
+// 16-byte aligned amplitudes), else the selected volumes one by one.  A is
+// then converted to double in fragment order, [m-tile][k-step pair][lane][2],
+// so that a lane's operands for two k-steps are one 16-byte load.  Fragment
+// layouts (PTX ISA, mma.m8n8k4 .f64): A a0 = A[lane / 4][lane % 4]; B b0 =
+// B[lane % 4][lane / 4]; C / D c_i = C[lane / 4][2 (lane % 4) + i].
+constexpr int kMmaWM = 2;    // warps along the voxels
+constexpr int kMmaMT = 4;    // m-tiles (8 voxels) a warp forms: 2 x 4 x 8 = 64
+constexpr int kMmaNTW = 1;   // n-tiles (8 columns) a warp forms
+constexpr int kMmaKSM = 16;  // k-steps (4 directions) a warp holds: nd <= 64
+constexpr int kMmaMaxWarps = kMmaWM * 6;  // nSH <= 48 (lmax <= 8): at most 6 warps along the columns
+constexpr int kMmaMaxRow = 256;           // longest voxel row staged whole (floats)
+
+__host__ __device__ inline int mma_ks2(int nd) { return ((nd + 3) / 4 + 1) / 2; }
+// staged floats a voxel: the whole row (contiguous volumes) or the selected ones
+__host__ inline int mma_row_floats(int nd, int nb0, bool whole_rows, long long vs) {
+  return whole_rows ? (int)std::max<long long>(vs, nd + nb0) : nd + nb0;
+}
+__host__ inline size_t mma_smem_bytes(int nd, int nb0, int row_floats) {
+  return ((size_t)kTileRows * mma_ks2(nd) * 8 + kTileRows) * sizeof(double) +
+         ((size_t)kTileRows * row_floats + nd + nb0) * sizeof(float);
+}
+
+__device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(c0), "+d"(c1)
+      : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__global__ void __launch_bounds__(kMmaMaxWarps * 32, 2) amp2sh_mma_kernel(const __grid_constant__ Amp2ShArgs a) {
+  extern __shared__ __align__(16) double msm_[];
+  const int ks = (a.nd + 3) / 4, ks2 = mma_ks2(a.nd);
+  double* Ap = msm_;                                              // [8][ks2][32][2]
+  double* nrm = Ap + kTileRows * ks2 * 8;                         // [kTileRows]
+  float* S = reinterpret_cast<float*>(nrm + kTileRows);          // [kTileRows][row_floats]
+  int* dw = reinterpret_cast<int*>(S + kTileRows * a.row_floats);  // [nd]
+  int* bz = dw + a.nd;                                            // [nb0]
+  __shared__ int max_index;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int wm = warp % kMmaWM, wn = warp / kMmaWM;
+  double b[kMmaKSM];
+  {
+    const int c = 8 * wn + (lane >> 2);
+#pragma unroll
+    for (int ks = 0; ks < kMmaKSM; ++ks) {
+      const int k = 4 * ks + (lane & 3);
+      b[ks] = (k < a.nd && c < a.nsh) ? __ldg(a.fit + (long long)c * a.nd + k) : 0.0;
+    }
+  }
+  if (threadIdx.x == 0) max_index = 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < a.nd; t += blockDim.x) {
+    dw[t] = a.dwis[t];
+    atomicMax(&max_index, dw[t]);
+  }
+  for (int t = threadIdx.x; t < a.nb0; t += blockDim.x) {
+    bz[t] = a.b0[t];
+    atomicMax(&max_index, bz[t]);
+  }
+  __syncthreads();
+  // whole rows only when every selected volume lies inside the row
+  const bool whole = a.contig && max_index < a.vs;
+  // staged row stride: the voxel stride for whole rows, else the selection
+  const int ls = whole ? (int)a.vs : a.nd + a.nb0;
+  // this lane's two conversion slots t = lane, lane + 32: the staged float it
+  // reads (-1: padding) and its place in an m-tile's fragment-ordered rows
+  int src[2], dst[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int t = lane + 32 * j;
+    src[j] = t < a.nd ? (whole ? dw[t] : t) : -1;
+    dst[j] = (t >> 3) * 64 + (t & 3) * 2 + ((t >> 2) & 1);
+  }
+  auto gather = [&](long long tile) {
+    const long long v0 = tile * kTileRows;
+    const int rows = a.n - v0 < kTileRows ? (int)(a.n - v0) : kTileRows;
+    if (whole) {
+      // rows v0 .. v0 + rows - 1 up to the last voxel's highest selected volume
+      const float* base = a.amp + v0 * a.vs;
+      const int nfl = (rows - 1) * (int)a.vs + max_index + 1;
+      const int nch = nfl >> 2;
+      for (int c = threadIdx.x; c < nch; c += blockDim.x) cp_async16(S + 4 * c, base + 4 * c);
+      for (int e = 4 * nch + threadIdx.x; e < nfl; e += blockDim.x) cp_async4(S + e, base + e);
+    } else {
+      for (int r = warp; r < rows; r += nwarps) {
+        const float* p = a.amp + (v0 + r) * a.vs;
+        for (int t = lane; t < a.nd; t += 32) cp_async4(S + r * ls + t, p + (long long)dw[t] * a.ts);
+        if (a.normalise)
+          for (int t = lane; t < a.nb0; t += 32) cp_async4(S + r * ls + a.nd + t, p + (long long)bz[t] * a.ts);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  const long long ntiles = (a.n + kTileRows - 1) / kTileRows;
+  if ((long long)blockIdx.x < ntiles) gather(blockIdx.x);
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long v0 = tile * kTileRows;
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();  // this tile's staging visible; the previous tile's A consumed
+    for (int r = warp; r < kTileRows; r += nwarps) {
+      const bool live = v0 + r < a.n;
+      const float* row = S + r * ls;
+      double* out = Ap + (r >> 3) * ks2 * 64 + (r & 7) * 8;
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        if (lane + 32 * j < 8 * ks2) out[dst[j]] = (live && src[j] >= 0) ? (double)row[src[j]] : 0.0;
+    }
+    if (a.normalise)
+      for (int r = threadIdx.x; r < kTileRows; r += blockDim.x) {
+        if (v0 + r >= a.n) continue;
+        // get_amps' sum, in its order: 1 + the b=0 amplitudes one by one
+        double s = 1.0;
+        for (int i = 0; i < a.nb0; ++i) s += (double)S[r * ls + (whole ? bz[i] : a.nd + i)];
+        nrm[r] = (double)a.nb0 / s;
+      }
+    __syncthreads();  // A and the norms ready; the staging free for the next tile
+    if (tile + gridDim.x < ntiles) gather(tile + gridDim.x);
+    double acc[kMmaMT][2];
+#pragma unroll
+    for (int m = 0; m < kMmaMT; ++m) acc[m][0] = acc[m][1] = 0.0;
+#pragma unroll
+    for (int kp = 0; kp < kMmaKSM / 2; ++kp) {
+      if (kp < ks2) {
+        double2 x[kMmaMT];
+#pragma unroll
+        for (int m = 0; m < kMmaMT; ++m)
+          x[m] = *reinterpret_cast<const double2*>(Ap + (((wm * kMmaMT + m) * ks2 + kp) * 32 + lane) * 2);
+#pragma unroll
+        for (int m = 0; m < kMmaMT; ++m) dmma_m8n8k4(acc[m][0], acc[m][1], x[m].x, b[2 * kp]);
+        if (2 * kp + 1 < ks)  // an odd k-step count leaves the last pair's second step empty
+#pragma unroll
+          for (int m = 0; m < kMmaMT; ++m) dmma_m8n8k4(acc[m][0], acc[m][1], x[m].y, b[2 * kp + 1]);
+      }
+    }
+    const int c = 8 * wn + 2 * (lane & 3);
+#pragma unroll
+    for (int m = 0; m < kMmaMT; ++m) {
+      const int r = (wm * kMmaMT + m) * 8 + (lane >> 2);
+      const long long v = v0 + r;
+      if (v < a.n) {
+        const double f = a.normalise ? nrm[r] : 1.0;
+        if (c < a.nsh) a.out[v * a.os + c] = (float)(acc[m][0] * f);
+        if (c + 1 < a.nsh) a.out[v * a.os + c + 1] = (float)(acc[m][1] * f);
       }
     }
   }
@@ -239,8 +404,36 @@ extern "C" int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stri
   if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_amp2sh: ") + cudaGetErrorString(e));
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int jc = (nsh + 31) / 32;
-  if (jc <= 3 && tile_smem_bytes(nd, nb0, jc) <= (size_t)smem_max / 2) {
-    // the whole fit in shared memory with room for two blocks an SM
+  const bool mma_ok = nd <= 4 * kMmaKSM && nsh <= 8 * kMmaNTW * (kMmaMaxWarps / kMmaWM) &&
+                      mma_smem_bytes(nd, nb0, mma_row_floats(nd, nb0, false, 0)) <= (size_t)smem_max / 2;
+  // the whole fit in shared memory with room for two blocks an SM
+  const bool tile_ok = jc <= 3 && tile_smem_bytes(nd, nb0, jc) <= (size_t)smem_max / 2;
+  const int want = csdb200::g_amp2sh_kind;
+  const int kind = want == 1 ? 1 : (want == 2 && tile_ok) ? 2 : (want == 3 && mma_ok) ? 3 : mma_ok ? 3 : tile_ok ? 2 : 1;
+  if (kind == 3) {
+    // whole voxel rows staged when the volumes are contiguous and each tile's
+    // first row is 16-byte aligned (tiles start 64 rows apart)
+    a.contig = volume_stride == 1 && voxel_stride >= 1 && voxel_stride <= kMmaMaxRow &&
+               (reinterpret_cast<uintptr_t>(amp) & 15) == 0;
+    a.row_floats = mma_row_floats(nd, nb0, a.contig, voxel_stride);
+    size_t smem = mma_smem_bytes(nd, nb0, a.row_floats);
+    if (smem > (size_t)smem_max / 2) {  // two blocks an SM or the selected volumes only
+      a.contig = 0;
+      a.row_floats = mma_row_floats(nd, nb0, false, voxel_stride);
+      smem = mma_smem_bytes(nd, nb0, a.row_floats);
+    }
+    const int wn = ((nsh + 7) / 8 + kMmaNTW - 1) / kMmaNTW;
+    const int threads = 32 * kMmaWM * wn;
+    int per_sm = 0;
+    e = cudaFuncSetAttribute(amp2sh_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, amp2sh_mma_kernel, threads, smem);
+    if (e == cudaSuccess) {
+      const long long tiles = (n_voxels + kTileRows - 1) / kTileRows;
+      const long long grid = std::max<long long>(1, std::min<long long>(tiles, (long long)nsm * std::max(1, per_sm)));
+      amp2sh_mma_kernel<<<(unsigned)grid, threads, smem, st>>>(a);
+      e = cudaGetLastError();
+    }
+  } else if (kind == 2) {
     const size_t smem = tile_smem_bytes(nd, nb0, jc);
     e = jc == 1 ? launch_tile<1>(a, smem, nsm, st) : jc == 2 ? launch_tile<2>(a, smem, nsm, st)
                                                       : launch_tile<3>(a, smem, nsm, st);

@@ -36,6 +36,7 @@ static int fail(int code, const std::string& msg) {
 }
 namespace csdb200 {
 extern int g_mlp_infer_kind;  // mlp.cu
+extern int g_amp2sh_kind;     // amp2sh.cu
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace csdb200
 
@@ -1539,6 +1540,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
     case 8:
       if (value > 16) return fail(CSD_ERR_INVALID, "csd_set_launch_config: at most 16 slabs");
       g_host_slabs = value;
+      break;
+    case 9:
+      if (value > 3) return fail(CSD_ERR_INVALID, "csd_set_launch_config: amp2sh kernel is 0, 1, 2 or 3");
+      csdb200::g_amp2sh_kind = value;
       break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }

@@ -2,7 +2,7 @@
 
     python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
         [--method warm|plain|persistent|persistent_warm|predict|peaks|amp2sh] [--reps 2]
-        [--projection mma|tcgen05] [--solve warp|group16|group8]
+        [--projection mma|tcgen05] [--solve warp|group16|group8] [--amp2sh-kernel auto|row|tile|mma]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
 (lmax 8) or 8 b=0 + 90 DW (lmax 10).  Prints the state's work / time
@@ -24,12 +24,14 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--projection", default="tcgen05", choices=["mma", "tcgen05"])
     ap.add_argument("--solve", default="warp", choices=["warp", "group16", "group8"])
+    ap.add_argument("--amp2sh-kernel", default="auto", choices=["auto", "row", "tile", "mma"])
     a = ap.parse_args()
     import torch
 
     from . import autotune, csd, synth
     autotune.set_knob(autotune.KNOB_TC_PROJECTION, 2 if a.projection == "tcgen05" else 1)
     autotune.set_knob(autotune.KNOB_SOLVE_KIND, {"warp": 1, "group16": 2, "group8": 3}[a.solve])
+    autotune.set_knob(autotune.KNOB_AMP2SH_KIND, ["auto", "row", "tile", "mma"].index(a.amp2sh_kernel))
     from .warmstart import WarmStartNet
     ndw, nb0 = (60, 6) if a.lmax <= 8 else (90, 8)
     v = synth.make_volume(tuple(a.dims), nb0, ndw, (15.0, 40.0), a.lmax, None, 5)

@@ -135,12 +135,26 @@ def test_amp2sh_command_line(cuda, tmp_path):
     _check(got2, _ref(amp[:, dwis], fit6, np.arange(60), [], False))
 
 
-@pytest.mark.parametrize("ndir,lmax", [(59, 4), (60, 8), (90, 10), (300, 12), (300, 16), (800, 8)])
-def test_amp2sh_fit_shapes(cuda, ndir, lmax):
-    """Odd direction counts (padded pairs), one to three column groups of 32
-    in the tile kernel, and fits too large for shared memory (the row kernel:
-    300 directions at lmax 12 / 16)."""
+@pytest.fixture
+def amp2sh_kernel():
+    from mrtrix3_b200 import autotune
+
+    def use(kind):
+        autotune.set_knob(autotune.KNOB_AMP2SH_KIND, kind)
+    yield use
+    use(0)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("ndir,lmax", [(30, 4), (59, 4), (60, 8), (64, 8), (90, 10), (300, 12), (300, 16), (800, 8)])
+def test_amp2sh_fit_shapes(cuda, amp2sh_kernel, ndir, lmax, kind):
+    """Every kernel (1 row, 2 tile, 3 FP64 tensor cores, 0 the automatic
+    choice; a kernel that does not apply falls back to one that does) on odd
+    direction counts (padded k-steps), one to three column groups of 32 in
+    the tile kernel, the tensor-core limits (64 directions, lmax 8) and fits
+    too large for shared memory (300 directions at lmax 12 / 16)."""
     import torch
+    amp2sh_kernel(kind)
     rng = np.random.default_rng(ndir + lmax)
     dirs = np.stack([rng.uniform(0, 2 * np.pi, ndir), np.arccos(rng.uniform(-1, 1, ndir))], axis=1)
     fit = np.linalg.pinv(O.init_transform(dirs, lmax))
@@ -153,3 +167,25 @@ def test_amp2sh_fit_shapes(cuda, ndir, lmax):
     for normalise in (False, True):
         got = csd.amp2sh(d, fit, dwis, bzeros, normalise=normalise).cpu().numpy().astype(np.float64)
         _check(got, _ref(amp, fit, dwis, bzeros, normalise))
+
+
+@pytest.mark.parametrize("kind", [0, 2])
+def test_amp2sh_row_layouts(cuda, amp2sh_kernel, kind):
+    """Voxel rows padded beyond the volumes (voxel stride 70 for 66 volumes),
+    rows that start off a 16-byte boundary (a column slice), and a voxel
+    stride above what the tensor-core kernel stages whole (300): all give the
+    fit of the selected volumes."""
+    import torch
+    amp2sh_kernel(kind)
+    grad = synth.config5_scheme()
+    fit, dwis, bzeros = _fit(grad)
+    rng = np.random.default_rng(17)
+    n = 5003
+    for width, first in ((70, 0), (70, 1), (300, 3)):
+        wide = rng.uniform(0.1, 2.0, (n, width)).astype(np.float32)
+        d = torch.from_numpy(wide).to(cuda)[:, first:first + grad.shape[0]]
+        assert d.stride() == (width, 1)
+        amp = wide[:, first:first + grad.shape[0]]
+        for normalise in (False, True):
+            got = csd.amp2sh(d, fit, dwis, bzeros, normalise=normalise).cpu().numpy().astype(np.float64)
+            _check(got, _ref(amp, fit, dwis, bzeros, normalise))

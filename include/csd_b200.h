@@ -252,9 +252,12 @@ int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t
  * built-in default, 7 the jump of exactly periodic two-cycles to their
  * last call (1 on, 2 off; by default on in the phased method, off in the
  * persistent kernel), 8 the most slabs csd_dwi2fod_host_phased cuts a volume
- * into (0 = 4).  Knobs 0-5, 7 and 8
+ * into (0 = 4), 9 the csd_amp2sh kernel (1 a dot product a thread, 2 FP64
+ * FMA tiles, 3 FP64 tensor cores where they apply: nd <= 64, nSH <= 48;
+ * 0 = the fastest that applies).  Knobs 0-5, 7 and 8
  * leave the outputs unchanged bit for bit; knob 6 changes the FP32
- * summation order of the logits. */
+ * summation order of the logits, knob 9 the FP64 summation order of the
+ * coefficients. */
 int csd_set_launch_config(int which, int value);
 
 /* Thread-local description of the last failure. */

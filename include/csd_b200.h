@@ -240,6 +240,37 @@ int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t
                int nsh, const int* dwis, int nd, const int* bzeros, int nb0, int normalise, float* sh_out,
                int64_t out_stride, void* stream);
 
+/* ---- inequality-constrained least squares, batched: the solver of
+ *      dwi2fod msmt_csd (src/dwi/sdeconv/msmt_csd.h:249-270) and of
+ *      Math::ICLS (core/math/constrained_least_squares.h).
+ *
+ * csd_icls_create replaces ICLS::Problem (constrained_least_squares.h:
+ * 90-151): min ||H x - b||^2 subject to A x >= t, the last num_eq rows of
+ * A as equalities; H [nmeas][nparam], A [ncons][nparam] row-major host FP64,
+ * t [ncons] or NULL (zeros); solution_reg scales the largest diagonal entry
+ * of H^T H added to its diagonal, constraint_reg is added to the diagonal of
+ * the active-set systems; max_niter 0 = 10 nparam; tol the violation below
+ * -tol that activates a constraint.  Set-up in FP64 on the host, tables
+ * uploaded to the current device.  Errors: CSD_ERR_INVALID (sizes, H^T H not
+ * positive definite, a zero constraint row).
+ *
+ * csd_icls_solve replaces ICLS::Solver::operator() (:241-370) for n
+ * right-hand sides b (device float, [n][voxel_stride], measurements
+ * meas_stride apart), FP64 inside: x (device float [n][x_stride], x_stride
+ * >= nparam), niter (device int32 [n] or NULL: the solver's rounds; -1 where
+ * an active set outgrew 512 rows, with x NaN).  mask (device uint8 [n] or
+ * NULL): 0 skips the voxel (x = 0).  A non-finite b gives x = NaN.  Returns
+ * without synchronising; grows a per-warp scratch buffer on first use. */
+typedef struct csd_icls csd_icls;
+int csd_icls_create(const double* H, int nmeas, int nparam, const double* A, int ncons, const double* t,
+                    int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol,
+                    csd_icls** out);
+void csd_icls_destroy(csd_icls* problem);
+/* out4 = {nmeas, nparam, ncons, max_niter} */
+int csd_icls_info(const csd_icls* problem, int* out4);
+int csd_icls_solve(csd_icls* problem, const float* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
+                   const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, void* stream);
+
 /* Launch-shape knobs (process-wide), chosen by the project's autotuner
  * (mrtrix3_b200/autotune.py): which = 0 warps per block of the persistent
  * kernel, 1 warps per block of the phased solve kernel, 2 projection blocks

@@ -32,7 +32,8 @@ EXPORTED = [
     "csd_shared_dwis", "csd_shared_matrix", "csd_solve", "csd_dwi2fod_host", "csd_state_create",
     "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_run",
     "csd_state_fod",
-    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_last_error",
+    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_icls_create",
+    "csd_icls_destroy", "csd_icls_info", "csd_icls_solve", "csd_last_error",
 ]
 
 
@@ -87,6 +88,13 @@ def lib():
         L.csd_state_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(i64), vp]
         L.csd_amp2sh.argtypes = [vp, i64, i64, i64, vp, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
                                  vp, i64, vp]
+        L.csd_icls_create.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                      ctypes.POINTER(vp)]
+        L.csd_icls_destroy.argtypes = [vp]
+        L.csd_icls_destroy.restype = None
+        L.csd_icls_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+        L.csd_icls_solve.argtypes = [vp, vp, i64, i64, i64, vp, vp, i64, vp, vp]
         L.csd_sh2peaks.argtypes = [vp, i64, i64, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                    vp, ctypes.c_int, vp, vp, vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]

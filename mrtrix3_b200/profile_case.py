@@ -1,7 +1,7 @@
 """Run one CSD method on a synthetic case, for profilers (ncu) and timing.
 
     python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
-        [--method warm|plain|persistent|persistent_warm|predict|peaks|amp2sh] [--reps 2]
+        [--method warm|plain|persistent|persistent_warm|predict|peaks|amp2sh|msmt] [--reps 2]
         [--projection mma|tcgen05] [--solve warp|group16|group8] [--amp2sh-kernel auto|row|tile|mma]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
@@ -20,7 +20,7 @@ def main():
     ap.add_argument("--dims", type=int, nargs=3, default=[64, 64, 64])
     ap.add_argument("--lmax", type=int, default=8)
     ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm", "predict", "peaks",
-                                                          "amp2sh"])
+                                                          "amp2sh", "msmt"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--projection", default="tcgen05", choices=["mma", "tcgen05"])
     ap.add_argument("--solve", default="warp", choices=["warp", "group16", "group8"])
@@ -32,6 +32,29 @@ def main():
     autotune.set_knob(autotune.KNOB_TC_PROJECTION, 2 if a.projection == "tcgen05" else 1)
     autotune.set_knob(autotune.KNOB_SOLVE_KIND, {"warp": 1, "group16": 2, "group8": 3}[a.solve])
     autotune.set_knob(autotune.KNOB_AMP2SH_KIND, ["auto", "row", "tile", "mma"].index(a.amp2sh_kernel))
+    if a.method == "msmt":  # 3-tissue MSMT-CSD on a 4-shell scheme (6 b=0 + 30/45/60 DW)
+        from . import msmt
+        s = msmt.MSMTShared(synth.msmt_scheme())
+        s.set_responses([synth.MSMT_RESPONSES[k] for k in ("wm", "gm", "csf")])
+        s.init()
+        rng = np.random.default_rng(5)
+        n = int(np.prod(a.dims))
+        clean = synth.msmt_truth(rng, n) @ s.C.T
+        dwi = synth.rician(rng, clean, rng.uniform(1000.0 / 40, 1000.0 / 15, n)).astype(np.float32)
+        d = torch.from_numpy(dwi).cuda()
+        x, it = s.solve(d)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.reps):
+            s.solve(d, out=x, niter=it)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+        itn = it.cpu().numpy()
+        print(f"msmt: {n} voxels in {ms:.3f} ms per call ({n / ms / 1e3:.2f}M voxels/s), solver rounds mean "
+              f"{itn.mean():.2f} max {itn.max()}")
+        return
     from .warmstart import WarmStartNet
     ndw, nb0 = (60, 6) if a.lmax <= 8 else (90, 8)
     v = synth.make_volume(tuple(a.dims), nb0, ndw, (15.0, 40.0), a.lmax, None, 5)

@@ -264,3 +264,62 @@ def load_hr_dirs() -> np.ndarray:
     import os
     p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "electrostatic_repulsion_300.txt")
     return np.loadtxt(p, dtype=np.float64)
+
+
+# ---- multi-shell, multi-tissue synthetic data (dwi2fod msmt_csd) ----------
+
+# Per-tissue responses on the shells b = 0, 1000, 2000, 3000 (rows), even
+# zonal coefficients l = 0, 2, .. (columns): white matter (anisotropic),
+# grey matter and CSF (isotropic).  Invented, of the usual shape.
+MSMT_BVALUES = (0.0, 1000.0, 2000.0, 3000.0)
+MSMT_RESPONSES = {
+    "wm": np.array([[3000.0, 0.0, 0.0, 0.0, 0.0],
+                    [1900.0, -650.0, 170.0, -30.0, 4.0],
+                    [1300.0, -700.0, 290.0, -85.0, 18.0],
+                    [950.0, -640.0, 340.0, -130.0, 35.0]]),
+    "gm": np.array([[2600.0], [1150.0], [620.0], [380.0]]),
+    "csf": np.array([[4200.0], [1550.0], [580.0], [230.0]]),
+}
+
+
+def msmt_scheme(n_b0: int = 6, ndir=(30, 45, 60)) -> np.ndarray:
+    """b = 0 volumes then one shell per entry of ``ndir`` at b = 1000, 2000,
+    3000 (Fibonacci hemispheres, each shell rotated about z)."""
+    rows = [np.zeros((n_b0, 4))]
+    for s, nd in enumerate(ndir):
+        d = fibonacci_hemisphere(nd)
+        a = 0.37 * (s + 1)
+        rot = np.array([[math.cos(a), -math.sin(a), 0.0], [math.sin(a), math.cos(a), 0.0], [0.0, 0.0, 1.0]])
+        rows.append(np.hstack([d @ rot.T, np.full((nd, 1), MSMT_BVALUES[s + 1])]))
+    return np.vstack(rows)
+
+
+def msmt_truth(rng: np.random.Generator, nv: int, lmax: int = 8) -> np.ndarray:
+    """[nv][nSH(lmax) + 2] true parameters: a white-matter ODF (fraction x the
+    SH of 1-3 fibre deltas, truncated at lmax), grey matter, CSF; fractions
+    Dirichlet(1, 1, 1), every tenth voxel pure CSF or pure grey matter."""
+    from . import sh
+    frac = rng.dirichlet([1.0, 1.0, 1.0], nv)
+    frac[::10] = [0.0, 0.0, 1.0]
+    frac[5::10] = [0.0, 1.0, 0.0]
+    k, u, w = _sample_fibres(rng, nv)
+    y00 = 1.0 / math.sqrt(4.0 * math.pi)
+    out = np.zeros((nv, sh.n_for_l(lmax) + 2))
+    for f in range(3):
+        d = u[:, f]
+        azel = np.stack([np.arctan2(d[:, 1], d[:, 0]), np.arccos(np.clip(d[:, 2], -1, 1))], axis=1)
+        Y = sh.init_transform(azel, lmax)
+        out[:, :-2] += (w[:, f] * (f < k))[:, None] * Y
+    out[:, :-2] *= frac[:, :1]
+    out[:, -2] = frac[:, 1] * y00
+    out[:, -1] = frac[:, 2] * y00
+    return out
+
+
+def rician(rng: np.random.Generator, clean: np.ndarray, sigma) -> np.ndarray:
+    sigma = np.asarray(sigma, np.float64)
+    if sigma.ndim == 1:
+        sigma = sigma[:, None]
+    re = clean + rng.normal(size=clean.shape) * sigma
+    im = rng.normal(size=clean.shape) * sigma
+    return np.sqrt(re * re + im * im)

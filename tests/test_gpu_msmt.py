@@ -1,0 +1,132 @@
+"""The batched GPU ICLS solver (csd_icls_create / csd_icls_solve) and
+multi-shell multi-tissue CSD on it, against the reference's golden ICLS
+vectors (testing/cmd/testing_unit_tests_icls.cpp, with its isApprox 1e-6
+test) and the FP64 restatements (oracle/icls_ref.py, oracle/msmt_ref.py).
+Outputs are float32: tolerances are relative to the voxel's largest
+parameter, 1e-5 (p99) and 1e-4 (max)."""
+import os
+
+import numpy as np
+import pytest
+
+from mrtrix3_b200 import msmt, synth
+from oracle import icls_ref, msmt_ref
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "icls_golden.npz"))
+RESP = [synth.MSMT_RESPONSES["wm"], synth.MSMT_RESPONSES["gm"], synth.MSMT_RESPONSES["csf"]]
+
+
+def _rows(cuda, b, n):
+    import torch
+    return torch.from_numpy(np.tile(np.asarray(b, np.float32), (n, 1))).to(cuda)
+
+
+@pytest.mark.parametrize("case", ["eq_t", "eq_zero", "ineq_t", "ineq_zero", "stacked"])
+def test_icls_golden_vectors(cuda, case):
+    G = GOLD
+    H, Ai, Ae = G["problem_matrix"], G["inequality_constraint_matrix"], G["equality_constraint_matrix"]
+    ti, te = G["inequality_constraint_vector"], G["equality_constraint_vector"]
+    if case == "eq_t":
+        P, want = msmt.ICLSProblem(H, np.vstack([Ai, Ae]), np.concatenate([ti, te]), num_eq=10), G["solution"]
+    elif case == "eq_zero":
+        P, want = msmt.ICLSProblem(H, np.vstack([Ai, Ae]), None, num_eq=10), G["solution_zero"]
+    elif case == "ineq_t":
+        P, want = msmt.ICLSProblem(H, Ai, ti), G["solution_no_eq"]
+    elif case == "ineq_zero":
+        P, want = msmt.ICLSProblem(H, Ai), G["solution_no_eq_zero"]
+    else:
+        A = np.vstack([Ai, Ae])
+        P, want = msmt.ICLSProblem(H, A, np.concatenate([ti, te]), num_eq=10), G["solution"]
+    # the problem vector is stored in float32 for the device: compare with the
+    # oracle on the same rounded vector, and with the golden solution
+    b32 = G["problem_vector"].astype(np.float32)
+    x, it = P.solve(_rows(cuda, b32, 37))
+    x = x.cpu().numpy().astype(np.float64)
+    it = it.cpu().numpy()
+    assert (it >= 0).all() and (it == it[0]).all()
+    for row in x:
+        assert icls_ref.is_approx(row, want, 1e-5)  # float32 b and x: the golden 1e-6 holds in FP64 (CPU test)
+    ref = icls_ref.Problem(H, np.vstack([Ai, Ae]) if case in ("eq_t", "eq_zero", "stacked") else Ai,
+                           None if case in ("eq_zero", "ineq_zero") else
+                           (np.concatenate([ti, te]) if case in ("eq_t", "stacked") else ti),
+                           num_eq=10 if case in ("eq_t", "eq_zero", "stacked") else 0)
+    xr, itr = icls_ref.solve(ref, b32.astype(np.float64))
+    assert icls_ref.is_approx(x[0], xr, 1e-6)
+    assert it[0] == itr
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_icls_batch_of_different_problems_vectors(cuda, seed):
+    """Non-negative least squares, one right-hand side a row."""
+    import torch
+    rng = np.random.default_rng(seed)
+    H = rng.normal(size=(60, 20))
+    P = msmt.ICLSProblem(H, np.eye(20))
+    ref = icls_ref.Problem(H, np.eye(20))
+    b = rng.normal(size=(257, 60)).astype(np.float32)
+    x, it = P.solve(torch.from_numpy(b).to(cuda))
+    x, it = x.cpu().numpy(), it.cpu().numpy()
+    same = 0
+    for i in range(len(b)):
+        xr, itr = icls_ref.solve(ref, b[i].astype(np.float64))
+        assert np.max(np.abs(x[i] - xr)) <= 1e-5 * max(1.0, np.abs(xr).max())
+        # with tol = 0 the last round stops on the sign of a multiplier's
+        # residual that is zero in exact arithmetic: rounding may add a round
+        # that changes nothing
+        assert abs(int(it[i]) - int(itr)) <= 1
+        same += it[i] == itr
+    assert same >= 0.8 * len(b)
+
+
+def _msmt_case(n, seed):
+    s = msmt.MSMTShared(synth.msmt_scheme())
+    s.set_responses(RESP)
+    s.init()
+    P = msmt_ref.problem(s.grad, s.shells, RESP, [8, 0, 0], s.HR_dirs)
+    rng = np.random.default_rng(seed)
+    truth = synth.msmt_truth(rng, n)
+    clean = truth @ P.H.T
+    sigma = rng.uniform(1000.0 / 40, 1000.0 / 15, n)
+    dwi = synth.rician(rng, clean, sigma).astype(np.float32)
+    return s, P, dwi
+
+
+def _rel(x, r):
+    return np.abs(x - r).max(1) / np.maximum(np.abs(r).max(1), 1e-30)
+
+
+def test_msmt_matches_oracle(cuda):
+    import torch
+    s, P, dwi = _msmt_case(3000, 21)
+    x, it = s.solve(torch.from_numpy(dwi).to(cuda))
+    torch.cuda.synchronize()
+    x, it = x.cpu().numpy().astype(np.float64), it.cpu().numpy()
+    assert x.shape == (3000, 47) and (it >= 1).any()
+    idx = np.arange(0, 3000, 10)
+    xr, itr = msmt_ref.solve(P, dwi[idx].astype(np.float64))
+    rel = _rel(x[idx], xr)
+    assert np.percentile(rel, 99) <= 1e-5 and rel.max() <= 1e-4
+    assert np.mean(it[idx] == itr) >= 0.9
+    assert (it <= s.max_niter()).all()
+    wm, gm, csf = s.split(x)
+    assert wm.shape[1] == 45 and gm.shape[1] == 1 and csf.shape[1] == 1
+
+
+def test_msmt_mask_nonfinite_and_layout(cuda):
+    import torch
+    s, P, dwi = _msmt_case(300, 22)
+    dwi[7, 3] = np.nan
+    mask = np.ones(300, np.uint8)
+    mask[::3] = 0
+    # volume-major storage: voxel stride 1, volume stride n
+    d = torch.from_numpy(np.ascontiguousarray(dwi.T)).to(cuda).t()
+    x, it = s.solve(d, mask=torch.from_numpy(mask).to(cuda))
+    x, it = x.cpu().numpy().astype(np.float64), it.cpu().numpy()
+    assert not x[mask == 0].any() and (it[mask == 0] == 0).all()
+    assert np.isnan(x[7]).all()
+    live = np.nonzero(mask)[0]
+    live = live[(live != 7)][:60]
+    xr, _ = msmt_ref.solve(P, dwi[live].astype(np.float64))
+    assert _rel(x[live], xr).max() <= 1e-4

@@ -249,7 +249,8 @@ int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t
  * A as equalities; H [nmeas][nparam], A [ncons][nparam] row-major host FP64,
  * t [ncons] or NULL (zeros); solution_reg scales the largest diagonal entry
  * of H^T H added to its diagonal, constraint_reg is added to the diagonal of
- * the active-set systems; max_niter 0 = 10 nparam; tol the violation below
+ * the active-set systems (nparam <= 256, ncons <= 4096, nmeas <= 4096, num_eq
+ * <= 512); max_niter 0 = 10 nparam; tol the violation below
  * -tol that activates a constraint.  Set-up in FP64 on the host, tables
  * uploaded to the current device.  Errors: CSD_ERR_INVALID (sizes, H^T H not
  * positive definite, a zero constraint row).

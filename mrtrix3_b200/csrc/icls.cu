@@ -18,7 +18,9 @@
 // The reference refactors B_a B_a^T from scratch for every solve, its rows in
 // constraint order.  Here the rows are kept in activation order and the
 // factor grows by one row per activation (a forward substitution, O(a^2));
-// removing row p recomputes rows p.. only.  The multipliers are the same
+// removing row p recomputes rows p.. only.  The factor's first 48 rows (the
+// active sets of multi-tissue CSD stay below the 47 parameters, in practice)
+// live in shared memory, later rows in a per-warp global scratch.  The multipliers are the same
 // (to rounding); ties in the choice of the constraint to drop still go to the
 // lowest constraint index, as the reference's ascending scan does.
 #include <cuda_runtime.h>
@@ -53,12 +55,21 @@ namespace {
 
 constexpr int kIclsWarps = 4;  // warps per block
 constexpr int kIclsMaxActive = 512;
+constexpr int kIclsMaxParam = 256;
+constexpr int kIclsSmemRows = 48;  // factor rows kept in shared memory (packed); later rows in global scratch
+constexpr int kIclsSmemFactor = kIclsSmemRows * (kIclsSmemRows + 1) / 2;
 
 // per-warp shared memory, in doubles: b, y_u, c_u, c, lam_prev, l, r (work,
 // max(ncons, nparam)), inv (the factor's reciprocal diagonal), then act and
 // pos (2 ncons ints in ncons doubles)
 __host__ __device__ inline size_t icls_warp_doubles(int nmeas, int nparam, int ncons) {
-  return (size_t)nmeas + nparam + 6 * (size_t)ncons + (size_t)(ncons > nparam ? ncons : nparam);
+  return (size_t)nmeas + nparam + 6 * (size_t)ncons + (size_t)(ncons > nparam ? ncons : nparam) + kIclsSmemFactor;
+}
+
+// Element (i, j <= i) of the active-set factor: rows below kIclsSmemRows
+// packed in shared memory, later rows row-major in the warp's global scratch.
+__device__ __forceinline__ double& lref(double* Ls, double* Lg, int ld, int i, int j) {
+  return i < kIclsSmemRows ? Ls[i * (i + 1) / 2 + j] : Lg[(long long)i * ld + j];
 }
 
 struct IclsArgs {
@@ -80,36 +91,72 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Appends row k of the active-set factor for constraint q: z = L^-1 S[k][0..k)
-// by column-oriented forward substitution (Lc column-major: Lc[j ld + i] =
-// L[i][j]; Lr row-major), then L[k][k] = sqrt(S_kk - |z|^2).
-__device__ __forceinline__ void factor_append(const IclsArgs& a, double* Lc, double* Lr, double* inv, double* r, const int* act,
-                              int k, int q, int lane) {
+// Appends row k of the active-set factor for constraint q: w = L^-1 S[k][0..k)
+// by column-oriented forward substitution, L[k][k] = sqrt(S_kk - |w|^2), and
+// extends z = L^-1 rhs by its new entry z_k = (rhs_q - w . z) / L[k][k].
+__device__ __forceinline__ void factor_append(const IclsArgs& a, double* Ls, double* Lg, double* inv, double* r,
+                                              double* z, const int* act, int k, int q, double rhs, int lane) {
   const double* Gq = a.G + (long long)q * a.ncons;
   for (int p = lane; p < k; p += 32) r[p] = Gq[act[p]];
   __syncwarp();
   for (int j = 0; j < k; ++j) {
-    const double zj = r[j] * inv[j];
+    const double wj = r[j] * inv[j];
     __syncwarp();
-    for (int i = j + 1 + lane; i < k; i += 32) r[i] -= Lc[(long long)j * a.ld + i] * zj;
-    if (lane == 0) r[j] = zj;
+    for (int i = j + 1 + lane; i < k; i += 32) r[i] -= lref(Ls, Lg, a.ld, i, j) * wj;
+    if (lane == 0) r[j] = wj;
     __syncwarp();
   }
-  double s = 0.0;
+  double s = 0.0, t = 0.0;
   for (int p = lane; p < k; p += 32) {
-    const double z = r[p];
-    s = fma(z, z, s);
-    Lc[(long long)p * a.ld + k] = z;
-    Lr[(long long)k * a.ld + p] = z;
+    const double w = r[p];
+    s = fma(w, w, s);
+    t = fma(w, z[p], t);
+    lref(Ls, Lg, a.ld, k, p) = w;
   }
   s = warp_sum(s);
+  t = warp_sum(t);
   const double d = sqrt(Gq[q] + a.reg - s);
   if (lane == 0) {
-    Lc[(long long)k * a.ld + k] = d;
-    Lr[(long long)k * a.ld + k] = d;
+    lref(Ls, Lg, a.ld, k, k) = d;
     inv[k] = 1.0 / d;
+    z[k] = (rhs - t) / d;
   }
   __syncwarp();
+}
+
+// Removes row p of the na-row factor: Givens rotations of columns (c, c + 1),
+// c = p .. na - 2, zero the diagonal of row c + 1 into column c (rows below
+// rotated alike, and z with them: L z = rhs stays true without equation p);
+// then rows p + 1.. move up one.
+__device__ __forceinline__ void factor_remove(const IclsArgs& a, double* Ls, double* Lg, double* inv, double* z,
+                                              int p, int na, int lane) {
+  for (int c = p; c + 1 < na; ++c) {
+    const int r0 = c + 1;
+    const double x = lref(Ls, Lg, a.ld, r0, c), y = lref(Ls, Lg, a.ld, r0, r0);
+    const double h = hypot(x, y);
+    const double cs = x / h, sn = y / h;
+    __syncwarp();
+    for (int r = r0 + lane; r < na; r += 32) {
+      double& u = lref(Ls, Lg, a.ld, r, c);
+      double& v = lref(Ls, Lg, a.ld, r, c + 1);
+      const double u0 = u, v0 = v;
+      u = cs * u0 + sn * v0;
+      v = cs * v0 - sn * u0;
+    }
+    if (lane == 0) {
+      const double z0 = z[c], z1 = z[c + 1];
+      z[c] = cs * z0 + sn * z1;
+      z[c + 1] = cs * z1 - sn * z0;
+      inv[c] = 1.0 / h;
+    }
+    __syncwarp();
+  }
+  // new row i (i >= p) = old row i + 1, columns 0..i (its column i + 1 is now 0)
+  for (int i = p; i + 1 < na; ++i) {
+    // (the two rows' storage does not overlap: packed row i ends where row i + 1 begins)
+    for (int j = lane; j <= i; j += 32) lref(Ls, Lg, a.ld, i, j) = lref(Ls, Lg, a.ld, i + 1, j);
+    __syncwarp();
+  }
 }
 
 __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __grid_constant__ IclsArgs a) {
@@ -121,15 +168,15 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
   double* cu = yu + a.nparam;
   double* c = cu + a.ncons;
   double* lp = c + a.ncons;   // lambda_prev, by constraint
-  double* l = lp + a.ncons;   // multipliers, by active position
-  double* r = l + a.ncons;    // work vector
+  double* z = lp + a.ncons;   // L^-1 (-c_u[act]), by active position
+  double* r = z + a.ncons;    // work vector; the multipliers after a solve
   double* inv = r + (a.ncons > a.nparam ? a.ncons : a.nparam);  // 1 / diagonal of the factor
-  int* act = reinterpret_cast<int*>(inv + a.ncons);  // active constraints, activation order
-  int* pos = act + a.ncons;                          // position of each constraint in act, -1 if inactive
+  double* Ls = inv + a.ncons;  // factor rows < kIclsSmemRows, packed
+  int* act = reinterpret_cast<int*>(Ls + kIclsSmemFactor);  // active constraints, activation order
+  int* pos = act + a.ncons;  // position of each constraint in act, -1 if inactive
   const long long gw = (long long)blockIdx.x * kIclsWarps + warp;
   const long long nw = (long long)gridDim.x * kIclsWarps;
-  double* Lc = a.scratch + gw * 2 * (long long)a.ld * a.ld;
-  double* Lr = Lc + (long long)a.ld * a.ld;
+  double* Lg = a.scratch + gw * (long long)a.ld * a.ld;  // factor rows >= kIclsSmemRows
   const int num_ineq = a.ncons - a.num_eq;
   for (long long v = gw; v < a.n; v += nw) {
     float* xo = a.x + v * a.xs;
@@ -170,8 +217,8 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
       pos[m] = -1;
     }
     __syncwarp();
-    int na = 0;        // active rows in the factor
-    bool solved = false;  // l holds a solution (else x = y_u)
+    int na = 0;           // active rows in the factor
+    bool solved = false;  // r holds the multipliers of a solve (else x = y_u)
     // the equalities are active from the start (constrained_least_squares.h:265-266)
     for (int e = 0; e < a.num_eq; ++e) {
       const int q = num_ineq + e;
@@ -180,7 +227,7 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
         pos[q] = na;
       }
       __syncwarp();
-      factor_append(a, Lc, Lr, inv, r, act, na, q, lane);
+      factor_append(a, Ls, Lg, inv, r, z, act, na, q, -cu[q], lane);
       ++na;
     }
     int niter = 0;
@@ -215,25 +262,17 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
           pos[imin] = na;
         }
         __syncwarp();
-        factor_append(a, Lc, Lr, inv, r, act, na, imin, lane);
+        factor_append(a, Ls, Lg, inv, r, z, act, na, imin, -cu[imin], lane);
         ++na;
       }
       while (true) {
-        // l = (L L^T)^-1 (-c_u[act]): forward (column-oriented on Lc), then
-        // backward (column-oriented on L^T = rows of Lr)
-        for (int p = lane; p < na; p += 32) r[p] = -cu[act[p]];
+        // the multipliers: L^T l = z by columns of L^T (rows of L)
+        for (int p = lane; p < na; p += 32) r[p] = z[p];
         __syncwarp();
-        for (int j = 0; j < na; ++j) {
-          const double zj = r[j] * inv[j];
-          __syncwarp();
-          for (int i = j + 1 + lane; i < na; i += 32) r[i] -= Lc[(long long)j * a.ld + i] * zj;
-          if (lane == 0) r[j] = zj;
-          __syncwarp();
-        }
         for (int j = na - 1; j >= 0; --j) {
           const double lj = r[j] * inv[j];
           __syncwarp();
-          for (int i = lane; i < j; i += 32) r[i] -= Lr[(long long)j * a.ld + i] * lj;
+          for (int i = lane; i < j; i += 32) r[i] -= lref(Ls, Lg, a.ld, j, i) * lj;
           if (lane == 0) r[j] = lj;
           __syncwarp();
         }
@@ -243,7 +282,6 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
         for (int p = lane; p < na; p += 32) {
           const int n = act[p];
           const double lv = r[p];
-          l[p] = lv;
           if (n < num_ineq && lv < 0.0) {
             const double s = lp[n] / (lp[n] - lv);
             if (s < smin || (s == smin && n < sidx)) {
@@ -269,8 +307,9 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
           solved = true;
           break;
         }
-        // drop it: shift the later rows down and rebuild their factor rows
+        // drop it: rotate its row out of the factor, shift the later rows
         changed = true;
+        factor_remove(a, Ls, Lg, inv, z, spos, na, lane);
         const int nact = na - 1;
         if (lane == 0) pos[sidx] = -1;
         for (int p0 = spos; p0 < nact; p0 += 32) {
@@ -285,16 +324,15 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
         }
         __syncwarp();
         na = nact;
-        for (int k = spos; k < na; ++k) factor_append(a, Lc, Lr, inv, r, act, k, act[k], lane);
       }
       // lambda_prev: the new multipliers on the active inequalities, 0 elsewhere
-      for (int m = lane; m < num_ineq; m += 32) lp[m] = pos[m] >= 0 ? l[pos[m]] : 0.0;
+      for (int m = lane; m < num_ineq; m += 32) lp[m] = pos[m] >= 0 ? r[pos[m]] : 0.0;
       __syncwarp();
       ++niter;
       if (!changed || niter > a.max_niter) break;
       for (int m = lane; m < a.ncons; m += 32) {
         double s = cu[m];
-        for (int p = 0; p < na; ++p) s = fma(a.G[(long long)act[p] * a.ncons + m], l[p], s);
+        for (int p = 0; p < na; ++p) s = fma(a.G[(long long)act[p] * a.ncons + m], r[p], s);
         c[m] = s;
       }
       __syncwarp();
@@ -304,13 +342,24 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
       if (a.niter && lane == 0) a.niter[v] = -1;
       continue;
     }
-    // x = y_u + B_a^T l, then L^T z = x by back substitution (rows of L)
-    for (int j = lane; j < a.nparam; j += 32) {
-      double s = yu[j];
-      if (solved)
-        for (int p = 0; p < na; ++p) s = fma(a.B[(long long)act[p] * a.nparam + j], l[p], s);
-      r[j] = s;
+    // x = y_u + B_a^T l (into registers: r still holds l), then L^T z = x by
+    // back substitution (rows of L)
+    double xj[kIclsMaxParam / 32];
+#pragma unroll
+    for (int h = 0; h < kIclsMaxParam / 32; ++h) {
+      const int j = lane + 32 * h;
+      xj[h] = 0.0;
+      if (j < a.nparam) {
+        double s = yu[j];
+        if (solved)
+          for (int p = 0; p < na; ++p) s = fma(a.B[(long long)act[p] * a.nparam + j], r[p], s);
+        xj[h] = s;
+      }
     }
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < kIclsMaxParam / 32; ++h)
+      if (lane + 32 * h < a.nparam) r[lane + 32 * h] = xj[h];
     __syncwarp();
     for (int j = a.nparam - 1; j >= 0; --j) {
       const double zj = r[j] / a.L[(long long)j * a.nparam + j];
@@ -366,7 +415,7 @@ extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const dou
                                int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol,
                                csd_icls** out) {
   if (!out || !H || !A || nmeas < 1 || nparam < 1 || ncons < 1 || num_eq < 0 || num_eq > ncons ||
-      solution_reg < 0.0 || constraint_reg < 0.0 || tol < 0.0 || max_niter < 0 || ncons > 4096 || nparam > 1024 ||
+      solution_reg < 0.0 || constraint_reg < 0.0 || tol < 0.0 || max_niter < 0 || ncons > 4096 || nparam > kIclsMaxParam ||
       nmeas > 4096 || num_eq > kIclsMaxActive)
     return csdb200::set_error(CSD_ERR_INVALID, "csd_icls_create: invalid argument");
   *out = nullptr;
@@ -475,11 +524,11 @@ extern "C" int csd_icls_solve(csd_icls* p, const float* b, int64_t n, int64_t vo
   const int ld = std::min(p->ncons, kIclsMaxActive);
   const size_t warps = (size_t)blocks * kIclsWarps;
   if (warps > p->scratch_warps) {
-    // the factor of each warp's active set, twice (column- and row-major)
+    // each warp's factor rows beyond the shared-memory part (row-major, ld)
     cudaFree(p->d_scratch);
     p->d_scratch = nullptr;
     p->scratch_warps = 0;
-    e = cudaMalloc(&p->d_scratch, warps * 2 * (size_t)ld * ld * sizeof(double));
+    e = cudaMalloc(&p->d_scratch, warps * (size_t)ld * ld * sizeof(double));
     if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_icls_solve: ") + cudaGetErrorString(e));
     p->scratch_warps = warps;
   }

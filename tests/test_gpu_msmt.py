@@ -130,3 +130,28 @@ def test_msmt_mask_nonfinite_and_layout(cuda):
     live = live[(live != 7)][:60]
     xr, _ = msmt_ref.solve(P, dwi[live].astype(np.float64))
     assert _rel(x[live], xr).max() <= 1e-4
+
+
+def test_icls_active_sets_beyond_the_shared_memory_rows(cuda):
+    """Non-negative least squares whose unconstrained solution is negative
+    almost everywhere: 60-80 active constraints, so the factor's rows past
+    the 48 kept in shared memory (and the Givens removals across that
+    boundary) are exercised."""
+    import torch
+    rng = np.random.default_rng(9)
+    H = rng.normal(size=(150, 80))
+    P = msmt.ICLSProblem(H, np.eye(80))
+    ref = icls_ref.Problem(H, np.eye(80))
+    u = rng.uniform(0.5, 1.5, size=(33, 80))
+    u[:, ::7] *= -1.0  # a few coordinates stay free
+    b = (-(u @ H.T) + rng.normal(scale=0.05, size=(33, 150))).astype(np.float32)
+    x, it = P.solve(torch.from_numpy(b).to(cuda))
+    x, it = x.cpu().numpy(), it.cpu().numpy()
+    big = 0
+    for i in range(len(b)):
+        tr = []
+        xr, itr = icls_ref.solve(ref, b[i].astype(np.float64), trace=tr)
+        big += max(len(t) for t in tr) > 48
+        assert np.max(np.abs(x[i] - xr)) <= 1e-5 * max(1.0, np.abs(xr).max())
+        assert abs(int(it[i]) - int(itr)) <= 1
+    assert big == len(b)

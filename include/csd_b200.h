@@ -259,9 +259,11 @@ int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t
  * right-hand sides b (device float, [n][voxel_stride], measurements
  * meas_stride apart), FP64 inside: x (device float [n][x_stride], x_stride
  * >= nparam), niter (device int32 [n] or NULL: the solver's rounds; -1 where
- * an active set outgrew 512 rows, with x NaN).  mask (device uint8 [n] or
- * NULL): 0 skips the voxel (x = 0).  A non-finite b gives x = NaN.  Returns
- * without synchronising; grows a per-warp scratch buffer on first use. */
+ * an active set outgrew 512 rows, with x NaN), pred (device float [n]
+ * [pred_stride] or NULL: the predicted measurements H x, dwi2fod msmt_csd's
+ * -predicted_signal).  mask (device uint8 [n] or NULL): 0 skips the voxel
+ * (x = 0, pred = 0).  A non-finite b gives x = NaN.  Returns without
+ * synchronising; grows a per-warp scratch buffer on first use. */
 typedef struct csd_icls csd_icls;
 int csd_icls_create(const double* H, int nmeas, int nparam, const double* A, int ncons, const double* t,
                     int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol,
@@ -270,7 +272,8 @@ void csd_icls_destroy(csd_icls* problem);
 /* out4 = {nmeas, nparam, ncons, max_niter} */
 int csd_icls_info(const csd_icls* problem, int* out4);
 int csd_icls_solve(csd_icls* problem, const float* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
-                   const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, void* stream);
+                   const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, float* pred,
+                   int64_t pred_stride, void* stream);
 
 /* Launch-shape knobs (process-wide), chosen by the project's autotuner
  * (mrtrix3_b200/autotune.py): which = 0 warps per block of the persistent

@@ -94,7 +94,7 @@ def lib():
         L.csd_icls_destroy.argtypes = [vp]
         L.csd_icls_destroy.restype = None
         L.csd_icls_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
-        L.csd_icls_solve.argtypes = [vp, vp, i64, i64, i64, vp, vp, i64, vp, vp]
+        L.csd_icls_solve.argtypes = [vp, vp, i64, i64, i64, vp, vp, i64, vp, vp, i64, vp]
         L.csd_sh2peaks.argtypes = [vp, i64, i64, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                    vp, ctypes.c_int, vp, vp, vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]

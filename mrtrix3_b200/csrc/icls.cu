@@ -47,6 +47,7 @@ struct csd_icls {
   double* d_G = nullptr;     // [ncons][ncons]
   double* d_t = nullptr;     // [ncons] or null
   double* d_L = nullptr;     // [nparam][nparam], lower, row-major
+  double* d_H = nullptr;     // [nmeas][nparam] (the predicted measurements H x)
   double* d_scratch = nullptr;  // per warp: two copies of the active-set factor
   size_t scratch_warps = 0;
 };
@@ -79,7 +80,9 @@ struct IclsArgs {
   float* x;
   long long xs;
   int* niter;
-  const double *b2dT, *B, *G, *t, *L;
+  float* pred;
+  long long ps;
+  const double *b2dT, *B, *G, *t, *L, *H;
   double* scratch;
   int nmeas, nparam, ncons, num_eq, max_niter, ld;
   double reg, tol;
@@ -182,6 +185,8 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
     float* xo = a.x + v * a.xs;
     if (a.mask && !a.mask[v]) {
       for (int j = lane; j < a.nparam; j += 32) xo[j] = 0.f;
+      if (a.pred)
+        for (int i = lane; i < a.nmeas; i += 32) a.pred[v * a.ps + i] = 0.f;
       if (a.niter && lane == 0) a.niter[v] = 0;
       continue;
     }
@@ -195,6 +200,8 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
     if (!__all_sync(0xffffffffu, finite)) {
       // a non-finite measurement propagates through b2d^T b to every output
       for (int j = lane; j < a.nparam; j += 32) xo[j] = __int_as_float(0x7fffffff);
+      if (a.pred)
+        for (int i = lane; i < a.nmeas; i += 32) a.pred[v * a.ps + i] = __int_as_float(0x7fffffff);
       if (a.niter && lane == 0) a.niter[v] = 0;
       continue;
     }
@@ -339,6 +346,8 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
     }
     if (fail) {
       for (int j = lane; j < a.nparam; j += 32) xo[j] = __int_as_float(0x7fffffff);
+      if (a.pred)
+        for (int i = lane; i < a.nmeas; i += 32) a.pred[v * a.ps + i] = __int_as_float(0x7fffffff);
       if (a.niter && lane == 0) a.niter[v] = -1;
       continue;
     }
@@ -369,6 +378,13 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
       __syncwarp();
     }
     for (int j = lane; j < a.nparam; j += 32) xo[j] = (float)r[j];
+    if (a.pred)  // the predicted measurements H x (MSMT_Processor's -predicted_signal, dwi2fod.cpp:212-216)
+      for (int i = lane; i < a.nmeas; i += 32) {
+        const double* h = a.H + (long long)i * a.nparam;
+        double s = 0.0;
+        for (int j = 0; j < a.nparam; ++j) s = fma(h[j], r[j], s);
+        a.pred[v * a.ps + i] = (float)s;
+      }
     if (a.niter && lane == 0) a.niter[v] = niter;
     __syncwarp();
   }
@@ -469,6 +485,7 @@ extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const dou
     if (e == cudaSuccess) e = upload(&p->d_B, B);
     if (e == cudaSuccess) e = upload(&p->d_G, G);
     if (e == cudaSuccess) e = upload(&p->d_L, L);
+    if (e == cudaSuccess) e = upload(&p->d_H, std::vector<double>(H, H + (size_t)nmeas * nparam));
     if (e == cudaSuccess && t) e = upload(&p->d_t, tt);
     if (e != cudaSuccess) {
       csd_icls_destroy(p);
@@ -488,6 +505,7 @@ extern "C" void csd_icls_destroy(csd_icls* p) {
   cudaFree(p->d_G);
   cudaFree(p->d_t);
   cudaFree(p->d_L);
+  cudaFree(p->d_H);
   cudaFree(p->d_scratch);
   delete p;
 }
@@ -502,8 +520,9 @@ extern "C" int csd_icls_info(const csd_icls* p, int* out4) {
 }
 
 extern "C" int csd_icls_solve(csd_icls* p, const float* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
-                              const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, void* stream) {
-  if (!p || n < 0 || (n > 0 && (!b || !x)) || x_stride < p->nparam)
+                              const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, float* pred,
+                              int64_t pred_stride, void* stream) {
+  if (!p || n < 0 || (n > 0 && (!b || !x)) || x_stride < p->nparam || (pred && pred_stride < p->nmeas))
     return csdb200::set_error(CSD_ERR_INVALID, "csd_icls_solve: invalid argument");
   if (n == 0) return CSD_OK;
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -541,6 +560,9 @@ extern "C" int csd_icls_solve(csd_icls* p, const float* b, int64_t n, int64_t vo
   a.x = x;
   a.xs = x_stride;
   a.niter = niter;
+  a.pred = pred;
+  a.ps = pred_stride;
+  a.H = p->d_H;
   a.b2dT = p->d_b2dT;
   a.B = p->d_B;
   a.G = p->d_G;

@@ -248,11 +248,12 @@ class MSMTShared:
         except Exception:
             pass
 
-    def solve(self, dwi, mask=None, out=None, niter=None, stream=None):
+    def solve(self, dwi, mask=None, out=None, niter=None, predicted=None, stream=None):
         """MSMT_Processor over every row of ``dwi`` (device float32 [n][volumes],
         any strides): the concatenated tissue ODFs, device float32 [n][N], and
-        the solver's rounds per voxel (device int32 [n])."""
-        return icls_solve(self.handle, dwi, int(sum(self.nparams())), mask, out, niter, stream)
+        the solver's rounds per voxel (device int32 [n]); ``predicted``
+        (device float32 [n][volumes], optional) receives C x."""
+        return icls_solve(self.handle, dwi, int(sum(self.nparams())), mask, out, niter, stream, predicted)
 
     def split(self, x):
         """The per-tissue parts of a [.., N] solution."""
@@ -263,7 +264,7 @@ class MSMTShared:
         return out
 
 
-def icls_solve(handle, b, nparam: int, mask=None, out=None, niter=None, stream=None):
+def icls_solve(handle, b, nparam: int, mask=None, out=None, niter=None, stream=None, predicted=None):
     import torch
     if b.dim() != 2 or b.dtype != torch.float32 or not b.is_cuda:
         raise ValueError("icls_solve: b must be a float32 CUDA tensor [n][measurements]")
@@ -274,10 +275,17 @@ def icls_solve(handle, b, nparam: int, mask=None, out=None, niter=None, stream=N
         niter = torch.empty(n, dtype=torch.int32, device=b.device)
     if mask is not None:
         mask = mask.to(torch.uint8)
+    if predicted is not None and (predicted.dtype != torch.float32 or predicted.dim() != 2 or
+                                  predicted.shape[0] != n or predicted.stride(1) != 1 or
+                                  predicted.device != b.device):
+        raise ValueError("icls_solve: predicted must be float32 [n][>= measurements] with contiguous rows")
     csd.check(csd.lib().csd_icls_solve(handle, ctypes.c_void_p(b.data_ptr()), n, b.stride(0), b.stride(1),
                                        ctypes.c_void_p(mask.data_ptr()) if mask is not None else None,
                                        ctypes.c_void_p(out.data_ptr()), out.stride(0),
-                                       ctypes.c_void_p(niter.data_ptr()), ctypes.c_void_p(csd._stream_ptr(stream))))
+                                       ctypes.c_void_p(niter.data_ptr()),
+                                       ctypes.c_void_p(predicted.data_ptr()) if predicted is not None else None,
+                                       predicted.stride(0) if predicted is not None else 0,
+                                       ctypes.c_void_p(csd._stream_ptr(stream))))
     return out, niter
 
 
@@ -298,8 +306,8 @@ class ICLSProblem:
                                             float(tol), ctypes.byref(h)))
         self._h = h
 
-    def solve(self, b, mask=None, out=None, niter=None, stream=None):
-        return icls_solve(self._h, b, self.nparam, mask, out, niter, stream)
+    def solve(self, b, mask=None, out=None, niter=None, stream=None, predicted=None):
+        return icls_solve(self._h, b, self.nparam, mask, out, niter, stream, predicted)
 
     def __del__(self):
         try:

@@ -155,3 +155,62 @@ def test_icls_active_sets_beyond_the_shared_memory_rows(cuda):
         assert np.max(np.abs(x[i] - xr)) <= 1e-5 * max(1.0, np.abs(xr).max())
         assert abs(int(it[i]) - int(itr)) <= 1
     assert big == len(b)
+
+
+def test_dwi2fod_msmt_csd_command_line(cuda, tmp_path):
+    """``dwi2fod msmt_csd`` on .mif files: one output per tissue (float32,
+    SH axis contiguous, the gradient table in prior_dw_scheme), equal voxel
+    for voxel to the library call, near the oracle; -mask, -lmax and
+    -predicted_signal."""
+    import torch
+    from mrtrix3_b200 import mif
+    from mrtrix3_b200.dwi2fod import run
+    s, P, dwi = _msmt_case(7 * 6 * 5, 23)
+    dims = (7, 6, 5)
+    data = dwi.reshape(dims[2], dims[1], dims[0], -1).transpose(2, 1, 0, 3)
+    mask = np.ones(dims[::-1], np.uint8)
+    mask[0, 0, :] = 0
+    p_dwi, p_mask = str(tmp_path / "dwi.mif"), str(tmp_path / "mask.mif")
+    mif.write(p_dwi, mif.Image(data=data, vox=[2.0, 2.0, 2.0, 1.0], transform=np.eye(4)[:3],
+                               keyval={"dw_scheme": mif.scheme_to_text(s.grad), "pe_scheme": "0,1,0,0.05"}),
+              layout=[-2, 3, 4, 1])
+    mif.write(p_mask, mif.Image(data=mask.transpose(2, 1, 0).astype(np.float64), vox=[2.0, 2.0, 2.0]),
+              datatype="UInt8")
+    resp = []
+    for k in ("wm", "gm", "csf"):
+        f = tmp_path / f"{k}.txt"
+        np.savetxt(f, synth.MSMT_RESPONSES[k])
+        resp.append(str(f))
+    outs = [str(tmp_path / f"{k}.mif") for k in ("wm", "gm", "csf")]
+    pred_path = str(tmp_path / "pred.mif")
+    args = ["msmt_csd", p_dwi, resp[0], outs[0], resp[1], outs[1], resp[2], outs[2], "-mask", p_mask,
+            "-predicted_signal", pred_path]
+    assert run(args) == 0
+    imgs = [mif.read(o) for o in outs]
+    assert [i.data.shape[3] for i in imgs] == [45, 1, 1]
+    for i in imgs:
+        assert i.layout[3] == 1 and i.datatype.startswith("Float32")
+        assert "dw_scheme" not in i.keyval and i.keyval["pe_scheme"] == "0,1,0,0.05"
+        np.testing.assert_allclose(mif.parse_scheme(i.keyval["prior_dw_scheme"]), s.grad)
+    got = np.concatenate([i.data.transpose(2, 1, 0, 3).reshape(-1, i.data.shape[3]) for i in imgs], axis=1)
+    flat_mask = mask.reshape(-1)
+    x, _ = s.solve(torch.from_numpy(dwi).to(cuda), mask=torch.from_numpy(flat_mask).to(cuda))
+    # the command line re-reads the scheme from the header text and normalises
+    # it again: the problem differs from this one's in the last bits only
+    xd = x.cpu().numpy()
+    assert np.all(np.abs(got - xd) <= 1e-6 * np.abs(xd).max(1, keepdims=True))
+    assert not got[flat_mask == 0].any()
+    live = np.nonzero(flat_mask)[0][:40]
+    xr, _ = msmt_ref.solve(P, dwi[live].astype(np.float64))
+    assert _rel(got[live], xr).max() <= 1e-4
+    pred = mif.read(pred_path).data.transpose(2, 1, 0, 3).reshape(-1, dwi.shape[1]).astype(np.float64)
+    want = xr @ P.H.T
+    assert np.abs(pred[live] - want).max() <= 1e-4 * np.abs(want).max()
+    assert not pred[flat_mask == 0].any()
+    # -lmax per tissue, and the argument rules
+    assert run(args[:8] + ["-lmax", "6,0,0", "-force"]) == 0
+    assert mif.read(outs[0]).data.shape[3] == 28
+    with pytest.raises(SystemExit, match="pairs"):
+        run(["msmt_csd", p_dwi, resp[0], outs[0], resp[1]])
+    with pytest.raises(SystemExit, match="already exists"):
+        run(args[:8])

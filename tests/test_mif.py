@@ -118,8 +118,10 @@ def test_output_layout_keeps_spatial_order():
 
 
 def test_cli_rejects_other_algorithms_and_arguments():
-    with pytest.raises(SystemExit, match="only the csd"):
-        run(["msmt_csd", "a", "b", "c", "d", "e"])
+    with pytest.raises(SystemExit, match="usage"):
+        run(["sdeconv", "a", "b", "c"])
+    with pytest.raises(SystemExit, match="pairs"):
+        run(["msmt_csd", "a", "b", "c", "d"])
     with pytest.raises(SystemExit, match="single input response"):
         run(["csd", "a", "b"])
     with pytest.raises(SystemExit, match="unknown option"):

@@ -179,6 +179,94 @@ def rel_errors(fod, F64):
     return np.abs(fod.astype(np.float64) - F64).max(axis=1) / np.where(den > 0, den, 1.0)
 
 
+def next_rows(dwi_dev, sample_idx):
+    """Measurements of the paths beyond the headline, on this GPU (rank 0,
+    N = 1): multi-tissue CSD (ICLS solver) with its C FP64 baseline on the
+    host cores, and amp2sh on the benchmark volume's amplitudes."""
+    import torch
+
+    from mrtrix3_b200 import msmt, sh, synth
+    from oracle import icls_ref, msmt_ref
+    out = {}
+    # ---- msmt_csd: 64x64x32 voxels, 4 shells, 3 tissues
+    resp = [synth.MSMT_RESPONSES[k] for k in ("wm", "gm", "csf")]
+    s = msmt.MSMTShared(synth.msmt_scheme())
+    s.set_responses(resp)
+    s.init()
+    rng = np.random.default_rng(5)
+    n = 64 * 64 * 32
+    dwi = synth.rician(rng, synth.msmt_truth(rng, n) @ s.C.T, rng.uniform(1000.0 / 40, 1000.0 / 15, n))
+    dwi = dwi.astype(np.float32)
+    d = torch.from_numpy(dwi).cuda()
+    x, it = s.solve(d)
+    for _ in range(2):
+        s.solve(d, out=x, niter=it)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    reps = 3
+    for _ in range(reps):
+        s.solve(d, out=x, niter=it)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    P = msmt_ref.problem(s.grad, s.shells, resp, [8, 0, 0], s.HR_dirs)
+    idx = np.random.default_rng(1).choice(n, 500, replace=False)
+    cores = os.cpu_count() or 1
+    xr, itr = icls_ref.solve_batch_c(P, dwi[idx].astype(np.float64), nthreads=cores)
+    xg = x.cpu().numpy()[idx].astype(np.float64)
+    rel = np.abs(xg - xr).max(1) / np.abs(xr).max(1)
+    # CPU baseline: the C restatement on all host cores, a bounded sample
+    m = min(n, 400 * cores)
+    t0 = time.perf_counter()
+    icls_ref.solve_batch_c(P, dwi[:m].astype(np.float64), nthreads=cores)
+    cpu_s = time.perf_counter() - t0
+    out["msmt_csd"] = {
+        "workload": "64x64x32 synthetic voxels (no mask: 131,072), 6 b=0 + 30/45/60 directions at b=1000/2000/3000, "
+                    "3 tissues (WM lmax 8, GM, CSF: 47 parameters, 302 constraints), Rician SNR U[15,40]",
+        "value": n / (ms / 1e3), "unit": "voxels/s", "ms": ms, "dtype": "f64",
+        "solver_rounds_mean": float(it.float().mean().item()),
+        "parity": {"vs": "oracle/icls_oracle.c (FP64)", "sample_voxels": len(idx),
+                   "p99_rel_err": float(np.percentile(rel, 99)), "max_rel_err": float(rel.max()),
+                   "rounds_equal": float(np.mean(it.cpu().numpy()[idx] == itr))},
+        "cpu_baseline": {"value": m / cpu_s, "unit": "voxels/s", "cores": cores, "kind": "port",
+                         "sample": f"the first {m} voxels through oracle/icls_oracle.c (FP64, refactoring per "
+                                   f"solve as the reference), {cores} threads, {cpu_s:.1f} s"}}
+    # ---- amp2sh: the benchmark volume's 66 amplitudes a voxel, 60-direction fit at lmax 8
+    grad = synth.config5_scheme()
+    from mrtrix3_b200 import csd as C
+    sch = C.Shared(grad)
+    sch.set_response(np.array([1.0, -0.5]))
+    sch.init()
+    dwis = np.asarray(sch.dwis)
+    bz = np.nonzero(grad[:, 3] <= 10.0)[0]
+    fit = sh.pinv(sh.init_transform(sh.cartesian_to_azel(grad[dwis, :3]), 8))
+    plan = C.Amp2SHCommon(fit, dwis, bz, normalise=True)
+    y = plan(dwi_dev)
+    for _ in range(3):
+        plan(dwi_dev, y)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(10):
+        plan(dwi_dev, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_a = e0.elapsed_time(e1) / 10
+    na = dwi_dev.shape[0]
+    sel = torch.from_numpy(np.asarray(sample_idx, np.int64)).to(dwi_dev.device)
+    a = dwi_dev[sel].cpu().numpy().astype(np.float64)
+    ref = (a[:, dwis] * (len(bz) / (1.0 + a[:, bz].sum(1)))[:, None]) @ fit.T
+    got = y[sel].cpu().numpy().astype(np.float64)
+    err = np.abs(got - ref).max(1) / np.abs(ref).max(1)
+    out["amp2sh"] = {
+        "workload": f"{na} voxels x 66 volumes (the benchmark volume), 60 directions, lmax 8, -normalise",
+        "value": na / (ms_a / 1e3), "unit": "voxels/s", "ms": ms_a, "dtype": "f64",
+        "achieved_tflops_fp64": na * 2 * 45 * 60 / (ms_a / 1e3) / 1e12,
+        "achieved_gbs": na * (66 + 45) * 4 / (ms_a / 1e3) / 1e9,
+        "parity": {"vs": "numpy FP64 fit", "sample_voxels": len(sample_idx), "max_rel_err": float(err.max())}}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -186,6 +274,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-next-rows", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -350,6 +439,8 @@ def main():
             "clocks": clk.summary(), "warm_start_net": net_src}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(vol)
+    if rank == 0 and world == 1 and not args.no_next_rows:
+        line["next_rows"] = next_rows(d, np.nonzero(vol.mask)[0][:2000])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -21,7 +21,14 @@ max_niter rounds; x = L^-T y.
 """
 from __future__ import annotations
 
+import ctypes
+import os
+import subprocess
+
 import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_CLIB = None
 
 
 class Problem:
@@ -128,3 +135,39 @@ def solve(P: Problem, b, trace: list | None = None):
 def is_approx(x, y, prec: float) -> bool:
     """Eigen's isApprox: ||x - y|| <= prec * min(||x||, ||y||)."""
     return bool(np.linalg.norm(x - y) <= prec * min(np.linalg.norm(x), np.linalg.norm(y)))
+
+
+def _clib():
+    """liboracle_icls.so (oracle/icls_oracle.c): the same solver in C, threaded."""
+    global _CLIB
+    if _CLIB is None:
+        so = os.path.join(HERE, "liboracle_icls.so")
+        src = os.path.join(HERE, "icls_oracle.c")
+        if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+            subprocess.check_call(["make", "-s", "-C", HERE, so])
+        L = ctypes.CDLL(so)
+        vp = ctypes.c_void_p
+        L.oracle_icls_solve.restype = ctypes.c_int
+        L.oracle_icls_solve.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_double, vp, vp, vp, vp, vp, ctypes.c_long, vp, vp,
+                                        ctypes.c_int]
+        _CLIB = L
+    return _CLIB
+
+
+def solve_batch_c(P: Problem, b, nthreads: int = 1):
+    """solve() for every row of ``b`` by the C restatement: (x [n][nparam], niter [n])."""
+    b = np.ascontiguousarray(b, np.float64)
+    b2d = np.ascontiguousarray(P.b2d)
+    B = np.ascontiguousarray(P.B)
+    L = np.ascontiguousarray(P.L)
+    t = None if P.t is None else np.ascontiguousarray(P.t)
+    x = np.zeros((len(b), P.H.shape[1]))
+    it = np.zeros(len(b), np.int32)
+    rc = _clib().oracle_icls_solve(P.H.shape[0], P.H.shape[1], P.num_constraints, P.num_eq, P.max_niter,
+                                   P.lambda_min_norm, P.tol, b2d.ctypes.data, B.ctypes.data,
+                                   t.ctypes.data if t is not None else None, L.ctypes.data, b.ctypes.data, len(b),
+                                   x.ctypes.data, it.ctypes.data, int(nthreads))
+    if rc != 0:
+        raise RuntimeError("oracle_icls_solve failed")
+    return x, it

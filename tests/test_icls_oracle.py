@@ -86,3 +86,22 @@ def test_nonnegative_least_squares_matches_scipy(seed):
     x, _ = R.solve(R.Problem(H, np.eye(20)), b)
     ref, _ = nnls(H, b)
     np.testing.assert_allclose(x, ref, atol=1e-9)
+
+
+def test_c_restatement_matches_python():
+    """oracle/icls_oracle.c (the CPU baseline) against the numpy restatement:
+    the golden problem and non-negative least squares, several threads."""
+    P = R.Problem.with_equalities(G["problem_matrix"], G["inequality_constraint_matrix"],
+                                  G["equality_constraint_matrix"], G["inequality_constraint_vector"],
+                                  G["equality_constraint_vector"])
+    x, it = R.solve_batch_c(P, G["problem_vector"][None, :], nthreads=1)
+    assert R.is_approx(x[0], G["solution"], 1e-6)
+    rng = np.random.default_rng(4)
+    H = rng.normal(size=(60, 20))
+    Q = R.Problem(H, np.eye(20))
+    b = rng.normal(size=(40, 60))
+    xc, itc = R.solve_batch_c(Q, b, nthreads=4)
+    for i in range(len(b)):
+        xp, itp = R.solve(Q, b[i])
+        np.testing.assert_allclose(xc[i], xp, atol=1e-10)
+        assert itc[i] == itp

@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcsd_b200.so")
 
 CSD_OK = 0
+CSD_ERR_INVALID, CSD_ERR_CUDA, CSD_ERR_TIMEOUT, CSD_ERR_NOMEM, CSD_ERR_UNSUPPORTED = -1, -2, -3, -4, -5
 STATUS_MASKED, STATUS_CONVERGED, STATUS_NITER, STATUS_NONFINITE = 0, 1, 2, 3
 STATUS_FP64, STATUS_CHOLFAIL, STATUS_WARM_RESTART = 0x10, 0x20, 0x40
 

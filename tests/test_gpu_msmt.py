@@ -214,3 +214,38 @@ def test_dwi2fod_msmt_csd_command_line(cuda, tmp_path):
         run(["msmt_csd", p_dwi, resp[0], outs[0], resp[1]])
     with pytest.raises(SystemExit, match="already exists"):
         run(args[:8])
+
+
+@pytest.mark.parametrize("tissues,lmax", [(("gm", "csf"), None), (("wm", "gm", "csf"), [10, 0, 0]),
+                                          (("wm", "csf"), [6, 0])])
+def test_msmt_tissue_sets(cuda, tissues, lmax):
+    """Isotropic tissues only (2 parameters, 2 constraints), white matter at
+    lmax 10 (its response padded with zeros), two tissues."""
+    import torch
+    resp = [synth.MSMT_RESPONSES[k] for k in tissues]
+    s = msmt.MSMTShared(synth.msmt_scheme())
+    if lmax:
+        s.parse_cmdline_options(lmax=lmax)
+    s.set_responses(resp)
+    s.init()
+    want_lmax = lmax or [0] * len(tissues)
+    assert s.lmax == want_lmax
+    pad = [np.pad(r, ((0, 0), (0, max(0, L // 2 + 1 - r.shape[1]))))[:, :L // 2 + 1] for r, L in zip(resp, want_lmax)]
+    P = msmt_ref.problem(s.grad, s.shells, pad, want_lmax, s.HR_dirs)
+    rng = np.random.default_rng(31)
+    truth = synth.msmt_truth(rng, 200)
+    cols = {"wm": list(range(45)), "gm": [45], "csf": [46]}
+    x_true = np.zeros((200, P.H.shape[1]))
+    c0 = 0
+    for k, L in zip(tissues, want_lmax):
+        n = (L + 1) * (L + 2) // 2
+        src = truth[:, cols[k]]
+        x_true[:, c0:c0 + min(n, src.shape[1])] = src[:, :n]
+        c0 += n
+    dwi = synth.rician(rng, x_true @ P.H.T, 30.0).astype(np.float32)
+    x, it = s.solve(torch.from_numpy(dwi).to(cuda))
+    x = x.cpu().numpy().astype(np.float64)
+    idx = np.arange(0, 200, 4)
+    xr, itr = msmt_ref.solve(P, dwi[idx].astype(np.float64))
+    assert _rel(x[idx], xr).max() <= 1e-4
+    assert (it.cpu().numpy() >= 0).all()

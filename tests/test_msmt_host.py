@@ -105,3 +105,21 @@ def test_oracle_solutions_are_optimal():
     for i in (0, 5):
         xi, _ = icls_ref.solve(P, clean[i])
         np.testing.assert_allclose(xi[-2:], truth[i, -2:], atol=1e-6 * np.abs(truth[i]).max())
+
+
+def test_icls_create_rejects_bad_problems():
+    """Argument checks of csd_icls_create run before any device work."""
+    import ctypes
+
+    from mrtrix3_b200 import csd
+    h = ctypes.c_void_p()
+    H = np.ones((4, 2))
+    A = np.ones((3, 2))
+    L = csd.lib()
+    for args in [(H.ctypes.data, 4, 0, A.ctypes.data, 3, None, 0, 0.0, 0.0, 0, 0.0),    # no parameters
+                 (H.ctypes.data, 4, 2, A.ctypes.data, 3, None, 4, 0.0, 0.0, 0, 0.0),    # more equalities than rows
+                 (H.ctypes.data, 4, 2, A.ctypes.data, 3, None, 0, -1.0, 0.0, 0, 0.0),   # negative regularisation
+                 (H.ctypes.data, 4, 2, A.ctypes.data, 3, None, 0, 0.0, 0.0, 0, -1.0),   # negative tolerance
+                 (H.ctypes.data, 4, 300, A.ctypes.data, 3, None, 0, 0.0, 0.0, 0, 0.0)]:  # too many parameters
+        assert L.csd_icls_create(*args, ctypes.byref(h)) == csd.CSD_ERR_INVALID
+        assert not h.value

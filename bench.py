@@ -210,6 +210,13 @@ def next_rows(dwi_dev, sample_idx):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    # end to end through the host-buffer C ABI call (csd_icls_solve_host):
+    # copies of the measurements in and the solutions out inside the timed region
+    s.solve_host(dwi)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        s.solve_host(dwi)
+    e2e_s = (time.perf_counter() - t0) / 2
     P = msmt_ref.problem(s.grad, s.shells, resp, [8, 0, 0], s.HR_dirs)
     idx = np.random.default_rng(1).choice(n, 500, replace=False)
     cores = os.cpu_count() or 1
@@ -226,6 +233,9 @@ def next_rows(dwi_dev, sample_idx):
                     "3 tissues (WM lmax 8, GM, CSF: 47 parameters, 302 constraints), Rician SNR U[15,40]",
         "value": n / (ms / 1e3), "unit": "voxels/s", "ms": ms, "dtype": "f64",
         "solver_rounds_mean": float(it.float().mean().item()),
+        "e2e": {"value": n / e2e_s, "unit": "voxels/s", "h2d_bytes_per_step": int(dwi.nbytes),
+                "d2h_bytes_per_step": int(n * (47 + 1) * 4),
+                "api": "csd_icls_solve_host (host buffers; device staging allocated and copies made inside)"},
         "parity": {"vs": "oracle/icls_oracle.c (FP64)", "sample_voxels": len(idx),
                    "p99_rel_err": float(np.percentile(rel, 99)), "max_rel_err": float(rel.max()),
                    "rounds_equal": float(np.mean(it.cpu().numpy()[idx] == itr))},

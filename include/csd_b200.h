@@ -274,6 +274,11 @@ int csd_icls_info(const csd_icls* problem, int* out4);
 int csd_icls_solve(csd_icls* problem, const float* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
                    const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, float* pred,
                    int64_t pred_stride, void* stream);
+/* csd_icls_solve on HOST buffers: b [n][voxel_stride] float (measurements
+ * contiguous), mask [n] or NULL, x [n][nparam], niter [n] or NULL, pred
+ * [n][nmeas] or NULL.  Stages through device memory; synchronous. */
+int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t voxel_stride, const uint8_t* mask,
+                        float* x, int32_t* niter, float* pred);
 
 /* Launch-shape knobs (process-wide), chosen by the project's autotuner
  * (mrtrix3_b200/autotune.py): which = 0 warps per block of the persistent

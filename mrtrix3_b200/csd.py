@@ -34,7 +34,7 @@ EXPORTED = [
     "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_run",
     "csd_state_fod",
     "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_icls_create",
-    "csd_icls_destroy", "csd_icls_info", "csd_icls_solve", "csd_last_error",
+    "csd_icls_destroy", "csd_icls_info", "csd_icls_solve", "csd_icls_solve_host", "csd_last_error",
 ]
 
 
@@ -96,6 +96,7 @@ def lib():
         L.csd_icls_destroy.restype = None
         L.csd_icls_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         L.csd_icls_solve.argtypes = [vp, vp, i64, i64, i64, vp, vp, i64, vp, vp, i64, vp]
+        L.csd_icls_solve_host.argtypes = [vp, vp, i64, i64, vp, vp, vp, vp]
         L.csd_sh2peaks.argtypes = [vp, i64, i64, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                    vp, ctypes.c_int, vp, vp, vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]

@@ -584,3 +584,45 @@ extern "C" int csd_icls_solve(csd_icls* p, const float* b, int64_t n, int64_t vo
   if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_icls_solve: ") + cudaGetErrorString(e));
   return CSD_OK;
 }
+
+// The solver on HOST buffers (b [n][voxel_stride] float, x [n][nparam],
+// niter / mask / pred optional): device staging, one solve, copies back;
+// synchronous.  The solve dominates (milliseconds per thousand voxels against
+// microseconds of transfer), so the copies are not overlapped.
+extern "C" int csd_icls_solve_host(csd_icls* p, const float* b, int64_t n, int64_t voxel_stride,
+                                   const uint8_t* mask, float* x, int32_t* niter, float* pred) {
+  if (!p || n < 0 || (n > 0 && (!b || !x)) || voxel_stride < p->nmeas)
+    return csdb200::set_error(CSD_ERR_INVALID, "csd_icls_solve_host: invalid argument");
+  if (n == 0) return CSD_OK;
+  const size_t nb = (size_t)n * voxel_stride * sizeof(float), nx = (size_t)n * p->nparam * sizeof(float);
+  const size_t np = pred ? (size_t)n * p->nmeas * sizeof(float) : 0, nm = mask ? (size_t)n : 0;
+  char* d = nullptr;
+  const size_t off_x = (nb + 255) / 256 * 256, off_i = off_x + (nx + 255) / 256 * 256,
+               off_p = off_i + ((size_t)n * sizeof(int32_t) + 255) / 256 * 256,
+               off_m = off_p + (np + 255) / 256 * 256, total = off_m + nm;
+  cudaError_t e = cudaMalloc(&d, total);
+  if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_NOMEM, std::string("csd_icls_solve_host: ") + cudaGetErrorString(e));
+  cudaStream_t st = nullptr;
+  e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d, b, nb, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && mask) e = cudaMemcpyAsync(d + off_m, mask, nm, cudaMemcpyHostToDevice, st);
+  int rc = CSD_OK;
+  if (e == cudaSuccess)
+    rc = csd_icls_solve(p, reinterpret_cast<const float*>(d), n, voxel_stride, 1,
+                        mask ? reinterpret_cast<const uint8_t*>(d + off_m) : nullptr, reinterpret_cast<float*>(d + off_x),
+                        p->nparam, reinterpret_cast<int32_t*>(d + off_i), pred ? reinterpret_cast<float*>(d + off_p) : nullptr,
+                        p->nmeas, st);
+  if (e == cudaSuccess && rc == CSD_OK) e = cudaMemcpyAsync(x, d + off_x, nx, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && rc == CSD_OK && niter)
+    e = cudaMemcpyAsync(niter, d + off_i, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && rc == CSD_OK && pred) e = cudaMemcpyAsync(pred, d + off_p, np, cudaMemcpyDeviceToHost, st);
+  if (st) {
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    cudaStreamDestroy(st);
+  }
+  cudaFree(d);
+  if (rc != CSD_OK) return rc;
+  if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_icls_solve_host: ") + cudaGetErrorString(e));
+  return CSD_OK;
+}

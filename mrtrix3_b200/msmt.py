@@ -255,6 +255,20 @@ class MSMTShared:
         (device float32 [n][volumes], optional) receives C x."""
         return icls_solve(self.handle, dwi, int(sum(self.nparams())), mask, out, niter, stream, predicted)
 
+    def solve_host(self, dwi: np.ndarray, mask: np.ndarray | None = None, predicted: bool = False):
+        """``solve`` on host arrays through csd_icls_solve_host (synchronous):
+        (x [n][N] float32, rounds [n] int32, predicted [n][volumes] or None)."""
+        dwi = np.ascontiguousarray(dwi, np.float32)
+        n = dwi.shape[0]
+        x = np.empty((n, int(sum(self.nparams()))), np.float32)
+        it = np.empty(n, np.int32)
+        pred = np.empty((n, self.grad.shape[0]), np.float32) if predicted else None
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        csd.check(csd.lib().csd_icls_solve_host(self.handle, dwi.ctypes.data, n, dwi.shape[1],
+                                                m.ctypes.data if m is not None else None, x.ctypes.data,
+                                                it.ctypes.data, pred.ctypes.data if pred is not None else None))
+        return x, it, pred
+
     def split(self, x):
         """The per-tissue parts of a [.., N] solution."""
         out, b = [], 0

@@ -249,3 +249,18 @@ def test_msmt_tissue_sets(cuda, tissues, lmax):
     xr, itr = msmt_ref.solve(P, dwi[idx].astype(np.float64))
     assert _rel(x[idx], xr).max() <= 1e-4
     assert (it.cpu().numpy() >= 0).all()
+
+
+def test_msmt_host_buffers_equal_device_call(cuda):
+    """csd_icls_solve_host (host arrays, staged through the device) gives the
+    device call's results bit for bit, with the mask and predicted signal."""
+    import torch
+    s, P, dwi = _msmt_case(500, 24)
+    mask = (np.arange(500) % 5 != 0).astype(np.uint8)
+    x_h, it_h, pred_h = s.solve_host(dwi, mask, predicted=True)
+    pred_d = torch.empty((500, dwi.shape[1]), dtype=torch.float32, device=cuda)
+    x_d, it_d = s.solve(torch.from_numpy(dwi).to(cuda), mask=torch.from_numpy(mask).to(cuda), predicted=pred_d)
+    np.testing.assert_array_equal(x_h, x_d.cpu().numpy())
+    np.testing.assert_array_equal(it_h, it_d.cpu().numpy())
+    np.testing.assert_array_equal(pred_h, pred_d.cpu().numpy())
+    assert not x_h[mask == 0].any()

@@ -235,10 +235,20 @@ int csd_sh2peaks(const float* sh, int64_t n_voxels, int64_t voxel_stride, int lm
  *      are device pointers; output float [n][out_stride].  The volume
  *      indices in `dwis` and `bzeros` must address volumes of the voxel (the
  *      kernel reads them unchecked; the Python binding checks them).  Returns
- *      without synchronising.  The -rician correction is not provided. */
+ *      without synchronising.  The -rician correction: csd_amp2sh_rician. */
 int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t volume_stride, const double* fit,
                int nsh, const int* dwis, int nd, const int* bzeros, int nb0, int normalise, float* sh_out,
                int64_t out_stride, void* stream);
+
+/* ---- amp2sh -rician (cmd/amp2sh.cpp:129-150, 180-197): csd_amp2sh's fit
+ *      reweighted for the Rician noise bias, up to 20 rounds per voxel, FP64;
+ *      sh2amp [nd][nsh] (double, device) is the SH-to-amplitude mapping whose
+ *      pinv is `fit`; noise: device float per voxel (noise[v * noise_stride]).
+ *      nsh <= 153.  Returns without synchronising. */
+int csd_amp2sh_rician(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t volume_stride,
+                      const double* fit, const double* sh2amp, int nsh, const int* dwis, int nd, const int* bzeros,
+                      int nb0, int normalise, const float* noise, int64_t noise_stride, float* sh_out,
+                      int64_t out_stride, void* stream);
 
 /* ---- inequality-constrained least squares, batched: the solver of
  *      dwi2fod msmt_csd (src/dwi/sdeconv/msmt_csd.h:249-270) and of

@@ -12,8 +12,9 @@ DWI::compute_SH2amp_mapping chooses (lmax from the direction count, at most
 8 unless ``-lmax`` asks, lowered while poorly conditioned); the output is
 float32 with the input's layout.
 
-Options: -lmax N, -normalise, -directions file, -grad file, -force.
-``-rician`` is not provided.
+Options: -lmax N, -normalise, -directions file, -grad file, -rician noise
+(a 3-D noise-level image: the fit reweighted for the Rician bias,
+amp2sh.cpp:129-150), -force.
 """
 from __future__ import annotations
 
@@ -46,8 +47,6 @@ def run(argv) -> int:
             i += 1
     if len(pos) != 2:
         raise SystemExit("usage: python -m mrtrix3_b200.amp2sh <amp> <SH> [options]")
-    if "-rician" in opt:
-        raise SystemExit("amp2sh: the -rician correction is not provided")
     in_path, out_path = pos
     if os.path.exists(out_path) and not opt.get("-force"):
         raise SystemExit(f"amp2sh: output image \"{out_path}\" already exists (use -force to replace it)")
@@ -97,7 +96,15 @@ def run(argv) -> int:
     from . import csd
     dev = torch.device("cuda", torch.cuda.current_device())
     amp = torch.from_numpy(np.ascontiguousarray(img.data.reshape(-1, nvol), np.float32)).to(dev)
-    out = csd.amp2sh(amp, fit, dwis, bzeros, normalise=bool(opt.get("-normalise"))).cpu().numpy()
+    noise = None
+    if "-rician" in opt:
+        nimg = mif.read(opt["-rician"])
+        if nimg.data.shape[:3] != (nx, ny, nz) or int(np.prod(nimg.data.shape[3:])) != 1:
+            raise SystemExit("amp2sh: the noise image must be 3-D, with the amplitude image's dimensions")
+        noise = torch.from_numpy(np.ascontiguousarray(nimg.data.reshape(-1), np.float32)).to(dev)
+    plan = csd.Amp2SHCommon(fit, dwis, bzeros, normalise=bool(opt.get("-normalise")), device=dev,
+                            sh2amp=mapping if noise is not None else None)
+    out = plan(amp, noise=noise).cpu().numpy()
     res = mif.Image(data=out.reshape(nx, ny, nz, -1), vox=img.vox, transform=img.transform, keyval=kv)
     mif.write(out_path, res, layout=img.layout, datatype="Float32LE" if np.little_endian else "Float32BE")
     return 0

@@ -33,7 +33,7 @@ EXPORTED = [
     "csd_shared_dwis", "csd_shared_matrix", "csd_solve", "csd_dwi2fod_host", "csd_state_create",
     "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_run",
     "csd_state_fod",
-    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_icls_create",
+    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_amp2sh_rician", "csd_icls_create",
     "csd_icls_destroy", "csd_icls_info", "csd_icls_solve", "csd_icls_solve_host", "csd_last_error",
 ]
 
@@ -89,6 +89,8 @@ def lib():
         L.csd_state_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(i64), vp]
         L.csd_amp2sh.argtypes = [vp, i64, i64, i64, vp, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
                                  vp, i64, vp]
+        L.csd_amp2sh_rician.argtypes = [vp, i64, i64, i64, vp, vp, ctypes.c_int, vp, ctypes.c_int, vp,
+                                         ctypes.c_int, ctypes.c_int, vp, i64, vp, i64, vp]
         L.csd_icls_create.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                       ctypes.POINTER(vp)]
@@ -386,7 +388,7 @@ class Amp2SHCommon:
     volumes it applies to, ``bzeros`` the b=0 volumes for ``normalise``.
     Calling it on amplitudes runs csd_amp2sh."""
 
-    def __init__(self, fit, dwis, bzeros=None, normalise: bool = False, device=None):
+    def __init__(self, fit, dwis, bzeros=None, normalise: bool = False, device=None, sh2amp=None):
         import torch
         fit = np.asarray(fit, np.float64)
         self.dwis = np.asarray(dwis, np.int64).reshape(-1)
@@ -404,11 +406,20 @@ class Amp2SHCommon:
         self.fit_d = torch.from_numpy(np.ascontiguousarray(fit)).to(dev)
         self.dwis_d = torch.from_numpy(np.ascontiguousarray(self.dwis, np.int32)).to(dev)
         self.b0_d = torch.from_numpy(np.ascontiguousarray(self.bzeros, np.int32)).to(dev) if len(self.bzeros) else None
+        # the mapping itself, for the Rician correction ([len(dwis)][nSH])
+        self.sh2amp_d = None
+        if sh2amp is not None:
+            sh2amp = np.asarray(sh2amp, np.float64)
+            if sh2amp.shape != (self.nd, self.nsh):
+                raise ValueError("amp2sh: sh2amp must be [selected volumes][nSH]")
+            self.sh2amp_d = torch.from_numpy(np.ascontiguousarray(sh2amp)).to(dev)
 
-    def __call__(self, amp, out=None, stream=None):
+    def __call__(self, amp, out=None, stream=None, noise=None):
         """SH coefficients of each row of ``amp`` (float32 CUDA tensor
         [n][volumes], any strides) into ``out`` (float32 [n][>= nSH], unit
-        column stride; allocated when None).  Returns ``out``."""
+        column stride; allocated when None).  ``noise`` (float32 CUDA [n]):
+        the Rician-corrected fit (needs ``sh2amp`` at construction).
+        Returns ``out``."""
         import torch
         if amp.dim() != 2 or amp.dtype != torch.float32 or amp.device != self.fit_d.device:
             raise ValueError("amp2sh: amplitudes must be a float32 tensor [n][volumes] on the fit's device")
@@ -419,6 +430,20 @@ class Amp2SHCommon:
         if (out.dim() != 2 or out.dtype != torch.float32 or out.device != amp.device or out.shape[0] != amp.shape[0]
                 or out.shape[1] < self.nsh or out.stride(1) != 1):
             raise ValueError("amp2sh: output must be float32 [n][>= nSH] with contiguous rows")
+        if noise is not None:
+            if self.sh2amp_d is None:
+                raise ValueError("amp2sh: the Rician correction needs the sh2amp mapping")
+            if noise.dtype != torch.float32 or noise.dim() != 1 or noise.shape[0] != amp.shape[0] or \
+                    noise.device != amp.device:
+                raise ValueError("amp2sh: noise must be a float32 tensor [n] on the amplitudes' device")
+            check(lib().csd_amp2sh_rician(
+                ctypes.c_void_p(amp.data_ptr()), amp.shape[0], amp.stride(0), amp.stride(1),
+                ctypes.c_void_p(self.fit_d.data_ptr()), ctypes.c_void_p(self.sh2amp_d.data_ptr()), self.nsh,
+                ctypes.c_void_p(self.dwis_d.data_ptr()), self.nd,
+                ctypes.c_void_p(self.b0_d.data_ptr()) if self.b0_d is not None else None, len(self.bzeros),
+                int(self.normalise), ctypes.c_void_p(noise.data_ptr()), noise.stride(0),
+                ctypes.c_void_p(out.data_ptr()), max(out.stride(0), self.nsh), ctypes.c_void_p(_stream_ptr(stream))))
+            return out
         check(lib().csd_amp2sh(ctypes.c_void_p(amp.data_ptr()), amp.shape[0], amp.stride(0), amp.stride(1),
                                ctypes.c_void_p(self.fit_d.data_ptr()), self.nsh,
                                ctypes.c_void_p(self.dwis_d.data_ptr()), self.nd,

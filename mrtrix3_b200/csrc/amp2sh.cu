@@ -450,3 +450,196 @@ extern "C" int csd_amp2sh(const float* amp, int64_t n_voxels, int64_t voxel_stri
   if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_amp2sh: ") + cudaGetErrorString(e));
   return CSD_OK;
 }
+
+// ---- amp2sh -rician (amp2sh.cpp:129-150, 180-197): the fit reweighted for
+// the Rician noise bias.  Per voxel, from c = fit a: up to 20 rounds of
+//   ap = SH2amp c, clamped at 0; t = (ap / noise)^2.25;
+//   w = ((t + 1.7) / (t + 1.12))^2; diff = a - noise (t + 1.65)^(1 / 2.25);
+//   stop when sum diff^2 / sum a^2 < 1e-8; else ap += diff and
+//   c = (H^T H)^-1 H^T ap with H = diag(w) SH2amp (Cholesky, as LLT there).
+// A warp a voxel, in FP64; per warp in shared memory: a, ap, w [nd], c, s
+// [nsh] and the packed lower triangle of H^T H.
+namespace {
+
+constexpr int kRicWarps = 4;
+constexpr int kRicRounds = 20;
+constexpr double kRicianPower = 2.25;
+
+__host__ __device__ inline size_t ric_warp_doubles(int nd, int nsh) {
+  return 3 * (size_t)nd + 2 * (size_t)nsh + (size_t)nsh * (nsh + 1) / 2;
+}
+
+struct RicianArgs {
+  Amp2ShArgs a;
+  const double* sh2amp;  // [nd][nsh]
+  const float* noise;    // [n] (noise[v * noise_stride])
+  long long noise_stride;
+};
+
+__device__ __forceinline__ double ric_warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kRicWarps * 32) amp2sh_rician_kernel(const __grid_constant__ RicianArgs ra) {
+  extern __shared__ __align__(16) double rsm_[];
+  const Amp2ShArgs& a = ra.a;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nd = a.nd, nsh = a.nsh;
+  double* av = rsm_ + warp * ric_warp_doubles(nd, nsh);
+  double* ap = av + nd;
+  double* w = ap + nd;
+  double* c = w + nd;
+  double* s = c + nsh;
+  double* Q = s + nsh;  // packed lower: Q[i (i + 1) / 2 + j]
+  const long long gw = (long long)blockIdx.x * kRicWarps + warp, nw = (long long)gridDim.x * kRicWarps;
+  for (long long v = gw; v < a.n; v += nw) {
+    const float* p = a.amp + v * a.vs;
+    double norm = 1.0;
+    if (a.normalise) {
+      double t = 1.0;  // get_amps' order
+      for (int i = 0; i < a.nb0; ++i) t += (double)p[(long long)a.b0[i] * a.ts];
+      norm = (double)a.nb0 / t;
+    }
+    for (int n = lane; n < nd; n += 32) av[n] = (double)p[(long long)a.dwis[n] * a.ts] * norm;
+    __syncwarp();
+    for (int j = lane; j < nsh; j += 32) {
+      const double* f = a.fit + (long long)j * nd;
+      double t = 0.0;
+      for (int n = 0; n < nd; ++n) t = fma(f[n], av[n], t);
+      c[j] = t;
+    }
+    __syncwarp();
+    const double noise = (double)ra.noise[v * ra.noise_stride];
+    for (int round = 0; round < kRicRounds; ++round) {
+      // get_rician_bias: ap, w, the convergence test, ap += diff
+      double nd2 = 0.0, na2 = 0.0;
+      for (int n = lane; n < nd; n += 32) {
+        const double* h = ra.sh2amp + (long long)n * nsh;
+        double t = 0.0;
+        for (int j = 0; j < nsh; ++j) t = fma(h[j], c[j], t);
+        t = fmax(t, 0.0);
+        const double tt = pow(t / noise, kRicianPower);
+        const double q = (tt + 1.7) / (tt + 1.12);
+        w[n] = q * q;
+        const double diff = av[n] - noise * pow(tt + 1.65, 1.0 / kRicianPower);
+        nd2 = fma(diff, diff, nd2);
+        na2 = fma(av[n], av[n], na2);
+        ap[n] = t + diff;
+      }
+      nd2 = ric_warp_sum(nd2);
+      na2 = ric_warp_sum(na2);
+      __syncwarp();
+      if (nd2 / na2 < 1.0e-8) break;
+      // s = H^T ap, Q = H^T H (lower), H = diag(w) SH2amp
+      for (int j = lane; j < nsh; j += 32) {
+        double t = 0.0;
+        for (int n = 0; n < nd; ++n) t = fma(ra.sh2amp[(long long)n * nsh + j] * w[n], ap[n], t);
+        s[j] = t;
+      }
+      const int nq = nsh * (nsh + 1) / 2;
+      for (int e = lane; e < nq; e += 32) {
+        int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+        while (i * (i + 1) / 2 > e) --i;
+        while ((i + 1) * (i + 2) / 2 <= e) ++i;
+        const int j = e - i * (i + 1) / 2;
+        double t = 0.0;
+        for (int n = 0; n < nd; ++n) {
+          const double wn = w[n];
+          t = fma(ra.sh2amp[(long long)n * nsh + i] * wn, ra.sh2amp[(long long)n * nsh + j] * wn, t);
+        }
+        Q[e] = t;
+      }
+      __syncwarp();
+      // Cholesky in place (left-looking by columns; lanes over the rows)
+      for (int k = 0; k < nsh; ++k) {
+        const int kk = k * (k + 1) / 2;
+        double d = 0.0;
+        for (int m = lane; m < k; m += 32) d = fma(Q[kk + m], Q[kk + m], d);
+        d = ric_warp_sum(d);
+        const double dk = sqrt(Q[kk + k] - d);
+        __syncwarp();
+        for (int i = k + 1 + lane; i < nsh; i += 32) {
+          const int ii = i * (i + 1) / 2;
+          double t = Q[ii + k];
+          for (int m = 0; m < k; ++m) t -= Q[ii + m] * Q[kk + m];
+          Q[ii + k] = t / dk;
+        }
+        __syncwarp();
+        if (lane == 0) Q[kk + k] = dk;
+        __syncwarp();
+      }
+      // c = L^-T L^-1 s (column-oriented substitutions)
+      for (int k = 0; k < nsh; ++k) {
+        const double zk = s[k] / Q[k * (k + 1) / 2 + k];
+        __syncwarp();
+        for (int i = k + 1 + lane; i < nsh; i += 32) s[i] -= Q[i * (i + 1) / 2 + k] * zk;
+        if (lane == 0) s[k] = zk;
+        __syncwarp();
+      }
+      for (int k = nsh - 1; k >= 0; --k) {
+        const int kk = k * (k + 1) / 2;
+        const double ck = s[k] / Q[kk + k];
+        __syncwarp();
+        for (int i = lane; i < k; i += 32) s[i] -= Q[kk + i] * ck;
+        if (lane == 0) s[k] = ck;
+        __syncwarp();
+      }
+      for (int j = lane; j < nsh; j += 32) c[j] = s[j];
+      __syncwarp();
+    }
+    for (int j = lane; j < nsh; j += 32) a.out[v * a.os + j] = (float)c[j];
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+extern "C" int csd_amp2sh_rician(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t volume_stride,
+                                 const double* fit, const double* sh2amp, int nsh, const int* dwis, int nd,
+                                 const int* bzeros, int nb0, int normalise, const float* noise, int64_t noise_stride,
+                                 float* sh_out, int64_t out_stride, void* stream) {
+  if (n_voxels < 0 || (n_voxels > 0 && (!amp || !sh_out || !noise)) || !fit || !sh2amp || !dwis || nd < 1 ||
+      nd > kA2sMaxDirs || nsh < 1 || nsh > 153 || out_stride < nsh || nb0 < 0 || (nb0 && !bzeros) ||
+      (normalise && nb0 == 0))
+    return csdb200::set_error(CSD_ERR_INVALID, "csd_amp2sh_rician: invalid argument");
+  if (n_voxels == 0) return CSD_OK;
+  RicianArgs ra{};
+  Amp2ShArgs& a = ra.a;
+  a.amp = amp;
+  a.n = n_voxels;
+  a.vs = voxel_stride;
+  a.ts = volume_stride;
+  a.fit = fit;
+  a.dwis = dwis;
+  a.b0 = bzeros;
+  a.nd = nd;
+  a.nb0 = nb0;
+  a.nsh = nsh;
+  a.normalise = normalise;
+  a.out = sh_out;
+  a.os = out_stride;
+  ra.sh2amp = sh2amp;
+  ra.noise = noise;
+  ra.noise_stride = noise_stride;
+  int dev = 0, nsm = 0, smem_max = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t smem = kRicWarps * ric_warp_doubles(nd, nsh) * sizeof(double);
+  if (e == cudaSuccess && smem > (size_t)smem_max)
+    return csdb200::set_error(CSD_ERR_INVALID, "csd_amp2sh_rician: problem too large for shared memory");
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(amp2sh_rician_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, amp2sh_rician_kernel, kRicWarps * 32, smem);
+  if (e == cudaSuccess) {
+    const long long blocks = std::max<long long>(
+        1, std::min<long long>((n_voxels + kRicWarps - 1) / kRicWarps, (long long)nsm * std::max(1, per_sm)));
+    amp2sh_rician_kernel<<<(unsigned)blocks, kRicWarps * 32, smem, static_cast<cudaStream_t>(stream)>>>(ra);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_amp2sh_rician: ") + cudaGetErrorString(e));
+  return CSD_OK;
+}

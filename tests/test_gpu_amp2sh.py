@@ -189,3 +189,52 @@ def test_amp2sh_row_layouts(cuda, amp2sh_kernel, kind):
         for normalise in (False, True):
             got = csd.amp2sh(d, fit, dwis, bzeros, normalise=normalise).cpu().numpy().astype(np.float64)
             _check(got, _ref(amp, fit, dwis, bzeros, normalise))
+
+
+@pytest.mark.parametrize("normalise", [False, True])
+def test_amp2sh_rician_matches_oracle(cuda, normalise):
+    """-rician: the reweighted fit against the FP64 restatement
+    (oracle/amp2sh_ref.py); a noise level of ~SNR 20 a voxel."""
+    import torch
+    from oracle import amp2sh_ref
+    grad = synth.config5_scheme()
+    fit, dwis, bzeros = _fit(grad)
+    m = O.init_transform(sh.cartesian_to_azel(grad[dwis, :3]), 8)
+    rng = np.random.default_rng(13)
+    n = 1003
+    amp = synth.voxel_signals(rng, grad, n, (15.0, 40.0)).astype(np.float32)
+    noise = (amp[:, bzeros].mean(1) / rng.uniform(10.0, 30.0, n)).astype(np.float32)
+    if normalise:
+        noise = noise * (len(bzeros) / (1.0 + amp[:, bzeros].sum(1))).astype(np.float32)
+    plan = csd.Amp2SHCommon(fit, dwis, bzeros, normalise=normalise, sh2amp=m)
+    got = plan(torch.from_numpy(amp).to(cuda), noise=torch.from_numpy(noise).to(cuda)).cpu().numpy()
+    plain = plan(torch.from_numpy(amp).to(cuda)).cpu().numpy()
+    for i in range(0, n, 17):
+        a = amp2sh_ref.amps(amp[i], dwis, bzeros, normalise)
+        ref = amp2sh_ref.fit_rician(a, m, fit, float(noise[i]))
+        assert np.abs(got[i] - ref).max() <= 1e-5 * np.abs(ref).max()
+    # the correction changes the fit (it is not the plain one)
+    assert np.abs(got - plain).max() > 1e-3 * np.abs(plain).max()
+
+
+def test_amp2sh_rician_command_line(cuda, tmp_path):
+    from mrtrix3_b200.amp2sh import run
+    from oracle import amp2sh_ref
+    grad = synth.config5_scheme()
+    dims = (5, 4, 3)
+    n = int(np.prod(dims))
+    rng = np.random.default_rng(6)
+    amp = synth.voxel_signals(rng, grad, n, (15.0, 40.0)).astype(np.float32)
+    noise = np.full(n, 60.0, np.float32)
+    data = amp.reshape(dims[2], dims[1], dims[0], -1).transpose(2, 1, 0, 3)
+    p, pn, out = str(tmp_path / "dwi.mif"), str(tmp_path / "noise.mif"), str(tmp_path / "sh.mif")
+    mif.write(p, mif.Image(data=data, vox=[2.0, 2.0, 2.0, 1.0], keyval={"dw_scheme": mif.scheme_to_text(grad)}))
+    mif.write(pn, mif.Image(data=noise.reshape(dims[2], dims[1], dims[0]).transpose(2, 1, 0),
+                            vox=[2.0, 2.0, 2.0]))
+    assert run([p, out, "-rician", pn]) == 0
+    got = mif.read(out).data.transpose(2, 1, 0, 3).reshape(n, -1).astype(np.float64)
+    fit, dwis, bzeros = _fit(grad)
+    m = O.init_transform(sh.cartesian_to_azel(grad[dwis, :3]), 8)
+    for i in range(0, n, 7):
+        ref = amp2sh_ref.fit_rician(amp2sh_ref.amps(amp[i], dwis), m, fit, 60.0)
+        assert np.abs(got[i] - ref).max() <= 1e-5 * np.abs(ref).max()

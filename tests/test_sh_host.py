@@ -95,8 +95,6 @@ def test_amp2sh_cli_rejects_options_before_any_device_work(tmp_path):
     mif.write(p, img)
     dirs = str(tmp_path / "dirs.txt")
     np.savetxt(dirs, _fib_dirs(6))
-    with pytest.raises(SystemExit, match="rician"):
-        amp2sh.run([p, str(tmp_path / "o.mif"), "-rician", "noise.mif"])
     with pytest.raises(SystemExit, match="normalise"):
         amp2sh.run([p, str(tmp_path / "o.mif"), "-directions", dirs, "-normalise"])
     with pytest.raises(SystemExit, match="directions or diffusion encoding"):

@@ -250,6 +250,22 @@ int csd_amp2sh_rician(const float* amp, int64_t n_voxels, int64_t voxel_stride, 
                       int nb0, int normalise, const float* noise, int64_t noise_stride, float* sh_out,
                       int64_t out_stride, void* stream);
 
+/* ---- amp2response (cmd/amp2response.cpp:152-190): accumulate, over the
+ *      voxels of `mask` (device uint8 [n] or NULL = all), the normal
+ *      equations of one shell's zonal response fit: M += T^T T (lower
+ *      triangle of [nz][nz], nz = lmax/2 + 1, lmax even <= 12) and b += T^T a,
+ *      T_i the normalised zonal Legendre values at the elevation of volume
+ *      `volumes[i]`'s direction `dirs[i]` ([n_dirs][3] device doubles) from the
+ *      voxel's fibre direction (fibre_dir[v * dir_stride + c * dir_comp_stride],
+ *      c = x y z, device float), folded into [0, pi/2]; a the amplitudes
+ *      (amp[v * voxel_stride + volumes[i] * volume_stride]).  M and b are
+ *      device doubles, added to (zero them first).  FP64.  Returns without
+ *      synchronising. */
+int csd_amp2response_accumulate(const float* amp, int64_t n_voxels, int64_t voxel_stride, int64_t volume_stride,
+                                const float* fibre_dir, int64_t dir_stride, int64_t dir_comp_stride,
+                                const uint8_t* mask, const double* dirs, int n_dirs, const int* volumes, int lmax,
+                                double* M, double* b, void* stream);
+
 /* ---- inequality-constrained least squares, batched: the solver of
  *      dwi2fod msmt_csd (src/dwi/sdeconv/msmt_csd.h:249-270) and of
  *      Math::ICLS (core/math/constrained_least_squares.h).
@@ -279,11 +295,22 @@ int csd_icls_create(const double* H, int nmeas, int nparam, const double* A, int
                     int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol,
                     csd_icls** out);
 void csd_icls_destroy(csd_icls* problem);
+/* The problem already in standard form (constrained_least_squares.h:67-70,
+ * 124-126, 139-140): HtH [nparam][nparam] (host, its lower triangle read) is
+ * H^T H, and the right-hand sides given to the solver are H^T b (nmeas =
+ * nparam).  As amp2response's constrained fit (amp2response.cpp:345-346). */
+int csd_icls_create_standard(const double* HtH, int nparam, const double* A, int ncons, const double* t,
+                             int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol,
+                             csd_icls** out);
 /* out4 = {nmeas, nparam, ncons, max_niter} */
 int csd_icls_info(const csd_icls* problem, int* out4);
 int csd_icls_solve(csd_icls* problem, const float* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
                    const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, float* pred,
                    int64_t pred_stride, void* stream);
+/* csd_icls_solve with FP64 right-hand sides and solutions (device
+ * pointers; no mask, no predicted measurements). */
+int csd_icls_solve_f64(csd_icls* problem, const double* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
+                       double* x, int64_t x_stride, int32_t* niter, void* stream);
 /* csd_icls_solve on HOST buffers: b [n][voxel_stride] float (measurements
  * contiguous), mask [n] or NULL, x [n][nparam], niter [n] or NULL, pred
  * [n][nmeas] or NULL.  Stages through device memory; synchronous. */

@@ -75,6 +75,8 @@ __device__ __forceinline__ double& lref(double* Ls, double* Lg, int ld, int i, i
 
 struct IclsArgs {
   const float* b;
+  const double* b64;  // FP64 right-hand sides instead of b (csd_icls_solve_f64)
+  double* x64;        // FP64 solutions instead of x
   long long n, vs, ms;
   const uint8_t* mask;
   float* x;
@@ -182,24 +184,31 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
   double* Lg = a.scratch + gw * (long long)a.ld * a.ld;  // factor rows >= kIclsSmemRows
   const int num_ineq = a.ncons - a.num_eq;
   for (long long v = gw; v < a.n; v += nw) {
-    float* xo = a.x + v * a.xs;
+    float* xo = a.x64 ? nullptr : a.x + v * a.xs;
+    double* xo64 = a.x64 ? a.x64 + v * a.xs : nullptr;
+    auto put = [&](int j, double val) {
+      if (xo64)
+        xo64[j] = val;
+      else
+        xo[j] = (float)val;
+    };
     if (a.mask && !a.mask[v]) {
-      for (int j = lane; j < a.nparam; j += 32) xo[j] = 0.f;
+      for (int j = lane; j < a.nparam; j += 32) put(j, 0.0);
       if (a.pred)
         for (int i = lane; i < a.nmeas; i += 32) a.pred[v * a.ps + i] = 0.f;
       if (a.niter && lane == 0) a.niter[v] = 0;
       continue;
     }
-    const float* bv = a.b + v * a.vs;
     bool finite = true;
     for (int i = lane; i < a.nmeas; i += 32) {
-      const float f = bv[(long long)i * a.ms];
+      const long long o = v * a.vs + (long long)i * a.ms;
+      const double f = a.b64 ? a.b64[o] : (double)a.b[o];
       finite &= isfinite(f);
-      bb[i] = (double)f;
+      bb[i] = f;
     }
     if (!__all_sync(0xffffffffu, finite)) {
       // a non-finite measurement propagates through b2d^T b to every output
-      for (int j = lane; j < a.nparam; j += 32) xo[j] = __int_as_float(0x7fffffff);
+      for (int j = lane; j < a.nparam; j += 32) put(j, __longlong_as_double(0x7ff8000000000000ll));
       if (a.pred)
         for (int i = lane; i < a.nmeas; i += 32) a.pred[v * a.ps + i] = __int_as_float(0x7fffffff);
       if (a.niter && lane == 0) a.niter[v] = 0;
@@ -345,7 +354,7 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
       __syncwarp();
     }
     if (fail) {
-      for (int j = lane; j < a.nparam; j += 32) xo[j] = __int_as_float(0x7fffffff);
+      for (int j = lane; j < a.nparam; j += 32) put(j, __longlong_as_double(0x7ff8000000000000ll));
       if (a.pred)
         for (int i = lane; i < a.nmeas; i += 32) a.pred[v * a.ps + i] = __int_as_float(0x7fffffff);
       if (a.niter && lane == 0) a.niter[v] = -1;
@@ -377,7 +386,7 @@ __global__ void __launch_bounds__(kIclsWarps * 32) icls_solve_kernel(const __gri
       if (lane == 0) r[j] = zj;
       __syncwarp();
     }
-    for (int j = lane; j < a.nparam; j += 32) xo[j] = (float)r[j];
+    for (int j = lane; j < a.nparam; j += 32) put(j, r[j]);
     if (a.pred)  // the predicted measurements H x (MSMT_Processor's -predicted_signal, dwi2fod.cpp:212-216)
       for (int i = lane; i < a.nmeas; i += 32) {
         const double* h = a.H + (long long)i * a.nparam;
@@ -427,9 +436,26 @@ cudaError_t upload(T** dst, const std::vector<T>& src) {
 
 }  // namespace
 
+namespace {
+int icls_build(const double* H, bool standard, int nmeas, int nparam, const double* A, int ncons, const double* t,
+               int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol, csd_icls** out);
+}
+
 extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const double* A, int ncons, const double* t,
                                int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol,
                                csd_icls** out) {
+  return icls_build(H, false, nmeas, nparam, A, ncons, t, num_eq, solution_reg, constraint_reg, max_niter, tol, out);
+}
+
+extern "C" int csd_icls_create_standard(const double* HtH, int nparam, const double* A, int ncons, const double* t,
+                                        int num_eq, double solution_reg, double constraint_reg, int max_niter,
+                                        double tol, csd_icls** out) {
+  return icls_build(HtH, true, nparam, nparam, A, ncons, t, num_eq, solution_reg, constraint_reg, max_niter, tol, out);
+}
+
+namespace {
+int icls_build(const double* H, bool standard, int nmeas, int nparam, const double* A, int ncons, const double* t,
+               int num_eq, double solution_reg, double constraint_reg, int max_niter, double tol, csd_icls** out) {
   if (!out || !H || !A || nmeas < 1 || nparam < 1 || ncons < 1 || num_eq < 0 || num_eq > ncons ||
       solution_reg < 0.0 || constraint_reg < 0.0 || tol < 0.0 || max_niter < 0 || ncons > 4096 || nparam > kIclsMaxParam ||
       nmeas > 4096 || num_eq > kIclsMaxActive)
@@ -441,7 +467,11 @@ extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const dou
     for (int i = 0; i < nparam; ++i)
       for (int j = 0; j <= i; ++j) {
         double s = 0.0;
-        for (int r = 0; r < nmeas; ++r) s += H[(size_t)r * nparam + i] * H[(size_t)r * nparam + j];
+        if (standard) {  // H^T H given (its lower triangle is read)
+          s = H[(size_t)i * nparam + j];
+        } else {
+          for (int r = 0; r < nmeas; ++r) s += H[(size_t)r * nparam + i] * H[(size_t)r * nparam + j];
+        }
         L[(size_t)i * nparam + j] = s;
       }
     double dmax = -INFINITY;
@@ -451,7 +481,8 @@ extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const dou
     // b2d^T = L^-1 H^T, B^T = L^-1 A^T (rows normalised)
     std::vector<double> b2dT((size_t)nparam * nmeas), B((size_t)ncons * nparam), tt, col(nparam), z(nparam);
     for (int r = 0; r < nmeas; ++r) {
-      for (int i = 0; i < nparam; ++i) col[i] = H[(size_t)r * nparam + i];
+      // b2d = H L^-T; in standard form the measurements are H^T b already: b2d = L^-T
+      for (int i = 0; i < nparam; ++i) col[i] = standard ? (i == r ? 1.0 : 0.0) : H[(size_t)r * nparam + i];
       forward(L, nparam, col.data(), z.data());
       for (int i = 0; i < nparam; ++i) b2dT[(size_t)i * nmeas + r] = z[i];
     }
@@ -461,7 +492,8 @@ extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const dou
       double nrm = 0.0;
       for (int i = 0; i < nparam; ++i) nrm += z[i] * z[i];
       nrm = std::sqrt(nrm);
-      if (!(nrm > 0.0)) throw std::runtime_error("ICLS constraint row is zero");
+      // a zero row normalises to NaN, as in the reference: its constraint
+      // value is NaN, which the "most violated" scan never selects
       for (int i = 0; i < nparam; ++i) B[(size_t)m * nparam + i] = z[i] / nrm;
       if (t) tt[m] /= nrm;
     }
@@ -485,7 +517,7 @@ extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const dou
     if (e == cudaSuccess) e = upload(&p->d_B, B);
     if (e == cudaSuccess) e = upload(&p->d_G, G);
     if (e == cudaSuccess) e = upload(&p->d_L, L);
-    if (e == cudaSuccess) e = upload(&p->d_H, std::vector<double>(H, H + (size_t)nmeas * nparam));
+    if (e == cudaSuccess && !standard) e = upload(&p->d_H, std::vector<double>(H, H + (size_t)nmeas * nparam));
     if (e == cudaSuccess && t) e = upload(&p->d_t, tt);
     if (e != cudaSuccess) {
       csd_icls_destroy(p);
@@ -497,6 +529,8 @@ extern "C" int csd_icls_create(const double* H, int nmeas, int nparam, const dou
   }
   return CSD_OK;
 }
+
+}  // namespace
 
 extern "C" void csd_icls_destroy(csd_icls* p) {
   if (!p) return;
@@ -519,11 +553,36 @@ extern "C" int csd_icls_info(const csd_icls* p, int* out4) {
   return CSD_OK;
 }
 
+namespace {
+int icls_solve(csd_icls* p, const float* b, const double* b64, int64_t n, int64_t voxel_stride, int64_t meas_stride,
+               const uint8_t* mask, float* x, double* x64, int64_t x_stride, int32_t* niter, float* pred,
+               int64_t pred_stride, void* stream);
+}
+
 extern "C" int csd_icls_solve(csd_icls* p, const float* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
                               const uint8_t* mask, float* x, int64_t x_stride, int32_t* niter, float* pred,
                               int64_t pred_stride, void* stream) {
-  if (!p || n < 0 || (n > 0 && (!b || !x)) || x_stride < p->nparam || (pred && pred_stride < p->nmeas))
+  if (!p || n < 0 || (n > 0 && (!b || !x)))
     return csdb200::set_error(CSD_ERR_INVALID, "csd_icls_solve: invalid argument");
+  return icls_solve(p, b, nullptr, n, voxel_stride, meas_stride, mask, x, nullptr, x_stride, niter, pred, pred_stride,
+                    stream);
+}
+
+extern "C" int csd_icls_solve_f64(csd_icls* p, const double* b, int64_t n, int64_t voxel_stride, int64_t meas_stride,
+                                  double* x, int64_t x_stride, int32_t* niter, void* stream) {
+  if (!p || n < 0 || (n > 0 && (!b || !x)))
+    return csdb200::set_error(CSD_ERR_INVALID, "csd_icls_solve_f64: invalid argument");
+  return icls_solve(p, nullptr, b, n, voxel_stride, meas_stride, nullptr, nullptr, x, x_stride, niter, nullptr, 0,
+                    stream);
+}
+
+namespace {
+int icls_solve(csd_icls* p, const float* b, const double* b64, int64_t n, int64_t voxel_stride, int64_t meas_stride,
+               const uint8_t* mask, float* x, double* x64, int64_t x_stride, int32_t* niter, float* pred,
+               int64_t pred_stride, void* stream) {
+  if (x_stride < p->nparam || (pred && (pred_stride < p->nmeas || !p->d_H)))
+    return csdb200::set_error(CSD_ERR_INVALID, "csd_icls_solve: invalid argument (predicted measurements need a "
+                                               "problem given by H)");
   if (n == 0) return CSD_OK;
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
   int nsm = 0, smem_max = 0;
@@ -553,6 +612,8 @@ extern "C" int csd_icls_solve(csd_icls* p, const float* b, int64_t n, int64_t vo
   }
   IclsArgs a{};
   a.b = b;
+  a.b64 = b64;
+  a.x64 = x64;
   a.n = n;
   a.vs = voxel_stride;
   a.ms = meas_stride;
@@ -584,6 +645,8 @@ extern "C" int csd_icls_solve(csd_icls* p, const float* b, int64_t n, int64_t vo
   if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_icls_solve: ") + cudaGetErrorString(e));
   return CSD_OK;
 }
+
+}  // namespace
 
 // The solver on HOST buffers (b [n][voxel_stride] float, x [n][nparam],
 // niter / mask / pred optional): device staging, one solve, copies back;

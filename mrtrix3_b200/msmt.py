@@ -308,20 +308,43 @@ class ICLSProblem:
     s.t. A x >= t, the last ``num_eq`` rows of A equalities."""
 
     def __init__(self, H, A, t=None, num_eq: int = 0, solution_reg: float = 0.0, constraint_reg: float = 0.0,
-                 max_niter: int = 0, tol: float = 0.0):
+                 max_niter: int = 0, tol: float = 0.0, standard_form: bool = False):
+        """``standard_form``: H is H^T H (square) and the right-hand sides are
+        H^T b (constrained_least_squares.h:67-70)."""
         H = np.ascontiguousarray(H, np.float64)
         A = np.ascontiguousarray(A, np.float64)
         t = None if t is None or len(t) == 0 else np.ascontiguousarray(t, np.float64)
         self.nparam = H.shape[1]
         h = ctypes.c_void_p()
-        csd.check(csd.lib().csd_icls_create(H.ctypes.data, H.shape[0], H.shape[1], A.ctypes.data, A.shape[0],
-                                            t.ctypes.data if t is not None else None, int(num_eq),
-                                            float(solution_reg), float(constraint_reg), int(max_niter),
-                                            float(tol), ctypes.byref(h)))
+        tp = t.ctypes.data if t is not None else None
+        if standard_form:
+            if H.shape[0] != H.shape[1]:
+                raise ValueError("ICLSProblem: a problem in standard form needs a square H^T H")
+            csd.check(csd.lib().csd_icls_create_standard(H.ctypes.data, H.shape[1], A.ctypes.data, A.shape[0], tp,
+                                                         int(num_eq), float(solution_reg), float(constraint_reg),
+                                                         int(max_niter), float(tol), ctypes.byref(h)))
+        else:
+            csd.check(csd.lib().csd_icls_create(H.ctypes.data, H.shape[0], H.shape[1], A.ctypes.data, A.shape[0],
+                                                tp, int(num_eq), float(solution_reg), float(constraint_reg),
+                                                int(max_niter), float(tol), ctypes.byref(h)))
         self._h = h
 
     def solve(self, b, mask=None, out=None, niter=None, stream=None, predicted=None):
         return icls_solve(self._h, b, self.nparam, mask, out, niter, stream, predicted)
+
+    def solve_f64(self, b, stream=None):
+        """FP64 right-hand sides (device float64 [n][measurements]) -> FP64
+        solutions [n][nparam] and rounds [n] (csd_icls_solve_f64)."""
+        import torch
+        if b.dim() != 2 or b.dtype != torch.float64 or not b.is_cuda:
+            raise ValueError("solve_f64: b must be a float64 CUDA tensor [n][measurements]")
+        x = torch.empty((b.shape[0], self.nparam), dtype=torch.float64, device=b.device)
+        it = torch.empty(b.shape[0], dtype=torch.int32, device=b.device)
+        csd.check(csd.lib().csd_icls_solve_f64(self._h, ctypes.c_void_p(b.data_ptr()), b.shape[0], b.stride(0),
+                                               b.stride(1), ctypes.c_void_p(x.data_ptr()), x.stride(0),
+                                               ctypes.c_void_p(it.data_ptr()),
+                                               ctypes.c_void_p(csd._stream_ptr(stream))))
+        return x, it
 
     def __del__(self):
         try:

@@ -53,7 +53,8 @@ class Problem:
         self.b2d = np.linalg.solve(self.L, rhs.T).T
         B = np.linalg.solve(self.L, A.T).T
         norms = np.linalg.norm(B, axis=1)
-        self.B = B / norms[:, None]
+        with np.errstate(invalid="ignore", divide="ignore"):  # a zero row becomes NaN, as there
+            self.B = B / norms[:, None]
         self.t = None if t is None or len(t) == 0 else np.asarray(t, np.float64) / norms
 
     @property
@@ -89,7 +90,7 @@ def solve(P: Problem, b, trace: list | None = None):
     x = y_u.copy()
     niter = 0
     while num_ineq > 0:
-        i_min = int(np.argmin(c[:num_ineq]))  # first index of the minimum, as Eigen's minCoeff
+        i_min = _min_coeff(c[:num_ineq])
         if not c[i_min] < -P.tol:
             break
         changed = not active[i_min]
@@ -130,6 +131,16 @@ def solve(P: Problem, b, trace: list | None = None):
             c = c - P.t
     x = np.linalg.solve(P.L.T, x)
     return x, niter
+
+
+def _min_coeff(v) -> int:
+    """Eigen's minCoeff(&index): a scan keeping the first strict minimum, so
+    NaN entries are never chosen (unless the first entry is NaN, which then
+    stays)."""
+    if np.isnan(v[0]):
+        return 0
+    with np.errstate(invalid="ignore"):
+        return int(np.nanargmin(v)) if np.isnan(v).any() else int(np.argmin(v))
 
 
 def is_approx(x, y, prec: float) -> bool:

@@ -235,7 +235,7 @@ def next_rows(dwi_dev, sample_idx):
         "solver_rounds_mean": float(it.float().mean().item()),
         "e2e": {"value": n / e2e_s, "unit": "voxels/s", "h2d_bytes_per_step": int(dwi.nbytes),
                 "d2h_bytes_per_step": int(n * (47 + 1) * 4),
-                "api": "csd_icls_solve_host (host buffers; device staging allocated and copies made inside)"},
+                "api": "csd_icls_solve_host (host buffers, pageable; copies made inside the timed region)"},
         "parity": {"vs": "oracle/icls_oracle.c (FP64)", "sample_voxels": len(idx),
                    "p99_rel_err": float(np.percentile(rel, 99)), "max_rel_err": float(rel.max()),
                    "rounds_equal": float(np.mean(it.cpu().numpy()[idx] == itr))},

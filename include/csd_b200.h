@@ -313,7 +313,9 @@ int csd_icls_solve_f64(csd_icls* problem, const double* b, int64_t n, int64_t vo
                        double* x, int64_t x_stride, int32_t* niter, void* stream);
 /* csd_icls_solve on HOST buffers: b [n][voxel_stride] float (measurements
  * contiguous), mask [n] or NULL, x [n][nparam], niter [n] or NULL, pred
- * [n][nmeas] or NULL.  Stages through device memory; synchronous. */
+ * [n][nmeas] or NULL.  Stages through device memory kept with the problem
+ * (grown as needed, freed by csd_icls_destroy); synchronous.  Calls on one
+ * problem must not overlap. */
 int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t voxel_stride, const uint8_t* mask,
                         float* x, int32_t* niter, float* pred);
 

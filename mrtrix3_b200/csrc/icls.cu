@@ -48,8 +48,11 @@ struct csd_icls {
   double* d_t = nullptr;     // [ncons] or null
   double* d_L = nullptr;     // [nparam][nparam], lower, row-major
   double* d_H = nullptr;     // [nmeas][nparam] (the predicted measurements H x)
-  double* d_scratch = nullptr;  // per warp: two copies of the active-set factor
+  double* d_scratch = nullptr;  // per warp: the factor rows past the shared-memory part
   size_t scratch_warps = 0;
+  char* d_host_ws = nullptr;  // csd_icls_solve_host's device staging, grown as needed
+  size_t host_ws_bytes = 0;
+  cudaStream_t host_stream = nullptr;
 };
 
 namespace {
@@ -541,6 +544,8 @@ extern "C" void csd_icls_destroy(csd_icls* p) {
   cudaFree(p->d_L);
   cudaFree(p->d_H);
   cudaFree(p->d_scratch);
+  cudaFree(p->d_host_ws);
+  if (p->host_stream) cudaStreamDestroy(p->host_stream);
   delete p;
 }
 
@@ -649,8 +654,8 @@ int icls_solve(csd_icls* p, const float* b, const double* b64, int64_t n, int64_
 }  // namespace
 
 // The solver on HOST buffers (b [n][voxel_stride] float, x [n][nparam],
-// niter / mask / pred optional): device staging, one solve, copies back;
-// synchronous.  The solve dominates (milliseconds per thousand voxels against
+// niter / mask / pred optional): device staging (kept with the problem for
+// later calls, with its stream), one solve, copies back; synchronous.  The solve dominates (milliseconds per thousand voxels against
 // microseconds of transfer), so the copies are not overlapped.
 extern "C" int csd_icls_solve_host(csd_icls* p, const float* b, int64_t n, int64_t voxel_stride,
                                    const uint8_t* mask, float* x, int32_t* niter, float* pred) {
@@ -659,14 +664,22 @@ extern "C" int csd_icls_solve_host(csd_icls* p, const float* b, int64_t n, int64
   if (n == 0) return CSD_OK;
   const size_t nb = (size_t)n * voxel_stride * sizeof(float), nx = (size_t)n * p->nparam * sizeof(float);
   const size_t np = pred ? (size_t)n * p->nmeas * sizeof(float) : 0, nm = mask ? (size_t)n : 0;
-  char* d = nullptr;
   const size_t off_x = (nb + 255) / 256 * 256, off_i = off_x + (nx + 255) / 256 * 256,
                off_p = off_i + ((size_t)n * sizeof(int32_t) + 255) / 256 * 256,
                off_m = off_p + (np + 255) / 256 * 256, total = off_m + nm;
-  cudaError_t e = cudaMalloc(&d, total);
-  if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_NOMEM, std::string("csd_icls_solve_host: ") + cudaGetErrorString(e));
-  cudaStream_t st = nullptr;
-  e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  cudaError_t e = cudaSuccess;
+  if (total > p->host_ws_bytes) {  // the staging buffer is kept for later calls
+    cudaFree(p->d_host_ws);
+    p->d_host_ws = nullptr;
+    p->host_ws_bytes = 0;
+    e = cudaMalloc(&p->d_host_ws, total);
+    if (e != cudaSuccess)
+      return csdb200::set_error(CSD_ERR_NOMEM, std::string("csd_icls_solve_host: ") + cudaGetErrorString(e));
+    p->host_ws_bytes = total;
+  }
+  if (!p->host_stream) e = cudaStreamCreateWithFlags(&p->host_stream, cudaStreamNonBlocking);
+  char* d = p->d_host_ws;
+  cudaStream_t st = p->host_stream;
   if (e == cudaSuccess) e = cudaMemcpyAsync(d, b, nb, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && mask) e = cudaMemcpyAsync(d + off_m, mask, nm, cudaMemcpyHostToDevice, st);
   int rc = CSD_OK;
@@ -682,9 +695,7 @@ extern "C" int csd_icls_solve_host(csd_icls* p, const float* b, int64_t n, int64
   if (st) {
     const cudaError_t e2 = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = e2;
-    cudaStreamDestroy(st);
   }
-  cudaFree(d);
   if (rc != CSD_OK) return rc;
   if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_icls_solve_host: ") + cudaGetErrorString(e));
   return CSD_OK;

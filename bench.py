@@ -54,6 +54,9 @@ WEIGHTS = os.path.join(ROOT, "mrtrix3_b200", "data", "warmstart_c5.npz")
 SOLVE_DRAM_BYTES_PER_VOXEL = (126.449152e6 + 47.146496e6) / 262144
 
 
+FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -419,7 +422,11 @@ def main():
                 "algorithmic_flops_per_launch": flops / solve_launches,
                 "avg_launch_ms": wstats["ms_solve"] / solve_launches,
                 "flops_counted": "sum over solves of k*n(n+1) + n^3/3 + 2n^2 (n=45, k=|negative set|)",
-                "kernel_share_of_step": wstats["ms_solve"] / ms_warm}
+                "kernel_share_of_step": wstats["ms_solve"] / ms_warm,
+                # context: the factorisation and substitutions run on the FP32 SIMT pipes
+                # (148 SMs x 128 FMA lanes x 2 flops x 1.965 GHz, nominal, not measured)
+                "fp32_simt_nominal_tflops": FP32_SIMT_NOMINAL_TFLOPS,
+                "frac_of_fp32_simt_nominal": achieved / FP32_SIMT_NOMINAL_TFLOPS}
 
     # ---- end to end through the host-buffer C ABI (pinned buffers) ---------
     pinned = torch.from_numpy(vol.dwi).pin_memory()

@@ -266,6 +266,21 @@ int csd_amp2response_accumulate(const float* amp, int64_t n_voxels, int64_t voxe
                                 const uint8_t* mask, const double* dirs, int n_dirs, const int* volumes, int lmax,
                                 double* M, double* b, void* stream);
 
+/* ---- dwi2tensor (cmd/dwi2tensor.cpp:106-135) with tensor2metric's FA and
+ *      principal eigenvector (cmd/tensor2metric.cpp:156-247), as dwi2response's
+ *      fa / manual algorithms use them: per voxel of dwi ([n][voxel_stride],
+ *      volumes volume_stride apart, device float) the iteratively reweighted
+ *      log-linear fit (iter reweightings, default 2; ols: unweighted start)
+ *      with bmat = -grad2bmatrix (device double [n_volumes][7], rows [-b gx^2,
+ *      -b gy^2, -b gz^2, -2b gx gy, -2b gx gz, -2b gy gz, 1]), FP64.  Outputs
+ *      (device float): dt [n][dt_stride] = Dxx Dyy Dzz Dxy Dxz Dyz; b0 [n],
+ *      fa [n] and vec [n][3] (the principal eigenvector times FA) or NULL.
+ *      Voxels outside `mask` (device uint8 or NULL) give zeros.  Returns
+ *      without synchronising. */
+int csd_dwi2tensor(const float* dwi, int64_t n_voxels, int64_t voxel_stride, int64_t volume_stride,
+                   const double* bmat, int n_volumes, const uint8_t* mask, int iter, int ols, float* dt,
+                   int64_t dt_stride, float* b0, float* fa, float* vec, void* stream);
+
 /* ---- inequality-constrained least squares, batched: the solver of
  *      dwi2fod msmt_csd (src/dwi/sdeconv/msmt_csd.h:249-270) and of
  *      Math::ICLS (core/math/constrained_least_squares.h).

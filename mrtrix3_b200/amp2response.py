@@ -103,6 +103,31 @@ def fit(M, b, lmax: int, constrained: bool = True) -> np.ndarray:
     return x.cpu().numpy()[0]
 
 
+def responses(amp, fibre_dir, mask, dirs_azel, volumes, lmax, constrained: bool = True) -> np.ndarray:
+    """The response rows for the shells given by their [az el] directions and
+    volume indices (device amp [n][volumes], fibre_dir [n][3], mask [n]):
+    [shells][lmax_max/2 + 1], each row padded with zeros."""
+    max_lmax = max(lmax)
+    rows = []
+    for s, (da, vols, L) in enumerate(zip(dirs_azel, volumes, lmax)):
+        if L and not np.isfinite(zonal_amp_transform(da[:, 1], L)).all():
+            raise ValueError(f"Unable to construct A2SH transformation for shell {s}; lmax ({L}) may be too large "
+                             "for this shell")
+        cart = np.stack([np.cos(da[:, 0]) * np.sin(da[:, 1]), np.sin(da[:, 0]) * np.sin(da[:, 1]), np.cos(da[:, 1])],
+                        axis=1)
+        M, b = accumulate(amp, fibre_dir, cart, vols, L, mask)
+        rf = fit(M, b, L, constrained=constrained)
+        row = np.zeros(max_lmax // 2 + 1)
+        row[:len(rf)] = rf
+        rows.append(row)
+    return np.array(rows)
+
+
+def default_lmax(n_shells: int, first_is_bzero: bool):
+    """amp2response.cpp:287-294: 0 for a b=0 first shell, else 10."""
+    return [0 if (i == 0 and first_is_bzero) else 10 for i in range(n_shells)]
+
+
 def _parse(argv):
     pos, opt = [], {}
     i = 0
@@ -169,8 +194,7 @@ def run(argv) -> int:
         if any(l % 2 for l in lmax):
             raise SystemExit("Values specified for lmax must be even")
     else:
-        lmax = [0 if (i == 0 and shells_b0) else 10 for i in range(len(dirs_azel))]
-    max_lmax = max(lmax)
+        lmax = default_lmax(len(dirs_azel), shells_b0)
     m = mif.read(mask_path)
     if m.data.shape[:3] != (nx, ny, nz_) or int(np.prod(m.data.shape[3:])) != 1:
         raise SystemExit("amp2response: the mask must be a 3-D image of the amplitude image's dimensions")
@@ -186,19 +210,11 @@ def run(argv) -> int:
     amp = torch.from_numpy(np.ascontiguousarray(img.data.reshape(-1, nvol), np.float32)).to(dev)
     fdir = torch.from_numpy(np.ascontiguousarray(dimg.data.reshape(-1, dimg.data.shape[3])[:, :3], np.float32)).to(dev)
     mk = torch.from_numpy(mask.astype(np.uint8)).to(dev)
-    rows = []
-    for s, (da, vols, L) in enumerate(zip(dirs_azel, volumes, lmax)):
-        if L and not np.isfinite(zonal_amp_transform(da[:, 1], L)).all():
-            raise SystemExit(f"Unable to construct A2SH transformation for shell {s}; lmax ({L}) may be too large "
-                             "for this shell")
-        cart = np.stack([np.cos(da[:, 0]) * np.sin(da[:, 1]), np.sin(da[:, 0]) * np.sin(da[:, 1]), np.cos(da[:, 1])],
-                        axis=1)
-        M, b = accumulate(amp, fdir, cart, vols, L, mk)
-        rf = fit(M, b, L, constrained=not opt.get("-noconstraint"))
-        row = np.zeros(max_lmax // 2 + 1)
-        row[:len(rf)] = rf
-        rows.append(row)
-    np.savetxt(out_path, np.array(rows), fmt="%.10g")
+    try:
+        rows = responses(amp, fdir, mk, dirs_azel, volumes, lmax, constrained=not opt.get("-noconstraint"))
+    except ValueError as e:
+        raise SystemExit(str(e))
+    np.savetxt(out_path, rows, fmt="%.10g")
     return 0
 
 

@@ -35,7 +35,7 @@ EXPORTED = [
     "csd_state_fod",
     "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_amp2sh_rician", "csd_icls_create",
     "csd_icls_destroy", "csd_icls_info", "csd_icls_solve", "csd_icls_solve_host", "csd_icls_create_standard", "csd_icls_solve_f64",
-    "csd_amp2response_accumulate", "csd_last_error",
+    "csd_amp2response_accumulate", "csd_dwi2tensor", "csd_last_error",
 ]
 
 
@@ -103,6 +103,8 @@ def lib():
         L.csd_icls_create_standard.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.POINTER(vp)]
         L.csd_icls_solve_f64.argtypes = [vp, vp, i64, i64, i64, vp, i64, vp, vp]
+        L.csd_dwi2tensor.argtypes = [vp, i64, i64, i64, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, i64,
+                                     vp, vp, vp, vp]
         L.csd_amp2response_accumulate.argtypes = [vp, i64, i64, i64, vp, i64, i64, vp, vp, ctypes.c_int, vp,
                                                   ctypes.c_int, vp, vp, vp]
         L.csd_sh2peaks.argtypes = [vp, i64, i64, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float,

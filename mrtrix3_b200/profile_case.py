@@ -1,7 +1,7 @@
 """Run one CSD method on a synthetic case, for profilers (ncu) and timing.
 
     python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
-        [--method warm|plain|persistent|persistent_warm|predict|peaks|amp2sh|msmt] [--reps 2]
+        [--method warm|plain|persistent|persistent_warm|predict|peaks|amp2sh|msmt|tensor|amp2response] [--reps 2]
         [--projection mma|tcgen05] [--solve warp|group16|group8] [--amp2sh-kernel auto|row|tile|mma]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
@@ -20,7 +20,7 @@ def main():
     ap.add_argument("--dims", type=int, nargs=3, default=[64, 64, 64])
     ap.add_argument("--lmax", type=int, default=8)
     ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm", "predict", "peaks",
-                                                          "amp2sh", "msmt"])
+                                                          "amp2sh", "msmt", "tensor", "amp2response"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--projection", default="tcgen05", choices=["mma", "tcgen05"])
     ap.add_argument("--solve", default="warp", choices=["warp", "group16", "group8"])
@@ -32,6 +32,37 @@ def main():
     autotune.set_knob(autotune.KNOB_TC_PROJECTION, 2 if a.projection == "tcgen05" else 1)
     autotune.set_knob(autotune.KNOB_SOLVE_KIND, {"warp": 1, "group16": 2, "group8": 3}[a.solve])
     autotune.set_knob(autotune.KNOB_AMP2SH_KIND, ["auto", "row", "tile", "mma"].index(a.amp2sh_kernel))
+    if a.method in ("tensor", "amp2response"):
+        # the tensor fit (FA, principal vector) of a 4-shell volume, then the
+        # amp2response accumulation over every voxel of its largest shell
+        from . import amp2response as AR
+        from . import msmt
+        from .tensor import dwi2tensor
+        grad = synth.msmt_scheme()
+        n = int(np.prod(a.dims))
+        rng = np.random.default_rng(3)
+        clean = 1000.0 * np.exp(-grad[:, 3] * 0.8e-3)[None, :].repeat(n, axis=0)
+        dwi = torch.from_numpy(synth.rician(rng, clean, 20.0)).float().cuda()  # isotropic, SNR 50 at b=0
+        g = msmt.normalise_scheme(grad)
+        vols = msmt.cluster_shells(g[:, 3])[-1]
+        da = msmt.direction_matrix(g, vols)
+        cart = np.stack([np.cos(da[:, 0]) * np.sin(da[:, 1]), np.sin(da[:, 0]) * np.sin(da[:, 1]), np.cos(da[:, 1])], 1)
+        _, _, _, vec = dwi2tensor(dwi, grad)
+        vec = vec + torch.tensor([0.0, 0.0, 1.0], device=vec.device)  # a direction everywhere
+        run = (lambda: dwi2tensor(dwi, grad)) if a.method == "tensor" else \
+            (lambda: AR.accumulate(dwi, vec, cart, vols, 10))
+        run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.reps):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+        print(f"{a.method}: {n} voxels x {grad.shape[0]} volumes in {ms:.3f} ms per call "
+              f"({n / ms / 1e3:.1f}M voxels/s)")
+        return
     if a.method == "msmt":  # 3-tissue MSMT-CSD on a 4-shell scheme (6 b=0 + 30/45/60 DW)
         from . import msmt
         s = msmt.MSMTShared(synth.msmt_scheme())

@@ -123,3 +123,29 @@ def test_icls_create_rejects_bad_problems():
                  (H.ctypes.data, 4, 300, A.ctypes.data, 3, None, 0, 0.0, 0.0, 0, 0.0)]:  # too many parameters
         assert L.csd_icls_create(*args, ctypes.byref(h)) == csd.CSD_ERR_INVALID
         assert not h.value
+
+
+def test_top_threshold_rule():
+    """mrthreshold -top N: the value at index size - N of the sorted finite
+    values, voxels >= it selected (ties at the threshold all kept)."""
+    from mrtrix3_b200.dwi2response import top_threshold
+    v = np.array([0.1, 0.5, np.nan, 0.3, 0.9, 0.5, 0.0])
+    assert top_threshold(v, 2) == 0.5
+    assert np.sum(v >= top_threshold(v, 2)) == 3  # the tie at 0.5 keeps both
+    assert top_threshold(v, 6) == 0.0
+    with pytest.raises(SystemExit, match="less than number of voxels"):
+        top_threshold(v, 7)
+
+
+def test_dwi2response_argument_errors(tmp_path):
+    from mrtrix3_b200.dwi2response import run
+    with pytest.raises(SystemExit, match="usage"):
+        run(["tournier", "a.mif", "r.txt"])
+    with pytest.raises(SystemExit, match="wrong number of arguments"):
+        run(["manual", "a.mif", "r.txt"])
+    with pytest.raises(SystemExit, match="-mask is required"):
+        run(["fa", "a.mif", str(tmp_path / "r.txt")])
+    out = tmp_path / "r.txt"
+    out.write_text("1\n")
+    with pytest.raises(SystemExit, match="already exists"):
+        run(["fa", "a.mif", str(out), "-mask", "m.mif"])

@@ -16,7 +16,7 @@ coefficients, padded to the largest lmax.
 
 Options: -lmax l1,l2,.. (one per shell; default 0 for a b=0 shell, else
 10), -isotropic (lmax 0 everywhere), -noconstraint, -directions file,
--grad file, -force.
+-shells b1,b2,.. (Shells::select_shells), -grad file, -force.
 """
 from __future__ import annotations
 
@@ -154,8 +154,6 @@ def run(argv) -> int:
     pos, opt = _parse(argv)
     if len(pos) != 4:
         raise SystemExit("usage: python -m mrtrix3_b200.amp2response <amps> <mask> <directions> <response> [options]")
-    if "-shells" in opt:
-        raise SystemExit("amp2response: -shells is not provided")
     amp_path, mask_path, dir_path, out_path = pos
     if os.path.exists(out_path) and not opt.get("-force"):
         raise SystemExit(f"amp2response: output file \"{out_path}\" already exists (use -force to replace it)")
@@ -181,6 +179,12 @@ def run(argv) -> int:
             raise SystemExit("amp2response: no directions or diffusion encoding found")
         grad = msmt.normalise_scheme(grad)
         shells = msmt.cluster_shells(grad[:, 3])
+        if "-shells" in opt:
+            try:
+                keep = msmt.select_shells(grad[:, 3], shells, [float(v) for v in opt["-shells"].split(",")])
+            except ValueError as e:
+                raise SystemExit(f"amp2response: {e}")
+            shells = [shells[i] for i in keep]
         shells_b0 = float(np.mean(grad[shells[0], 3])) <= 10.0
         volumes = shells
         dirs_azel = [msmt.direction_matrix(grad, v) for v in shells]

@@ -29,7 +29,8 @@ Options (csd.cpp:318-346, dwi2fod.cpp:38-59, gradient.cpp:36-60):
 
 msmt_csd (dwi2fod.cpp:283-326, msmt_csd.cpp:24-48): one response file per
 tissue ([shells][even zonal coefficients]) and one output per tissue, every
-b-value shell used; -lmax takes one value per tissue; -norm_lambda /
+b-value shell used (or those -shells b1,b2,.. selects); -lmax takes one
+value per tissue; -norm_lambda /
 -neg_lambda default 1e-10; -predicted_signal image writes the modelled DW
 signal (float32, the input's layout); -mask, -directions, -grad as above.
 """
@@ -43,7 +44,7 @@ import numpy as np
 from . import mif
 
 _VALUED = {"-mask", "-lmax", "-directions", "-filter", "-neg_lambda", "-norm_lambda", "-threshold", "-niter",
-           "-grad", "-warm_start", "-nthreads", "-predicted_signal"}
+           "-grad", "-warm_start", "-nthreads", "-predicted_signal", "-shells"}
 _FLAGS = {"-force", "-quiet", "-info"}
 
 
@@ -101,6 +102,8 @@ def run(argv) -> int:
     if os.path.exists(out_path) and not opt.get("-force"):
         raise SystemExit(f"dwi2fod: output image \"{out_path}\" already exists (use -force to replace it)")
 
+    if "-shells" in opt:
+        raise SystemExit("dwi2fod csd: -shells is not provided (the largest non-b=0 shell is used)")
     from . import csd
     img = mif.read(dwi_path)
     if img.data.ndim != 4:
@@ -200,7 +203,11 @@ def run_msmt(pos, opt) -> int:
             raise SystemExit(f"dwi2fod: output image \"{o}\" already exists (use -force to replace it)")
     from . import msmt
     img, grad, mask = _load_dwi(pos[1], opt)
-    shared = msmt.MSMTShared(grad)
+    try:
+        shared = msmt.MSMTShared(grad, shells=[float(v) for v in opt["-shells"].split(",")] if "-shells" in opt
+                                 else None)
+    except ValueError as e:
+        raise SystemExit(f"dwi2fod: {e}")
     kw = {}
     if "-lmax" in opt:
         kw["lmax"] = [int(v) for v in opt["-lmax"].split(",")]

@@ -94,6 +94,75 @@ def cluster_shells(b, bzero_threshold: float = 10.0, bvalue_epsilon: float = 80.
     return shells
 
 
+def _shell_stats(b, vols):
+    """Shell::Shell (dwi/shells.cpp:52-70): mean, sample stdev, min and --
+    as computed there -- "max" = max(running min, b) of the last volume."""
+    bv = np.asarray(b, np.float64)[np.asarray(vols)]
+    mean = float(bv.mean())
+    with np.errstate(invalid="ignore", divide="ignore"):
+        stdev = float(np.sqrt(np.sum((bv - mean) ** 2) / (len(bv) - 1))) if len(bv) > 1 else float("nan")
+    lo = hi = np.inf
+    for x in bv:
+        lo = min(lo, x)
+        hi = max(lo, x)
+    return mean, stdev, float(lo), float(hi)
+
+
+def select_shells(b, shells, requested, bzero_threshold: float = 10.0):
+    """Shells::select_shells with the -shells option (dwi/shells.cpp:100-215):
+    the indices of the shells to keep for the requested b-values."""
+    b = np.asarray(b, np.float64)
+    stats = [_shell_stats(b, v) for v in shells]
+    has_b0 = stats[0][0] <= bzero_threshold
+    keep = [False] * len(shells)
+    b0_selected = False
+
+    def take(s, stat):
+        if keep[s]:
+            raise ValueError(f"User selected a shell more than once: {stat[0]} +- {stat[1]} with {len(shells[s])} "
+                             "volumes")
+        keep[s] = True
+
+    for want in requested:
+        want = float(want)
+        if want < 0:
+            raise ValueError("Cannot select shells corresponding to negative b-values")
+        if want <= bzero_threshold:
+            if not has_b0:
+                raise ValueError("User selected b=0 shell, but no such data was found")
+            if b0_selected:
+                raise ValueError("User selected b=0 shell more than once")
+            keep[0] = True
+            b0_selected = True
+            continue
+        selected = False
+        for s, st in enumerate(stats):
+            if st[2] <= want <= st[3]:
+                take(s, st)
+                selected = True
+        if selected:
+            continue
+        near = [s for s, st in enumerate(stats) if abs(want - st[0]) <= 1.0]
+        if len(near) == 1:
+            take(near[0], stats[near[0]])
+            continue
+        zero_stdev = any(not (st[0] <= bzero_threshold) and st[1] < 1.0 for st in stats)
+        best, best_n, ambiguous = 0, np.inf, False
+        for s, st in enumerate(stats):
+            sd = 0.5 * bzero_threshold if st[0] <= bzero_threshold else (np.sqrt(st[0]) if zero_stdev else st[1])
+            n = abs((want - st[0]) / sd)
+            if n < best_n:
+                ambiguous = n >= 0.1 * best_n
+                best, best_n = s, n
+            else:
+                ambiguous = n < 10.0 * best_n
+        if ambiguous:
+            raise ValueError(f"Unable to robustly select desired shell b={want:g} (detected shells are: "
+                             + ", ".join(f"{st[0]:g} +- {st[1]:g}" for st in stats) + ")")
+        take(best, stats[best])
+    return [s for s in range(len(shells)) if keep[s]]
+
+
 def direction_matrix(grad, vols) -> np.ndarray:
     """DWI::gen_direction_matrix (gradient.h:77-95): [az el] per volume; a
     zero vector gives a NaN elevation, as there."""
@@ -121,9 +190,13 @@ def load_hr_dirs() -> np.ndarray:
 class MSMTShared:
     """MSMT_CSD::Shared.  ``grad`` is the [volumes][4] gradient table."""
 
-    def __init__(self, grad, bzero_threshold: float = 10.0, bvalue_epsilon: float = 80.0):
+    def __init__(self, grad, bzero_threshold: float = 10.0, bvalue_epsilon: float = 80.0, shells=None):
+        """``shells``: the -shells b-values to keep (select_shells); default all."""
         self.grad = normalise_scheme(grad)
         self.shells = cluster_shells(self.grad[:, 3], bzero_threshold, bvalue_epsilon)
+        if shells is not None:
+            keep = select_shells(self.grad[:, 3], self.shells, shells, bzero_threshold)
+            self.shells = [self.shells[i] for i in keep]
         self.HR_dirs = load_hr_dirs()
         self.lmax = None
         self.lmax_response = []

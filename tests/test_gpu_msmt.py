@@ -264,3 +264,23 @@ def test_msmt_host_buffers_equal_device_call(cuda):
     np.testing.assert_array_equal(it_h, it_d.cpu().numpy())
     np.testing.assert_array_equal(pred_h, pred_d.cpu().numpy())
     assert not x_h[mask == 0].any()
+
+
+def test_msmt_shell_subset(cuda):
+    """-shells 0,1000,3000: the volumes of the other shell take no part
+    (their rows of the forward matrix are zero, as in the reference)."""
+    import torch
+    resp = [r[[0, 1, 3]] for r in RESP]
+    s = msmt.MSMTShared(synth.msmt_scheme(), shells=[0, 1000, 3000])
+    assert [len(v) for v in s.shells] == [6, 30, 60]
+    s.set_responses(resp)
+    s.init()
+    assert not s.C[s.grad[:, 3] == 2000.0].any()
+    P = msmt_ref.problem(s.grad, s.shells, resp, [8, 0, 0], s.HR_dirs)
+    rng = np.random.default_rng(25)
+    full = msmt_ref.problem(s.grad, msmt.cluster_shells(s.grad[:, 3]), RESP, [8, 0, 0], s.HR_dirs)
+    dwi = synth.rician(rng, synth.msmt_truth(rng, 200) @ full.H.T, 25.0).astype(np.float32)
+    x, _ = s.solve(torch.from_numpy(dwi).to(cuda))
+    idx = np.arange(0, 200, 5)
+    xr, _ = msmt_ref.solve(P, dwi[idx].astype(np.float64))
+    assert _rel(x.cpu().numpy()[idx].astype(np.float64), xr).max() <= 1e-4

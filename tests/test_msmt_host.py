@@ -149,3 +149,32 @@ def test_dwi2response_argument_errors(tmp_path):
     out.write_text("1\n")
     with pytest.raises(SystemExit, match="already exists"):
         run(["fa", "a.mif", str(out), "-mask", "m.mif"])
+
+
+def test_shell_selection_rules():
+    """Shells::select_shells with -shells (dwi/shells.cpp:100-215): exact
+    range, within 1 of a mean, nearest in standard deviations, the
+    ambiguity rule (the last shell's verdict, as there), b=0, repeats."""
+    g = msmt.normalise_scheme(synth.msmt_scheme())
+    sh = msmt.cluster_shells(g[:, 3])
+    assert msmt.select_shells(g[:, 3], sh, [0, 3000]) == [0, 3]
+    assert msmt.select_shells(g[:, 3], sh, [2000.5]) == [2]
+    assert msmt.select_shells(g[:, 3], sh, [1000, 2000]) == [1, 2]
+    with pytest.raises(ValueError, match="robustly"):
+        msmt.select_shells(g[:, 3], sh, [2100])
+    with pytest.raises(ValueError, match="more than once"):
+        msmt.select_shells(g[:, 3], sh, [1000, 1000.4])
+    with pytest.raises(ValueError, match="b=0 shell more than once"):
+        msmt.select_shells(g[:, 3], sh, [0, 5])
+    with pytest.raises(ValueError, match="negative"):
+        msmt.select_shells(g[:, 3], sh, [-1])
+    g2 = g.copy()
+    g2[6:, 3] += np.random.default_rng(0).uniform(-40, 40, len(g) - 6)
+    sh2 = msmt.cluster_shells(g2[:, 3])
+    assert msmt.select_shells(g2[:, 3], sh2, [1000, 3000]) == [1, 3]
+    # a shell's "max" is its last volume's b-value (shells.cpp:63-64)
+    mean, sd, lo, hi = msmt._shell_stats(g2[:, 3], sh2[1])
+    assert lo == g2[sh2[1], 3].min() and hi == max(lo, g2[sh2[1][-1], 3])
+    # the multi-tissue set-up keeps only the selected shells
+    s = msmt.MSMTShared(synth.msmt_scheme(), shells=[0, 3000])
+    assert [len(v) for v in s.shells] == [6, 60]

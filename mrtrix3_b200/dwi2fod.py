@@ -22,6 +22,7 @@ Options (csd.cpp:318-346, dwi2fod.cpp:38-59, gradient.cpp:36-60):
   -threshold v       amplitude below which a direction is constrained (0)
   -niter N           maximum iterate() calls per voxel (50)
   -grad file         gradient table [x y z b] rows, instead of dw_scheme
+  -fslgrad bvecs bvals   FSL gradient files (image-axis directions)
   -warm_start file   a warm-start network (.npz) trained for this scheme
                      (no counterpart in MRtrix3; off by default)
   -force             overwrite the output
@@ -55,6 +56,12 @@ def _parse(argv):
         a = argv[i]
         if a.startswith("-") and len(a) > 1 and not _is_number(a):
             key = "-" + a.lstrip("-")
+            if key == "-fslgrad":
+                if i + 2 >= len(argv):
+                    raise SystemExit("dwi2fod: option \"-fslgrad\" expects two values (bvecs bvals)")
+                opt[key] = (argv[i + 1], argv[i + 2])
+                i += 3
+                continue
             if key in _VALUED:
                 if i + 1 >= len(argv):
                     raise SystemExit(f"dwi2fod: option \"{a}\" expects a value")
@@ -108,12 +115,10 @@ def run(argv) -> int:
     img = mif.read(dwi_path)
     if img.data.ndim != 4:
         raise SystemExit(f"dwi2fod: input image \"{dwi_path}\" is not 4-D")
-    if "-grad" in opt:
-        grad = mif.load_matrix(opt["-grad"])
-    elif "dw_scheme" in img.keyval:
-        grad = mif.parse_scheme(img.keyval["dw_scheme"])
-    else:
-        raise SystemExit(f"dwi2fod: no diffusion encoding found in image \"{dwi_path}\"")
+    try:
+        grad = mif.dw_scheme(img, opt)
+    except ValueError as e:
+        raise SystemExit(f"dwi2fod: {e} (\"{dwi_path}\")")
     nx, ny, nz, nvol = img.data.shape
     if grad.shape != (nvol, 4):
         raise SystemExit(f"dwi2fod: number of volumes in the gradient table ({grad.shape[0]}) does not match the "
@@ -172,12 +177,10 @@ def _load_dwi(dwi_path, opt):
     img = mif.read(dwi_path)
     if img.data.ndim != 4:
         raise SystemExit(f"dwi2fod: input image \"{dwi_path}\" is not 4-D")
-    if "-grad" in opt:
-        grad = mif.load_matrix(opt["-grad"])
-    elif "dw_scheme" in img.keyval:
-        grad = mif.parse_scheme(img.keyval["dw_scheme"])
-    else:
-        raise SystemExit(f"dwi2fod: no diffusion encoding found in image \"{dwi_path}\"")
+    try:
+        grad = mif.dw_scheme(img, opt)
+    except ValueError as e:
+        raise SystemExit(f"dwi2fod: {e} (\"{dwi_path}\")")
     nvol = img.data.shape[3]
     if grad.shape != (nvol, 4):
         raise SystemExit(f"dwi2fod: number of volumes in the gradient table ({grad.shape[0]}) does not match the "

@@ -17,7 +17,7 @@ each (``-lmax`` one per shell; default 0 for b=0, else 10).
 Options: -mask (required by fa: the brain mask the script would otherwise
 make with dwi2mask, which is not provided here, and which it would then
 erode), -number, -threshold, -lmax, -dirs, -voxels image, -grad file,
--force.
+-fslgrad bvecs bvals, -force.
 """
 from __future__ import annotations
 
@@ -40,6 +40,12 @@ def _parse(argv):
     while i < len(argv):
         a = argv[i]
         key = "-" + a.lstrip("-") if a.startswith("-") and len(a) > 1 else None
+        if key == "-fslgrad":
+            if i + 2 >= len(argv):
+                raise SystemExit("dwi2response: option \"-fslgrad\" expects two values (bvecs bvals)")
+            opt[key] = (argv[i + 1], argv[i + 2])
+            i += 3
+            continue
         if key in _VALUED:
             if i + 1 >= len(argv):
                 raise SystemExit(f"dwi2response: option \"{a}\" expects a value")
@@ -71,12 +77,10 @@ def _load(path, opt):
     img = mif.read(path)
     if img.data.ndim != 4:
         raise SystemExit("dwi2response: the DW image must be 4-D")
-    if "-grad" in opt:
-        grad = mif.load_matrix(opt["-grad"])
-    elif "dw_scheme" in img.keyval:
-        grad = mif.parse_scheme(img.keyval["dw_scheme"])
-    else:
-        raise SystemExit("dwi2response: no diffusion encoding found")
+    try:
+        grad = mif.dw_scheme(img, opt)
+    except ValueError as e:
+        raise SystemExit(f"dwi2response: {e}")
     return img, grad
 
 

@@ -267,3 +267,75 @@ def scheme_to_text(grad: np.ndarray) -> str:
 def parse_scheme(text: str) -> np.ndarray:
     return np.array([[float(v) for v in re.split(r"[ ,;\t]+", line.strip()) if v]
                      for line in text.split("\n") if line.strip()], np.float64)
+
+
+def load_bvecs_bvals(bvecs_path: str, bvals_path: str, transform=None, n_volumes: int | None = None) -> np.ndarray:
+    """An FSL bvecs / bvals pair as an [n][4] gradient table in scanner
+    space (DWI::load_bvecs_bvals, core/dwi/gradient.cpp:127-200): bvals one
+    row (or column), bvecs three rows (or columns), both one entry a volume;
+    the bvecs are in the image axes of a left-handed frame, so the first is
+    negated when the transform's 3x3 part has a positive determinant, then
+    rotated by that part; rows with NaN become b=0 rows (a NaN bval with a
+    valid direction, or a NaN direction with b > 0, is an error)."""
+    try:
+        bvals = load_matrix(bvals_path)
+        bvecs = load_matrix(bvecs_path)
+    except (OSError, ValueError) as e:
+        raise ValueError(f"Unable to import files \"{bvecs_path}\" and \"{bvals_path}\" as FSL bvecs/bvals pair "
+                         f"({e})")
+    if bvals.shape[0] != 1:
+        if bvals.shape[1] == 1:
+            bvals = bvals.T
+        else:
+            raise ValueError(f"bvals file must contain 1 row or column only (file \"{bvals_path}\" has "
+                             f"{bvals.shape[0]})")
+    if bvecs.shape[0] != 3:
+        if bvecs.shape[1] == 3:
+            bvecs = bvecs.T
+        else:
+            raise ValueError(f"bvecs file must contain exactly 3 rows or columns (file \"{bvecs_path}\" has "
+                             f"{bvecs.shape[0]})")
+    if bvals.shape[1] != bvecs.shape[1]:
+        raise ValueError("bvecs and bvals files must have same number of diffusion directions")
+    if n_volumes is not None and bvals.shape[1] != n_volumes:
+        raise ValueError(f"bvecs and bvals files must have same number of diffusion directions as DW-image "
+                         f"(gradients: {bvecs.shape[1]}, image: {n_volumes})")
+    R = np.eye(3) if transform is None else np.asarray(transform, np.float64)[:3, :3]
+    bvecs = bvecs.copy()
+    if np.linalg.det(R) > 0.0:
+        bvecs[0] *= -1.0
+    grad = np.zeros((bvecs.shape[1], 4))
+    grad[:, :3] = (R @ bvecs).T
+    grad[:, 3] = bvals[0]
+    for n in range(len(grad)):
+        zero = False
+        if np.isnan(grad[n, 3]):
+            if np.sum(grad[n, :3] ** 2) > 0.0:
+                raise ValueError("Corrupt content in bvecs/bvals data (NaN present in bval but valid direction in "
+                                 "bvec)")
+            zero = True
+        if np.isnan(grad[n, :3]).any():
+            if grad[n, 3] > 0.0:
+                raise ValueError("Corrupt content in bvecs/bvals data (NaN bvec direction but non-zero value in "
+                                 "bval)")
+            zero = True
+        if zero:
+            grad[n] = 0.0
+    return grad
+
+
+def dw_scheme(img: Image, opt: dict) -> np.ndarray:
+    """The gradient table of a DW image (DWI::get_raw_DW_scheme,
+    gradient.cpp:250-273): -grad file, -fslgrad (bvecs, bvals), else the
+    header's dw_scheme."""
+    if "-grad" in opt and "-fslgrad" in opt:
+        raise ValueError("Diffusion gradient table can be provided using either -grad or -fslgrad option, but NOT "
+                         "both")
+    if "-grad" in opt:
+        return load_matrix(opt["-grad"])
+    if "-fslgrad" in opt:
+        bvecs, bvals = opt["-fslgrad"]
+        return load_bvecs_bvals(bvecs, bvals, img.transform, img.data.shape[3] if img.data.ndim > 3 else 1)
+    if "dw_scheme" in img.keyval:
+        return parse_scheme(img.keyval["dw_scheme"])
+    raise ValueError("no diffusion encoding information found in image")

@@ -126,3 +126,42 @@ def test_cli_rejects_other_algorithms_and_arguments():
         run(["csd", "a", "b"])
     with pytest.raises(SystemExit, match="unknown option"):
         run(["csd", "a", "b", "c", "-bogus"])
+
+
+def test_fsl_bvecs_bvals_import(tmp_path):
+    """DWI::load_bvecs_bvals (core/dwi/gradient.cpp:127-200): rows or
+    columns, the first axis negated for a transform with positive
+    determinant, rotation into scanner space, NaN rows as b=0, errors."""
+    bvecs = np.array([[1.0, 0.0, 0.0, np.nan], [0.0, 1.0, 0.0, np.nan], [0.0, 0.0, 1.0, np.nan]])
+    bvals = np.array([1000.0, 2000.0, 3000.0, 0.0])
+    pv, pb = str(tmp_path / "bvecs"), str(tmp_path / "bvals")
+    np.savetxt(pv, bvecs)
+    np.savetxt(pb, bvals[None, :])
+    # identity transform (det 1 > 0): x negated
+    g = mif.load_bvecs_bvals(pv, pb, np.eye(4)[:3], 4)
+    np.testing.assert_allclose(g[:3], [[-1, 0, 0, 1000], [0, 1, 0, 2000], [0, 0, 1, 3000]])
+    np.testing.assert_array_equal(g[3], 0.0)
+    # a transform with negative determinant (x flipped): no negation, rotation applied
+    T = np.diag([-1.0, 1.0, 1.0, 1.0])[:3]
+    g2 = mif.load_bvecs_bvals(pv, pb, T, 4)
+    np.testing.assert_allclose(g2[:3, :3], [[-1, 0, 0], [0, 1, 0], [0, 0, 1]])
+    # a rotation of 90 degrees about z (det 1): x negated, then rotated
+    Rz = np.array([[0.0, -1.0, 0.0, 5.0], [1.0, 0.0, 0.0, 6.0], [0.0, 0.0, 1.0, 7.0]])
+    g3 = mif.load_bvecs_bvals(pv, pb, Rz, 4)
+    np.testing.assert_allclose(g3[0, :3], Rz[:, :3] @ [-1.0, 0.0, 0.0])
+    # column layout accepted; size checks
+    np.savetxt(pv, bvecs.T)
+    np.savetxt(pb, bvals[:, None])
+    np.testing.assert_allclose(mif.load_bvecs_bvals(pv, pb, np.eye(4)[:3], 4), g)
+    with pytest.raises(ValueError, match="same number of diffusion directions as DW-image"):
+        mif.load_bvecs_bvals(pv, pb, None, 5)
+    # a NaN bval with a valid direction is corrupt
+    bv = bvals.copy()
+    bv[0] = np.nan
+    np.savetxt(pb, bv[None, :])
+    with pytest.raises(ValueError, match="NaN present in bval"):
+        mif.load_bvecs_bvals(pv, pb, None, 4)
+    # the CLI helper: -grad and -fslgrad together are refused
+    img = mif.Image(data=np.zeros((2, 2, 2, 4)), vox=[1.0] * 4, transform=np.eye(4)[:3])
+    with pytest.raises(ValueError, match="NOT both"):
+        mif.dw_scheme(img, {"-grad": "g.txt", "-fslgrad": (pv, pb)})

@@ -178,3 +178,20 @@ def test_shell_selection_rules():
     # the multi-tissue set-up keeps only the selected shells
     s = msmt.MSMTShared(synth.msmt_scheme(), shells=[0, 3000])
     assert [len(v) for v in s.shells] == [6, 60]
+
+
+@pytest.mark.parametrize("lmax", [0, 2, 8, 10, 12])
+def test_amp2response_host_transforms_match_oracle(lmax):
+    """ZSH::init_amp_transform / init_deriv_transform (ZSH.h:66-99) and the
+    constraint matrix at 0..90 degrees (amp2response.cpp:337-344)."""
+    from mrtrix3_b200 import amp2response as AR
+    from oracle import amp2response_ref as AREF
+    els = np.linspace(0.0, np.pi, 37)
+    assert np.abs(AR.zonal_amp_transform(els, lmax) - AREF._zonal(els, lmax, 0)).max() <= 1e-12
+    if lmax:
+        d = AR.zonal_deriv_transform(els, lmax)
+        dr = AREF._zonal(els, lmax, 1)
+        assert np.abs(d[:, 1:] - dr[:, 1:]).max() <= 1e-12 and not d[:, 0].any()
+        C = AR.constraint_matrix(lmax)
+        assert C.shape == (182, lmax // 2 + 1)
+        assert np.abs(C - AREF.constraints(lmax)).max() <= 1e-12

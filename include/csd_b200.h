@@ -354,6 +354,58 @@ int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t vo
  * coefficients. */
 int csd_set_launch_config(int which, int value);
 
+/* ---- fod2fixel's FMLS FOD segmenter (src/dwi/fmls.cpp:118-311,
+ *      cmd/fod2fixel.cpp).
+ *
+ * csd_fmls_tables carries what Segmenter's constructor (fmls.cpp:118-140)
+ * builds, as host arrays: the ndir unit directions [ndir][3] (the 1281-
+ * direction set), their neighbour lists (adj_off [ndir + 1] into adj,
+ * at most 16 a direction), the integration weights [ndir], the SH ->
+ * amplitude matrix [ndir][nsh] of lmax (<= 16), SH::PrecomputedAL's table
+ * [al_ndir][n_al] at elevations n al_inc, FastLookupSet's grid (num_az x
+ * num_el cells from az_begin / el_begin in steps az_step / el_step, cell c
+ * listing grid[grid_off[c] .. grid_off[c + 1])), and the lobe thresholds
+ * (-fmls_integral, -fmls_peak_value, -fmls_lobe_merge_ratio). */
+typedef struct csd_fmls_tables {
+  int ndir, lmax, nsh;
+  const double* unit;
+  const double* weight;
+  const int32_t* adj_off;
+  const int32_t* adj;
+  int n_adj;
+  const double* sh2amp;
+  int al_ndir, n_al;
+  double al_inc;
+  const double* al;
+  int num_az, num_el;
+  double az_begin, el_begin, az_step, el_step;
+  const int32_t* grid_off;
+  const int32_t* grid;
+  int n_grid;
+  double integral_threshold, peak_value_threshold, merge_ratio;
+} csd_fmls_tables;
+
+/* csd_fmls_create replaces FMLS::Segmenter's constructor: checks the tables
+ * and copies them to the current device.  Errors: CSD_ERR_INVALID. */
+typedef struct csd_fmls csd_fmls;
+int csd_fmls_create(const csd_fmls_tables* tables, csd_fmls** out);
+void csd_fmls_destroy(csd_fmls* segmenter);
+
+/* csd_fmls_segment replaces Segmenter::operator() (fmls.cpp:159-311) for n
+ * voxels of SH coefficients (device float [n][voxel_stride], coefficients
+ * coef_stride apart; FP64 inside).  counts (device int32 [n]): the number of
+ * lobes kept in each voxel (0 where mask, device uint8 [n] or NULL, is 0);
+ * fixels (device float [n][max_fixels][8]): per lobe, in the reference's
+ * order, the unit mean direction (3), the direction of the largest peak
+ * (3), the integral (AFD) and the largest peak amplitude; only the first
+ * max_fixels lobes of a voxel are written, so a count above max_fixels asks
+ * for another pass with more room.  A voxel with a non-finite coefficient
+ * has no lobes.  Returns without synchronising; grows a per-warp scratch
+ * buffer on first use. */
+int csd_fmls_segment(csd_fmls* segmenter, const float* fod, int64_t n_voxels, int64_t voxel_stride,
+                     int64_t coef_stride, const uint8_t* mask, int max_fixels, int32_t* counts, float* fixels,
+                     void* stream);
+
 /* Thread-local description of the last failure. */
 const char* csd_last_error(void);
 

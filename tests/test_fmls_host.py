@@ -1,0 +1,229 @@
+"""CPU tests of fod2fixel's FMLS segmenter: the direction set and its tables
+(mrtrix3_b200.directions / fmls), and the segmentation core
+(csrc/fmls_core.cuh) built for the host and compared with the oracle's
+literal restatement of Segmenter::operator() (oracle/fmls_ref.py)."""
+import ctypes
+import math
+import os
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from mrtrix3_b200 import directions, fmls, sh  # noqa: E402
+from oracle import fmls_ref  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def dirset():
+    u = directions.unit_vectors(directions.load_tessellation_1281())
+    return u, directions.adjacency_1281()
+
+
+def test_tessellation_and_adjacency(dirset):
+    u, adj = dirset
+    assert u.shape == (1281, 3)
+    np.testing.assert_allclose(np.linalg.norm(u, axis=1), 1.0, atol=1e-12)
+    deg = np.array([len(a) for a in adj])
+    # a geodesic sphere of 2562 points, antipodes merged: 12 / 2 vertices of
+    # degree 5, the rest 6; 7680 / 2 edges
+    assert (deg == 5).sum() == 6 and (deg == 6).sum() == 1275 and deg.sum() // 2 == 3840
+    for i, a in enumerate(adj):
+        assert i not in a and list(a) == sorted(a)
+        for j in a:
+            assert i in adj[j]
+
+
+def test_adjacency_file_matches_hull(dirset):
+    u, adj = dirset
+    again = directions.hull_adjacency(u)
+    assert all(np.array_equal(a, b) for a, b in zip(adj, again))
+
+
+def test_integration_weights(dirset):
+    u, _ = dirset
+    w = directions.integration_weights(u)
+    # a least-squares fit over 1326 basis functions (lmax 50) with 1281 weights
+    assert abs(w.sum() - 4.0 * math.pi) < 1e-6
+    azel = np.stack([np.arctan2(u[:, 1], u[:, 0]), np.arccos(u[:, 2])], axis=1)
+    Y = sh.init_transform(azel, 16)
+    integ = w @ Y
+    assert abs(integ[0] - 2.0 * math.sqrt(math.pi)) < 1e-6
+    assert np.abs(integ[1:]).max() < 1e-6
+
+
+def test_fast_lookup_matches_exhaustive(dirset):
+    u, adj = dirset
+    look = directions.FastLookup(u, adj)
+    rng = np.random.default_rng(3)
+    p = rng.normal(size=(3000, 3))
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    for q in p:
+        assert look.select_direction(q) == int(np.argmax(np.abs(u @ q)))
+    for i in range(0, 1281, 97):  # the set's own directions
+        assert look.select_direction(u[i]) == i
+
+
+def test_precomputed_al_rows():
+    tab = directions.precomputed_al(8, 2562)
+    el = 100 * math.pi / 2561
+    for m in range(9):
+        P = sh.plm_sph(8, m, np.array([math.cos(el)]))
+        for l in range(m + (m & 1), 9, 2):
+            assert abs(tab[100, l * l // 4 + m] - P[l][0]) < 1e-13
+    assert np.all(tab[0, [l * l // 4 + m for l in range(0, 9, 2) for m in range(1, l + 1)]] == 0.0)
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    out = tmp_path_factory.mktemp("fmls") / "libfmls_host.so"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-o", str(out),
+                    os.path.join(ROOT, "tests", "fmls_host_harness.cpp")], check=True)
+    return ctypes.CDLL(str(out))
+
+
+def synthetic_fods(n, lmax, seed, noise):
+    """Sums of 1-3 truncated delta functions with random weights and
+    directions, DC scaled into [0.1, 0.5], plus Gaussian noise on every
+    coefficient (which makes small positive and negative lobes)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        k = int(rng.integers(1, 4))
+        azel = np.stack([rng.uniform(-np.pi, np.pi, k), np.arccos(rng.uniform(-1, 1, k))], 1)
+        c = (rng.uniform(0.3, 1.0, k)[:, None] * sh.init_transform(azel, lmax)).sum(0)
+        c = c / c[0] * rng.uniform(0.1, 0.5)
+        c = c + rng.normal(0.0, noise, c.shape)
+        c[0] = abs(c[0])
+        out.append(c)
+    return np.array(out)
+
+
+def host_segment(lib, tables, rows, max_out=64):
+    ct = fmls.c_tables(tables)
+    rows = np.ascontiguousarray(rows, np.float64)
+    counts = np.zeros(len(rows), np.int32)
+    fx = np.zeros((len(rows), max_out, 8), np.float32)
+    lib.fmls_host_segment(ctypes.byref(ct), ctypes.c_void_p(rows.ctypes.data), len(rows), max_out,
+                          ctypes.c_void_p(counts.ctypes.data), ctypes.c_void_p(fx.ctypes.data))
+    return counts, fx
+
+
+def oracle_rows(seg, rows):
+    return [seg(r) for r in rows]
+
+
+def compare(counts, fx, ref, atol=1e-6):
+    for v, lobes in enumerate(ref):
+        assert counts[v] == len(lobes), f"voxel {v}: {counts[v]} lobes, oracle {len(lobes)}"
+        for q, lb in enumerate(lobes[:fx.shape[1]]):
+            want = np.concatenate([lb["mean_dir"], lb["peak_dir"], [lb["integral"], lb["max_peak"]]])
+            np.testing.assert_allclose(fx[v, q], want.astype(np.float32), rtol=1e-6, atol=atol)
+
+
+@pytest.mark.parametrize("lmax,noise,merge,integral,peak", [
+    (8, 0.01, 1.0, 0.0, 0.1),     # fod2fixel's defaults
+    (8, 0.05, 1.0, 0.0, 0.0),     # -fmls_no_thresholds: every positive lobe
+    (8, 0.02, 0.5, 0.0, 0.1),     # lobes merged across bridges
+    (12, 0.02, 0.3, 0.01, 0.05),
+    (6, 0.003, 0.8, 0.0, 0.1),
+    (10, 0.03, 0.0, 0.0, 0.1),    # merge ratio 0: every bridge merges
+])
+def test_core_matches_oracle(harness, lmax, noise, merge, integral, peak):
+    T = fmls.FMLSTables(lmax, integral, peak, merge)
+    seg = fmls_ref.Segmenter(lmax, integral, peak, merge)
+    rows = synthetic_fods(24, lmax, seed=lmax * 100 + int(noise * 1000), noise=noise)
+    counts, fx = host_segment(harness, T, rows)
+    compare(counts, fx, oracle_rows(seg, rows))
+    assert counts.sum() > 0
+
+
+def test_core_merges_lobes(harness):
+    # at merge ratio 0 a lobe holds the peaks of the lobes it absorbed: fewer,
+    # larger lobes than with the default ratio 1
+    rows = synthetic_fods(16, 8, seed=11, noise=0.03)
+    c1, _ = host_segment(harness, fmls.FMLSTables(8, 0.0, 0.0, 1.0), rows)
+    c0, _ = host_segment(harness, fmls.FMLSTables(8, 0.0, 0.0, 0.0), rows)
+    assert c0.sum() < c1.sum()
+
+
+def test_core_edge_cases(harness):
+    T = fmls.FMLSTables(8)
+    seg = fmls_ref.Segmenter(8)
+    n = sh.n_for_l(8)
+    iso = np.zeros(n)
+    iso[0] = 1.0                       # constant amplitude: every direction tied, taken in index order
+    neg_dc = synthetic_fods(1, 8, 5, 0.01)[0]
+    neg_dc[0] = -neg_dc[0]             # DC not positive: no lobes
+    nan_row = synthetic_fods(1, 8, 6, 0.01)[0]
+    nan_row[7] = np.nan                # a non-finite coefficient: no lobes
+    neg_fod = -synthetic_fods(1, 8, 7, 0.0)[0]
+    neg_fod[0] = 1e-3                  # the largest-magnitude amplitude negative: no lobes
+    zero = np.zeros(n)
+    rows = np.array([iso, neg_dc, nan_row, neg_fod, zero])
+    counts, fx = host_segment(harness, T, rows)
+    assert list(counts[1:]) == [0, 0, 0, 0]
+    # ties break by index, so directions that are not neighbours seed lobes of
+    # their own (hundreds of them) and the bridges between them are assigned
+    # afterwards: as the reference's ordered multimap does
+    ref = seg(iso)
+    assert len(ref) > 100
+    compare(counts[:1], fx[:1], [ref])
+    assert abs(sum(lb["integral"] for lb in ref) - 4.0 * math.pi * sh.init_transform(np.zeros((1, 2)), 8)[0, 0]) < 1e-5
+
+
+def test_core_max_out_counts_all(harness):
+    rows = synthetic_fods(8, 8, seed=9, noise=0.05)
+    T = fmls.FMLSTables(8, 0.0, 0.0, 1.0)
+    c_all, f_all = host_segment(harness, T, rows, max_out=64)
+    c2, f2 = host_segment(harness, T, rows, max_out=2)
+    assert np.array_equal(c_all, c2)   # the count is every lobe kept, whatever fits
+    np.testing.assert_array_equal(f2, f_all[:, :2])
+
+
+def test_pack_offsets_and_disp():
+    counts = np.array([2, 0, 1])
+    fx = np.zeros((3, 2, 8), np.float32)
+    fx[0, 0] = [1, 0, 0, 0, 1, 0, 2.0, 4.0]
+    fx[0, 1] = [0, 1, 0, 0, 0, 1, 1.0, 3.0]
+    fx[2, 0] = [0, 0, 1, 1, 0, 0, 0.5, 0.25]
+    c, off, d, afd, pk, disp = fmls.pack(counts, fx)
+    assert list(off) == [0, 2, 2] and list(afd) == [2.0, 1.0, 0.5]
+    np.testing.assert_array_equal(d[2], [0, 0, 1])
+    np.testing.assert_array_equal(disp, np.float32([0.5, 1.0 / 3.0, 2.0]))
+    _, _, dp, _, _, _ = fmls.pack(counts, fx, dirpeak=True)
+    np.testing.assert_array_equal(dp[2], [1, 0, 0])
+
+
+def test_cli_argument_errors(tmp_path):
+    from mrtrix3_b200 import fod2fixel, mif
+    with pytest.raises(SystemExit, match="usage"):
+        fod2fixel.run(["only_one"])
+    with pytest.raises(SystemExit, match="nii"):
+        fod2fixel.run(["a.mif", "b", "-nii"])
+    bad = tmp_path / "bad.mif"
+    mif.write(str(bad), mif.Image(data=np.zeros((2, 2, 2, 7), np.float32), vox=[1, 1, 1, 1]))
+    with pytest.raises(SystemExit, match="SH series"):
+        fod2fixel.run([str(bad), str(tmp_path / "out")])
+    with pytest.raises(SystemExit, match="merge_ratio"):
+        fod2fixel.thresholds({"-fmls_lobe_merge_ratio": "1.5"})
+    assert fod2fixel.thresholds({"-fmls_no_thresholds": True, "-fmls_peak_value": "0.3"}) == (0.0, 0.0, 1.0)
+    # unambiguous prefixes, as dwi2response's scripts pass "-peak" for -peak_amp
+    pos, opt = fod2fixel._parse(["f.mif", "d", "-peak", "p.mif", "-fmls_no_thr"])
+    assert pos == ["f.mif", "d"] and opt == {"-peak_amp": "p.mif", "-fmls_no_thresholds": True}
+    with pytest.raises(SystemExit, match="unknown option"):
+        fod2fixel._parse(["-fmls"])
+    full = tmp_path / "full"
+    full.mkdir()
+    (full / "x").write_text("")
+    good = tmp_path / "good.mif"
+    mif.write(str(good), mif.Image(data=np.zeros((2, 2, 2, 15), np.float32), vox=[1, 1, 1, 1]))
+    with pytest.raises(SystemExit, match="not empty"):
+        fod2fixel.run([str(good), str(full)])

@@ -1,0 +1,135 @@
+"""GPU parity of fod2fixel's FMLS segmenter (csd_fmls_segment through the C
+ABI) against the oracle's restatement of Segmenter::operator()
+(oracle/fmls_ref.py): per voxel the same lobes in the same order.  The
+amplitudes are FP64 on both sides but summed in another order, so a lobe
+boundary may move where two amplitudes tie to rounding: counts must agree
+on at least 98% of voxels and the values of agreeing voxels to 1e-4."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+pytestmark = pytest.mark.gpu
+
+
+def _fods(n, lmax, seed, noise):
+    from test_fmls_host import synthetic_fods
+    return synthetic_fods(n, lmax, seed, noise)
+
+
+def _segment(rows, lmax, mask=None, max_fixels=0, **kw):
+    import torch
+
+    from mrtrix3_b200 import fmls
+    seg = fmls.Segmenter(lmax, **kw)
+    c, f = seg.segment(torch.from_numpy(np.ascontiguousarray(rows, np.float32)).cuda(),
+                       None if mask is None else torch.from_numpy(mask.astype(np.uint8)).cuda(),
+                       max_fixels=max_fixels)
+    torch.cuda.synchronize()
+    return c.cpu().numpy(), f.cpu().numpy()
+
+
+def _check(counts, fx, rows, lmax, atol=1e-4, min_agree=0.98, **kw):
+    from oracle import fmls_ref
+    seg = fmls_ref.Segmenter(lmax, **{k: v for k, v in kw.items()})
+    agree = 0
+    for v, r in enumerate(rows.astype(np.float32).astype(np.float64)):
+        lobes = seg(r)
+        if len(lobes) != counts[v]:
+            continue
+        agree += 1
+        for q, lb in enumerate(lobes[:fx.shape[1]]):
+            want = np.concatenate([lb["mean_dir"], lb["peak_dir"], [lb["integral"], lb["max_peak"]]])
+            np.testing.assert_allclose(fx[v, q], want, rtol=1e-4, atol=atol)
+    assert agree >= min_agree * len(rows), f"{agree} of {len(rows)} voxels agree"
+
+
+@pytest.mark.parametrize("lmax,noise", [(8, 0.01), (8, 0.04), (6, 0.02), (10, 0.02)])
+def test_segment_matches_oracle(lmax, noise):
+    rows = _fods(60, lmax, seed=lmax + int(noise * 100), noise=noise)
+    counts, fx = _segment(rows, lmax)
+    assert counts.sum() > 0
+    _check(counts, fx, rows, lmax)
+
+
+def test_segment_thresholds_and_merging():
+    rows = _fods(40, 8, seed=21, noise=0.03)
+    kw = dict(integral_threshold=0.01, peak_value_threshold=0.05, merge_ratio=0.4)
+    counts, fx = _segment(rows, 8, **kw)
+    _check(counts, fx, rows, 8, **kw)
+
+
+def test_segment_mask_layout_and_invalid_rows():
+    import torch
+
+    from mrtrix3_b200 import fmls, sh
+    n = sh.n_for_l(8)
+    rows = _fods(30, 8, seed=4, noise=0.01).astype(np.float32)
+    rows[3, 0] = -1.0
+    rows[5, 9] = np.nan
+    mask = np.ones(30, bool)
+    mask[[1, 7]] = False
+    c_ref, f_ref = _segment(rows, 8, mask=mask)
+    assert c_ref[1] == 0 and c_ref[7] == 0 and c_ref[3] == 0 and c_ref[5] == 0
+    # coefficient-major storage ([nsh][n], coefficients n apart)
+    t = torch.from_numpy(np.ascontiguousarray(rows.T)).cuda().t()
+    seg = fmls.Segmenter(8)
+    c2, f2 = seg.segment(t, torch.from_numpy(mask.astype(np.uint8)).cuda())
+    np.testing.assert_array_equal(c2.cpu().numpy(), c_ref)
+    np.testing.assert_array_equal(f2.cpu().numpy(), f_ref)
+    assert t.shape[1] == n
+
+
+def test_segment_overflow_and_maxnum():
+    # an isotropic FOD (every amplitude tied: hundreds of lobes) among others
+    rows = _fods(12, 8, seed=8, noise=0.06)
+    rows[4] = 0.0
+    rows[4, 0] = 0.5
+    kw = dict(integral_threshold=0.0, peak_value_threshold=0.0)
+    counts, fx = _segment(rows, 8, **kw)
+    assert counts.max() > 16        # voxels run again with room for all their lobes
+    assert fx.shape[1] == counts.max()
+    _check(counts, fx, rows, 8, **kw)
+    c3, f3 = _segment(rows, 8, max_fixels=3, **kw)
+    np.testing.assert_array_equal(c3, np.minimum(counts, 3))
+    np.testing.assert_array_equal(f3, fx[:, :3])
+
+
+def test_fod2fixel_cli(tmp_path):
+    from mrtrix3_b200 import fmls, fod2fixel, mif
+    from oracle import fmls_ref
+    nx, ny, nz = 4, 3, 2
+    rows = _fods(nx * ny * nz, 8, seed=31, noise=0.01).astype(np.float32)
+    data = rows.reshape(nz, ny, nx, -1).transpose(2, 1, 0, 3)
+    src = tmp_path / "fod.mif"
+    mif.write(str(src), mif.Image(data=data, vox=[2.0, 2.0, 2.0, 1.0]))
+    out = tmp_path / "fixels"
+    assert fod2fixel.run([str(src), str(out), "-afd", "afd.mif", "-peak_amp", "peak.mif", "-disp", "disp.mif"]) == 0
+    index = mif.read(str(out / "index.mif"))
+    dirs = mif.read(str(out / "directions.mif")).data
+    afd = mif.read(str(out / "afd.mif")).data.reshape(-1)
+    peak = mif.read(str(out / "peak.mif")).data.reshape(-1)
+    disp = mif.read(str(out / "disp.mif")).data.reshape(-1)
+    assert index.data.shape == (nx, ny, nz, 2) and int(index.keyval["nfixels"]) == len(afd)
+    assert dirs.shape == (len(afd), 3, 1)
+    np.testing.assert_array_equal(disp, (afd / peak).astype(np.float32))
+    seg = fmls_ref.Segmenter(8)
+    agree = 0
+    for x in range(nx):
+        for y in range(ny):
+            for z in range(nz):
+                cnt, off = index.data[x, y, z]
+                lobes = seg(data[x, y, z].astype(np.float64))
+                if len(lobes) != cnt:
+                    continue
+                agree += 1
+                for q, lb in enumerate(lobes):
+                    np.testing.assert_allclose(dirs[off + q, :, 0], lb["mean_dir"], atol=1e-4)
+                    np.testing.assert_allclose(afd[off + q], lb["integral"], rtol=1e-4)
+    assert agree >= 0.9 * nx * ny * nz
+    assert fmls.FIXEL_FIELDS == 8

@@ -277,7 +277,65 @@ def next_rows(dwi_dev, sample_idx):
         "achieved_tflops_fp64": na * 2 * 45 * 60 / (ms_a / 1e3) / 1e12,
         "achieved_gbs": na * (66 + 45) * 4 / (ms_a / 1e3) / 1e9,
         "parity": {"vs": "numpy FP64 fit", "sample_voxels": len(sample_idx), "max_rel_err": float(err.max())}}
+    try:
+        out["fod2fixel"] = fod2fixel_row()
+    except Exception as ex:  # the headline line is printed whatever happens here
+        out["fod2fixel"] = {"error": f"{type(ex).__name__}: {ex}"}
     return out
+
+
+def fod2fixel_row():
+    """fod2fixel's FMLS segmentation (csd_fmls_segment) of 65,536 synthetic
+    FODs at lmax 8, default thresholds; parity and the CPU baseline from the
+    oracle's restatement on a sample."""
+    import torch
+
+    from mrtrix3_b200 import fmls, sh
+    from oracle import fmls_ref
+    rng = np.random.default_rng(17)
+    n, lmax = 65536, 8
+    k = rng.integers(1, 4, n)
+    c = np.zeros((n, sh.n_for_l(lmax)))
+    for j in range(3):
+        azel = np.stack([rng.uniform(-np.pi, np.pi, n), np.arccos(rng.uniform(-1, 1, n))], 1)
+        c += ((j < k) * rng.uniform(0.3, 1.0, n))[:, None] * sh.init_transform(azel, lmax)
+    c = c / c[:, :1] * rng.uniform(0.1, 0.5, (n, 1)) + rng.normal(0.0, 0.01, c.shape)
+    c[:, 0] = np.abs(c[:, 0])
+    rows = c.astype(np.float32)
+    seg = fmls.Segmenter(lmax)
+    d = torch.from_numpy(rows).cuda()
+    counts, fx = seg.segment(d, max_fixels=16)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    reps = 2
+    for _ in range(reps):
+        seg.segment(d, max_fixels=16)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    counts, fx = counts.cpu().numpy(), fx.cpu().numpy()
+    ref = fmls_ref.Segmenter(lmax)
+    sample = 40
+    t0 = time.perf_counter()
+    lobes = [ref(r) for r in rows[:sample].astype(np.float64)]
+    cpu_s = time.perf_counter() - t0
+    agree, maxd = 0, 0.0
+    for v, lb in enumerate(lobes):
+        if min(len(lb), 16) != counts[v]:
+            continue
+        agree += 1
+        for q, x in enumerate(lb[:16]):
+            want = np.concatenate([x["mean_dir"], x["peak_dir"], [x["integral"], x["max_peak"]]])
+            maxd = max(maxd, float(np.abs(fx[v, q] - want).max()))
+    return {"workload": f"{n} synthetic FODs (lmax 8, 1-3 fibres + N(0, 0.01) on each coefficient), 1281 "
+                        "directions, default thresholds, at most 16 fixels a voxel",
+            "value": n / (ms / 1e3), "unit": "voxels/s", "ms": ms, "dtype": "f64",
+            "fixels_per_voxel": float(np.minimum(counts, 16).mean()),
+            "parity": {"vs": "oracle/fmls_ref.py (FP64)", "sample_voxels": sample,
+                       "counts_equal": agree / sample, "max_abs_diff": maxd},
+            "cpu_baseline": {"value": sample / cpu_s, "unit": "voxels/s", "cores": 1, "kind": "port",
+                             "sample": f"the first {sample} voxels through oracle/fmls_ref.py (Python), {cpu_s:.1f} s"}}
 
 
 def main():

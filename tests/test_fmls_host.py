@@ -220,6 +220,12 @@ def test_cli_argument_errors(tmp_path):
     assert pos == ["f.mif", "d"] and opt == {"-peak_amp": "p.mif", "-fmls_no_thresholds": True}
     with pytest.raises(SystemExit, match="unknown option"):
         fod2fixel._parse(["-fmls"])
+    # the reference's own test command lines (testing/binaries/tests/fod2fixel)
+    pos, opt = fod2fixel._parse("-nthread 1 -fmls_no_thresholds fod.mif tmp-fod2fixel3 -afd afd.mif -peak peak.mif "
+                                "-disp disp.mif -force".split())
+    assert pos == ["fod.mif", "tmp-fod2fixel3"]
+    assert opt == {"-nthreads": "1", "-fmls_no_thresholds": True, "-afd": "afd.mif", "-peak_amp": "peak.mif",
+                   "-disp": "disp.mif", "-force": True}
     full = tmp_path / "full"
     full.mkdir()
     (full / "x").write_text("")

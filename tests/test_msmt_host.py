@@ -140,7 +140,7 @@ def test_top_threshold_rule():
 def test_dwi2response_argument_errors(tmp_path):
     from mrtrix3_b200.dwi2response import run
     with pytest.raises(SystemExit, match="usage"):
-        run(["tournier", "a.mif", "r.txt"])
+        run(["dhollander", "a.mif", "r.txt"])
     with pytest.raises(SystemExit, match="wrong number of arguments"):
         run(["manual", "a.mif", "r.txt"])
     with pytest.raises(SystemExit, match="-mask is required"):

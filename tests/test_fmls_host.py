@@ -233,3 +233,35 @@ def test_cli_argument_errors(tmp_path):
     mif.write(str(good), mif.Image(data=np.zeros((2, 2, 2, 15), np.float32), vox=[1, 1, 1, 1]))
     with pytest.raises(SystemExit, match="not empty"):
         fod2fixel.run([str(good), str(full)])
+
+
+def test_c_abi_rejects_bad_tables():
+    """csd_fmls_create / csd_fmls_segment check their arguments before any
+    device call (no GPU needed)."""
+    from mrtrix3_b200 import csd
+    L = csd.lib()
+    T = fmls.FMLSTables(8)
+    h = ctypes.c_void_p()
+
+    def create(**over):
+        ct = fmls.c_tables(T)
+        for k, v in over.items():
+            setattr(ct, k, v)
+        return L.csd_fmls_create(ctypes.byref(ct), ctypes.byref(h))
+
+    assert L.csd_fmls_create(None, ctypes.byref(h)) == csd.CSD_ERR_INVALID
+    assert create(lmax=7) == csd.CSD_ERR_INVALID          # odd lmax
+    assert create(nsh=44) == csd.CSD_ERR_INVALID          # nsh not NforL(lmax)
+    assert create(ndir=4096) == csd.CSD_ERR_INVALID       # more directions than the sort's width
+    assert create(n_al=10) == csd.CSD_ERR_INVALID         # PrecomputedAL rows of another lmax
+    assert create(n_adj=T.adj_off[-1] - 1) == csd.CSD_ERR_INVALID  # offsets and list disagree
+    bad = T.adj.copy()
+    bad[5] = 1281                                          # a neighbour out of range
+    keep = T.adj
+    T.adj = bad
+    assert create() == csd.CSD_ERR_INVALID
+    T.adj = keep
+    assert b"neighbour" in L.csd_last_error()
+    assert create(merge_ratio=-0.5) == csd.CSD_ERR_INVALID
+    assert h.value is None
+    assert L.csd_fmls_segment(None, None, 0, 45, 1, None, 16, None, None, None) == csd.CSD_ERR_INVALID

@@ -1,7 +1,8 @@
 """Run one CSD method on a synthetic case, for profilers (ncu) and timing.
 
     python -m mrtrix3_b200.profile_case [--dims 64 64 64] [--lmax 8]
-        [--method warm|plain|persistent|persistent_warm|predict|peaks|amp2sh|msmt|tensor|amp2response] [--reps 2]
+        [--method warm|plain|persistent|persistent_warm|predict|peaks|fod2fixel|amp2sh|msmt|tensor|amp2response]
+        [--reps 2]
         [--projection mma|tcgen05] [--solve warp|group16|group8] [--amp2sh-kernel auto|row|tile|mma]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
@@ -20,7 +21,7 @@ def main():
     ap.add_argument("--dims", type=int, nargs=3, default=[64, 64, 64])
     ap.add_argument("--lmax", type=int, default=8)
     ap.add_argument("--method", default="warm", choices=["warm", "plain", "persistent", "persistent_warm", "predict", "peaks",
-                                                          "amp2sh", "msmt", "tensor", "amp2response"])
+                                                          "fod2fixel", "amp2sh", "msmt", "tensor", "amp2response"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--projection", default="tcgen05", choices=["mma", "tcgen05"])
     ap.add_argument("--solve", default="warp", choices=["warp", "group16", "group8"])
@@ -94,7 +95,7 @@ def main():
     net = None
     if a.method in ("warm", "persistent_warm", "predict"):
         net = WarmStartNet.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_c5.npz"))
-    st = csd.State(s, d.shape[0]) if a.method in ("warm", "plain", "peaks") else None
+    st = csd.State(s, d.shape[0]) if a.method in ("warm", "plain", "peaks", "fod2fixel") else None
     fod = None
     if a.method == "amp2sh":  # the SH fit of this volume's DW amplitudes (normalised by its b=0 volumes)
         from . import sh
@@ -115,9 +116,24 @@ def main():
         print(f"amp2sh: {d.shape[0]} voxels in {ms:.3f} ms per call, {nbytes / ms / 1e6:.0f} GB/s "
               f"({d.shape[0] / ms / 1e3:.1f}M voxels/s)")
         return
-    if a.method == "peaks":  # sh2peaks on this volume's FODs
+    if a.method in ("peaks", "fod2fixel"):  # sh2peaks / FMLS segmentation of this volume's FODs
         st.run(d)
         fod = st.fod(as_numpy=False)["fod"]
+    if a.method == "fod2fixel":
+        from . import fmls
+        seg = fmls.Segmenter(a.lmax)
+        counts, _ = seg.segment(fod, max_fixels=16)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.reps):
+            seg.segment(fod, max_fixels=16)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.reps
+        print(f"fod2fixel: {fod.shape[0]} voxels in {ms:.3f} ms per call ({fod.shape[0] / ms / 1e3:.3f}M voxels/s), "
+              f"{counts.float().mean().item():.2f} fixels a voxel")
+        return
     t0 = time.perf_counter()
     for _ in range(a.reps):
         if a.method == "predict":

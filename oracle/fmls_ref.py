@@ -11,6 +11,13 @@ the segmenter uses (2 x 1281 elevations, linear interpolation); and
 fod2fixel's per-fixel outputs (cmd/fod2fixel.cpp:109-125, 250-286).  The
 direction set, its adjacency, grid lookup and integration weights come from
 mrtrix3_b200.directions (data tables, checked by their own tests).
+
+Pinning: parity unpinned against reference-run output.  The reference's
+golden fixel directories (testing/binaries/tests/fod2fixel, fod2fixel/out1-3)
+live in a test-data submodule that is absent, and the reference cannot be
+built here.  Only the PrecomputedAL interpolation is pinned, by the
+reference's own known-answer test (testing_unit_tests_sh_precomputer.cpp,
+restated in tests/test_fmls_host.py).
 """
 from __future__ import annotations
 

@@ -265,3 +265,32 @@ def test_c_abi_rejects_bad_tables():
     assert create(merge_ratio=-0.5) == csd.CSD_ERR_INVALID
     assert h.value is None
     assert L.csd_fmls_segment(None, None, 0, 45, 1, None, 16, None, None, None) == csd.CSD_ERR_INVALID
+
+
+def test_precomputed_al_matches_exact_values():
+    """The reference's own known-answer test for SH::PrecomputedAL
+    (testing/cmd/testing_unit_tests_sh_precomputer.cpp): random lmax-8
+    coefficients in [-1, 1], 10,000 random unit directions, the value
+    through the 512-elevation table within 1e-3 of the exact one.  Here with
+    the oracle's interpolation (fmls_ref._AL, SH.h:435-460) on the host
+    table (directions.precomputed_al)."""
+    lmax = 8
+    rng = np.random.default_rng(2)
+    coefs = rng.uniform(-1.0, 1.0, sh.n_for_l(lmax))
+    al = fmls_ref._AL(directions.precomputed_al(lmax, 512))
+    p = rng.uniform(-1.0, 1.0, (10000, 3))
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    az = np.arctan2(p[:, 1], p[:, 0])
+    el = np.arccos(p[:, 2])
+    exact = sh.init_transform(np.stack([az, el], axis=1), lmax) @ coefs
+    for i in range(len(p)):
+        A = al.get(el[i])
+        v = 0.0
+        for l in range(0, lmax + 1, 2):
+            v += A[l * l // 4] * coefs[l * (l + 1) // 2]
+        for m in range(1, lmax + 1):
+            c, s = math.cos(m * az[i]), math.sin(m * az[i])
+            for l in range(m + (m & 1), lmax + 1, 2):
+                v += A[l * l // 4 + m] * math.sqrt(2.0) * (c * coefs[l * (l + 1) // 2 + m] +
+                                                          s * coefs[l * (l + 1) // 2 - m])
+        assert abs(v - exact[i]) <= 1e-3

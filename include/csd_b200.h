@@ -389,6 +389,13 @@ typedef struct csd_fmls_tables {
  * and copies them to the current device.  Errors: CSD_ERR_INVALID. */
 typedef struct csd_fmls csd_fmls;
 int csd_fmls_create(const csd_fmls_tables* tables, csd_fmls** out);
+/* csd_fmls_create_default: the same on the built-in 1281-direction set (its
+ * hull adjacency and integration weights compiled in; the SH transform,
+ * Legendre table and lookup grid built on the host), as fod2fixel's
+ * Segmenter (dirs (1281), lmax) with load_fmls_thresholds' values.
+ * Errors: CSD_ERR_INVALID (lmax odd, negative or above 16). */
+int csd_fmls_create_default(int lmax, double integral_threshold, double peak_value_threshold, double merge_ratio,
+                            csd_fmls** out);
 void csd_fmls_destroy(csd_fmls* segmenter);
 
 /* csd_fmls_segment replaces Segmenter::operator() (fmls.cpp:159-311) for n

@@ -49,6 +49,37 @@ def gen_hr_inc():
                 "  return std::vector<double>(kBuiltinHR, kBuiltinHR + %d);\n}\n" % len(vals))
 
 
+def gen_fmls_inc():
+    """fmls_builtin.inc: the 1281 tessellation directions (verbatim text),
+    their hull neighbours and the integration weights (least squares, numpy
+    FP64, printed with 17 significant digits) for csd_fmls_create_default."""
+    src = [os.path.join(HERE, "data", f) for f in ("tessellation_1281.txt", "tessellation_1281_adjacency.txt")]
+    dst = os.path.join(CSRC, "fmls_builtin.inc")
+    if os.path.exists(dst) and all(os.path.getmtime(dst) >= os.path.getmtime(f) for f in src):
+        return
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    from mrtrix3_b200 import directions
+    azel = [line.split() for line in open(src[0]) if line.strip() and not line.startswith("#")]
+    adj = directions.adjacency_1281()
+    w = directions.integration_weights(directions.unit_vectors(directions.load_tessellation_1281()))
+    off = [0]
+    for a in adj:
+        off.append(off[-1] + len(a))
+    with open(dst, "w") as f:
+        f.write("// generated by mrtrix3_b200/build.py from data/tessellation_1281*.txt\n")
+        f.write("static const double kTess1281AzEl[%d] = {\n" % (2 * len(azel)))
+        for a, e in azel:
+            f.write("  %s, %s,\n" % (a, e))
+        f.write("};\n")
+        f.write("static const int kTess1281AdjOff[%d] = {%s};\n" % (len(off), ", ".join(str(v) for v in off)))
+        f.write("static const int kTess1281Adj[%d] = {%s};\n" % (off[-1], ", ".join(str(int(v)) for a in adj for v in a)))
+        f.write("static const double kTess1281Weight[%d] = {\n" % len(w))
+        for v in w:
+            f.write("  %.17g,\n" % v)
+        f.write("};\n")
+
+
 def _stale(out, deps):
     if not os.path.exists(out):
         return True
@@ -70,6 +101,7 @@ def sources():
 def build(force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     gen_hr_inc()
+    gen_fmls_inc()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".inc", ".h"))]
     headers.append(os.path.join(os.path.dirname(HERE), "include", "csd_b200.h"))
     cu, cpp = sources()

@@ -35,7 +35,8 @@ EXPORTED = [
     "csd_state_fod",
     "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_amp2sh_rician", "csd_icls_create",
     "csd_icls_destroy", "csd_icls_info", "csd_icls_solve", "csd_icls_solve_host", "csd_icls_create_standard", "csd_icls_solve_f64",
-    "csd_amp2response_accumulate", "csd_dwi2tensor", "csd_fmls_create", "csd_fmls_destroy", "csd_fmls_segment",
+    "csd_amp2response_accumulate", "csd_dwi2tensor", "csd_fmls_create", "csd_fmls_create_default", "csd_fmls_destroy",
+    "csd_fmls_segment",
     "csd_last_error",
 ]
 
@@ -114,6 +115,8 @@ def lib():
         L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_dwi2fod_host_phased.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
         L.csd_fmls_create.argtypes = [vp, ctypes.POINTER(vp)]
+        L.csd_fmls_create_default.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                              ctypes.POINTER(vp)]
         L.csd_fmls_destroy.argtypes = [vp]
         L.csd_fmls_destroy.restype = None
         L.csd_fmls_segment.argtypes = [vp, vp, i64, i64, i64, vp, ctypes.c_int, vp, vp, vp]

@@ -84,13 +84,19 @@ class Segmenter:
 
     def __init__(self, lmax: int, integral_threshold: float = INTEGRAL_THRESHOLD_DEFAULT,
                  peak_value_threshold: float = PEAK_VALUE_THRESHOLD_DEFAULT,
-                 merge_ratio: float = MERGE_RATIO_DEFAULT):
+                 merge_ratio: float = MERGE_RATIO_DEFAULT, builtin: bool = False):
+        """builtin: let the library build the tables itself
+        (csd_fmls_create_default) instead of passing these host tables."""
         from . import csd
         self.tables = FMLSTables(lmax, integral_threshold, peak_value_threshold, merge_ratio)
         self._lib = csd.lib()
         h = ctypes.c_void_p()
-        ct = c_tables(self.tables)
-        csd.check(self._lib.csd_fmls_create(ctypes.byref(ct), ctypes.byref(h)))
+        if builtin:
+            csd.check(self._lib.csd_fmls_create_default(lmax, float(integral_threshold), float(peak_value_threshold),
+                                                        float(merge_ratio), ctypes.byref(h)))
+        else:
+            ct = c_tables(self.tables)
+            csd.check(self._lib.csd_fmls_create(ctypes.byref(ct), ctypes.byref(h)))
         self._h = h
 
     def close(self):

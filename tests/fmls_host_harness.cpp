@@ -6,8 +6,43 @@
 #include <cstdint>
 #include <vector>
 
+#include <stdexcept>
+#include <string>
+
 #include "../include/csd_b200.h"
 #include "../mrtrix3_b200/csrc/fmls_core.cuh"
+#include "../mrtrix3_b200/csrc/fmls_tables.hpp"
+
+// the library's error recorder and device upload are not part of this build
+namespace csdb200 {
+int set_error(int code, const std::string&) { return code; }
+}
+extern "C" int csd_fmls_create(const csd_fmls_tables*, csd_fmls**) { return 0; }
+
+// The C++ table builder's output (csd_fmls_create_default's tables), for
+// comparison with the Python host tables: sizes into dims[7], the arrays
+// copied into the caller's buffers when they are not null.
+extern "C" int fmls_host_default_tables(int lmax, int* dims, double* steps, double* unit, double* weight,
+                                        double* sh2amp, double* al, int32_t* adj_off, int32_t* adj,
+                                        int32_t* grid_off, int32_t* grid) {
+  try {
+    const csdb200::FmlsHostTables T = csdb200::build_fmls_tables(lmax);
+    dims[0] = T.ndir; dims[1] = T.nsh; dims[2] = T.al_ndir; dims[3] = T.n_al; dims[4] = T.num_az;
+    dims[5] = T.num_el; dims[6] = (int)T.grid.size();
+    steps[0] = T.al_inc; steps[1] = T.az_begin; steps[2] = T.el_begin; steps[3] = T.az_step; steps[4] = T.el_step;
+    if (unit) std::copy(T.unit.begin(), T.unit.end(), unit);
+    if (weight) std::copy(T.weight.begin(), T.weight.end(), weight);
+    if (sh2amp) std::copy(T.sh2amp.begin(), T.sh2amp.end(), sh2amp);
+    if (al) std::copy(T.al.begin(), T.al.end(), al);
+    if (adj_off) std::copy(T.adj_off.begin(), T.adj_off.end(), adj_off);
+    if (adj) std::copy(T.adj.begin(), T.adj.end(), adj);
+    if (grid_off) std::copy(T.grid_off.begin(), T.grid_off.end(), grid_off);
+    if (grid) std::copy(T.grid.begin(), T.grid.end(), grid);
+    return 0;
+  } catch (const std::exception&) {
+    return -1;
+  }
+}
 
 extern "C" int fmls_host_segment(const csd_fmls_tables* c, const double* sh_rows, int n, int max_out,
                                  int32_t* counts, float* fixels) {

@@ -83,9 +83,13 @@ def test_precomputed_al_rows():
 def harness(tmp_path_factory):
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
+    from mrtrix3_b200 import build
+    build.gen_fmls_inc()
     out = tmp_path_factory.mktemp("fmls") / "libfmls_host.so"
+    csrc = os.path.join(ROOT, "mrtrix3_b200", "csrc")
     subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-o", str(out),
-                    os.path.join(ROOT, "tests", "fmls_host_harness.cpp")], check=True)
+                    os.path.join(ROOT, "tests", "fmls_host_harness.cpp"), os.path.join(csrc, "fmls_tables.cpp"),
+                    os.path.join(csrc, "shared_init.cpp")], check=True)
     return ctypes.CDLL(str(out))
 
 
@@ -263,6 +267,9 @@ def test_c_abi_rejects_bad_tables():
     T.adj = keep
     assert b"neighbour" in L.csd_last_error()
     assert create(merge_ratio=-0.5) == csd.CSD_ERR_INVALID
+    assert L.csd_fmls_create_default(7, 0.0, 0.1, 1.0, ctypes.byref(h)) == csd.CSD_ERR_INVALID
+    assert b"lmax" in L.csd_last_error()
+    assert L.csd_fmls_create_default(8, 0.0, 0.1, 1.0, None) == csd.CSD_ERR_INVALID
     assert h.value is None
     assert L.csd_fmls_segment(None, None, 0, 45, 1, None, 16, None, None, None) == csd.CSD_ERR_INVALID
 
@@ -294,3 +301,34 @@ def test_precomputed_al_matches_exact_values():
                 v += A[l * l // 4 + m] * math.sqrt(2.0) * (c * coefs[l * (l + 1) // 2 + m] +
                                                           s * coefs[l * (l + 1) // 2 - m])
         assert abs(v - exact[i]) <= 1e-3
+
+
+@pytest.mark.parametrize("lmax", [8, 12])
+def test_cpp_default_tables_equal_host_tables(harness, lmax):
+    """csd_fmls_create_default's C++ tables (fmls_tables.cpp) against the
+    Python host tables the GPU tests use (mrtrix3_b200.fmls.FMLSTables)."""
+    T = fmls.FMLSTables(lmax)
+    dims = np.zeros(7, np.int32)
+    steps = np.zeros(5)
+    assert harness.fmls_host_default_tables(lmax, ctypes.c_void_p(dims.ctypes.data),
+                                            ctypes.c_void_p(steps.ctypes.data), *([None] * 8)) == 0
+    nd, nsh, al_ndir, n_al, num_az, num_el, n_grid = (int(v) for v in dims)
+    assert (nd, nsh, al_ndir, n_al, num_az, num_el, n_grid) == (T.ndir, T.nsh, T.al_ndir, T.n_al, T.num_az,
+                                                                T.num_el, len(T.grid))
+    np.testing.assert_allclose(steps, [T.al_inc, T.az_begin, T.el_begin, T.az_step, T.el_step], rtol=1e-15)
+    unit, weight = np.zeros((nd, 3)), np.zeros(nd)
+    sh2amp, al = np.zeros((nd, nsh)), np.zeros((al_ndir, n_al))
+    adj_off, adj = np.zeros(nd + 1, np.int32), np.zeros(len(T.adj), np.int32)
+    grid_off, grid = np.zeros(num_az * num_el + 1, np.int32), np.zeros(n_grid, np.int32)
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    assert harness.fmls_host_default_tables(lmax, p(dims), p(steps), p(unit), p(weight), p(sh2amp), p(al), p(adj_off),
+                                            p(adj), p(grid_off), p(grid)) == 0
+    np.testing.assert_allclose(unit, T.unit, rtol=0, atol=1e-15)
+    np.testing.assert_array_equal(weight, T.weight)
+    np.testing.assert_allclose(sh2amp, T.sh2amp, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(al, T.al, rtol=0, atol=1e-13)
+    np.testing.assert_array_equal(adj_off, T.adj_off)
+    np.testing.assert_array_equal(adj, T.adj)
+    np.testing.assert_array_equal(grid_off, T.grid_off)
+    np.testing.assert_array_equal(grid, T.grid)
+    assert harness.fmls_host_default_tables(7, p(dims), p(steps), *([None] * 8)) == -1

@@ -133,3 +133,20 @@ def test_fod2fixel_cli(tmp_path):
                     np.testing.assert_allclose(afd[off + q], lb["integral"], rtol=1e-4)
     assert agree >= 0.9 * nx * ny * nz
     assert fmls.FIXEL_FIELDS == 8
+
+
+def test_builtin_tables_give_the_same_lobes():
+    """csd_fmls_create_default (tables built by the library) against the
+    host tables: the same lobes, values to 1e-5 (the SH transform and
+    Legendre table agree to 1e-13)."""
+    import torch
+
+    from mrtrix3_b200 import fmls
+    rows = _fods(80, 8, seed=77, noise=0.02).astype(np.float32)
+    d = torch.from_numpy(rows).cuda()
+    c1, f1 = fmls.Segmenter(8).segment(d, max_fixels=16)
+    c2, f2 = fmls.Segmenter(8, builtin=True).segment(d, max_fixels=16)
+    c1, f1, c2, f2 = (t.cpu().numpy() for t in (c1, f1, c2, f2))
+    same = c1 == c2
+    assert same.mean() >= 0.98
+    np.testing.assert_allclose(f2[same], f1[same], rtol=1e-5, atol=1e-6)

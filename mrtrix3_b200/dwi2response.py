@@ -167,6 +167,7 @@ def tax_loop(step, fit, mask, init_rf, peak_ratio=0.1, max_iters=20, convergence
         if it > 0:
             reiterate = False
             for old, new in zip(rf, new_rf):
+                old, new = float(old), float(new)  # as the script's floats: a zero mean raises
                 mean = 0.5 * (old + new)
                 diff = abs(0.5 * (old - new))
                 if diff / mean > change:
@@ -289,7 +290,11 @@ def run(argv) -> int:
         mask = rows(mif.read(opt["-mask"]).data.reshape(dims) != 0)
         if not mask.any():
             raise SystemExit("Provided mask image does not contain any voxels")
-        resp, voxels, _ = iterative(algo, opt, g, shells, dwi, mask, dims)
+        try:
+            resp, voxels, _ = iterative(algo, opt, g, shells, dwi, mask, dims)
+        except ZeroDivisionError:
+            raise SystemExit(f"dwi2response {algo}: a response coefficient's mean over two rounds is zero "
+                             "(the script stops with a division by zero there)")
         np.savetxt(out_path, resp.reshape(1, -1), fmt="%.10g")
         if "-voxels" in opt:
             vox = voxels.reshape(nz, ny, nx).transpose(2, 1, 0).astype(np.float64)

@@ -125,6 +125,10 @@ def test_tax_convergence_rule():
     # the mask of each iteration is the previous single-fibre set
     np.testing.assert_array_equal(f.calls[1][1], sf)
     np.testing.assert_array_equal(f.calls[0][0], [90.0, -45.0, 5.0])
+    # a coefficient whose old and new values cancel: the script divides by zero
+    fz = FakeSteps(p1, p2, rf_fn=lambda it, sf: [np.array([100.0, 0.0]), np.array([110.0, 0.0])][min(it, 1)])
+    with pytest.raises(ZeroDivisionError):
+        D.tax_loop(fz.step, fz.fit, mask, [90.0, -45.0, 5.0])
     f0 = FakeSteps(np.zeros(n), np.zeros(n))
     with pytest.raises(SystemExit, match="excluded"):
         D.tax_loop(f0.step, f0.fit, mask, [1.0, 0.0, 0.0])

@@ -332,3 +332,29 @@ def test_cpp_default_tables_equal_host_tables(harness, lmax):
     np.testing.assert_array_equal(grid_off, T.grid_off)
     np.testing.assert_array_equal(grid, T.grid)
     assert harness.fmls_host_default_tables(7, p(dims), p(steps), *([None] * 8)) == -1
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "fmls_golden.npz")
+GOLDEN_CASES = {"default": (0.0, 0.1, 1.0), "no_thresholds": (0.0, 0.0, 1.0), "merge_0.5": (0.0, 0.1, 0.5)}
+
+
+@pytest.mark.parametrize("case", sorted(GOLDEN_CASES))
+def test_core_reproduces_golden(harness, case):
+    """The host-built core against the committed oracle fixtures
+    (tests/golden/make_fmls_golden.py), bit for bit in float32."""
+    g = np.load(GOLDEN)
+    counts, fx = host_segment(harness, fmls.FMLSTables(8, *GOLDEN_CASES[case]), g["rows"].astype(np.float64),
+                              max_out=24)
+    np.testing.assert_array_equal(counts, g[case + "_counts"])
+    np.testing.assert_array_equal(fx, g[case + "_fixels"])
+
+
+def test_oracle_reproduces_golden():
+    g = np.load(GOLDEN)
+    seg = fmls_ref.Segmenter(8, *GOLDEN_CASES["merge_0.5"])
+    for v in range(0, 48, 12):
+        lobes = seg(g["rows"][v].astype(np.float64))
+        assert len(lobes) == g["merge_0.5_counts"][v]
+        for q, lb in enumerate(lobes[:24]):
+            want = np.concatenate([lb["mean_dir"], lb["peak_dir"], [lb["integral"], lb["max_peak"]]]).astype(np.float32)
+            np.testing.assert_array_equal(g["merge_0.5_fixels"][v, q], want)

@@ -150,3 +150,17 @@ def test_builtin_tables_give_the_same_lobes():
     same = c1 == c2
     assert same.mean() >= 0.98
     np.testing.assert_allclose(f2[same], f1[same], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("case,kw", [("default", {}),
+                                     ("no_thresholds", dict(integral_threshold=0.0, peak_value_threshold=0.0)),
+                                     ("merge_0.5", dict(merge_ratio=0.5))])
+def test_segment_matches_golden(case, kw):
+    """Against the committed oracle fixtures (tests/golden/fmls_golden.npz):
+    counts equal on >= 98% of voxels, values of those to 1e-4."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "fmls_golden.npz"))
+    counts, fx = _segment(g["rows"], 8, max_fixels=24, **kw)
+    want_c = np.minimum(g[case + "_counts"], 24)
+    same = counts == want_c
+    assert same.mean() >= 0.98
+    np.testing.assert_allclose(fx[same], g[case + "_fixels"][same], rtol=1e-4, atol=1e-4)

@@ -35,7 +35,7 @@ def main(ref):
     print("wrote", out)
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
     from mrtrix3_b200 import directions
-    adj = directions.hull_adjacency(directions.unit_vectors(directions.load_tessellation_1281(cached=False)))
+    adj = directions.hull_adjacency(directions.unit_vectors(directions.load_tessellation_1281()))
     out2 = os.path.join(HERE, "tessellation_1281_adjacency.txt")
     with open(out2, "w") as f:
         f.write("# neighbours of each of the 1281 tessellation directions (0-based, ascending), one line each\n")

@@ -28,8 +28,8 @@ from . import sh
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 
 
-def load_tessellation_1281(cached: bool = True) -> np.ndarray:
-    del cached  # the directions are always read from the shipped table
+def load_tessellation_1281() -> np.ndarray:
+    """[1281][2] azimuth / elevation of the shipped tessellation."""
     return np.loadtxt(os.path.join(DATA, "tessellation_1281.txt"), dtype=np.float64)
 
 

@@ -12,6 +12,7 @@ in one kernel launch (fmls.cu).
 from __future__ import annotations
 
 import ctypes
+import functools
 import math
 
 import numpy as np
@@ -24,6 +25,35 @@ MERGE_RATIO_DEFAULT = 1.0           # fmls.h: FMLS_MERGE_RATIO_BRIDGE_TO_PEAK_DE
 FIXEL_FIELDS = 8                    # mean dir (3), peak dir (3), integral, max peak
 
 
+@functools.lru_cache(maxsize=None)
+def _direction_set():
+    """The lmax-independent tables of the 1281-direction set, built once per
+    process: unit vectors, neighbour lists (CSR), integration weights, the
+    lookup grid."""
+    unit = np.ascontiguousarray(directions.unit_vectors(directions.load_tessellation_1281()))
+    adj = directions.adjacency_1281()
+    adj_off = np.zeros(len(unit) + 1, np.int32)
+    adj_off[1:] = np.cumsum([len(a) for a in adj])
+    weight = np.ascontiguousarray(directions.integration_weights(unit))
+    look = directions.FastLookup(unit, adj)
+    for a in (unit, adj_off, weight, look.offsets, look.entries):
+        a.setflags(write=False)
+    return unit, adj_off, np.concatenate(adj).astype(np.int32), weight, look
+
+
+@functools.lru_cache(maxsize=None)
+def _lmax_tables(lmax: int):
+    """The SH -> amplitude matrix and PrecomputedAL table of one lmax."""
+    unit = _direction_set()[0]
+    az = np.arctan2(unit[:, 1], unit[:, 0])
+    el = np.arccos(unit[:, 2])
+    sh2amp = np.ascontiguousarray(sh.init_transform(np.stack([az, el], axis=1), lmax))
+    al = np.ascontiguousarray(directions.precomputed_al(lmax, 2 * len(unit)))
+    sh2amp.setflags(write=False)
+    al.setflags(write=False)
+    return sh2amp, al
+
+
 class FMLSTables:
     def __init__(self, lmax: int, integral_threshold: float = INTEGRAL_THRESHOLD_DEFAULT,
                  peak_value_threshold: float = PEAK_VALUE_THRESHOLD_DEFAULT,
@@ -32,21 +62,12 @@ class FMLSTables:
             raise ValueError("fod2fixel: lmax must be even and at most 16")
         self.lmax = lmax
         self.nsh = sh.n_for_l(lmax)
-        self.unit = np.ascontiguousarray(directions.unit_vectors(directions.load_tessellation_1281()))
+        self.unit, self.adj_off, self.adj, self.weight, look = _direction_set()
         self.ndir = len(self.unit)
-        adj = directions.adjacency_1281()
-        self.adj_off = np.zeros(self.ndir + 1, np.int32)
-        self.adj_off[1:] = np.cumsum([len(a) for a in adj])
-        self.adj = np.concatenate(adj).astype(np.int32)
-        self.weight = np.ascontiguousarray(directions.integration_weights(self.unit))
-        az = np.arctan2(self.unit[:, 1], self.unit[:, 0])
-        el = np.arccos(self.unit[:, 2])
-        self.sh2amp = np.ascontiguousarray(sh.init_transform(np.stack([az, el], axis=1), lmax))
-        self.al_ndir = 2 * self.ndir
-        self.al = np.ascontiguousarray(directions.precomputed_al(lmax, self.al_ndir))
+        self.sh2amp, self.al = _lmax_tables(lmax)
+        self.al_ndir = self.al.shape[0]
         self.n_al = self.al.shape[1]
         self.al_inc = math.pi / (self.al_ndir - 1)
-        look = directions.FastLookup(self.unit, adj)
         self.num_az, self.num_el = look.num_az, look.num_el
         self.az_begin, self.el_begin = look.az_begin, look.el_begin
         self.az_step, self.el_step = look.az_step, look.el_step

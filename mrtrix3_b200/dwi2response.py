@@ -206,11 +206,16 @@ def iterative(algo, opt, g, shells, dwi, mask, dims):
     lmax = int(opt["-lmax"]) if "-lmax" in opt else None
     dev = dwi.device
 
+    segmenters = {}  # one per FOD lmax (4 in tournier's first round, then the CSD's lmax)
+
     def step(rf, voxels):
         s = csd.make_shared(grad, np.asarray(rf, np.float64))
         m = torch.from_numpy(np.asarray(voxels, np.uint8)).to(dev)
         fod = csd.dwi2fod_csd(s, dw_dev, m)["fod"]
-        seg = fmls.Segmenter(sh.l_for_n(s.nSH()), 0.0, 0.0, fmls.MERGE_RATIO_DEFAULT)  # -fmls_no_thresholds
+        L = sh.l_for_n(s.nSH())
+        if L not in segmenters:
+            segmenters[L] = fmls.Segmenter(L, 0.0, 0.0, fmls.MERGE_RATIO_DEFAULT)  # -fmls_no_thresholds
+        seg = segmenters[L]
         counts, fx = seg.segment(fod, m, max_fixels=2)
         c = counts.cpu().numpy()
         f = fx.cpu().numpy()

@@ -21,9 +21,15 @@ restated in tests/test_fmls_host.py).
 """
 from __future__ import annotations
 
+import ctypes
 import math
+import os
+import subprocess
 
 import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_CLIB = None
 
 MAX_DIR_CHANGE = 0.2
 ANGLE_TOLERANCE = 1e-4
@@ -256,3 +262,46 @@ def fod2fixel(fod_rows, lmax, mask=None, maxnum=0, dirpeak=False, **thresholds):
             afd, pk = np.float32(lb["integral"]), np.float32(lb["max_peak"])
             fixels.append([d[0], d[1], d[2], afd, pk, np.float32(afd / pk)])
     return counts, np.array(fixels, np.float32).reshape(-1, 6)
+
+
+def _clib():
+    """liboracle_fmls.so (oracle/fmls_oracle.c): the segmenter in C, threaded."""
+    global _CLIB
+    if _CLIB is None:
+        so = os.path.join(HERE, "liboracle_fmls.so")
+        src = os.path.join(HERE, "fmls_oracle.c")
+        if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+            subprocess.check_call(["make", "-s", "-C", HERE, so])
+        L = ctypes.CDLL(so)
+        vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.oracle_fmls_segment.restype = ci
+        L.oracle_fmls_segment.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, ci, ci, cd, vp, ci, ci, cd, cd, cd, cd, vp,
+                                          vp, cd, cd, cd, vp, ctypes.c_long, ci, vp, vp, ci]
+        _CLIB = L
+    return _CLIB
+
+
+def segment_batch_c(seg: Segmenter, rows, max_out: int = 16, nthreads: int = 1):
+    """Segmenter.__call__ for every row of ``rows`` [n][nsh] by the C
+    restatement (oracle/fmls_oracle.c): (counts [n], fixels [n][max_out][8]:
+    mean dir, peak dir, integral, max peak; float32)."""
+    rows = np.ascontiguousarray(rows, np.float64)
+    unit = np.ascontiguousarray(seg.unit, np.float64)
+    adj_off = np.zeros(len(seg.adj) + 1, np.int32)
+    adj_off[1:] = np.cumsum([len(a) for a in seg.adj])
+    adj = np.concatenate(seg.adj).astype(np.int32)
+    w = np.ascontiguousarray(seg.weights, np.float64)
+    sh2amp = np.ascontiguousarray(seg.sh2amp, np.float64)
+    al = np.ascontiguousarray(seg.al.table, np.float64)
+    lk = seg.lookup
+    counts = np.zeros(len(rows), np.int32)
+    fixels = np.zeros((len(rows), max_out, 8), np.float32)
+    p = lambda a: a.ctypes.data  # noqa: E731
+    rc = _clib().oracle_fmls_segment(len(unit), seg.lmax, sh2amp.shape[1], p(unit), p(w), p(adj_off), p(adj),
+                                     p(sh2amp), al.shape[0], al.shape[1], seg.al.inc, p(al), lk.num_az, lk.num_el,
+                                     lk.az_begin, lk.el_begin, lk.az_step, lk.el_step, p(lk.offsets), p(lk.entries),
+                                     seg.integral_threshold, seg.peak_value_threshold, seg.merge_ratio, p(rows),
+                                     len(rows), max_out, p(counts), p(fixels), int(nthreads))
+    if rc != 0:
+        raise RuntimeError("oracle_fmls_segment failed")
+    return counts, fixels

@@ -358,3 +358,23 @@ def test_oracle_reproduces_golden():
         for q, lb in enumerate(lobes[:24]):
             want = np.concatenate([lb["mean_dir"], lb["peak_dir"], [lb["integral"], lb["max_peak"]]]).astype(np.float32)
             np.testing.assert_array_equal(g["merge_0.5_fixels"][v, q], want)
+
+
+@pytest.mark.parametrize("case", sorted(GOLDEN_CASES))
+def test_c_oracle_reproduces_golden(case):
+    """The C restatement (oracle/fmls_oracle.c: the reference's vector of
+    lobes with masks, erased on merges) against the same fixtures, threaded."""
+    g = np.load(GOLDEN)
+    seg = fmls_ref.Segmenter(8, *GOLDEN_CASES[case])
+    counts, fx = fmls_ref.segment_batch_c(seg, g["rows"].astype(np.float64), max_out=24, nthreads=4)
+    np.testing.assert_array_equal(counts, g[case + "_counts"])
+    np.testing.assert_array_equal(fx, g[case + "_fixels"])
+
+
+def test_c_oracle_matches_host_core(harness):
+    rows = synthetic_fods(64, 10, seed=31, noise=0.03)
+    kw = (0.0, 0.0, 0.3)
+    c1, f1 = fmls_ref.segment_batch_c(fmls_ref.Segmenter(10, *kw), rows, max_out=32, nthreads=2)
+    c2, f2 = host_segment(harness, fmls.FMLSTables(10, *kw), rows, max_out=32)
+    np.testing.assert_array_equal(c1, c2)
+    np.testing.assert_allclose(f1, f2, rtol=1e-6, atol=1e-6)

@@ -164,3 +164,19 @@ def test_segment_matches_golden(case, kw):
     same = counts == want_c
     assert same.mean() >= 0.98
     np.testing.assert_allclose(fx[same], g[case + "_fixels"][same], rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("kw", [{}, dict(integral_threshold=0.0, peak_value_threshold=0.0, merge_ratio=0.6)])
+def test_segment_matches_c_oracle_large(kw):
+    """4096 voxels against the threaded C restatement (oracle/fmls_oracle.c):
+    counts equal on >= 99%, values of those to 1e-4."""
+    import os as _os
+
+    from oracle import fmls_ref
+    rows = _fods(4096, 8, seed=123, noise=0.015).astype(np.float32)
+    counts, fx = _segment(rows, 8, max_fixels=16, **kw)
+    rc, rf = fmls_ref.segment_batch_c(fmls_ref.Segmenter(8, **kw), rows.astype(np.float64), max_out=16,
+                                      nthreads=_os.cpu_count() or 1)
+    same = np.minimum(rc, 16) == counts
+    assert same.mean() >= 0.99
+    np.testing.assert_allclose(fx[same], rf[same], rtol=1e-4, atol=1e-4)

@@ -237,6 +237,14 @@ def test_cli_argument_errors(tmp_path):
     mif.write(str(good), mif.Image(data=np.zeros((2, 2, 2, 15), np.float32), vox=[1, 1, 1, 1]))
     with pytest.raises(SystemExit, match="not empty"):
         fod2fixel.run([str(good), str(full)])
+    with pytest.raises(SystemExit, match="maxnum"):
+        fod2fixel.run([str(good), str(tmp_path / "o1"), "-maxnum", "0"])
+    small = tmp_path / "small_mask.mif"
+    mif.write(str(small), mif.Image(data=np.ones((2, 2, 1), np.float32), vox=[1, 1, 1]))
+    with pytest.raises(SystemExit, match="dimensions do not match"):
+        fod2fixel.run([str(good), str(tmp_path / "o2"), "-mask", str(small)])
+    with pytest.raises(SystemExit, match="non-negative"):
+        fod2fixel.run([str(good), str(tmp_path / "o3"), "-fmls_peak_value", "-1"])
 
 
 def test_c_abi_rejects_bad_tables():

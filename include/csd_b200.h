@@ -8,6 +8,14 @@
  *   the ThreadedLoop over voxels in cmd/dwi2fod.cpp:275-281
  *     with CSD_Processor (cmd/dwi2fod.cpp:120-176)                -> csd_solve,
  *                                                                    csd_dwi2fod_host
+ * and, for the commands around it:
+ *   sh2peaks (cmd/sh2peaks.cpp)                                   -> csd_sh2peaks
+ *   amp2sh (cmd/amp2sh.cpp)                                       -> csd_amp2sh[_rician]
+ *   Math::ICLS (core/math/constrained_least_squares.h), the solver
+ *     of dwi2fod msmt_csd and amp2response                        -> csd_icls_*
+ *   amp2response's accumulation (cmd/amp2response.cpp)            -> csd_amp2response_accumulate
+ *   dwi2tensor + tensor2metric -fa -vector                        -> csd_dwi2tensor
+ *   FMLS::Segmenter (src/dwi/fmls.cpp), fod2fixel's segmentation  -> csd_fmls_*
  * Plain pointers and sizes only.  Device pointers are CUDA global memory on
  * the current device; a `stream` argument is a cudaStream_t (NULL = legacy
  * default stream).  All functions return 0 on success or a negative CSD_ERR_*

@@ -6,13 +6,15 @@ The loops themselves are mrtrix3_b200.dwi2response.tournier_loop / tax_loop
 (restating lib/mrtrix3/dwi2response/tournier.py:53-150 and tax.py:53-160;
 their control flow is tested on the CPU with fake steps).  Here their steps
 are ``dwi2fod csd`` by oracle/oracle.py (csd.h), ``fod2fixel
--fmls_no_thresholds`` by oracle/fmls_ref.py (fmls.cpp) and ``amp2response``
+-fmls_no_thresholds`` by oracle/fmls_oracle.c (fmls.cpp; equal to the
+literal restatement oracle/fmls_ref.py on its fixtures) and ``amp2response``
 by oracle/amp2response_ref.py (amp2response.cpp), so that the GPU run and
-this one differ only in the steps' arithmetic.  Small volumes only (the
-segmentation restatement takes ~80 ms a voxel).  Parity unpinned against
+this one differ only in the steps' arithmetic.  Parity unpinned against
 reference-run output (the scripts' test data are absent).
 """
 from __future__ import annotations
+
+import os
 
 import numpy as np
 
@@ -36,6 +38,8 @@ def iterative_ref(algo, grad_shell, dwi_shell, mask, dims, hr_dirs, number=300, 
     cart = np.stack([np.cos(dirs[:, 0]) * np.sin(dirs[:, 1]), np.sin(dirs[:, 0]) * np.sin(dirs[:, 1]),
                      np.cos(dirs[:, 1])], axis=1)
 
+    segs = {}
+
     def step(rf, voxels):
         v = np.asarray(voxels, bool)
         sh_lmax = _csd_lmax(rf)
@@ -45,17 +49,17 @@ def iterative_ref(algo, grad_shell, dwi_shell, mask, dims, hr_dirs, number=300, 
             F[v] = O.OracleShared(grad_shell, np.asarray(rf, np.float64), hr_dirs).solve(
                 dwi[v].astype(np.float32))["F"]
         F = F.astype(np.float32).astype(np.float64)   # the FOD image is float32
-        seg = fmls_ref.Segmenter(sh_lmax, 0.0, 0.0, 1.0)
+        if sh_lmax not in segs:
+            segs[sh_lmax] = fmls_ref.Segmenter(sh_lmax, 0.0, 0.0, 1.0)
         p1 = np.zeros(len(dwi), np.float32)
         p2 = np.zeros(len(dwi), np.float32)
         d1 = np.full((len(dwi), 3), np.nan, np.float32)
-        for i in np.nonzero(v)[0]:
-            lobes = seg(F[i])
-            if lobes:
-                p1[i] = lobes[0]["max_peak"]
-                d1[i] = lobes[0]["mean_dir"]
-            if len(lobes) > 1:
-                p2[i] = lobes[1]["max_peak"]
+        idx = np.nonzero(v)[0]
+        if len(idx):
+            c, fx = fmls_ref.segment_batch_c(segs[sh_lmax], F[idx], max_out=2, nthreads=os.cpu_count() or 1)
+            p1[idx] = np.where(c >= 1, fx[:, 0, 7], 0.0)
+            p2[idx] = np.where(c >= 2, fx[:, 1, 7], 0.0)
+            d1[idx] = np.where((c >= 1)[:, None], fx[:, 0, 0:3], np.nan)
         return p1, p2, d1
 
     def fit(sf, first_dir, L):

@@ -145,3 +145,21 @@ def test_iterative_cli_argument_errors(tmp_path):
         D.run(["fa", "dwi.mif", str(tmp_path / "out.txt"), "-mask", "m.mif", "-shells", "1000"])
     with pytest.raises(SystemExit, match="wrong number"):
         D.run(["tax", "dwi.mif", "x", str(tmp_path / "out.txt")])
+
+
+@pytest.mark.parametrize("algo,kw", [("tournier", dict(number=10, iter_voxels=30)), ("tax", dict(max_iters=4))])
+def test_loops_on_the_restatements_recover_the_response(algo, kw):
+    """The loops over the FP64 restatements of CSD, FMLS and amp2response
+    (oracle/dwi2response_ref.py, the reference side of the GPU parity test)
+    on a 60-voxel phantom made with synth.RESPONSE."""
+    from mrtrix3_b200 import msmt, synth
+    from oracle import dwi2response_ref as R
+    rng = np.random.default_rng(5)
+    grad = synth.grad_table(6, synth.fibonacci_hemisphere(60))
+    dwi = synth.voxel_signals(rng, grad, 60, 50.0)
+    g = msmt.normalise_scheme(grad)
+    vols = msmt.cluster_shells(g[:, 3])[-1]
+    rf, sf, it = R.iterative_ref(algo, g[vols], dwi[:, vols], np.ones(60, bool), (5, 4, 3), synth.load_hr_dirs(),
+                                 lmax=8, **kw)
+    assert 2 <= it <= 4 and sf.sum() >= 10
+    assert np.abs(rf - synth.RESPONSE).max() <= 0.1 * synth.RESPONSE[0]

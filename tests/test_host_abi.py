@@ -99,13 +99,14 @@ def test_errors_follow_reference_messages():
 
 def test_cpp_shim_compiles():
     """The C++ drop-in headers (CSD::Shared / CSD, csd.h:46-271; ICLS::Problem
-    / Solver, constrained_least_squares.h:71-370) and their examples, with the
-    fod2fixel segmentation example, compile against the C ABI."""
+    / Solver, constrained_least_squares.h:71-370; FMLS::Segmenter, fmls.h:60-291)
+    and their examples compile against the C ABI."""
     ex = os.path.join(ROOT, "mrtrix3_b200", "csrc", "examples", "dwi2fod_csd_example.cpp")
     if not os.path.exists(ex):
         pytest.skip("C++ shim example not present")
     for src in (ex, os.path.join(ROOT, "mrtrix3_b200", "csrc", "examples", "icls_example.cpp"),
-                os.path.join(ROOT, "mrtrix3_b200", "csrc", "examples", "fod2fixel_example.cpp")):
+                os.path.join(ROOT, "mrtrix3_b200", "csrc", "examples", "fod2fixel_example.cpp"),
+                os.path.join(ROOT, "mrtrix3_b200", "csrc", "examples", "fmls_segmenter_example.cpp")):
         r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-I", os.path.join(ROOT, "include"), "-I",
                             os.path.join(ROOT, "mrtrix3_b200", "csrc"), "-I", "/usr/local/cuda/include", src],
                            capture_output=True, text=True)

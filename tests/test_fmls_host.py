@@ -386,3 +386,58 @@ def test_c_oracle_matches_host_core(harness):
     c2, f2 = host_segment(harness, fmls.FMLSTables(10, *kw), rows, max_out=32)
     np.testing.assert_array_equal(c1, c2)
     np.testing.assert_allclose(f1, f2, rtol=1e-6, atol=1e-6)
+
+
+def test_cli_writes_the_fixel_directory(tmp_path, monkeypatch):
+    """fod2fixel's command line end to end on the CPU, the device segmenter
+    replaced by the C restatement: index (count, offset), directions and the
+    metric images in voxel order, x fastest; offset 0 where a voxel has no
+    fixels (the reference leaves those index entries unwritten)."""
+    import torch
+
+    from mrtrix3_b200 import fod2fixel, mif
+
+    class HostSegmenter:
+        def __init__(self, lmax, integral, peak, merge):
+            self.ref = fmls_ref.Segmenter(lmax, integral, peak, merge)
+
+        def segment(self, fod, mask=None, max_fixels=0):
+            rows = fod.numpy().astype(np.float64)
+            c, f = fmls_ref.segment_batch_c(self.ref, rows, max_out=64, nthreads=2)
+            if mask is not None:
+                c = np.where(mask.numpy() != 0, c, 0)
+            if max_fixels:
+                c = np.minimum(c, max_fixels)
+            return torch.from_numpy(c), torch.from_numpy(f)
+
+    monkeypatch.setattr(fmls, "Segmenter", HostSegmenter)
+    monkeypatch.setattr(torch.cuda, "current_device", lambda: 0)
+    monkeypatch.setattr(torch.Tensor, "to", lambda self, *a, **k: self)
+    nx, ny, nz = 3, 2, 2
+    rows = synthetic_fods(nx * ny * nz, 8, seed=41, noise=0.01).astype(np.float32)
+    rows[5] = 0.0  # no lobes
+    data = rows.reshape(nz, ny, nx, -1).transpose(2, 1, 0, 3)
+    src = tmp_path / "fod.mif"
+    mif.write(str(src), mif.Image(data=data, vox=[2.0, 2.0, 2.0, 1.0], keyval={"comments": "x"}))
+    out = tmp_path / "fixels"
+    assert fod2fixel.run([str(src), str(out), "-afd", "afd.mif", "-peak", "pk.mif", "-disp", "disp.mif",
+                          "-maxnum", "3"]) == 0
+    index = mif.read(str(out / "index.mif"))
+    dirs = mif.read(str(out / "directions.mif")).data
+    afd = mif.read(str(out / "afd.mif")).data.reshape(-1)
+    pk = mif.read(str(out / "pk.mif")).data.reshape(-1)
+    c, f = fmls_ref.segment_batch_c(fmls_ref.Segmenter(8), rows.astype(np.float64), max_out=64, nthreads=2)
+    c = np.minimum(c, 3)
+    assert int(index.keyval["nfixels"]) == c.sum() == len(afd)
+    assert index.keyval["comments"] == "x"
+    off = 0
+    for v in range(nx * ny * nz):
+        z, r = divmod(v, nx * ny)
+        y, x = divmod(r, nx)
+        cnt, o = index.data[x, y, z]
+        assert cnt == c[v] and o == (off if c[v] else 0)
+        for q in range(c[v]):
+            np.testing.assert_array_equal(dirs[off + q, :, 0], f[v, q, 0:3])
+            assert afd[off + q] == f[v, q, 6] and pk[off + q] == f[v, q, 7]
+        off += c[v]
+    np.testing.assert_array_equal(mif.read(str(out / "disp.mif")).data.reshape(-1), (afd / pk).astype(np.float32))

@@ -56,6 +56,14 @@ SOLVE_DRAM_BYTES_PER_VOXEL = (126.449152e6 + 47.146496e6) / 262144
 
 FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
+# The numerics of the timed path (csd_params defaults, include/csd_b200.h).
+PRECISION = {
+    "projection": "tcgen05, fp16 hi+lo splits of HR_trans and F (3 products, fp32 accumulate: 22 bits)",
+    "assembly": "mma.sync m16n8k16 on the fp16 hi+lo split of HR_trans, fp32 accumulate",
+    "factorisation": "fp32 Cholesky; fp64 re-factorisation when a pivot fails or (max L_ii/min L_ii)^2 > 1e6",
+    "refine": "policy 3: one fp64-residual refinement after every solve of a voxel whose set cycles in fp32",
+}
+
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -149,9 +157,9 @@ def cpu_baseline(vol, sample_target_s: float = 12.0):
                       f"(oracle/csd_oracle.c), {cores} threads, {dt:.1f} s"}
 
 
-def workload_config(vol, method):
+def workload_config(vol):
     return {"workload": WORKLOAD, "dims": list(vol.dims), "n_voxels": vol.n_voxels, "n_masked": vol.n_masked,
-            "nsh": 45, "n_hr": 300, "method": method,
+            "nsh": 45, "n_hr": 300,
             "l2": "inputs larger than L2 (dwi 497 MB + per-voxel state ~1 GB per step); no flush needed"}
 
 
@@ -169,7 +177,7 @@ def run_reference(args):
     v = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(vol, "FP64 CPU restatement of dwi2fod csd, all host cores"),
+            "config": workload_config(vol), "method": "FP64 CPU restatement of dwi2fod csd, all host cores",
             "cpu_baseline": {**last, "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "vs_baseline": None}
@@ -284,6 +292,141 @@ def next_rows(dwi_dev, sample_idx):
     return out
 
 
+def config_rows(net):
+    """The benchmark's other workloads on this GPU (rank 0, N = 1), each with
+    its FP64 oracle parity and CPU baseline: (1) 32x32x20, 64 directions,
+    plain; (2) 96x96x60, 60 directions, plain and warm-started (the
+    network's scheme); (3) 140x140x96, 90 directions, lmax 10, plain, with the
+    per-voxel iteration counts; (4) 16 uneven volumes with independent random
+    direction sets in one persistent work-queue launch replayed from a
+    captured CUDA graph, the launch shape picked by the project's autotuner,
+    beside the phased method run volume by volume."""
+    import torch
+
+    from mrtrix3_b200 import autotune, csd, synth
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    hr = synth.load_hr_dirs()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed_ms(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def parity(fod, negmask, ref):
+        r = rel_errors(fod, ref["F"])
+        return {"p99_rel_err": float(f"{np.percentile(r, 99):.3g}"), "max_rel_err": float(f"{r.max():.3g}"),
+                "negset_match": float(np.mean(np.all(negmask.view(np.uint32) == ref["negmask"], axis=1))),
+                "sample_voxels": int(len(r))}
+
+    def cpu(osh, rows, target_s=3.0):
+        probe = rows[:min(len(rows), 100 * cores)]
+        t0 = time.perf_counter()
+        osh.solve(probe, nthreads=cores)
+        rate = len(probe) / (time.perf_counter() - t0)
+        m = int(min(len(rows), max(len(probe), rate * target_s)))
+        t0 = time.perf_counter()
+        osh.solve(rows[:m], nthreads=cores)
+        dt = time.perf_counter() - t0
+        return {"value": float(f"{m / dt:.4g}"), "unit": UNIT, "cores": cores, "kind": "port",
+                "sample": f"{m} masked voxels, FP64 oracle restatement, {cores} threads, {dt:.1f} s"}
+
+    def solve_tflops(stt, n):
+        fl = stt["sum_neg"] * n * (n + 1) + (stt["solved"] - stt["reuse_solved"]) * (n ** 3 / 3.0 + 2 * n * n)
+        ms = stt["ms_solve"] - stt["ms_reuse"]
+        return float(f"{fl / max(1e-9, ms / 1e3) / 1e12:.4g}")
+
+    def phased(v, s, lmax, warm_net=None, n_sample=3000, seed=0, reps=3):
+        d = torch.from_numpy(v.dwi).cuda()
+        m = torch.from_numpy(v.mask).cuda() if v.mask is not None else None
+        n = v.n_masked
+        st = csd.State(s, v.n_voxels)
+        row = {}
+        runs = [("plain", None)] + ([("warm", warm_net)] if warm_net is not None else [])
+        outs = {}
+        for name, nt in runs:
+            ms = timed_ms(lambda: st.run(d, mask=m, warm=nt.predict(d, mask=m) if nt is not None else None), reps)
+            stt = st.stats()
+            outs[name] = st.fod()
+            row[name] = {"voxels_per_s": float(f"{n / ms * 1e3:.4g}"), "ms": float(f"{ms:.4g}"),
+                         "solves_per_voxel": float(f"{stt['solved'] / n:.3g}"),
+                         "solve_kernel_tflops": solve_tflops(stt, s.nSH())}
+        if warm_net is not None:
+            row["warm_vs_plain"] = float(f"{row['plain']['ms'] / row['warm']['ms']:.4g}")
+        st.close()
+        inside = np.nonzero(v.mask)[0] if v.mask is not None else np.arange(v.n_voxels)
+        idx = np.sort(np.random.default_rng(seed).choice(inside, min(n_sample, len(inside)), replace=False))
+        osh = O.OracleShared(v.grad, synth.RESPONSE, hr, lmax=lmax)
+        ref = osh.solve(v.dwi[idx], nthreads=cores)
+        row["parity"] = {k: parity(o["fod"][idx], o["negmask"][idx], ref) for k, o in outs.items()}
+        row["cpu_baseline"] = cpu(osh, v.dwi[inside])
+        return row, outs
+
+    out = {}
+    v = synth.config1()
+    out["1"], _ = phased(v, csd.make_shared(v.grad, synth.RESPONSE), 8, n_sample=v.n_voxels)
+    out["1"]["workload"] = "32x32x20 (20,480 voxels), 6 b=0 + 64 DW, SNR 30, lmax 8"
+    v = synth.config2()
+    out["2"], _ = phased(v, csd.make_shared(v.grad, synth.RESPONSE), 8, warm_net=net, n_sample=4000)
+    out["2"]["workload"] = "96x96x60, ellipsoid mask 50% (276,344 voxels), 6 b=0 + 60 DW, SNR U[15,40], lmax 8"
+    v = synth.config3()
+    out["3"], o3 = phased(v, csd.make_shared(v.grad, synth.RESPONSE, lmax=10), 10, n_sample=3000, reps=2)
+    it = o3["plain"]["iterations"][v.mask.astype(bool)]
+    out["3"]["iterations_per_voxel"] = {"mean": float(f"{it.mean():.3g}"), "p99": int(np.percentile(it, 99)),
+                                        "max": int(it.max()),
+                                        "histogram": {int(k): int(c) for k, c in enumerate(np.bincount(it)) if c}}
+    out["3"]["workload"] = "140x140x96, mask 45% (846,816 voxels), 8 b=0 + 90 DW, SNR U[15,40], lmax 10"
+    del v, o3
+    # config 4: 16 uneven volumes in one persistent launch, captured and replayed
+    vols = synth.config4(workers=min(16, cores))
+    shs = [csd.make_shared(v.grad, synth.RESPONSE) for v in vols]
+    ds = [torch.from_numpy(v.dwi).cuda() for v in vols]
+    ms_ = [torch.from_numpy(v.mask).cuda() for v in vols]
+    n4 = int(sum(v.n_masked for v in vols))
+    big = max(range(len(vols)), key=lambda i: vols[i].n_voxels)
+    tuned = autotune.tune(shs[big], ds[big][:262144], use_cache=False)
+    s4 = torch.cuda.Stream()
+    with torch.cuda.stream(s4):
+        csd.solve_volumes(shs, ds, masks=ms_, want_negmask=True, stream=s4)  # workspace before capture
+    s4.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s4):
+        outs4 = csd.solve_volumes(shs, ds, masks=ms_, want_negmask=True, stream=s4)
+    ms_graph = timed_ms(g.replay, 3)
+    ms_phased = 0.0
+    for sh_i, d_i, m_i, v in zip(shs, ds, ms_, vols):
+        st = csd.State(sh_i, v.n_voxels)
+        ms_phased += timed_ms(lambda: st.run(d_i, mask=m_i), 1)
+        st.close()
+    refs, gots = [], []
+    for i, (v, o) in enumerate(zip(vols, outs4)):
+        inside = np.nonzero(v.mask)[0]
+        idx = np.sort(np.random.default_rng(i).choice(inside, 200, replace=False))
+        osh = O.OracleShared(v.grad, synth.RESPONSE, hr)
+        r = osh.solve(v.dwi[idx], nthreads=cores)
+        refs.append(r)
+        gots.append((o["fod"].cpu().numpy()[idx], o["negmask"].cpu().numpy()[idx]))
+    ref4 = {"F": np.concatenate([r["F"] for r in refs]), "negmask": np.concatenate([r["negmask"] for r in refs])}
+    rows4 = np.concatenate([v.dwi[np.nonzero(v.mask)[0][:400]] for v in vols[:1]])
+    out["4"] = {"workload": f"16 volumes, dims U[64^3 .. 128x128x80] ({sum(v.n_voxels for v in vols):,} voxels, "
+                            f"{n4:,} masked), 6 b=0 + 60 random DW each, SNR U[15,40], lmax 8",
+                "persistent_graph": {"voxels_per_s": float(f"{n4 / ms_graph * 1e3:.4g}"), "ms": float(f"{ms_graph:.4g}"),
+                                     "launches": 1, "tuned_shape": tuned["config"]},
+                "phased_per_volume": {"voxels_per_s": float(f"{n4 / ms_phased * 1e3:.4g}"),
+                                      "ms": float(f"{ms_phased:.4g}")},
+                "parity": parity(np.concatenate([a for a, _ in gots]), np.concatenate([b for _, b in gots]), ref4),
+                "cpu_baseline": cpu(O.OracleShared(vols[0].grad, synth.RESPONSE, hr), rows4, target_s=2.0)}
+    autotune.apply({str(k): 0 for k in autotune.CANDIDATES})
+    del g
+    return out
+
+
 def fod2fixel_row():
     """fod2fixel's FMLS segmentation (csd_fmls_segment) of 65,536 synthetic
     FODs at lmax 8, default thresholds; parity and the CPU baseline from the
@@ -346,6 +489,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-next-rows", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other workloads (configs 1-4)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -353,7 +497,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from mrtrix3_b200 import csd, synth
+    from mrtrix3_b200 import autotune, csd, synth
     from mrtrix3_b200.warmstart import WarmStartNet, train_warm_start
     from oracle import oracle as O
 
@@ -435,56 +579,84 @@ def main():
     ms_plain = timed(plain_step, args.steps)
     pstats = st.stats()
     plain_out = st.fod()
+    # ablation: the network's first sets without the factor reuse of the later solves
+    autotune.set_knob(autotune.KNOB_REUSE, 2)
+    try:
+        ms_warm_noreuse = timed(warm_step, args.steps)
+        nstats = st.stats()
+    finally:
+        autotune.set_knob(autotune.KNOB_REUSE, 0)
     ms_pers_plain = timed(lambda: persistent_step(False), max(2, args.steps // 2))
     ms_pers_warm = timed(lambda: persistent_step(True), max(2, args.steps // 2))
 
     def rate(ms):
         return vol.n_masked * world / (ms / 1e3)
 
+    def r4(x):
+        return float(f"{x:.4g}")
+
     methods = {
-        "warm_phased": {"voxels_per_s": value, "ms": ms_warm, "passes": wstats["passes"],
-                        "solves_per_voxel": wstats["solved"] / vol.n_masked},
-        "plain_phased": {"voxels_per_s": rate(ms_plain), "ms": ms_plain, "passes": pstats["passes"],
-                         "solves_per_voxel": pstats["solved"] / vol.n_masked},
-        "persistent_plain": {"voxels_per_s": rate(ms_pers_plain), "ms": ms_pers_plain},
-        "persistent_warm": {"voxels_per_s": rate(ms_pers_warm), "ms": ms_pers_warm},
-        "warm_vs_plain": ms_plain / ms_warm,
+        "warm_vs_plain": r4(ms_plain / ms_warm),
+        "warm_phased": {"voxels_per_s": r4(value), "ms": r4(ms_warm), "passes": wstats["passes"],
+                        "solves_per_voxel": r4(wstats["solved"] / vol.n_masked),
+                        "reuse_solves_per_voxel": r4(wstats["reuse_solved"] / vol.n_masked),
+                        "mean_changed_dirs": r4(wstats["reuse_sum_changes"] / max(1.0, wstats["reuse_solved"]))},
+        "warm_phased_no_reuse": {"voxels_per_s": r4(rate(ms_warm_noreuse)), "ms": r4(ms_warm_noreuse),
+                                 "solves_per_voxel": r4(nstats["solved"] / vol.n_masked)},
+        "plain_phased": {"voxels_per_s": r4(rate(ms_plain)), "ms": r4(ms_plain), "passes": pstats["passes"],
+                         "solves_per_voxel": r4(pstats["solved"] / vol.n_masked)},
+        "persistent_plain_ms": r4(ms_pers_plain),
+        "persistent_warm_ms": r4(ms_pers_warm),
     }
 
     # ---- parity of the warm and plain outputs on a sample ------------------
     inside = np.nonzero(vol.mask)[0]
     idx = np.random.default_rng(1).choice(inside, 4000, replace=False)
     ref = O.OracleShared(vol.grad, synth.RESPONSE, synth.load_hr_dirs()).solve(vol.dwi[idx])
-    parity = {}
+    parity = {"vs": "FP64 oracle (oracle/csd_oracle.c)", "sample_voxels": len(idx)}
     for name, out in (("warm", warm_out), ("plain", plain_out)):
         r = rel_errors(out["fod"][idx], ref["F"])
-        parity[name] = {"p99_rel_err": float(np.percentile(r, 99)), "max_rel_err": float(r.max()),
+        parity[name] = {"p99_rel_err": float(f"{np.percentile(r, 99):.3g}"), "max_rel_err": float(f"{r.max():.3g}"),
                         "negset_match": float(np.mean(np.all(out["negmask"][idx].view(np.uint32) == ref["negmask"],
-                                                             axis=1))),
-                        "sample_voxels": len(idx)}
+                                                             axis=1)))}
 
-    # ---- roofline of the dominant kernel (csd_solve_kernel<45>) ------------
+    # ---- roofline of the solve kernels --------------------------------------
+    # csd_solve_kernel<45> (assembly + factorisation): per solve k n(n+1) +
+    # n^3/3 + 2n^2 (k = |negative set|); csd_solve_reuse_kernel<45> (warm-set
+    # factor + Woodbury correction by r changed directions): per solve
+    # r n(n-1) + r(r+1) n + 4 r n + n^2 + r^3.  Each against its own device time.
     n = 45
-    flops = wstats["sum_neg"] * n * (n + 1) + wstats["solved"] * (n ** 3 / 3.0 + 2 * n * n)
-    solve_s = wstats["ms_solve"] / 1e3
     peaks, peak_kind = load_peaks()
-    achieved = flops / solve_s / 1e12
+    full_solves = wstats["solved"] - wstats["reuse_solved"]
+    full_ms = wstats["ms_solve"] - wstats["ms_reuse"]
+    full_flops = wstats["sum_neg"] * n * (n + 1) + full_solves * (n ** 3 / 3.0 + 2 * n * n)
+    rr = wstats["reuse_sum_changes"] / max(1.0, wstats["reuse_solved"])
+    reuse_flops = wstats["reuse_solved"] * (rr * n * (n - 1) + rr * (rr + 1) * n + 4 * rr * n + n * n + rr ** 3)
     solve_launches = max(1.0, wstats["passes"])
+    kernels = {
+        "csd_solve_kernel<45>": {"ms_per_step": full_ms, "solves": full_solves, "flops": full_flops},
+        "csd_solve_reuse_kernel<45>": {"ms_per_step": wstats["ms_reuse"], "solves": wstats["reuse_solved"],
+                                       "flops": reuse_flops},
+    }
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    kd = kernels[dom]
+    achieved = kd["flops"] / max(1e-9, kd["ms_per_step"] / 1e3) / 1e12
     traffic = None
-    if SOLVE_DRAM_BYTES_PER_VOXEL is not None:
-        traffic = SOLVE_DRAM_BYTES_PER_VOXEL * wstats["solved"] / solve_launches
+    if dom == "csd_solve_kernel<45>" and SOLVE_DRAM_BYTES_PER_VOXEL is not None:
+        traffic = SOLVE_DRAM_BYTES_PER_VOXEL * full_solves / solve_launches
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                "frac": achieved / peaks["bf16_tflops"], "traffic": traffic,
-                "kernel": "csd_solve_kernel<45>",
+                "frac": achieved / peaks["bf16_tflops"], "traffic": traffic, "kernel": dom,
                 "peak_source": f"dense bf16 tensor peak, burst ({peak_kind})",
-                "algorithmic_flops_per_launch": flops / solve_launches,
-                "avg_launch_ms": wstats["ms_solve"] / solve_launches,
-                "flops_counted": "sum over solves of k*n(n+1) + n^3/3 + 2n^2 (n=45, k=|negative set|)",
-                "kernel_share_of_step": wstats["ms_solve"] / ms_warm,
-                # context: the factorisation and substitutions run on the FP32 SIMT pipes
+                "algorithmic_flops_per_launch": kd["flops"] / solve_launches,
+                "avg_launch_ms": kd["ms_per_step"] / solve_launches,
+                "kernel_share_of_step": kd["ms_per_step"] / ms_warm,
+                # context: the factorisations and substitutions run on the FP32 SIMT pipes
                 # (148 SMs x 128 FMA lanes x 2 flops x 1.965 GHz, nominal, not measured)
                 "fp32_simt_nominal_tflops": FP32_SIMT_NOMINAL_TFLOPS,
-                "frac_of_fp32_simt_nominal": achieved / FP32_SIMT_NOMINAL_TFLOPS}
+                "frac_of_fp32_simt_nominal": achieved / FP32_SIMT_NOMINAL_TFLOPS,
+                "kernels": {k: {"ms_per_step": r4(v["ms_per_step"]), "solves": int(v["solves"]),
+                                "tflops": r4(v["flops"] / max(1e-9, v["ms_per_step"] / 1e3) / 1e12)}
+                            for k, v in kernels.items()}}
 
     # ---- end to end through the host-buffer C ABI (pinned buffers) ---------
     pinned = torch.from_numpy(vol.dwi).pin_memory()
@@ -508,14 +680,24 @@ def main():
             "vs_baseline": None,
             "dtype": "fp32 (tensor-core projection/assembly on fp16 hi+lo splits, fp64 fallback/refinement)",
             "data": "synthetic",
-            "config": workload_config(vol, "warm-started phased CSD (network first sets + plain iteration)"),
-            "methods": methods, "parity": parity, "roofline": roofline, "e2e": e2e,
+            "config": workload_config(vol),
+            "method": "warm-started phased CSD (network first sets + plain iteration)",
+            "roofline": roofline, "e2e": e2e,
             "gpu_launches": int(wstats["launches"] + mlp_launches) * args.steps,
             "clocks": clk.summary(), "warm_start_net": net_src}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(vol)
     if rank == 0 and world == 1 and not args.no_next_rows:
         line["next_rows"] = next_rows(d, np.nonzero(vol.mask)[0][:2000])
+    if rank == 0 and world == 1 and not args.no_configs:
+        try:
+            line["configs"] = config_rows(net)
+        except Exception as ex:  # the headline line is printed whatever happens here
+            line["configs"] = {"error": f"{type(ex).__name__}: {ex}"}
+    # the metric's own figures last: a reader of the line's tail sees them
+    line["precision"] = PRECISION
+    line["methods"] = methods
+    line["parity"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -163,10 +163,21 @@ int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream);
  * be NULL) receives how many voxels are still iterating (synchronises). */
 int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, void* stream);
 /* Work and device time since the last csd_state_set: out[8] = passes, voxels
- * projected, voxels solved, sum of |negative set| over the solves, then the
- * device milliseconds of the set / projection / solve kernels, and the
- * number of kernel launches. */
+ * projected, voxels solved, sum of |negative set| over the solves that
+ * assembled their system (not those of csd_state_reuse_stats), then the
+ * device milliseconds of the set / projection / solve kernels (the solve
+ * time includes the reuse kernel's), and the number of kernel launches. */
 int csd_state_stats(const csd_state* st, double* out);
+/* Factor reuse of a warm-started state since the last csd_state_set: out[3]
+ * = solves that went through the warm set's stored Cholesky factor (a
+ * Woodbury correction by the directions added to / dropped from the warm set,
+ * at most 24; more, a voxel whose set cycles, or a first solve that needed
+ * FP64 take the full assembly + factorisation), the sum of those changed-
+ * direction counts, and the device milliseconds of that kernel.  No
+ * counterpart in the reference: the iteration and its sets are csd.h:245-269's,
+ * only the arithmetic of each later W^-1 b differs.  csd_state_warm allocates
+ * the factor storage (capacity x ~4.8 KB at lmax 8) on a state's first warm use. */
+int csd_state_reuse_stats(const csd_state* st, double* out);
 /* CSD::FOD(): copy F (float) out, plus optional status/iterations/negmask. */
 int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride, uint8_t* status,
                   uint8_t* iterations, uint32_t* negmask, void* stream);
@@ -356,10 +367,12 @@ int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t vo
  * persistent kernel), 8 the most slabs csd_dwi2fod_host_phased cuts a volume
  * into (0 = 4), 9 the csd_amp2sh kernel (1 a dot product a thread, 2 FP64
  * FMA tiles, 3 FP64 tensor cores where they apply: nd <= 64, nSH <= 48;
- * 0 = the fastest that applies).  Knobs 0-5, 7 and 8
- * leave the outputs unchanged bit for bit; knob 6 changes the FP32
- * summation order of the logits, knob 9 the FP64 summation order of the
- * coefficients. */
+ * 0 = the fastest that applies), 10 the warm-started phased method's later
+ * solves from the warm set's stored factor (0 default = 1 on, 2 off).
+ * Knobs 0-5, 7 and 8 leave the outputs unchanged bit for bit; knob 6 changes
+ * the FP32 summation order of the logits, knob 9 the FP64 summation order of
+ * the coefficients, knob 10 the FP32 arithmetic of the later solves (same
+ * iteration, results within the parity tolerance). */
 int csd_set_launch_config(int which, int value);
 
 /* ---- fod2fixel's FMLS FOD segmenter (src/dwi/fmls.cpp:118-311,

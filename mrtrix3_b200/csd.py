@@ -113,6 +113,7 @@ def lib():
                                    vp, ctypes.c_int, vp, vp, vp]
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]
         L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.csd_state_reuse_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_dwi2fod_host_phased.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
         L.csd_fmls_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.csd_fmls_create_default.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -518,7 +519,11 @@ class State:
         out = (ctypes.c_double * 8)()
         check(lib().csd_state_stats(self._h, out))
         keys = ("passes", "projected", "solved", "sum_neg", "ms_set", "ms_project", "ms_solve", "launches")
-        return dict(zip(keys, list(out)))
+        d = dict(zip(keys, list(out)))
+        r = (ctypes.c_double * 3)()
+        check(lib().csd_state_reuse_stats(self._h, r))
+        d.update(reuse_solved=r[0], reuse_sum_changes=r[1], ms_reuse=r[2])
+        return d
 
     def iterate_all(self, max_passes: int = 0, stream=None) -> int:
         """iterate() until no voxel is active (csd_state_run: passes batched on

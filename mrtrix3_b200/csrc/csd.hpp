@@ -149,7 +149,14 @@ class CSD {
     cudaFree(d_rec_);
   }
 
-  // csd.h:237-243: DW_signals are the samples of the selected shell (dwis order)
+  // csd.h:237-243: DW_signals are the samples of the selected shell (dwis order).
+  // Unlike the reference's set(), which takes the samples as given, this one
+  // goes through csd_state_set and so also applies dwi2fod's load_data rules
+  // (cmd/dwi2fod.cpp:156-173): negative samples are clamped to zero, and a
+  // non-finite sample leaves F at zero with iterate() never returning true.
+  // dwi2fod applies the same rules before calling set(), so its results are
+  // unchanged; a caller that hands set() negative samples directly gets the
+  // fit of the clamped samples.
   template <class VectorType>
   void set(const VectorType& DW_signals) {
     const size_t nvol = shared.grad.size() / 4;

@@ -101,10 +101,30 @@ struct Dims {
 #endif
 };
 
+// Exact power of two 2^k as a float (k clamped to the normal range).
+__host__ __device__ __forceinline__ float pow2f(int k) {
+  k = k < -126 ? -126 : (k > 127 ? 127 : k);
+  union {
+    unsigned u;
+    float f;
+  } x;
+  x.u = (unsigned)(k + 127) << 23;
+  return x.f;
+}
+
+// Exponent that brings the largest of n values (>= 0) into [2^14, 2^15):
+// scaling by 2^-e keeps FP16 hi halves below 65504 and lo halves of the
+// large entries normal, at any scale of the caller's data (the reference's
+// FOD is scale-covariant: F(a S, b r) = (a / b) F(S, r)).  0 for all-zero data.
+__device__ __forceinline__ int fp16_split_exponent(float maxabs) {
+  if (!(maxabs > 0.f) || !isfinite(maxabs)) return 0;
+  return ((__float_as_int(maxabs) >> 23) & 0xFF) - 127 - 14;
+}
+
 // Everything a voxel of one image needs, by device pointer.
 struct Scheme {
   const float* H32;       // [nhr][HS] HR_trans, fp32, zero padded
-  const __half* H16;      // [2][nhr+1][HS16] HR_trans hi then lo, fp16, row nhr = 0
+  const __half* H16;      // [2][nhr+1][HS16] HR_trans / hscale, hi then lo, fp16, row nhr = 0
   const double* H64;      // [nhr][nsh] HR_trans, fp64 (FP64 fallback)
   const float* MtMp;      // packed-padded lower Mt_M, fp32
   const double* MtM64;    // [nsh][nsh] full Mt_M, fp64 (refinement residual)
@@ -113,6 +133,7 @@ struct Scheme {
   const int* dwis;        // [ndw]
   int ndw, ninit, niter;
   float threshold;
+  float hscale;           // power of two: the FP16 tables hold HR_trans / hscale
 };
 
 struct VolumeDesc {
@@ -156,6 +177,7 @@ struct HTab {
   const __half* hl;   // [nhr+1][HS16]
   int nhr;
   bool use32;         // read FP32 values from h32 (else re-sum the FP16 pair)
+  float hs;           // power of two the FP16 pair is scaled down by
 
   // FP32 values of row d, columns 4j..4j+3
   __device__ __forceinline__ float4 quad(int d, int j) const {
@@ -168,14 +190,14 @@ struct HTab {
       const float2 a1 = __half22float2(*reinterpret_cast<const __half2*>(&a.y));
       const float2 b0 = __half22float2(*reinterpret_cast<const __half2*>(&b.x));
       const float2 b1 = __half22float2(*reinterpret_cast<const __half2*>(&b.y));
-      return make_float4(a0.x + b0.x, a0.y + b0.y, a1.x + b1.x, a1.y + b1.y);
+      return make_float4((a0.x + b0.x) * hs, (a0.y + b0.y) * hs, (a1.x + b1.x) * hs, (a1.y + b1.y) * hs);
     }
   }
   __device__ __forceinline__ float val(int d, int i) const {
     if (Dims<N>::KEEP32 && use32) {
       return h32[d * Dims<N>::HS + i];
     } else {
-      return __half2float(hh[d * Dims<N>::HS16 + i]) + __half2float(hl[d * Dims<N>::HS16 + i]);
+      return (__half2float(hh[d * Dims<N>::HS16 + i]) + __half2float(hl[d * Dims<N>::HS16 + i])) * hs;
     }
   }
 };
@@ -186,6 +208,7 @@ __device__ HTab<N> load_htab(unsigned char* smem, const Scheme& sc, int nhr, boo
   HTab<N> t;
   t.nhr = nhr;
   t.use32 = Dims<N>::KEEP32 && use32;
+  t.hs = sc.hscale;
   const int b32 = htab_bytes_32<N>(nhr, use32);
   t.h32 = reinterpret_cast<const float*>(smem);
   if (t.use32) {
@@ -426,6 +449,7 @@ __device__ __forceinline__ void assemble_pass(const HTab<N>& H, const float* MtM
     }
   }
   const int gid = lane >> 2, tig = lane & 3;
+  const float ws = H.hs * H.hs;  // exact: the tables are HR_trans / hs
 #pragma unroll
   for (int ib = IB0; ib < IB1; ++ib) {
 #pragma unroll
@@ -439,7 +463,7 @@ __device__ __forceinline__ void assemble_pass(const HTab<N>& H, const float* MtM
             const int j = 8 * jb + 2 * tig + c;
             if (i < N && j <= i) {
               const int o = packoff(i) + j;
-              w.W[o] = __ldg(MtMp + o) + acc[ib - IB0][jb][2 * r + c];
+              w.W[o] = __ldg(MtMp + o) + acc[ib - IB0][jb][2 * r + c] * ws;
             }
           }
         }

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -63,6 +64,8 @@ static int g_set_kind = 0;    // phased set kernel: 0 default, 1 warp per voxel,
 // 87.9 ms per benchmark volume)
 static int g_fast_cycles = 0;
 static int g_host_slabs = 0;  // host-buffer phased entry point: most slabs per call (knob 8; 0 = 4)
+static int g_reuse = 0;       // later solves of warm-started voxels from their warm-set factor (knob 10: 0 default
+                              // = on, 1 on, 2 off)
 static constexpr int kSetDefault = 2;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
 
@@ -261,17 +264,51 @@ namespace csdb200 {
 // only the voxels whose set changed.
 
 constexpr int kProjRows = 64;       // voxels per projection tile
-constexpr float kProjFScale = 256.f;  // F is scaled by 2^8 before the FP16 split
+// Before the FP16 split each voxel's F is scaled by the power of two that
+// puts its largest coefficient in [2^14, 2^15) (fp16_split_exponent), and the
+// tables are HR_trans * 2^-hexp: the sign test is unchanged and a threshold
+// is compared after the same exact scaling.
 
 // status byte while iterating: low nibble 0xF, high bits = flags; 0x80 marks
 // a voxel whose set cycles in FP32 (its solves are refined)
 constexpr uint8_t kActive = 0x0F;
 constexpr uint8_t kCycling = 0x80;
 
+// ---- factor reuse for warm-started voxels ----------------------------------
+// A warm-started voxel's first solve factorises W0 = Mt_M + H[S0]^T H[S0] for
+// the network's set S0 (csd.h:255-264 with S0 in place of the projected set).
+// Every later set S of that voxel differs from S0 by a few directions (9 of
+// 300 on average on the benchmark volume), so with C = [h_d : d in S xor S0]
+// (n x r) and D = +1 for a direction S adds, -1 for one it drops,
+//   W_S = W0 + C D C^T,   F = W_S^-1 b = L0^-T (y0 - U t),
+// where L0 is W0's Cholesky factor, U = L0^-1 C, y0 = L0^-1 b, and t solves the
+// r x r system (D + U^T U) t = U^T y0 (the Woodbury identity).  That system is
+// quasi-definite -- I + U_a^T U_a > 0 on the added block, U_r^T U_r - I < 0 on
+// the dropped one because W0 >= Mt_M + C_r C_r^T -- so it is eliminated on its
+// diagonal without pivoting.  The iteration, its sets and its stopping rule
+// are the plain method's; only the way each later W_S^-1 b is computed
+// changes (r^2 n + r n^2 / 2 + n^2 operations instead of k n^2 / 2 + n^3 / 3).
+constexpr int kReuseMaxR = 24;   // more changed directions than this: full solve
+constexpr int kReuseKS = 25;     // row stride of [K | rhs] in shared memory (rhs in column 24)
+constexpr int kReusePack = 4;    // voxels a warp solves together (their columns side by side in the lanes)
+
+template <int N>
+struct ReuseLayout {
+  static constexpr int LSZ = packoff(N + 1) + ((N + 3) / 4) * 4;  // factor rows 0..N (row N = y0), then 1/L_ii
+  static constexpr int US = hr_stride(N);                         // column stride of U (odd number of float4s)
+  // per warp: the pack's factors, U's 32 columns, 32 rows of [K | rhs], the 32 changed directions
+  static constexpr int WARP_FLOATS = kReusePack * LSZ + 32 * US + 32 * kReuseKS + 32;
+  // threads per block (shared memory allows fewer warps than this at every lmax)
+  static constexpr int THREADS = 256;
+};
+
 struct StateParams {
   Scheme sc;
   int nhr, nw, n_in, use_warm, npd;
-  float cond_thr, thr_scaled;
+  float* Lst;           // [cap][ReuseLayout<N>::LSZ] first-solve factors of warm-started voxels, or NULL
+  uint8_t* fac;         // [cap] 1 = Lst holds the factor of the voxel's warm set
+  float cond_thr, thr;  // thr: the threshold (csd.h:179) in HR_trans F units
+  int hexp;             // the projection tables hold HR_trans * 2^-hexp
   const __half* Hp16;   // [2][npd][HS16] projection table (hi, lo), zero rows past nhr
   const __half* Htc16;  // [2][K chunks][320 rows][8] tcgen05 projection table (hi, lo), core-matrix layout
   float* F;             // [cap][HS]
@@ -510,6 +547,314 @@ __device__ __forceinline__ int cycle_jump(const StateParams& P, long long v, int
   return ((P.sc.niter - (it + 1)) & 1) ? 2 : 1;
 }
 
+// Whether voxel v's solve in this pass goes through its stored warm-set
+// factor.  Warp-collective (every lane returns the same answer); lane p < nw
+// receives word p of the added / dropped directions, r their total.  The
+// reuse and the full solve kernels evaluate it on the same state, the reuse
+// kernel first: a voxel it cannot finish has fac cleared and so falls to the
+// full kernel in the same pass.
+__device__ __forceinline__ bool reuse_route(const StateParams& P, long long v, int lane, uint32_t& add,
+                                            uint32_t& rem, int& r) {
+  add = rem = 0u;
+  r = 0;
+  if (!P.fac || !P.warm || !P.use_warm) return false;
+  if (!P.fac[v] || P.iters[v] < 2 || (P.status[v] & kCycling)) return false;
+  if (lane < P.nw) {
+    const uint32_t nb = P.newm[v * P.nw + lane];
+    uint32_t wb = P.warm[v * P.nw + lane];
+    if (lane == P.nw - 1 && (P.nhr & 31)) wb &= (1u << (P.nhr & 31)) - 1u;
+    add = nb & ~wb;
+    rem = wb & ~nb;
+  }
+  r = __reduce_add_sync(0xffffffffu, __popc(add) + __popc(rem));
+  return r <= kReuseMaxR;
+}
+
+// Later solves of warm-started voxels from the stored factor of their warm
+// set (see ReuseLayout).  A warp takes the list in chunks of kReusePack
+// entries and solves the chunk's reuse-routed voxels in packs whose changed
+// directions fit in the 32 lanes together: lane l carries one column of C
+// (the FP32 constraint row of a changed direction of one packed voxel, added
+// ones first) through the forward substitution with that voxel's L0, so a
+// voxel with r changed directions occupies r lanes.  The pairs of every
+// packed voxel's K = D + U^T U are spread over the lanes; each lane then
+// eliminates its own row of its voxel's [K | rhs]; finally 8-lane group g
+// forms x = y0 - U t for packed voxel g and back-substitutes F = L0^-T x.
+// Bookkeeping of sets, counts and the next active list is the full solve
+// kernel's.  A voxel whose elimination meets a zero or non-finite pivot is
+// left to the full solve kernel of the same pass (its fac is cleared).
+template <int N>
+__global__ void __launch_bounds__(ReuseLayout<N>::THREADS, 1)
+    csd_solve_reuse_kernel(const __grid_constant__ StateParams P) {
+  using RL = ReuseLayout<N>;
+  constexpr int HS = Dims<N>::HS;
+  constexpr int NQ = Dims<N>::NQ;
+  constexpr int G = 8;  // lanes per voxel in the back substitution
+  constexpr int CQG = GroupDims<N, G>::CQG;
+  extern __shared__ __align__(16) float rsm[];
+  const int nwarps = blockDim.x >> 5;
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
+  if ((long long)blockIdx.x * nwarps * kReusePack >= n_in) return;  // the grid is an upper bound
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = lane >> 3, sl = lane & 7;
+  float* wb = rsm + (size_t)warp * RL::WARP_FLOATS;  // [kReusePack][LSZ] the packed voxels' factors
+  float* Ub = wb + kReusePack * RL::LSZ;            // [32][US] column `lane` of U
+  float* Kb = Ub + 32 * RL::US;                     // [32][kReuseKS] row `lane` of its voxel's [K | rhs]
+  int* dl = reinterpret_cast<int*>(Kb + 32 * kReuseKS);  // [32] the pack's changed directions
+  unsigned long long n_solved = 0, sum_r = 0;  // work counters (stats[2], [3]), added once per warp
+  const long long stride = (long long)gridDim.x * nwarps * kReusePack;
+  for (long long c0 = ((long long)blockIdx.x * nwarps + warp) * kReusePack; c0 < n_in; c0 += stride) {
+    // the chunk's entries that go through their stored factor
+    unsigned pend = 0u;
+    int rq[kReusePack];
+    long long vq[kReusePack];
+    uint32_t aq[kReusePack], mq[kReusePack];  // lane p < nw: word p of the added / dropped directions
+#pragma unroll
+    for (int q = 0; q < kReusePack; ++q) {
+      rq[q] = 0;
+      vq[q] = 0;
+      aq[q] = mq[q] = 0u;
+      if (c0 + q < n_in) {
+        vq[q] = P.act_in[c0 + q];
+        if (reuse_route(P, vq[q], lane, aq[q], mq[q], rq[q])) pend |= 1u << q;
+      }
+    }
+    while (pend) {
+      // a pack: the pending entries, in order, while their columns fit in 32 lanes
+      int off[kReusePack], rg[kReusePack], na[kReusePack], npk = 0, used = 0;
+      long long vg[kReusePack];
+      uint32_t ag[kReusePack], mg[kReusePack];
+#pragma unroll
+      for (int g = 0; g < kReusePack; ++g) {
+        off[g] = 32;
+        rg[g] = 0;
+        na[g] = 0;
+        vg[g] = 0;
+        ag[g] = mg[g] = 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < kReusePack; ++q) {
+        if (((pend >> q) & 1u) && used + rq[q] <= 32) {
+          pend &= ~(1u << q);
+#pragma unroll
+          for (int g = 0; g < kReusePack; ++g)
+            if (g == npk) {
+              off[g] = used;
+              rg[g] = rq[q];
+              vg[g] = vq[q];
+              ag[g] = aq[q];
+              mg[g] = mq[q];
+            }
+          used += rq[q];
+          ++npk;
+        }
+      }
+      // the packed voxels' changed directions (added first) and their factors
+#pragma unroll
+      for (int g = 0; g < kReusePack; ++g) {
+        if (g < npk) {
+          int base = off[g];
+          for (int p = 0; p < P.nw; ++p) {
+            const uint32_t w = __shfl_sync(0xffffffffu, ag[g], p);
+            if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
+            base += __popc(w);
+          }
+          na[g] = base - off[g];
+          for (int p = 0; p < P.nw; ++p) {
+            const uint32_t w = __shfl_sync(0xffffffffu, mg[g], p);
+            if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
+            base += __popc(w);
+          }
+          const float4* src = reinterpret_cast<const float4*>(P.Lst + (size_t)vg[g] * RL::LSZ);
+          float4* dst = reinterpret_cast<float4*>(wb + g * RL::LSZ);
+          for (int i = lane; i < RL::LSZ / 4; i += 32) dst[i] = src[i];
+        }
+      }
+      __syncwarp();
+      // this lane's column: packed voxel gl, column c
+      int gl = 0, c = 0, rl = 0, nal = 0, ol = 0;
+      bool col = false;
+#pragma unroll
+      for (int g = 0; g < kReusePack; ++g)
+        if (g < npk && lane >= off[g] && lane < off[g] + rg[g]) {
+          gl = g;
+          col = true;
+          c = lane - off[g];
+          rl = rg[g];
+          nal = na[g];
+          ol = off[g];
+        }
+      const float* L = wb + gl * RL::LSZ;
+      const float* rd = L + packoff(N + 1);
+      const float* y0 = L + packoff(N);
+      const int d = col ? dl[lane] : 0;
+      // U = L0^-1 C, column `lane` in registers
+      float u[N];
+      {
+        const float4* h = reinterpret_cast<const float4*>(P.sc.H32 + (size_t)d * HS);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          const float4 x = col ? __ldg(h + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+          if (4 * q < N) u[4 * q] = x.x;
+          if (4 * q + 1 < N) u[4 * q + 1] = x.y;
+          if (4 * q + 2 < N) u[4 * q + 2] = x.z;
+          if (4 * q + 3 < N) u[4 * q + 3] = x.w;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const float* Li = L + packoff(i);
+        float s0 = u[i], s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+        for (int k4 = 0; k4 < i; k4 += 4) {
+          const float4 l = *reinterpret_cast<const float4*>(Li + k4);
+          s0 = fmaf(-l.x, u[k4], s0);
+          if (k4 + 1 < i) s1 = fmaf(-l.y, u[k4 + 1], s1);
+          if (k4 + 2 < i) s2 = fmaf(-l.z, u[k4 + 2], s2);
+          if (k4 + 3 < i) s3 = fmaf(-l.w, u[k4 + 3], s3);
+        }
+        u[i] = ((s0 + s1) + (s2 + s3)) * rd[i];
+      }
+      // rhs = u . y0; the column to shared memory (zero padded to US)
+      float rhs0 = 0.f, rhs1 = 0.f;
+#pragma unroll
+      for (int i = 0; i < N; i += 2) {
+        rhs0 = fmaf(u[i], y0[i], rhs0);
+        if (i + 1 < N) rhs1 = fmaf(u[i + 1], y0[i + 1], rhs1);
+      }
+      {
+        float4* uc = reinterpret_cast<float4*>(Ub + lane * RL::US);
+#pragma unroll
+        for (int q = 0; q < RL::US / 4; ++q)
+          uc[q] = make_float4(4 * q < N ? u[4 * q] : 0.f, 4 * q + 1 < N ? u[4 * q + 1] : 0.f,
+                              4 * q + 2 < N ? u[4 * q + 2] : 0.f, 4 * q + 3 < N ? u[4 * q + 3] : 0.f);
+      }
+      __syncwarp();
+      // K = D + U^T U of every packed voxel: its pairs i <= j in one index
+      // space after the earlier voxels' pairs, spread over the lanes
+      int npair = 0;
+#pragma unroll
+      for (int g = 0; g < kReusePack; ++g) npair += rg[g] * (rg[g] + 1) / 2;
+      for (int p = lane; p < npair; p += 32) {
+        // the voxel of pair p (o, ng: its first lane and added count) and p's place in its list
+        int o = 0, ng = 0, pp = p, acc = 0;
+#pragma unroll
+        for (int g = 0; g < kReusePack; ++g) {
+          const int pg = rg[g] * (rg[g] + 1) / 2;
+          if (p >= acc && p < acc + pg) {
+            o = off[g];
+            ng = na[g];
+            pp = p - acc;
+          }
+          acc += pg;
+        }
+        int j = (int)((sqrtf(8.f * (float)pp + 1.f) - 1.f) * 0.5f);
+        while ((j + 1) * (j + 2) / 2 <= pp) ++j;
+        while (j * (j + 1) / 2 > pp) --j;
+        const int i = pp - j * (j + 1) / 2;
+        const float4* ci = reinterpret_cast<const float4*>(Ub + (o + i) * RL::US);
+        const float4* cj = reinterpret_cast<const float4*>(Ub + (o + j) * RL::US);
+        float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+        for (int qq = 0; qq < NQ; ++qq) {
+          const float4 x = ci[qq], y = cj[qq];
+          a0 = fmaf(x.x, y.x, a0);
+          a1 = fmaf(x.y, y.y, a1);
+          a0 = fmaf(x.z, y.z, a0);
+          a1 = fmaf(x.w, y.w, a1);
+        }
+        const float kij = a0 + a1 + (i == j ? (i < ng ? 1.f : -1.f) : 0.f);
+        Kb[(o + i) * kReuseKS + j] = kij;
+        Kb[(o + j) * kReuseKS + i] = kij;
+      }
+      if (col) Kb[lane * kReuseKS + kReuseMaxR] = rhs0 + rhs1;
+      __syncwarp();
+      // Gauss-Jordan elimination on the diagonal (quasi-definite): lane
+      // `lane` owns row c of its voxel's [K | rhs]
+      int rmax = 0;
+#pragma unroll
+      for (int g = 0; g < kReusePack; ++g) rmax = max(rmax, rg[g]);
+      bool okl = true;
+      for (int p = 0; p < rmax; ++p) {
+        const bool step = col && p < rl;
+        const float piv = step ? Kb[(ol + p) * kReuseKS + p] : 1.f;
+        okl = okl && isfinite(piv) && piv != 0.f;
+        if (step && okl && c != p) {
+          const float f = Kb[lane * kReuseKS + p] / piv;
+          for (int cc = p; cc < rl; ++cc)
+            Kb[lane * kReuseKS + cc] = fmaf(-f, Kb[(ol + p) * kReuseKS + cc], Kb[lane * kReuseKS + cc]);
+          Kb[lane * kReuseKS + kReuseMaxR] =
+              fmaf(-f, Kb[(ol + p) * kReuseKS + kReuseMaxR], Kb[lane * kReuseKS + kReuseMaxR]);
+        }
+        __syncwarp();
+      }
+      const float t = (col && okl) ? Kb[lane * kReuseKS + kReuseMaxR] / Kb[lane * kReuseKS + c] : 0.f;
+      const unsigned bad = __ballot_sync(0xffffffffu, col && !(okl && isfinite(t)));
+      // 8-lane group grp: x = y0 - U t and F = L0^-T x for packed voxel grp
+      int og = 0, rgg = 0;
+      long long vgg = 0;
+#pragma unroll
+      for (int g = 0; g < kReusePack; ++g)
+        if (g == grp) {
+          og = off[g];
+          rgg = rg[g];
+          vgg = vg[g];
+        }
+      const bool gact = grp < npk;
+      const bool gok = gact && ((rgg == 0) || ((bad >> og) & ((rgg >= 32) ? 0xffffffffu : ((1u << rgg) - 1u))) == 0u);
+      const float* Lg = wb + (gact ? grp : 0) * RL::LSZ;
+      float x[CQG];
+#pragma unroll
+      for (int q = 0; q < CQG; ++q) {
+        const int i = sl + G * q;
+        x[q] = i < N ? Lg[packoff(N) + i] : 0.f;
+      }
+      for (int j = 0; j < rmax; ++j) {
+        const float tj = __shfl_sync(0xffffffffu, t, (og + j) & 31);
+        if (j < rgg) {
+#pragma unroll
+          for (int q = 0; q < CQG; ++q) {
+            const int i = sl + G * q;
+            if (i < N) x[q] = fmaf(-Ub[(og + j) * RL::US + i], tj, x[q]);
+          }
+        }
+      }
+      chol_back_group_f32<N, G>(Lg, Lg + packoff(N + 1), x, sl);
+      if (gok) {
+#pragma unroll
+        for (int q = 0; q < CQG; ++q) {
+          const int i = sl + G * q;
+          if (i < N) P.F[vgg * HS + i] = x[q];
+        }
+        for (int p = sl; p < P.nw; p += G) {
+          P.old2[vgg * P.nw + p] = P.old[vgg * P.nw + p];
+          P.old[vgg * P.nw + p] = P.newm[vgg * P.nw + p];
+        }
+        if (sl == 0) {
+          const uint8_t flags = (uint8_t)(P.status[vgg] & 0x70);
+          if (P.iters[vgg] >= P.sc.niter) {
+            P.status[vgg] = (uint8_t)(CSD_STATUS_NITER | flags);
+          } else {
+            P.status[vgg] = (uint8_t)(kActive | flags);
+            P.act_out[atomicAdd(P.n_out, 1)] = (int)vgg;
+          }
+          ++n_solved;
+          sum_r += (unsigned long long)rgg;
+        }
+      } else if (gact && sl == 0) {
+        P.fac[vgg] = 0;  // left to the full solve kernel of this pass
+      }
+      __syncwarp();
+    }
+  }
+  n_solved = __reduce_add_sync(0xffffffffu, (unsigned)n_solved);
+  sum_r = __reduce_add_sync(0xffffffffu, (unsigned)sum_r);
+  if (lane == 0 && P.stats && n_solved) {
+    atomicAdd(P.stats + 2, n_solved);
+    atomicAdd(P.stats + 3, sum_r);
+  }
+}
+
 // Projection pass: tiles of 64 active voxels.  Warp w computes rows
 // 16 (w & 3) .. +15 against half (w >> 2) of the directions with mma.sync
 // m16n8k16 (F hi/lo from shared memory as A, the direction table as B, both
@@ -528,6 +873,8 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
   __half* Fh = Hl + npd * D::HS16;
   __half* Fl = Fh + kProjRows * D::HS16;
   uint32_t* bm = reinterpret_cast<uint32_t*>(Fl + kProjRows * D::HS16);  // [64][kMaxWords]
+  float* rowscale = reinterpret_cast<float*>(bm + kProjRows * kMaxWords);  // [64] F scale of each row
+  float* rowthr = rowscale + kProjRows;                                     // [64] threshold in scaled units
   const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
   if ((long long)blockIdx.x * kProjRows >= n_in) return;  // the grid is an upper bound
   {
@@ -543,11 +890,25 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * kProjRows;
     __syncthreads();
+    // per-row power-of-two scale of F (warp w: rows w, w + 8, ...)
+    for (int r = warp; r < kProjRows; r += 8) {
+      float mx = 0.f;
+      if (e0 + r < n_in)
+        for (int c = lane; c < N; c += 32) mx = fmaxf(mx, fabsf(P.F[(long long)P.act_in[e0 + r] * D::HS + c]));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (lane == 0) {
+        const float sc = pow2f(-fp16_split_exponent(mx));
+        rowscale[r] = sc;
+        rowthr[r] = P.thr * sc * pow2f(-P.hexp);
+      }
+    }
+    __syncthreads();
     // F rows -> scaled FP16 hi / lo
     for (int i = threadIdx.x; i < kProjRows * D::HS16; i += blockDim.x) {
       const int r = i / D::HS16, c = i - r * D::HS16;
       float f = 0.f;
-      if (e0 + r < n_in && c < N) f = P.F[(long long)P.act_in[e0 + r] * D::HS + c] * kProjFScale;
+      if (e0 + r < n_in && c < N) f = P.F[(long long)P.act_in[e0 + r] * D::HS + c] * rowscale[r];
       const __half h = __float2half_rn(f);
       Fh[i] = h;
       Fl[i] = __float2half_rn(f - __half2float(h));
@@ -590,7 +951,7 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
         for (int e = 0; e < 4; ++e) {
           const int r = mrow + gid + 8 * (e >> 1);
           const int c = c0 + 8 * (half * tpw + t) + 2 * tig + (e & 1);
-          if (c < P.nhr && acc[t][e] < P.thr_scaled) atomicOr(&bm[r * kMaxWords + (c >> 5)], 1u << (c & 31));
+          if (c < P.nhr && acc[t][e] < rowthr[r]) atomicOr(&bm[r * kMaxWords + (c >> 5)], 1u << (c & 31));
         }
       }
     }
@@ -689,6 +1050,7 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
   bool failed = false;
   for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
     const int e0 = tile * kTcRows;
+    float thr_v = 0.f;  // this row's threshold in the scaled units of its amplitudes
     // this thread's voxel row -> scaled FP16 hi / lo chunks in the core-matrix layout
     {
       const int r = tid;
@@ -708,12 +1070,17 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
           }
         }
       }
+      float mx = 0.f;
+#pragma unroll
+      for (int c = 0; c < KC * 8; ++c) mx = fmaxf(mx, fabsf(f[c]));
+      const float fscale = pow2f(-fp16_split_exponent(mx));
+      thr_v = P.thr * fscale * pow2f(-P.hexp);
 #pragma unroll
       for (int kc = 0; kc < KC; ++kc) {
         __align__(16) __half hi[8], lo[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-          const float v = f[8 * kc + e] * kProjFScale;
+          const float v = f[8 * kc + e] * fscale;
           hi[e] = __float2half_rn(v);
           lo[e] = __float2half_rn(v - __half2float(hi[e]));
         }
@@ -779,7 +1146,7 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
 #pragma unroll
       for (int e = 0; e < 16; ++e) {
         const int c = 16 * j + e;
-        if (c < P.nhr && __uint_as_float(v[e]) < P.thr_scaled) words[c >> 5] |= 1u << (c & 31);
+        if (c < P.nhr && __uint_as_float(v[e]) < thr_v) words[c >> 5] |= 1u << (c & 31);
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -844,6 +1211,11 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
   for (int e = gw; e < n_in; e += nwt) {
     CSD_T0(tl);
     const long long v = P.act_in[e];
+    {
+      uint32_t a_, r_;
+      int nr_;
+      if (reuse_route(P, v, lane, a_, r_, nr_)) continue;  // solved by csd_solve_reuse_kernel
+    }
     for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
     for (int c = lane; c < HS; c += 32) w.F[c] = 0.f;
     uint32_t bits[kMaxWords];
@@ -855,9 +1227,23 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
     sum_k += (unsigned long long)k;
     ++n_solved;
     CSD_T1(tacc, kPhList, tl);
-    const int fl =
-        assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot, tacc) & 0x70;
+    const int fl_all =
+        assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot, tacc);
+    const int fl = fl_all & 0x70;
     CSD_T0(tw);
+    if (P.Lst && P.use_warm && P.warm && P.iters[v] == 1) {
+      // first solve of a warm-started voxel: keep the FP32 factor of its warm
+      // set (rows 0..N, row N = L^-1 b, then 1/L_ii) for its later solves
+      const bool keep = !(fl_all & 0x100);
+      if (keep) {
+        constexpr int LSZ = ReuseLayout<N>::LSZ, WQ = packoff(N + 1) / 4;
+        float4* dst = reinterpret_cast<float4*>(P.Lst + (size_t)v * LSZ);
+        const float4* W4 = reinterpret_cast<const float4*>(w.W);
+        const float4* R4 = reinterpret_cast<const float4*>(w.rdiag);
+        for (int i = lane; i < LSZ / 4; i += 32) dst[i] = i < WQ ? W4[i] : R4[i - WQ];
+      }
+      if (lane == 0) P.fac[v] = keep ? 1 : 0;
+    }
     for (int c = lane; c < N; c += 32) P.F[v * HS + c] = w.F[c];
     if (lane < P.nw) {
       P.old2[v * P.nw + lane] = P.old[v * P.nw + lane];
@@ -920,12 +1306,23 @@ __global__ void __launch_bounds__(GroupSolveThreads<G>::value, 1)
   const long long stride = (long long)gridDim.x * nwarps * V;
   unsigned long long sum_k = 0, n_solved = 0;  // work counters, added once per warp
   for (long long e0 = ((long long)blockIdx.x * nwarps + warp) * V; e0 < n_in; e0 += stride) {
-    // 1. assembly of each voxel's system (+ its right-hand side as row N)
+    // 1. assembly of each voxel's system (+ its right-hand side as row N);
+    // a voxel solved from its warm-set factor (csd_solve_reuse_kernel) leaves
+    // its slot idle
+    unsigned idle = 0u;
 #pragma unroll 1
     for (int g = 0; g < V; ++g) {
       if (e0 + g >= n_in) break;
       const WarpWS<N> w = group_slot_ws<N, V>(base, g);
       const long long v = P.act_in[e0 + g];
+      {
+        uint32_t a_, r_;
+        int nr_;
+        if (reuse_route(P, v, lane, a_, r_, nr_)) {
+          idle |= 1u << g;
+          continue;
+        }
+      }
       for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
       for (int c = lane; c < HS; c += 32) w.F[c] = 0.f;
       uint32_t bits[kMaxWords];
@@ -965,10 +1362,22 @@ __global__ void __launch_bounds__(GroupSolveThreads<G>::value, 1)
 #pragma unroll 1
     for (int g = 0; g < V; ++g) {
       if (e0 + g >= n_in) break;
+      if ((idle >> g) & 1u) continue;
       const WarpWS<N> w = group_slot_ws<N, V>(base, g);
       const long long v = P.act_in[e0 + g];
       const uint8_t st = P.status[v];
       const bool ok = (good >> (g * G)) & 1u;
+      if (P.Lst && P.use_warm && P.warm && P.iters[v] == 1) {
+        // first solve of a warm-started voxel: keep its FP32 factor, as csd_solve_kernel does
+        if (ok) {
+          constexpr int LSZ = ReuseLayout<N>::LSZ, WQ = packoff(N + 1) / 4;
+          float4* dst = reinterpret_cast<float4*>(P.Lst + (size_t)v * LSZ);
+          const float4* W4 = reinterpret_cast<const float4*>(w.W);
+          const float4* R4 = reinterpret_cast<const float4*>(w.rdiag);
+          for (int i = lane; i < LSZ / 4; i += 32) dst[i] = i < WQ ? W4[i] : R4[i - WQ];
+        }
+        if (lane == 0) P.fac[v] = ok ? 1 : 0;
+      }
       int fl = 0;
       if (!ok || (st & kCycling)) {
         // the shared list holds the last voxel's set: rebuild this one's
@@ -1037,6 +1446,7 @@ struct csd_shared {
   int device = -1;               // device holding the tables (-1: not uploaded yet)
   std::mutex upload_mu;
   int HS = 0, WSZ = 0;
+  int hexp = 0;                    // the FP16 tables hold HR_trans * 2^-hexp (largest entry in [2^14, 2^15))
   std::vector<float> H32_host;
   std::vector<__half> H16_host;    // [2][nhr+1][HS16]: hi then lo
   std::vector<__half> Hp16_host;   // [2][npd][HS16]: projection table, hi then lo
@@ -1130,12 +1540,23 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
   s->H32_host.assign((size_t)h.nhr * s->HS, 0.f);
   for (int d = 0; d < h.nhr; ++d)
     for (int c = 0; c < n; ++c) s->H32_host[(size_t)d * s->HS + c] = (float)h.HR[(size_t)d * n + c];
-  // FP16 hi/lo split of HR_trans for the tensor-core assembly, plus a zero row
+  // FP16 hi/lo split of HR_trans for the tensor-core assembly, plus a zero
+  // row.  HR_trans grows with the response (csd.h:175-180: the constraint
+  // multiplier is 50 r0 / 300), so the split is taken of HR_trans * 2^-hexp,
+  // an exact power of two that puts the largest entry in [2^14, 2^15): the
+  // hi halves stay below FP16's 65504 and the lo halves of the entries that
+  // matter stay normal at any response scale.  The kernels scale back exactly.
+  double hmax = 0.0;
+  for (double x : h.HR) hmax = std::max(hmax, std::fabs(x));
+  if (!(hmax > 0.0) || !std::isfinite(hmax)) return fail(CSD_ERR_INVALID, "constraint matrix is zero or not finite");
+  s->hexp = std::ilogb(hmax) - 14;
+  if (s->hexp < -60 || s->hexp > 60) return fail(CSD_ERR_UNSUPPORTED, "response scale out of the supported range");
+  const double hdown = std::ldexp(1.0, -s->hexp);
   const int HS16 = hr_stride16(n);
   s->H16_host.assign((size_t)2 * (h.nhr + 1) * HS16, __float2half_rn(0.f));
   for (int d = 0; d < h.nhr; ++d)
     for (int c = 0; c < n; ++c) {
-      const double x = h.HR[(size_t)d * n + c];
+      const double x = h.HR[(size_t)d * n + c] * hdown;
       const __half hi = __float2half_rn((float)x);
       const __half lo = __float2half_rn((float)(x - (double)__half2float(hi)));
       s->H16_host[(size_t)d * HS16 + c] = hi;
@@ -1369,6 +1790,7 @@ static Scheme scheme_of(const csd_shared* s) {
   sc.ninit = s->h.ninit;
   sc.niter = s->h.niter;
   sc.threshold = (float)s->h.threshold;
+  sc.hscale = pow2f(s->hexp);
   return sc;
 }
 
@@ -1545,6 +1967,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 3) return fail(CSD_ERR_INVALID, "csd_set_launch_config: amp2sh kernel is 0, 1, 2 or 3");
       csdb200::g_amp2sh_kind = value;
       break;
+    case 10:
+      if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: factor reuse is 0 (default), 1 on or 2 off");
+      g_reuse = value;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -1593,6 +2019,11 @@ struct csd_state {
   uint8_t* status = nullptr;
   uint16_t* iters = nullptr;
   uint16_t* cyc = nullptr;
+  float* Lst = nullptr;       // first-solve factors of warm-started voxels (allocated on first warm use)
+  uint8_t* fac = nullptr;     // 1 = Lst holds the voxel's warm-set factor
+  size_t lst_floats = 0;      // ReuseLayout<nSH>::LSZ
+  int reuse_warps = 0;        // launch shape of csd_solve_reuse_kernel
+  size_t reuse_smem = 0;
   int* act[2] = {nullptr, nullptr};
   int* slist = nullptr;
   int* counter = nullptr;
@@ -1609,8 +2040,9 @@ struct csd_state {
   unsigned long long* stats = nullptr;              // device: sum |neg|, solves
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int* pcount = nullptr;                            // device: per-pass counts of csd_state_run
-  cudaEvent_t bev[2 * kRunBatch + 1] = {};          // pass boundaries of one csd_state_run batch
+  cudaEvent_t bev[3 * kRunBatch + 1] = {};          // kernel boundaries of one csd_state_run batch
   double ms_set = 0, ms_project = 0, ms_solve = 0;  // device time of the kernels since the last set()
+  double ms_reuse = 0;                              // of which in csd_solve_reuse_kernel
   long long launches = 0;
 };
 
@@ -1661,7 +2093,7 @@ int state_shape(csd_state* st) {
   CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const size_t psm = (size_t)2 * st->sh->npd * Dims<N>::HS16 * 2 + (size_t)2 * kProjRows * Dims<N>::HS16 * 2 +
-                     (size_t)kProjRows * kMaxWords * 4;
+                     (size_t)kProjRows * kMaxWords * 4 + (size_t)2 * kProjRows * 4;
   if (psm > (size_t)smem_max) return fail(CSD_ERR_UNSUPPORTED, "projection tables too large for shared memory");
   st->proj_smem = psm;
   st->proj_blocks = nsm * std::max(1, (int)(smem_max / psm));
@@ -1675,6 +2107,16 @@ int state_shape(csd_state* st) {
       CUDA_TRY(cudaFuncSetAttribute(csd_state_set_tile_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
     }
   }
+  {
+    using RL = ReuseLayout<N>;
+    const size_t per = (size_t)RL::WARP_FLOATS * sizeof(float);
+    st->lst_floats = RL::LSZ;
+    st->reuse_warps = (int)std::min<size_t>(RL::THREADS / 32, (size_t)smem_max / per);
+    st->reuse_smem = per * st->reuse_warps;
+    if (st->reuse_warps > 0)
+      CUDA_TRY(cudaFuncSetAttribute(csd_solve_reuse_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)st->reuse_smem));
+  }
   return 0;
 }
 
@@ -1687,7 +2129,8 @@ StateParams state_params(const csd_state* st) {
   P.npd = st->sh->npd;
   P.Hp16 = st->sh->Hp16;
   P.Htc16 = st->sh->Htc16;
-  P.thr_scaled = (float)(st->sh->h.threshold * kProjFScale);
+  P.thr = (float)st->sh->h.threshold;
+  P.hexp = st->sh->hexp;
   P.cond_thr = (float)st->sh->cond_thr;
   P.F = st->F;
   P.b = st->b;
@@ -1699,6 +2142,9 @@ StateParams state_params(const csd_state* st) {
   P.status = st->status;
   P.iters = st->iters;
   P.cyc = st->cyc;
+  const bool reuse = g_reuse != 2 && st->use_warm && st->Lst;
+  P.Lst = reuse ? st->Lst : nullptr;
+  P.fac = reuse ? st->fac : nullptr;
   P.fast_cycles = g_fast_cycles != 2;
   P.n_out = st->counter;
   P.err = st->counter + 1;
@@ -1779,6 +2225,13 @@ int state_solve_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
   return 0;
 }
 template <int N>
+int state_reuse_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
+  const int need = (int)std::min<long long>(st->blocks, (P.n_in + st->reuse_warps - 1) / st->reuse_warps);
+  csd_solve_reuse_kernel<N><<<std::max(need, 1), st->reuse_warps * 32, st->reuse_smem, s>>>(P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+template <int N>
 int state_fod_launch(const csd_state* st, float* fod, int64_t fs, uint8_t* so, uint8_t* io, uint32_t* no,
                      cudaStream_t s) {
   const long long tot = st->n * N;
@@ -1825,7 +2278,7 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->act[0], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->act[1], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->counter, 2 * sizeof(int)));
-  CUDA_TRY(cudaMalloc(&st->stats, 2 * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMalloc(&st->stats, 4 * sizeof(unsigned long long)));
   CUDA_TRY(cudaMalloc(&st->pcount, (2 * kRunBatch + 2) * sizeof(int)));
   for (auto& e : st->ev) CUDA_TRY(cudaEventCreate(&e));
   for (auto& e : st->bev) CUDA_TRY(cudaEventCreate(&e));
@@ -1848,6 +2301,8 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->status);
   cudaFree(st->iters);
   cudaFree(st->cyc);
+  cudaFree(st->Lst);
+  cudaFree(st->fac);
   cudaFree(st->act[0]);
   cudaFree(st->act[1]);
   cudaFree(st->counter);
@@ -1870,10 +2325,10 @@ extern "C" int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, 
   st->use_warm = 0;
   st->cur = 0;
   st->passes = st->projected = st->solved = 0;
-  st->ms_set = st->ms_project = st->ms_solve = 0;
+  st->ms_set = st->ms_project = st->ms_solve = st->ms_reuse = 0;
   st->launches = 0;
   CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
-  CUDA_TRY(cudaMemsetAsync(st->stats, 0, 2 * sizeof(unsigned long long), s));
+  CUDA_TRY(cudaMemsetAsync(st->stats, 0, 4 * sizeof(unsigned long long), s));
   if (n_voxels == 0) {
     st->n_active = 0;
     return CSD_OK;
@@ -1904,10 +2359,31 @@ extern "C" int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, 
 extern "C" int csd_state_warm(csd_state* st, const uint32_t* negmask, void* stream) {
   if (!st || !negmask) return fail(CSD_ERR_INVALID, "csd_state_warm: invalid argument");
   const int nw = (st->sh->h.nhr + 31) / 32;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (st->n > 0)
-    CUDA_TRY(cudaMemcpyAsync(st->warm, negmask, (size_t)st->n * nw * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                             static_cast<cudaStream_t>(stream)));
+    CUDA_TRY(cudaMemcpyAsync(st->warm, negmask, (size_t)st->n * nw * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  if (g_reuse != 2 && !st->Lst && st->reuse_warps > 0) {
+    // storage for the warm sets' factors, on first warm use of the state
+    if (cudaMalloc(&st->Lst, (size_t)st->cap * st->lst_floats * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&st->fac, (size_t)st->cap) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(st->Lst);
+      st->Lst = nullptr;
+      return fail(CSD_ERR_NOMEM, "csd_state_warm: no device memory for the warm-set factors");
+    }
+  }
+  if (st->fac && st->n > 0) CUDA_TRY(cudaMemsetAsync(st->fac, 0, (size_t)st->n, s));
   st->use_warm = 1;
+  return CSD_OK;
+}
+
+extern "C" int csd_state_reuse_stats(const csd_state* st, double* out) {
+  if (!st || !out) return fail(CSD_ERR_INVALID, "csd_state_reuse_stats: invalid argument");
+  unsigned long long d[4] = {0, 0, 0, 0};
+  CUDA_TRY(cudaMemcpy(d, st->stats, sizeof(d), cudaMemcpyDeviceToHost));
+  out[0] = (double)d[2];
+  out[1] = (double)d[3];
+  out[2] = st->ms_reuse;
   return CSD_OK;
 }
 
@@ -1945,14 +2421,24 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
       Q.act_out = st->act[st->cur ^ 1];
       CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
       CUDA_TRY(cudaEventRecord(st->ev[2], s));
+      // later solves of warm-started voxels from their stored factor first;
+      // the full kernel then takes every other voxel (and any the first gave up)
+      if (Q.Lst) {
+        CSD_DISPATCH(st->sh->h.nsh, rc = state_reuse_launch<NN>(st, Q, s));
+        if (rc) return rc;
+        st->launches += 1;
+      }
+      CUDA_TRY(cudaEventRecord(st->ev[3], s));
       CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Q, s));
       if (rc) return rc;
-      CUDA_TRY(cudaEventRecord(st->ev[3], s));
+      CUDA_TRY(cudaEventRecord(st->ev[1], s));
       CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
       CUDA_TRY(cudaStreamSynchronize(s));
-      float ms2 = 0.f;
-      CUDA_TRY(cudaEventElapsedTime(&ms2, st->ev[2], st->ev[3]));
+      float ms2 = 0.f, ms3 = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&ms2, st->ev[2], st->ev[1]));
+      CUDA_TRY(cudaEventElapsedTime(&ms3, st->ev[2], st->ev[3]));
       st->ms_solve += ms2;
+      st->ms_reuse += ms3;
       st->launches += 1;
       st->solved += ns;
     }
@@ -1985,6 +2471,7 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
     CUDA_TRY(cudaMemsetAsync(st->counter + 1, 0, sizeof(int), s));
     CUDA_TRY(cudaEventRecord(st->bev[0], s));
     int rc = 0;
+    bool reuse = false;
     for (int p = 0; p < K; ++p) {
       StateParams P = state_params(st);
       P.n_in = U;  // grid size; the count itself comes from the device after the first pass
@@ -1994,16 +2481,24 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
       P.n_out = st->pcount + 2 * p + 1;
       CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
       if (rc) return rc;
-      CUDA_TRY(cudaEventRecord(st->bev[2 * p + 1], s));
+      CUDA_TRY(cudaEventRecord(st->bev[3 * p + 1], s));
       StateParams Q = state_params(st);
       Q.n_in = U;
       Q.n_in_dev = st->pcount + 2 * p + 1;
       Q.act_in = st->slist;
       Q.act_out = st->act[st->cur ^ 1];
       Q.n_out = st->pcount + 2 * p + 2;
+      // later solves of warm-started voxels from their stored factor first;
+      // the full kernel then takes every other voxel (and any the first gave up)
+      if (Q.Lst) {
+        reuse = true;
+        CSD_DISPATCH(st->sh->h.nsh, rc = state_reuse_launch<NN>(st, Q, s));
+        if (rc) return rc;
+      }
+      CUDA_TRY(cudaEventRecord(st->bev[3 * p + 2], s));
       CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Q, s));
       if (rc) return rc;
-      CUDA_TRY(cudaEventRecord(st->bev[2 * p + 2], s));
+      CUDA_TRY(cudaEventRecord(st->bev[3 * p + 3], s));
       st->cur ^= 1;
     }
     int cnt[2 * kRunBatch + 1];
@@ -2013,14 +2508,16 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
     CUDA_TRY(cudaStreamSynchronize(s));
     if (err) return fail(CSD_ERR_TIMEOUT, "projection: a bounded wait on the tensor cores timed out");
     cnt[0] = U;
-    st->launches += 2 * K;  // every enqueued pass launches both kernels (empty ones return at once)
+    st->launches += (reuse ? 3 : 2) * K;  // every enqueued pass launches its kernels (empty ones return at once)
     for (int p = 0; p < K; ++p) {
       if (cnt[2 * p] == 0) break;
-      float a = 0.f, b = 0.f;
-      CUDA_TRY(cudaEventElapsedTime(&a, st->bev[2 * p], st->bev[2 * p + 1]));
-      CUDA_TRY(cudaEventElapsedTime(&b, st->bev[2 * p + 1], st->bev[2 * p + 2]));
+      float a = 0.f, b = 0.f, c = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&a, st->bev[3 * p], st->bev[3 * p + 1]));
+      CUDA_TRY(cudaEventElapsedTime(&b, st->bev[3 * p + 1], st->bev[3 * p + 2]));
+      CUDA_TRY(cudaEventElapsedTime(&c, st->bev[3 * p + 2], st->bev[3 * p + 3]));
       st->ms_project += a;
-      st->ms_solve += b;
+      st->ms_reuse += b;
+      st->ms_solve += b + c;
       st->projected += cnt[2 * p];
       st->solved += cnt[2 * p + 1];
       st->passes += 1;
@@ -2147,6 +2644,7 @@ static int noalloc_launch(const csd_shared* s, const csd_volume* v, cudaStream_t
   d.sc.ninit = h.ninit;
   d.sc.niter = h.niter;
   d.sc.threshold = (float)h.threshold;
+  d.sc.hscale = pow2f(s->hexp);
   d.dwi = v->dwi;
   d.n_voxels = v->n_voxels;
   d.vox_stride = v->voxel_stride;

@@ -4,12 +4,15 @@
 // (1281) directions in FP64 (SH -> amplitude matrix, L2-resident) into
 // shared memory and sort the direction indices by |amplitude| descending,
 // index ascending (the reference's multimap order), by a bitonic network
-// over the next power of two in shared memory.  Lane 0 then runs the
-// segmentation core (fmls_core.cuh: the region growing, the pending
-// assignments, thresholds and Newton refinement of the peaks), its per-lobe
-// state in the warp's slot of a global scratch buffer, and writes the
-// voxel's lobes.  The core is the same source the CPU tests build for the
-// host and compare with the oracle.
+// over the next power of two in shared memory.  Lane 0 then grows the lobes
+// (fmls_core.cuh: the region growing and the pending assignments) with the
+// direction labels and the lobes' state in the warp's shared memory (up to
+// kFmlsLobes lobes; a voxel that makes more is grown again from its global
+// slot).  The Newton refinements of the candidate peaks are independent of
+// one another, so the lanes compute them in parallel, and lane 0 finishes
+// the lobes (thresholds, the nearest-peak test, the fixels) from those
+// results.  The core is the same source the CPU tests build for the host and
+// compare with the oracle.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,9 +29,10 @@ int set_error(int code, const std::string& msg);  // csd_solver.cu
 
 namespace {
 
-constexpr int kFmlsWarps = 4;
+constexpr int kFmlsWarps = 1;  // ~38 KB of shared memory a warp: five warps an SM
 constexpr int kFmlsMaxSort = 2048;  // directions at most (the sort's width)
 constexpr int kFmlsMaxNsh = 153;    // lmax 16
+constexpr int kFmlsLobes = 128;     // lobes a voxel may create in shared memory (more: the global slot)
 
 int next_pow2(int n) {
   int p = 1;
@@ -36,9 +40,19 @@ int next_pow2(int n) {
   return p;
 }
 
-// per warp slot: ints label parent neg head tail next retro_dir retro_lobe,
-// doubles max_peak mean(3) integral peak_dir(3)
+// per warp slot in global memory: ints label parent neg head tail next
+// retro_dir retro_lobe, doubles max_peak mean(3) integral peak_dir(3) -- one
+// entry per direction; the shared-memory lobes use only the retro lists
 constexpr int kSlotInts = 8, kSlotDoubles = 8;
+
+// Shared memory of one warp: values [nd] and sh [nsh] doubles, the sort keys
+// [sort_n] and labels [nd] ints, then for kFmlsLobes lobes the ints parent
+// neg head tail next and the doubles max_peak integral mean(3) peak_dir(3)
+// and the refined peaks' values (1) and directions (3).
+__host__ __device__ inline size_t fmls_warp_bytes(int nd, int nsh, int sort_n) {
+  const size_t a = ((size_t)(nd + nsh) * sizeof(double) + (size_t)(sort_n + nd) * sizeof(int) + 15) & ~(size_t)15;
+  return a + (size_t)5 * kFmlsLobes * sizeof(int) + (size_t)12 * kFmlsLobes * sizeof(double);
+}
 
 struct FmlsArgs {
   fmls::Tables t;
@@ -57,32 +71,49 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nd = a.t.ndir, nsh = a.t.nsh;
-  // per warp: values [nd] doubles, sh [nsh] doubles, keys [sort_n] ints
-  const size_t warp_bytes = ((size_t)(nd + nsh) * sizeof(double) + (size_t)a.sort_n * sizeof(int) + 15) & ~(size_t)15;
-  unsigned char* base = smem_raw + wib * warp_bytes;
+  unsigned char* base = smem_raw + wib * fmls_warp_bytes(nd, nsh, a.sort_n);
   double* values = reinterpret_cast<double*>(base);
   double* sh = values + nd;
   int* keys = reinterpret_cast<int*>(sh + nsh);
+  int* slabel = keys + a.sort_n;
+  int* li = reinterpret_cast<int*>(base + (((size_t)(nd + nsh) * sizeof(double) +
+                                            (size_t)(a.sort_n + nd) * sizeof(int) + 15) & ~(size_t)15));
+  double* ld = reinterpret_cast<double*>(li + 5 * kFmlsLobes);
+  double* pre_val = ld + 8 * kFmlsLobes;
+  double* pre_u = pre_val + kFmlsLobes;
 
   const long long gw = (long long)blockIdx.x * kFmlsWarps + wib;
   char* slot = a.scratch + gw * a.slot_bytes;
   int* ib = reinterpret_cast<int*>(slot);
   double* db = reinterpret_cast<double*>(slot + (((size_t)kSlotInts * nd * sizeof(int) + 15) & ~(size_t)15));
-  fmls::Work w;
-  w.values = values;
-  w.order = keys;
-  w.label = ib;
-  w.parent = ib + nd;
-  w.neg = ib + 2 * nd;
-  w.peak_head = ib + 3 * nd;
-  w.peak_tail = ib + 4 * nd;
-  w.peak_next = ib + 5 * nd;
-  w.retro_dir = ib + 6 * nd;
-  w.retro_lobe = ib + 7 * nd;
-  w.max_peak = db;
-  w.mean = db + nd;
-  w.integral = db + 4 * nd;
-  w.peak_dir = db + 5 * nd;
+  // the global slot's workspace (every array one entry per direction)
+  fmls::Work wg;
+  wg.values = values;
+  wg.order = keys;
+  wg.label = ib;
+  wg.parent = ib + nd;
+  wg.neg = ib + 2 * nd;
+  wg.peak_head = ib + 3 * nd;
+  wg.peak_tail = ib + 4 * nd;
+  wg.peak_next = ib + 5 * nd;
+  wg.retro_dir = ib + 6 * nd;
+  wg.retro_lobe = ib + 7 * nd;
+  wg.max_peak = db;
+  wg.mean = db + nd;
+  wg.integral = db + 4 * nd;
+  wg.peak_dir = db + 5 * nd;
+  // the shared-memory workspace: labels and up to kFmlsLobes lobes
+  fmls::Work ws = wg;
+  ws.label = slabel;
+  ws.parent = li;
+  ws.neg = li + kFmlsLobes;
+  ws.peak_head = li + 2 * kFmlsLobes;
+  ws.peak_tail = li + 3 * kFmlsLobes;
+  ws.peak_next = li + 4 * kFmlsLobes;
+  ws.max_peak = ld;
+  ws.integral = ld + kFmlsLobes;
+  ws.mean = ld + 2 * kFmlsLobes;
+  ws.peak_dir = ld + 5 * kFmlsLobes;
 
   const long long nwarps = (long long)gridDim.x * kFmlsWarps;
   for (long long v = gw; v < a.n; v += nwarps) {
@@ -123,16 +154,42 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
         __syncwarp();
       }
     }
-    if (lane == 0) {
-      int count = 0;
-      if (values[keys[0]] > 0.0) {
-        int nr = 0;
-        const int nl = fmls::grow(a.t, w, &nr);
-        count = fmls::finish(a.t, w, sh, nl, nr,
-                             reinterpret_cast<fmls::Fixel*>(a.fixels + v * (long long)a.max_fixels * 8), a.max_fixels);
+    // lane 0: the region growing and the pending assignments
+    int nl = 0;
+    bool in_smem = true;
+    if (lane == 0 && values[keys[0]] > 0.0) {
+      int nr = 0;
+      nl = fmls::grow(a.t, ws, &nr, kFmlsLobes);
+      if (nl < 0) {  // more lobes than the shared arrays hold
+        in_smem = false;
+        nl = fmls::grow(a.t, wg, &nr);
       }
-      a.counts[v] = count;
+      fmls::assign_pending(a.t, in_smem ? ws : wg, nr);
     }
+    nl = __shfl_sync(0xffffffffu, nl, 0);
+    in_smem = __shfl_sync(0xffffffffu, in_smem ? 1 : 0, 0) != 0;
+    if (nl == 0) {
+      if (lane == 0) a.counts[v] = 0;
+      __syncwarp();
+      continue;
+    }
+    __syncwarp();
+    const fmls::Work& w = in_smem ? ws : wg;
+    // the candidate peaks' Newton refinements, spread over the lanes (in the
+    // global slot's case lane 0 refines them itself, in finish_lobes)
+    if (in_smem) {
+      for (int p = lane; p < nl; p += 32) {
+        if (!fmls::peak_candidate(a.t, w, p)) continue;
+        double u[3] = {w.peak_dir[3 * p], w.peak_dir[3 * p + 1], w.peak_dir[3 * p + 2]};
+        pre_val[p] = fmls::get_peak(a.t, sh, u);
+        for (int k = 0; k < 3; ++k) pre_u[3 * p + k] = u[k];
+      }
+    }
+    __syncwarp();
+    if (lane == 0)
+      a.counts[v] = fmls::finish_lobes(a.t, w, sh, nl,
+                                       reinterpret_cast<fmls::Fixel*>(a.fixels + v * (long long)a.max_fixels * 8),
+                                       a.max_fixels, in_smem ? pre_val : nullptr, in_smem ? pre_u : nullptr);
     __syncwarp();
   }
 }
@@ -224,8 +281,7 @@ extern "C" int csd_fmls_segment(csd_fmls* p, const float* fod, int64_t n, int64_
     return csdb200::set_error(CSD_ERR_INVALID, "csd_fmls_segment: invalid argument");
   if (n == 0) return CSD_OK;
   const int nd = p->t.ndir, nsh = p->t.nsh, sort_n = next_pow2(nd);
-  const size_t warp_bytes = ((size_t)(nd + nsh) * sizeof(double) + (size_t)sort_n * sizeof(int) + 15) & ~(size_t)15;
-  const size_t smem = kFmlsWarps * warp_bytes;
+  const size_t smem = kFmlsWarps * fmls_warp_bytes(nd, nsh, sort_n);
   int nsm = 0, smem_max = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p->device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);

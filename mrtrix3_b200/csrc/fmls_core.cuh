@@ -123,7 +123,9 @@ FMLS_HD inline void lobe_merge(const Work& w, int a, int b) {
 
 // The region growing of fmls.cpp:178-246 over the directions in w.order.
 // Returns the number of lobes created; *n_retro the pending assignments.
-FMLS_HD inline int grow(const Tables& t, const Work& w, int* n_retro) {
+// max_lobes bounds the lobe arrays of w: a voxel that would create more
+// returns -1 (the caller repeats it with larger arrays).
+FMLS_HD inline int grow(const Tables& t, const Work& w, int* n_retro, int max_lobes = 1 << 30) {
   int nl = 0, nr = 0;
   for (int d = 0; d < t.ndir; ++d) w.label[d] = -1;
   for (int k = 0; k < t.ndir; ++k) {
@@ -150,6 +152,7 @@ FMLS_HD inline int grow(const Tables& t, const Work& w, int* n_retro) {
     }
     if (na == 0) {
       // FOD_lobe constructor (fmls.h:60-72)
+      if (nl >= max_lobes) return -1;
       const double* u = t.unit + 3 * d;
       const double av = fabs(v), wt = t.weight[d];
       w.parent[nl] = nl;
@@ -304,15 +307,30 @@ FMLS_HD inline int select_direction(const Tables& t, const double* p) {
   return best;
 }
 
-// fmls.cpp:248-301 after the growing: the pending assignments, then per
-// surviving lobe (creation order) the thresholds and the Newton refinement of
-// its peaks.  Writes at most max_out fixels; returns how many lobes survive.
-FMLS_HD inline int finish(const Tables& t, const Work& w, const double* sh, int nl, int nr, Fixel* out,
-                          int max_out) {
+// fmls.cpp:248-256: the pending ("retrospective") assignments, in order.
+FMLS_HD inline void assign_pending(const Tables& t, const Work& w, int nr) {
   for (int q = 0; q < nr; ++q) {
     const int d = w.retro_dir[q];
     lobe_add(t, w, root(w, w.retro_lobe[q]), d, w.values[d]);
   }
+}
+
+// Whether peak p (created with lobe p) is refined by finish_lobes: its lobe
+// (the root of p after the merges) is positive and passes the integral
+// threshold (fmls.cpp:258-262).  A peak's starting direction is the one the
+// growing left, which finish_lobes changes only after refining that peak, so
+// the refinements of all such peaks can be computed beforehand, in parallel.
+FMLS_HD inline bool peak_candidate(const Tables& t, const Work& w, int p) {
+  const int r = root(w, p);
+  return !w.neg[r] && !(w.integral[r] < t.integral_threshold);
+}
+
+// fmls.cpp:258-301: per surviving lobe (creation order) the thresholds and
+// the Newton refinement of its peaks.  pre_val / pre_u (nullable): the
+// results of get_peak for every candidate peak p, computed beforehand.
+// Writes at most max_out fixels; returns how many lobes survive.
+FMLS_HD inline int finish_lobes(const Tables& t, const Work& w, const double* sh, int nl, Fixel* out, int max_out,
+                                const double* pre_val = nullptr, const double* pre_u = nullptr) {
   int nout = 0;
   for (int r = 0; r < nl; ++r) {
     if (w.parent[r] != r) continue;
@@ -320,7 +338,13 @@ FMLS_HD inline int finish(const Tables& t, const Work& w, const double* sh, int 
     int pi = 0;
     for (int p = w.peak_head[r]; p >= 0; p = w.peak_next[p], ++pi) {
       double u[3] = {w.peak_dir[3 * p], w.peak_dir[3 * p + 1], w.peak_dir[3 * p + 2]};
-      const double val = get_peak(t, sh, u);
+      double val;
+      if (pre_val) {
+        val = pre_val[p];
+        for (int k = 0; k < 3; ++k) u[k] = pre_u[3 * p + k];
+      } else {
+        val = get_peak(t, sh, u);
+      }
       if (!(finite(val) && finite(u[0]) && finite(u[1]) && finite(u[2]))) continue;
       double max_dp = 0.0;
       int nearest = -1, j = 0;
@@ -354,6 +378,13 @@ FMLS_HD inline int finish(const Tables& t, const Work& w, const double* sh, int 
     ++nout;
   }
   return nout;
+}
+
+// fmls.cpp:248-301 after the growing: the pending assignments, then the lobes.
+FMLS_HD inline int finish(const Tables& t, const Work& w, const double* sh, int nl, int nr, Fixel* out,
+                          int max_out) {
+  assign_pending(t, w, nr);
+  return finish_lobes(t, w, sh, nl, out, max_out);
 }
 
 // True when the voxel has no lobes at all (fmls.cpp:166-167, 178-179):

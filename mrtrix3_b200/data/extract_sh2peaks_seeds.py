@@ -31,4 +31,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MRTRIX_REF")
+    if not root:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <MRtrix3 source tree>  (or set MRTRIX_REF)")
+    main(root)

@@ -230,17 +230,34 @@ def config3(seed=3, voxel_limit=None):
     return make_volume((140, 140, 96), 8, 90, (15.0, 40.0), 10, 0.45, seed, voxel_limit=voxel_limit)
 
 
-def config4(seed=4, n_volumes=16, scale=1.0):
-    """16 volumes, dims uniform in [64^3, 128x128x80], 6 b=0 + 60 DW each with an
-    independent random direction set, SNR U[15,40], lmax 8, mask ~50%."""
+def _config4_specs(seed, n_volumes, scale):
     rng = np.random.default_rng(seed)
-    vols = []
+    specs = []
     for i in range(n_volumes):
         dims = (int(rng.integers(64, 129) * scale), int(rng.integers(64, 129) * scale),
                 int(rng.integers(64, 81) * scale))
-        dims = tuple(max(4, d) for d in dims)
-        vols.append(make_volume(dims, 6, 60, (15.0, 40.0), 8, 0.5, seed * 1000 + i, random_dirs=True))
-    return vols
+        specs.append((tuple(max(4, d) for d in dims), seed * 1000 + i))
+    return specs
+
+
+def _config4_volume(spec):
+    dims, vseed = spec
+    return make_volume(dims, 6, 60, (15.0, 40.0), 8, 0.5, vseed, random_dirs=True)
+
+
+def config4(seed=4, n_volumes=16, scale=1.0, workers: int = 0):
+    """16 volumes, dims uniform in [64^3, 128x128x80], 6 b=0 + 60 DW each with an
+    independent random direction set, SNR U[15,40], lmax 8, mask ~50%.  With
+    workers > 1 the volumes are generated by that many spawned processes (the
+    same volumes: each has its own seed)."""
+    specs = _config4_specs(seed, n_volumes, scale)
+    if workers <= 1:
+        return [_config4_volume(sp) for sp in specs]
+    import concurrent.futures
+    import multiprocessing
+    with concurrent.futures.ProcessPoolExecutor(max_workers=workers,
+                                                mp_context=multiprocessing.get_context("spawn")) as ex:
+        return list(ex.map(_config4_volume, specs))
 
 
 def config5(seed=5, voxel_limit=None):

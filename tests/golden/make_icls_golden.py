@@ -30,7 +30,9 @@ SHAPES = {
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MRTRIX_REF")
+    if not root:
+        sys.exit("usage: python make_icls_golden.py <MRtrix3 source tree>  (or set MRTRIX_REF)")
     src = open(os.path.join(root, "testing", "cmd", "testing_unit_tests_icls.cpp")).read()
     for k, v in SIZES.items():
         m = re.search(r"const size_t %s = (\d+);" % k, src)

@@ -181,7 +181,9 @@ def test_cycle_jump_equals_full_iteration(cuda):
     that two-cycle until niter.  Jumping such a cycle to its last call once
     it is exactly periodic gives the FODs, sets, statuses and iteration
     counts of running every call -- plain and warm-started -- while the
-    number of passes drops."""
+    number of passes drops.  The warm-started run assembles every solve
+    (factor reuse off): its FP32 arithmetic is the one with cycling voxels
+    on this volume."""
     import os
 
     import torch
@@ -198,6 +200,7 @@ def test_cycle_jump_equals_full_iteration(cuda):
     st = csd.State(s, v.n_voxels)
     outs, passes = {}, {}
     try:
+        autotune.set_knob(autotune.KNOB_REUSE, 2)
         for knob in (2, 1):
             autotune.set_knob(autotune.KNOB_CYCLE_JUMP, knob)
             for name, w in (("plain", None), ("warm", warm)):
@@ -206,6 +209,7 @@ def test_cycle_jump_equals_full_iteration(cuda):
                 passes[(knob, name)] = st.stats()["passes"]
     finally:
         autotune.set_knob(autotune.KNOB_CYCLE_JUMP, 0)
+        autotune.set_knob(autotune.KNOB_REUSE, 0)
     for name in ("plain", "warm"):
         a, b = outs[(2, name)], outs[(1, name)]
         for k in ("fod", "negmask", "status", "iterations"):
@@ -215,6 +219,7 @@ def test_cycle_jump_equals_full_iteration(cuda):
     # the persistent kernel's per-voxel loop jumps the same cycles
     pers = {}
     try:
+        autotune.set_knob(autotune.KNOB_REUSE, 2)
         for knob in (2, 1):
             autotune.set_knob(autotune.KNOB_CYCLE_JUMP, knob)
             o = csd.dwi2fod_csd(s, d, mask=m, want_negmask=True)
@@ -224,3 +229,30 @@ def test_cycle_jump_equals_full_iteration(cuda):
     for k in ("fod", "negmask", "status", "iterations"):
         assert np.array_equal(pers[2][k], pers[1][k]), ("persistent", k)
     assert ((pers[1]["status"] & 0x0F) == csd.STATUS_NITER).sum() >= 1
+
+
+def test_benchmark_volume_shipped_network(cuda, hr_dirs):
+    """The configuration bench.py times: the 140x140x96 benchmark volume
+    (seed 5, 846,816 masked voxels, 6 b=0 + 60 DW, lmax 8) warm-started by
+    the shipped network (data/warmstart_c5.npz) through State.run.  Every
+    solved voxel is a fixed point of its own set; 4000 sampled voxels match
+    the FP64 oracle (p99 <= 1e-4, >= 99.5% identical final sets); the warm
+    start needs fewer solves than the plain start on the same volume."""
+    import os
+
+    import torch
+
+    from mrtrix3_b200.warmstart import WarmStartNet
+    v = synth.config5(seed=5)
+    s = csd.make_shared(v.grad, synth.RESPONSE)
+    d = torch.from_numpy(v.dwi).cuda()
+    m = torch.from_numpy(v.mask).cuda()
+    net = WarmStartNet.load(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                         "mrtrix3_b200", "data", "warmstart_c5.npz"))
+    st = csd.State(s, v.n_voxels)
+    st.run(d, mask=m, warm=net.predict(d, mask=m))
+    warm_solves = st.stats()["solved"]
+    _check(st.fod(), v, s, hr_dirs, 8, n_sample=4000, seed=5)
+    st.run(d, mask=m)
+    plain_solves = st.stats()["solved"]
+    assert warm_solves < 0.75 * plain_solves, (warm_solves, plain_solves)

@@ -1,0 +1,111 @@
+"""GPU parity of the warm-started phased method's factor reuse.
+
+A warm-started voxel's later solves go through the Cholesky factor of its
+first (warm) set and a Woodbury correction by the directions added to or
+dropped from that set (csd_solve_reuse_kernel); the iteration is still the
+reference's (csd.h:245-269) and must end where the FP64 oracle ends.  The
+warm sets here are the oracle's own final sets with 0-40 random directions
+flipped, so the corrections add and drop directions, and some exceed the
+24-direction limit and take the full solve instead.  Checked with the reuse
+on and off (launch knob 10): both against the oracle started from the same
+sets (p99 relative error <= 1e-4, >= 99.5% identical final sets), and
+against each other.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from mrtrix3_b200 import csd, synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _knob(value):
+    csd.check(csd.lib().csd_set_launch_config(10, value))
+
+
+def _perturbed(negmask, n_hr, rng, max_flips=40):
+    bits = csd.negmask_to_bool(negmask, n_hr)
+    for v in range(len(bits)):
+        k = int(rng.integers(0, max_flips + 1))
+        bits[v, rng.choice(n_hr, k, replace=False)] ^= True
+    nw = (n_hr + 31) // 32
+    pad = np.zeros((len(bits), nw * 32), bool)
+    pad[:, :n_hr] = bits
+    return np.packbits(pad, axis=1, bitorder="little").view(np.uint32).reshape(len(bits), nw)
+
+
+def _rel(fod, F):
+    den = np.abs(F).max(axis=1)
+    return np.abs(fod.astype(np.float64) - F).max(axis=1) / np.where(den > 0, den, 1.0)
+
+
+@pytest.mark.parametrize("lmax,nb0,ndw", [(8, 6, 60), (10, 8, 90), (6, 6, 45)])
+def test_reuse_matches_oracle_and_full_solves(cuda, hr_dirs, lmax, nb0, ndw):
+    import torch
+    rng = np.random.default_rng(900 + lmax)
+    grad = synth.grad_table(nb0, synth.fibonacci_hemisphere(ndw))
+    dwi = synth.voxel_signals(rng, grad, 3000, (15.0, 40.0))
+    osh = O.OracleShared(grad, synth.RESPONSE, hr_dirs, lmax=lmax)
+    s = csd.make_shared(grad, synth.RESPONSE, lmax=lmax)
+    warm = _perturbed(osh.solve(dwi)["negmask"], s.n_hr, rng)
+    # the oracle from the same first sets: a warm start may end on another
+    # fixed point than the plain start, and that is not what is tested here
+    ref = osh.solve(dwi, warm=warm)
+    d = torch.from_numpy(dwi).cuda()
+    w = torch.from_numpy(warm.view(np.int32)).cuda()
+    st = csd.State(s, len(dwi))
+    outs, stats = {}, {}
+    try:
+        for name, knob in (("reuse", 1), ("full", 2)):
+            _knob(knob)
+            st.run(d, warm=w)
+            outs[name] = st.fod()
+            stats[name] = st.stats()
+    finally:
+        _knob(0)
+        st.close()
+    assert stats["reuse"]["reuse_solved"] > 0.5 * len(dwi)
+    assert stats["full"]["reuse_solved"] == 0
+    for name, out in outs.items():
+        r = _rel(out["fod"], ref["F"])
+        assert np.all(np.isfinite(out["fod"])), name
+        assert np.percentile(r, 99) <= 1e-4, (name, np.percentile(r, 99), r.max())
+        m = np.all(out["negmask"].view(np.uint32) == ref["negmask"], axis=1)
+        assert m.mean() >= 0.995, (name, m.mean())
+        assert np.mean((out["status"] & 0x0F) == (ref["status"] & 0x0F)) >= 0.999, name
+    # the same iteration: same call counts and sets on (almost) every voxel
+    a, b = outs["reuse"], outs["full"]
+    assert np.mean(a["iterations"] == b["iterations"]) >= 0.995
+    assert np.mean(np.all(a["negmask"] == b["negmask"], axis=1)) >= 0.995
+    assert np.percentile(_rel(a["fod"], b["fod"].astype(np.float64)), 99) <= 1e-4
+
+
+def test_reuse_on_the_shipped_network(cuda, hr_dirs):
+    """The benchmark's scheme warm-started by the shipped network: the reuse
+    takes most later solves and leaves the results on the oracle's."""
+    import torch
+
+    from mrtrix3_b200.warmstart import WarmStartNet
+    net = WarmStartNet.load(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                         "mrtrix3_b200", "data", "warmstart_c5.npz"))
+    grad = synth.config5_scheme()
+    dwi = synth.voxel_signals(np.random.default_rng(31), grad, 8192, (15.0, 40.0))
+    ref = O.OracleShared(grad, synth.RESPONSE, hr_dirs).solve(dwi)
+    s = csd.make_shared(grad, synth.RESPONSE)
+    d = torch.from_numpy(dwi).cuda()
+    st = csd.State(s, len(dwi))
+    try:
+        _knob(0)
+        st.run(d, warm=net.predict(d))
+        out = st.fod()
+        stt = st.stats()
+    finally:
+        st.close()
+    later = stt["solved"] - len(dwi)
+    assert stt["reuse_solved"] >= 0.95 * later, (stt["reuse_solved"], later)
+    r = _rel(out["fod"], ref["F"])
+    assert np.percentile(r, 99) <= 1e-4, (np.percentile(r, 99), r.max())
+    assert np.mean(np.all(out["negmask"].view(np.uint32) == ref["negmask"], axis=1)) >= 0.995

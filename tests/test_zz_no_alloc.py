@@ -6,8 +6,11 @@ a library allocate mid-run.  csd_solve_noalloc keeps all of its device
 scratch in one static array of the library instead.  This test calls it
 through the C ABI twice in a row (the array keeps the previous call's
 contents, so the second call checks that everything that must start from
-zero is cleared) and compares each result with csd_solve's, within the
-tolerance the other GPU tests use.  This file is collected last on purpose.
+zero is cleared) and compares each result with csd_solve's and with the FP64
+oracle's, within the tolerance the other GPU tests use: at lmax 8, 10 and 12
+(at 10 and 12 the array holds fewer blocks' FP64 slots than the GPU has SMs,
+so the grid shrinks to fit), and with every factorisation forced through the
+FP64 slots.  This file is collected last on purpose.
 """
 import ctypes
 
@@ -15,6 +18,7 @@ import numpy as np
 import pytest
 
 from mrtrix3_b200 import csd, synth
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -40,15 +44,33 @@ def _noalloc(shared, dwi, mask, fod, status, iters, negmask):
     csd.check(fn(shared.handle, ctypes.byref(v), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
 
 
-def test_noalloc_matches_solve_twice(cuda):
+CASES = {
+    # name: (dims, b=0 volumes, DW directions, lmax, force FP64)
+    "lmax8": ((48, 40, 8), 6, 60, 8, False),
+    "lmax10": ((40, 24, 8), 8, 90, 10, False),
+    "lmax12": ((32, 16, 8), 8, 90, 12, False),
+    "lmax8_fp64": ((24, 16, 4), 6, 60, 8, True),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_noalloc_matches_solve_twice(cuda, hr_dirs, case):
     import torch
-    v = synth.make_volume((48, 40, 8), 6, 60, (15.0, 40.0), 8, 0.5, 4242)
-    s = csd.make_shared(v.grad, synth.RESPONSE)
+    dims, nb0, ndw, lmax, force64 = CASES[case]
+    v = synth.make_volume(dims, nb0, ndw, (15.0, 40.0), lmax, 0.5, 4242 + lmax)
+    s = csd.Shared(v.grad)
+    s.parse_cmdline_options(lmax=lmax)
+    if force64:
+        s.fp64_condition = 1.0  # every factorisation goes to the FP64 slots of the static array
+    s.set_response(synth.RESPONSE)
+    s.init()
     dwi = torch.from_numpy(v.dwi).cuda()
     mask = torch.from_numpy(v.mask).cuda()
     ref = csd.dwi2fod_csd(s, dwi, mask=mask, want_negmask=True)
     torch.cuda.synchronize()
     ref = {k: t.cpu().numpy() for k, t in ref.items()}
+    inside = np.nonzero(v.mask)[0]
+    o64 = O.OracleShared(v.grad, synth.RESPONSE, hr_dirs, lmax=lmax).solve(v.dwi[inside])
     n = dwi.shape[0]
     for call in range(2):
         fod = torch.full((n, s.nSH()), float("nan"), dtype=torch.float32, device=cuda)
@@ -63,6 +85,15 @@ def test_noalloc_matches_solve_twice(cuda):
         rel[np.abs(ref["fod"]).max(axis=1) == 0] = np.abs(got).max(axis=1)[np.abs(ref["fod"]).max(axis=1) == 0]
         assert np.isfinite(got).all(), call
         assert np.percentile(rel, 99) <= 1e-4 and rel.max() <= 1e-3, (call, rel.max())
-        assert np.array_equal(status.cpu().numpy(), ref["status"]), call
+        st = status.cpu().numpy()
+        assert np.array_equal(st, ref["status"]), call
+        if force64:
+            assert np.all(st[inside] & csd.STATUS_FP64), call
         assert np.array_equal(iters.cpu().numpy(), ref["iterations"]), call
-        assert np.mean(np.all(negmask.cpu().numpy() == ref["negmask"], axis=1)) >= 0.995, call
+        neg = negmask.cpu().numpy()
+        assert np.mean(np.all(neg == ref["negmask"], axis=1)) >= 0.995, call
+        # against the FP64 oracle, as the parity tests
+        r64 = np.abs(got[inside] - o64["F"]).max(axis=1) / np.abs(o64["F"]).max(axis=1)
+        assert np.percentile(r64, 99) <= 1e-4, (call, np.percentile(r64, 99))
+        assert np.mean(np.all(neg[inside].view(np.uint32) == o64["negmask"], axis=1)) >= 0.995, call
+        assert np.mean((st[inside] & 0x0F) == (o64["status"] & 0x0F)) >= 0.999, call

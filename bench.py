@@ -572,6 +572,22 @@ def main():
         barrier()
     ms_warm = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     wstats = st.stats()
+    # the inference alone (the rest of the step is in the state's counters)
+    barrier()
+    e0.record(stream)
+    for _ in range(3):
+        net.predict(d, mask=m, stream=stream)
+    e1.record(stream)
+    barrier()
+    ms_infer = e0.elapsed_time(e1) / 3
+    # the FP64 final residual check of the last step's voxels (csd_state_check), timed on its own
+    barrier()
+    e0.record(stream)
+    checked, resolved = st.check(1e-6, stream=stream)
+    e1.record(stream)
+    barrier()
+    fp64_check = {"ms": float(f"{e0.elapsed_time(e1):.4g}"), "checked": checked, "resolved": resolved,
+                  "tol": "max|b - W_S F| <= 1e-6 max|b| in FP64, else FP64 re-solve"}
     warm_out = st.fod()
     value = vol.n_masked * world / (ms_warm / 1e3)
 
@@ -597,6 +613,10 @@ def main():
 
     methods = {
         "warm_vs_plain": r4(ms_plain / ms_warm),
+        "warm_phase_ms": {"set": r4(wstats["ms_set"]), "infer": r4(ms_infer), "project": r4(wstats["ms_project"]),
+                          "solve_full": r4(wstats["ms_solve"] - wstats["ms_reuse"]), "solve_reuse": r4(wstats["ms_reuse"])},
+        "plain_phase_ms": {"set": r4(pstats["ms_set"]), "project": r4(pstats["ms_project"]),
+                           "solve_full": r4(pstats["ms_solve"])},
         "warm_phased": {"voxels_per_s": r4(value), "ms": r4(ms_warm), "passes": wstats["passes"],
                         "solves_per_voxel": r4(wstats["solved"] / vol.n_masked),
                         "reuse_solves_per_voxel": r4(wstats["reuse_solved"] / vol.n_masked),
@@ -605,6 +625,7 @@ def main():
                                  "solves_per_voxel": r4(nstats["solved"] / vol.n_masked)},
         "plain_phased": {"voxels_per_s": r4(rate(ms_plain)), "ms": r4(ms_plain), "passes": pstats["passes"],
                          "solves_per_voxel": r4(pstats["solved"] / vol.n_masked)},
+        "fp64_check": fp64_check,
         "persistent_plain_ms": r4(ms_pers_plain),
         "persistent_warm_ms": r4(ms_pers_warm),
     }

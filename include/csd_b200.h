@@ -178,6 +178,15 @@ int csd_state_stats(const csd_state* st, double* out);
  * only the arithmetic of each later W^-1 b differs.  csd_state_warm allocates
  * the factor storage (capacity x ~4.8 KB at lmax 8) on a state's first warm use. */
 int csd_state_reuse_stats(const csd_state* st, double* out);
+/* FP64 check of every finished voxel (converged or at niter): the residual
+ * r = b - (Mt_M + HR_trans[S]^T HR_trans[S]) F of the voxel's final set S
+ * (csd.h:255-264) in FP64; a voxel with max|r| > tol max|b| has its system
+ * re-assembled and solved in FP64 (status gains CSD_STATUS_FP64); tol 0
+ * re-solves every finished voxel.
+ * *n_checked / *n_resolved (may be NULL; otherwise the call synchronises)
+ * receive the counts.  No counterpart in the reference, which solves in
+ * FP64 throughout. */
+int csd_state_check(csd_state* st, double tol, int64_t* n_checked, int64_t* n_resolved, void* stream);
 /* CSD::FOD(): copy F (float) out, plus optional status/iterations/negmask. */
 int csd_state_fod(const csd_state* st, float* fod, int64_t fod_stride, uint8_t* status,
                   uint8_t* iterations, uint32_t* negmask, void* stream);

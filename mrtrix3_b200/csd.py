@@ -114,6 +114,7 @@ def lib():
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]
         L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_state_reuse_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.csd_state_check.argtypes = [vp, ctypes.c_double, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
         L.csd_dwi2fod_host_phased.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
         L.csd_fmls_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.csd_fmls_create_default.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -540,6 +541,18 @@ class State:
             self.warm(warm, stream=stream)
         self.iterate_all(stream=stream)
         return int(self.stats()["passes"])
+
+    def check(self, tol: float = 1e-6, stream=None, counts: bool = True):
+        """FP64 residual check of every finished voxel's last solve; voxels with
+        max|r| > tol max|b| are re-solved in FP64 (csd_state_check).  Returns
+        (checked, re-solved) when ``counts`` (synchronises), else None."""
+        if not counts:
+            check(lib().csd_state_check(self._h, float(tol), None, None, ctypes.c_void_p(_stream_ptr(stream))))
+            return None
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().csd_state_check(self._h, float(tol), ctypes.byref(a), ctypes.byref(b),
+                                    ctypes.c_void_p(_stream_ptr(stream))))
+        return a.value, b.value
 
     def fod(self, stream=None, as_numpy=True):
         import torch

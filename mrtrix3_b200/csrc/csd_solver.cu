@@ -274,6 +274,25 @@ constexpr int kProjRows = 64;       // voxels per projection tile
 constexpr uint8_t kActive = 0x0F;
 constexpr uint8_t kCycling = 0x80;
 
+// A warp's appends to the next active list, gathered in its lanes and
+// written 32 at a time with one atomic on the list's counter (every voxel of
+// a pass goes through that one counter).
+struct WarpAppend {
+  int v = 0, n = 0;
+  __device__ __forceinline__ void push(int voxel, int* list, int* counter, int lane) {
+    if (lane == n) v = voxel;
+    if (++n == 32) flush(list, counter, lane);
+  }
+  __device__ __forceinline__ void flush(int* list, int* counter, int lane) {
+    if (n == 0) return;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(counter, n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (lane < n) list[base + lane] = v;
+    n = 0;
+  }
+};
+
 // ---- factor reuse for warm-started voxels ----------------------------------
 // A warm-started voxel's first solve factorises W0 = Mt_M + H[S0]^T H[S0] for
 // the network's set S0 (csd.h:255-264 with S0 in place of the projected set).
@@ -290,16 +309,14 @@ constexpr uint8_t kCycling = 0x80;
 // changes (r^2 n + r n^2 / 2 + n^2 operations instead of k n^2 / 2 + n^3 / 3).
 constexpr int kReuseMaxR = 24;   // more changed directions than this: full solve
 constexpr int kReuseKS = 25;     // row stride of [K | rhs] in shared memory (rhs in column 24)
-constexpr int kReusePack = 4;    // voxels a warp solves together (their columns side by side in the lanes)
 
 template <int N>
 struct ReuseLayout {
   static constexpr int LSZ = packoff(N + 1) + ((N + 3) / 4) * 4;  // factor rows 0..N (row N = y0), then 1/L_ii
   static constexpr int US = hr_stride(N);                         // column stride of U (odd number of float4s)
-  // per warp: the pack's factors, U's 32 columns, 32 rows of [K | rhs], the 32 changed directions
-  static constexpr int WARP_FLOATS = kReusePack * LSZ + 32 * US + 32 * kReuseKS + 32;
-  // threads per block (shared memory allows fewer warps than this at every lmax)
-  static constexpr int THREADS = 256;
+  static constexpr int WARP_FLOATS = LSZ + kReuseMaxR * US + kReuseMaxR * kReuseKS;
+  // threads per block (bounds the registers: U's column lives in N of them)
+  static constexpr int THREADS = N <= 45 ? 512 : (N <= 66 ? 384 : 256);
 };
 
 struct StateParams {
@@ -307,6 +324,8 @@ struct StateParams {
   int nhr, nw, n_in, use_warm, npd;
   float* Lst;           // [cap][ReuseLayout<N>::LSZ] first-solve factors of warm-started voxels, or NULL
   uint8_t* fac;         // [cap] 1 = Lst holds the factor of the voxel's warm set
+  int* rest_out;        // csd_solve_reuse_kernel: the listed voxels it leaves to the full solve kernel
+  int* n_rest;
   float cond_thr, thr;  // thr: the threshold (csd.h:179) in HR_trans F units
   int hexp;             // the projection tables hold HR_trans * 2^-hexp
   const __half* Hp16;   // [2][npd][HS16] projection table (hi, lo), zero rows past nhr
@@ -571,284 +590,199 @@ __device__ __forceinline__ bool reuse_route(const StateParams& P, long long v, i
 }
 
 // Later solves of warm-started voxels from the stored factor of their warm
-// set (see ReuseLayout).  A warp takes the list in chunks of kReusePack
-// entries and solves the chunk's reuse-routed voxels in packs whose changed
-// directions fit in the 32 lanes together: lane l carries one column of C
-// (the FP32 constraint row of a changed direction of one packed voxel, added
-// ones first) through the forward substitution with that voxel's L0, so a
-// voxel with r changed directions occupies r lanes.  The pairs of every
-// packed voxel's K = D + U^T U are spread over the lanes; each lane then
-// eliminates its own row of its voxel's [K | rhs]; finally 8-lane group g
-// forms x = y0 - U t for packed voxel g and back-substitutes F = L0^-T x.
-// Bookkeeping of sets, counts and the next active list is the full solve
-// kernel's.  A voxel whose elimination meets a zero or non-finite pivot is
-// left to the full solve kernel of the same pass (its fac is cleared).
+// set (see ReuseLayout): warp per voxel.  Lane j < r carries column j of C
+// (the FP32 constraint row of the j-th changed direction, added ones first)
+// through the forward substitution with L0; the pairs of K = D + U^T U are
+// spread over the lanes; [K | U^T y0] is eliminated by the lanes (one row
+// each); then x = y0 - U t and F = L0^-T x.  Bookkeeping of sets, counts and
+// the next active list is the full solve kernel's.  (Packing several voxels
+// into one warp's lanes fills the idle lanes of the forward substitution but
+// needs their factors in shared memory together: at 7 warps an SM it ran
+// 1.6x slower than this form at 16.)
 template <int N>
 __global__ void __launch_bounds__(ReuseLayout<N>::THREADS, 1)
     csd_solve_reuse_kernel(const __grid_constant__ StateParams P) {
   using RL = ReuseLayout<N>;
   constexpr int HS = Dims<N>::HS;
+  constexpr int CQ = Dims<N>::CQ;
   constexpr int NQ = Dims<N>::NQ;
-  constexpr int G = 8;  // lanes per voxel in the back substitution
-  constexpr int CQG = GroupDims<N, G>::CQG;
   extern __shared__ __align__(16) float rsm[];
   const int nwarps = blockDim.x >> 5;
   const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
-  if ((long long)blockIdx.x * nwarps * kReusePack >= n_in) return;  // the grid is an upper bound
+  if ((long long)blockIdx.x * nwarps >= n_in) return;  // the grid is an upper bound
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int grp = lane >> 3, sl = lane & 7;
-  float* wb = rsm + (size_t)warp * RL::WARP_FLOATS;  // [kReusePack][LSZ] the packed voxels' factors
-  float* Ub = wb + kReusePack * RL::LSZ;            // [32][US] column `lane` of U
-  float* Kb = Ub + 32 * RL::US;                     // [32][kReuseKS] row `lane` of its voxel's [K | rhs]
-  int* dl = reinterpret_cast<int*>(Kb + 32 * kReuseKS);  // [32] the pack's changed directions
+  float* Lb = rsm + (size_t)warp * RL::WARP_FLOATS;  // factor rows 0..N (row N = y0), then 1/L_ii
+  float* Ub = Lb + RL::LSZ;                          // [kReuseMaxR][US] columns of U
+  float* Kb = Ub + kReuseMaxR * RL::US;              // [kReuseMaxR][kReuseKS] rows of [K | rhs]
+  const float* rd = Lb + packoff(N + 1);
+  const float* y0 = Lb + packoff(N);
+  int* dl = reinterpret_cast<int*>(Kb);              // changed directions (before K is formed)
   unsigned long long n_solved = 0, sum_r = 0;  // work counters (stats[2], [3]), added once per warp
-  const long long stride = (long long)gridDim.x * nwarps * kReusePack;
-  for (long long c0 = ((long long)blockIdx.x * nwarps + warp) * kReusePack; c0 < n_in; c0 += stride) {
-    // the chunk's entries that go through their stored factor
-    unsigned pend = 0u;
-    int rq[kReusePack];
-    long long vq[kReusePack];
-    uint32_t aq[kReusePack], mq[kReusePack];  // lane p < nw: word p of the added / dropped directions
-#pragma unroll
-    for (int q = 0; q < kReusePack; ++q) {
-      rq[q] = 0;
-      vq[q] = 0;
-      aq[q] = mq[q] = 0u;
-      if (c0 + q < n_in) {
-        vq[q] = P.act_in[c0 + q];
-        if (reuse_route(P, vq[q], lane, aq[q], mq[q], rq[q])) pend |= 1u << q;
+  WarpAppend app;
+  for (int e = blockIdx.x * nwarps + warp; e < n_in; e += gridDim.x * nwarps) {
+    const long long v = P.act_in[e];
+    // the stored factor into shared memory (coalesced 16-byte copies), issued
+    // before the routing test so that both round trips overlap (the host
+    // launches this kernel only on passes where nearly every listed voxel
+    // has a factor)
+    {
+      const float4* src = reinterpret_cast<const float4*>(P.Lst + (size_t)v * RL::LSZ);
+      float4* dst = reinterpret_cast<float4*>(Lb);
+      for (int i = lane; i < RL::LSZ / 4; i += 32) dst[i] = __ldcs(src + i);
+    }
+    uint32_t add, rem;
+    int r;
+    if (!reuse_route(P, v, lane, add, rem, r)) {
+      if (lane == 0 && P.rest_out) P.rest_out[atomicAdd(P.n_rest, 1)] = (int)v;
+      __syncwarp();
+      continue;
+    }
+    // the changed directions in order: added ones, then dropped ones
+    int na = 0;
+    {
+      int base = 0;
+      for (int p = 0; p < P.nw; ++p) {
+        const uint32_t w = __shfl_sync(0xffffffffu, add, p);
+        if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
+        base += __popc(w);
+      }
+      na = base;
+      for (int p = 0; p < P.nw; ++p) {
+        const uint32_t w = __shfl_sync(0xffffffffu, rem, p);
+        if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
+        base += __popc(w);
       }
     }
-    while (pend) {
-      // a pack: the pending entries, in order, while their columns fit in 32 lanes
-      int off[kReusePack], rg[kReusePack], na[kReusePack], npk = 0, used = 0;
-      long long vg[kReusePack];
-      uint32_t ag[kReusePack], mg[kReusePack];
+    __syncwarp();
+    const int d = lane < r ? dl[lane] : 0;
+    __syncwarp();
+    // U = L0^-1 C, column `lane` in registers
+    float u[N];
+    {
+      const float4* h = reinterpret_cast<const float4*>(P.sc.H32 + (size_t)d * HS);
 #pragma unroll
-      for (int g = 0; g < kReusePack; ++g) {
-        off[g] = 32;
-        rg[g] = 0;
-        na[g] = 0;
-        vg[g] = 0;
-        ag[g] = mg[g] = 0u;
+      for (int q = 0; q < NQ; ++q) {
+        const float4 x = lane < r ? __ldg(h + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (4 * q < N) u[4 * q] = x.x;
+        if (4 * q + 1 < N) u[4 * q + 1] = x.y;
+        if (4 * q + 2 < N) u[4 * q + 2] = x.z;
+        if (4 * q + 3 < N) u[4 * q + 3] = x.w;
       }
+    }
 #pragma unroll
-      for (int q = 0; q < kReusePack; ++q) {
-        if (((pend >> q) & 1u) && used + rq[q] <= 32) {
-          pend &= ~(1u << q);
+    for (int i = 0; i < N; ++i) {
+      const float* Li = Lb + packoff(i);
+      float s0 = u[i], s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
-          for (int g = 0; g < kReusePack; ++g)
-            if (g == npk) {
-              off[g] = used;
-              rg[g] = rq[q];
-              vg[g] = vq[q];
-              ag[g] = aq[q];
-              mg[g] = mq[q];
-            }
-          used += rq[q];
-          ++npk;
-        }
+      for (int k4 = 0; k4 < i; k4 += 4) {
+        const float4 l = *reinterpret_cast<const float4*>(Li + k4);
+        s0 = fmaf(-l.x, u[k4], s0);
+        if (k4 + 1 < i) s1 = fmaf(-l.y, u[k4 + 1], s1);
+        if (k4 + 2 < i) s2 = fmaf(-l.z, u[k4 + 2], s2);
+        if (k4 + 3 < i) s3 = fmaf(-l.w, u[k4 + 3], s3);
       }
-      // the packed voxels' changed directions (added first) and their factors
+      u[i] = ((s0 + s1) + (s2 + s3)) * rd[i];
+    }
+    // rhs_j = u_j . y0; U's columns to shared memory (zero padded to US)
+    float rhs0 = 0.f, rhs1 = 0.f;
 #pragma unroll
-      for (int g = 0; g < kReusePack; ++g) {
-        if (g < npk) {
-          int base = off[g];
-          for (int p = 0; p < P.nw; ++p) {
-            const uint32_t w = __shfl_sync(0xffffffffu, ag[g], p);
-            if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
-            base += __popc(w);
-          }
-          na[g] = base - off[g];
-          for (int p = 0; p < P.nw; ++p) {
-            const uint32_t w = __shfl_sync(0xffffffffu, mg[g], p);
-            if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
-            base += __popc(w);
-          }
-          const float4* src = reinterpret_cast<const float4*>(P.Lst + (size_t)vg[g] * RL::LSZ);
-          float4* dst = reinterpret_cast<float4*>(wb + g * RL::LSZ);
-          for (int i = lane; i < RL::LSZ / 4; i += 32) dst[i] = src[i];
-        }
+    for (int i = 0; i < N; i += 2) {
+      rhs0 = fmaf(u[i], y0[i], rhs0);
+      if (i + 1 < N) rhs1 = fmaf(u[i + 1], y0[i + 1], rhs1);
+    }
+    if (lane < r) {
+      float4* uc = reinterpret_cast<float4*>(Ub + lane * RL::US);
+#pragma unroll
+      for (int q = 0; q < RL::US / 4; ++q)
+        uc[q] = make_float4(4 * q < N ? u[4 * q] : 0.f, 4 * q + 1 < N ? u[4 * q + 1] : 0.f,
+                            4 * q + 2 < N ? u[4 * q + 2] : 0.f, 4 * q + 3 < N ? u[4 * q + 3] : 0.f);
+    }
+    __syncwarp();
+    // K = D + U^T U: pair p = j (j + 1) / 2 + i, i <= j, spread over the lanes
+    const int npair = r * (r + 1) / 2;
+    for (int p = lane; p < npair; p += 32) {
+      int j = (int)((sqrtf(8.f * (float)p + 1.f) - 1.f) * 0.5f);
+      while ((j + 1) * (j + 2) / 2 <= p) ++j;
+      while (j * (j + 1) / 2 > p) --j;
+      const int i = p - j * (j + 1) / 2;
+      const float4* ci = reinterpret_cast<const float4*>(Ub + i * RL::US);
+      const float4* cj = reinterpret_cast<const float4*>(Ub + j * RL::US);
+      float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const float4 x = ci[q], y = cj[q];
+        a0 = fmaf(x.x, y.x, a0);
+        a1 = fmaf(x.y, y.y, a1);
+        a0 = fmaf(x.z, y.z, a0);
+        a1 = fmaf(x.w, y.w, a1);
       }
-      __syncwarp();
-      // this lane's column: packed voxel gl, column c
-      int gl = 0, c = 0, rl = 0, nal = 0, ol = 0;
-      bool col = false;
-#pragma unroll
-      for (int g = 0; g < kReusePack; ++g)
-        if (g < npk && lane >= off[g] && lane < off[g] + rg[g]) {
-          gl = g;
-          col = true;
-          c = lane - off[g];
-          rl = rg[g];
-          nal = na[g];
-          ol = off[g];
-        }
-      const float* L = wb + gl * RL::LSZ;
-      const float* rd = L + packoff(N + 1);
-      const float* y0 = L + packoff(N);
-      const int d = col ? dl[lane] : 0;
-      // U = L0^-1 C, column `lane` in registers
-      float u[N];
-      {
-        const float4* h = reinterpret_cast<const float4*>(P.sc.H32 + (size_t)d * HS);
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-          const float4 x = col ? __ldg(h + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-          if (4 * q < N) u[4 * q] = x.x;
-          if (4 * q + 1 < N) u[4 * q + 1] = x.y;
-          if (4 * q + 2 < N) u[4 * q + 2] = x.z;
-          if (4 * q + 3 < N) u[4 * q + 3] = x.w;
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        const float* Li = L + packoff(i);
-        float s0 = u[i], s1 = 0.f, s2 = 0.f, s3 = 0.f;
-#pragma unroll
-        for (int k4 = 0; k4 < i; k4 += 4) {
-          const float4 l = *reinterpret_cast<const float4*>(Li + k4);
-          s0 = fmaf(-l.x, u[k4], s0);
-          if (k4 + 1 < i) s1 = fmaf(-l.y, u[k4 + 1], s1);
-          if (k4 + 2 < i) s2 = fmaf(-l.z, u[k4 + 2], s2);
-          if (k4 + 3 < i) s3 = fmaf(-l.w, u[k4 + 3], s3);
-        }
-        u[i] = ((s0 + s1) + (s2 + s3)) * rd[i];
-      }
-      // rhs = u . y0; the column to shared memory (zero padded to US)
-      float rhs0 = 0.f, rhs1 = 0.f;
-#pragma unroll
-      for (int i = 0; i < N; i += 2) {
-        rhs0 = fmaf(u[i], y0[i], rhs0);
-        if (i + 1 < N) rhs1 = fmaf(u[i + 1], y0[i + 1], rhs1);
-      }
-      {
-        float4* uc = reinterpret_cast<float4*>(Ub + lane * RL::US);
-#pragma unroll
-        for (int q = 0; q < RL::US / 4; ++q)
-          uc[q] = make_float4(4 * q < N ? u[4 * q] : 0.f, 4 * q + 1 < N ? u[4 * q + 1] : 0.f,
-                              4 * q + 2 < N ? u[4 * q + 2] : 0.f, 4 * q + 3 < N ? u[4 * q + 3] : 0.f);
-      }
-      __syncwarp();
-      // K = D + U^T U of every packed voxel: its pairs i <= j in one index
-      // space after the earlier voxels' pairs, spread over the lanes
-      int npair = 0;
-#pragma unroll
-      for (int g = 0; g < kReusePack; ++g) npair += rg[g] * (rg[g] + 1) / 2;
-      for (int p = lane; p < npair; p += 32) {
-        // the voxel of pair p (o, ng: its first lane and added count) and p's place in its list
-        int o = 0, ng = 0, pp = p, acc = 0;
-#pragma unroll
-        for (int g = 0; g < kReusePack; ++g) {
-          const int pg = rg[g] * (rg[g] + 1) / 2;
-          if (p >= acc && p < acc + pg) {
-            o = off[g];
-            ng = na[g];
-            pp = p - acc;
-          }
-          acc += pg;
-        }
-        int j = (int)((sqrtf(8.f * (float)pp + 1.f) - 1.f) * 0.5f);
-        while ((j + 1) * (j + 2) / 2 <= pp) ++j;
-        while (j * (j + 1) / 2 > pp) --j;
-        const int i = pp - j * (j + 1) / 2;
-        const float4* ci = reinterpret_cast<const float4*>(Ub + (o + i) * RL::US);
-        const float4* cj = reinterpret_cast<const float4*>(Ub + (o + j) * RL::US);
-        float a0 = 0.f, a1 = 0.f;
-#pragma unroll
-        for (int qq = 0; qq < NQ; ++qq) {
-          const float4 x = ci[qq], y = cj[qq];
-          a0 = fmaf(x.x, y.x, a0);
-          a1 = fmaf(x.y, y.y, a1);
-          a0 = fmaf(x.z, y.z, a0);
-          a1 = fmaf(x.w, y.w, a1);
-        }
-        const float kij = a0 + a1 + (i == j ? (i < ng ? 1.f : -1.f) : 0.f);
-        Kb[(o + i) * kReuseKS + j] = kij;
-        Kb[(o + j) * kReuseKS + i] = kij;
-      }
-      if (col) Kb[lane * kReuseKS + kReuseMaxR] = rhs0 + rhs1;
-      __syncwarp();
-      // Gauss-Jordan elimination on the diagonal (quasi-definite): lane
-      // `lane` owns row c of its voxel's [K | rhs]
-      int rmax = 0;
-#pragma unroll
-      for (int g = 0; g < kReusePack; ++g) rmax = max(rmax, rg[g]);
-      bool okl = true;
-      for (int p = 0; p < rmax; ++p) {
-        const bool step = col && p < rl;
-        const float piv = step ? Kb[(ol + p) * kReuseKS + p] : 1.f;
-        okl = okl && isfinite(piv) && piv != 0.f;
-        if (step && okl && c != p) {
-          const float f = Kb[lane * kReuseKS + p] / piv;
-          for (int cc = p; cc < rl; ++cc)
-            Kb[lane * kReuseKS + cc] = fmaf(-f, Kb[(ol + p) * kReuseKS + cc], Kb[lane * kReuseKS + cc]);
-          Kb[lane * kReuseKS + kReuseMaxR] =
-              fmaf(-f, Kb[(ol + p) * kReuseKS + kReuseMaxR], Kb[lane * kReuseKS + kReuseMaxR]);
-        }
-        __syncwarp();
-      }
-      const float t = (col && okl) ? Kb[lane * kReuseKS + kReuseMaxR] / Kb[lane * kReuseKS + c] : 0.f;
-      const unsigned bad = __ballot_sync(0xffffffffu, col && !(okl && isfinite(t)));
-      // 8-lane group grp: x = y0 - U t and F = L0^-T x for packed voxel grp
-      int og = 0, rgg = 0;
-      long long vgg = 0;
-#pragma unroll
-      for (int g = 0; g < kReusePack; ++g)
-        if (g == grp) {
-          og = off[g];
-          rgg = rg[g];
-          vgg = vg[g];
-        }
-      const bool gact = grp < npk;
-      const bool gok = gact && ((rgg == 0) || ((bad >> og) & ((rgg >= 32) ? 0xffffffffu : ((1u << rgg) - 1u))) == 0u);
-      const float* Lg = wb + (gact ? grp : 0) * RL::LSZ;
-      float x[CQG];
-#pragma unroll
-      for (int q = 0; q < CQG; ++q) {
-        const int i = sl + G * q;
-        x[q] = i < N ? Lg[packoff(N) + i] : 0.f;
-      }
-      for (int j = 0; j < rmax; ++j) {
-        const float tj = __shfl_sync(0xffffffffu, t, (og + j) & 31);
-        if (j < rgg) {
-#pragma unroll
-          for (int q = 0; q < CQG; ++q) {
-            const int i = sl + G * q;
-            if (i < N) x[q] = fmaf(-Ub[(og + j) * RL::US + i], tj, x[q]);
-          }
-        }
-      }
-      chol_back_group_f32<N, G>(Lg, Lg + packoff(N + 1), x, sl);
-      if (gok) {
-#pragma unroll
-        for (int q = 0; q < CQG; ++q) {
-          const int i = sl + G * q;
-          if (i < N) P.F[vgg * HS + i] = x[q];
-        }
-        for (int p = sl; p < P.nw; p += G) {
-          P.old2[vgg * P.nw + p] = P.old[vgg * P.nw + p];
-          P.old[vgg * P.nw + p] = P.newm[vgg * P.nw + p];
-        }
-        if (sl == 0) {
-          const uint8_t flags = (uint8_t)(P.status[vgg] & 0x70);
-          if (P.iters[vgg] >= P.sc.niter) {
-            P.status[vgg] = (uint8_t)(CSD_STATUS_NITER | flags);
-          } else {
-            P.status[vgg] = (uint8_t)(kActive | flags);
-            P.act_out[atomicAdd(P.n_out, 1)] = (int)vgg;
-          }
-          ++n_solved;
-          sum_r += (unsigned long long)rgg;
-        }
-      } else if (gact && sl == 0) {
-        P.fac[vgg] = 0;  // left to the full solve kernel of this pass
+      const float kij = a0 + a1 + (i == j ? (i < na ? 1.f : -1.f) : 0.f);
+      Kb[i * kReuseKS + j] = kij;
+      Kb[j * kReuseKS + i] = kij;
+    }
+    if (lane < r) Kb[lane * kReuseKS + kReuseMaxR] = rhs0 + rhs1;
+    __syncwarp();
+    // Gauss-Jordan elimination of [K | rhs] on the diagonal (quasi-definite)
+    bool ok = true;
+    for (int p = 0; p < r; ++p) {
+      const float piv = Kb[p * kReuseKS + p];
+      ok = ok && isfinite(piv) && piv != 0.f;
+      const float rpiv = __frcp_rn(piv);
+      if (ok && lane < r && lane != p) {
+        const float f = Kb[lane * kReuseKS + p] * rpiv;
+        for (int c = p; c < r; ++c) Kb[lane * kReuseKS + c] = fmaf(-f, Kb[p * kReuseKS + c], Kb[lane * kReuseKS + c]);
+        Kb[lane * kReuseKS + kReuseMaxR] =
+            fmaf(-f, Kb[p * kReuseKS + kReuseMaxR], Kb[lane * kReuseKS + kReuseMaxR]);
       }
       __syncwarp();
     }
+    const float t = (ok && lane < r) ? Kb[lane * kReuseKS + kReuseMaxR] / Kb[lane * kReuseKS + lane] : 0.f;
+    if (!__all_sync(0xffffffffu, ok && isfinite(t))) {
+      // leave this voxel to the full solve kernel of the same pass
+      if (lane == 0) {
+        P.fac[v] = 0;
+        if (P.rest_out) P.rest_out[atomicAdd(P.n_rest, 1)] = (int)v;
+      }
+      __syncwarp();
+      continue;
+    }
+    // x = y0 - U t, then F = L0^-T x
+    float x[CQ];
+#pragma unroll
+    for (int q = 0; q < CQ; ++q) {
+      const int i = lane + 32 * q;
+      x[q] = i < N ? y0[i] : 0.f;
+    }
+    for (int j = 0; j < r; ++j) {
+      const float tj = __shfl_sync(0xffffffffu, t, j);
+#pragma unroll
+      for (int q = 0; q < CQ; ++q) {
+        const int i = lane + 32 * q;
+        if (i < N) x[q] = fmaf(-Ub[j * RL::US + i], tj, x[q]);
+      }
+    }
+    chol_back_f32<N>(Lb, rd, x, lane);
+#pragma unroll
+    for (int q = 0; q < CQ; ++q) {
+      const int i = lane + 32 * q;
+      if (i < N) P.F[v * HS + i] = x[q];
+    }
+    if (lane < P.nw) {
+      P.old2[v * P.nw + lane] = P.old[v * P.nw + lane];
+      P.old[v * P.nw + lane] = P.newm[v * P.nw + lane];
+    }
+    sum_r += (unsigned long long)r;
+    ++n_solved;
+    {
+      const uint8_t flags = (uint8_t)(P.status[v] & 0x70);
+      const bool last = P.iters[v] >= P.sc.niter;
+      __syncwarp();
+      if (lane == 0) P.status[v] = last ? (uint8_t)(CSD_STATUS_NITER | flags) : (uint8_t)(kActive | flags);
+      if (!last) app.push((int)v, P.act_out, P.n_out, lane);
+    }
+    __syncwarp();
   }
-  n_solved = __reduce_add_sync(0xffffffffu, (unsigned)n_solved);
-  sum_r = __reduce_add_sync(0xffffffffu, (unsigned)sum_r);
+  app.flush(P.act_out, P.n_out, lane);
   if (lane == 0 && P.stats && n_solved) {
     atomicAdd(P.stats + 2, n_solved);
     atomicAdd(P.stats + 3, sum_r);
@@ -1152,8 +1086,10 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
     // per-voxel decision (csd.h:246-253), one thread per voxel
     const int r = tid;
+    bool append = false;
+    long long v = 0;
     if (e0 + r < n_in) {
-      const long long v = P.act_in[e0 + r];
+      v = P.act_in[e0 + r];
       const int it = P.iters[v];
       const bool warm = it == 0 && P.use_warm && P.warm;
       bool same = true, back = true;
@@ -1177,8 +1113,16 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
         for (int w = 0; w < P.nw; ++w)
           P.newm[v * P.nw + w] = ff == 2 ? P.old[v * P.nw + w] : words[w < kTcDirs / 32 ? w : 0];
         P.status[v] = st;
-        P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
+        append = true;
       }
+    }
+    // the solve list, one atomic per warp (a single counter takes every append)
+    {
+      const unsigned bal = __ballot_sync(0xffffffffu, append);
+      int base = 0;
+      if ((tid & 31) == 0 && bal) base = atomicAdd(P.n_out, __popc(bal));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (append) P.act_out[base + __popc(bal & ((1u << (tid & 31)) - 1u))] = (int)v;
     }
     __syncthreads();
   }
@@ -1208,6 +1152,7 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
   long long* tacc = nullptr;
 #endif
   unsigned long long sum_k = 0, n_solved = 0;  // work counters, added once per warp
+  WarpAppend app;
   for (int e = gw; e < n_in; e += nwt) {
     CSD_T0(tl);
     const long long v = P.act_in[e];
@@ -1249,17 +1194,15 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
       P.old2[v * P.nw + lane] = P.old[v * P.nw + lane];
       P.old[v * P.nw + lane] = P.newm[v * P.nw + lane];
     }
-    if (lane == 0) {
+    {
       const uint8_t flags = (uint8_t)((st & 0xF0) | fl);
-      if (P.iters[v] >= P.sc.niter) {
-        P.status[v] = (uint8_t)(CSD_STATUS_NITER | (flags & 0x70));
-      } else {
-        P.status[v] = (uint8_t)(kActive | flags);
-        P.act_out[atomicAdd(P.n_out, 1)] = (int)v;
-      }
+      const bool last = P.iters[v] >= P.sc.niter;
+      if (lane == 0) P.status[v] = last ? (uint8_t)(CSD_STATUS_NITER | (flags & 0x70)) : (uint8_t)(kActive | flags);
+      if (!last) app.push((int)v, P.act_out, P.n_out, lane);
     }
     CSD_T1(tacc, kPhSet, tw);
   }
+  app.flush(P.act_out, P.n_out, lane);
   if (lane == 0 && P.stats && n_solved) {
     atomicAdd(P.stats, sum_k);
     atomicAdd(P.stats + 1, n_solved);
@@ -1410,6 +1353,121 @@ __global__ void __launch_bounds__(GroupSolveThreads<G>::value, 1)
   if (lane == 0 && P.stats && n_solved) {
     atomicAdd(P.stats, sum_k);
     atomicAdd(P.stats + 1, n_solved);
+  }
+}
+
+// FP64 check of every finished voxel's last solve: the residual
+// r = b - (Mt_M + H_S^T H_S) F of its final set S (csd.h:255-264) in FP64 with
+// the FP64 tables, and rho = max|r| / max|b|.  A voxel with rho above `tol`
+// has its system re-assembled, factorised and solved in FP64 (its status
+// gains CSD_STATUS_FP64).  Warp per voxel: the lanes first take the
+// directions of S (a_d = h_d . F), then the coefficients
+// (sum_d a_d h_d + Mt_M F).  Up to lmax 8 the block keeps HR_trans and Mt_M
+// (FP64) in shared memory.  ctr[0] += voxels checked, ctr[1] += re-solved.
+template <int N>
+struct CheckLayout {
+  static constexpr bool STAGE = N <= 45;  // FP64 tables in shared memory
+  static constexpr int WARP = warp_ws_bytes<N>() + (kMaxHR + Dims<N>::HS) * 8;
+  static constexpr int WARPS = STAGE ? 8 : 4;
+  static size_t table_bytes(int nhr) { return STAGE ? ((size_t)nhr * N + (size_t)N * N) * 8 : 0; }
+};
+
+template <int N>
+__global__ void __launch_bounds__(256) csd_state_check_kernel(const __grid_constant__ StateParams P, long long n,
+                                                               double tol, unsigned long long* ctr) {
+  using CL = CheckLayout<N>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double* H = P.sc.H64;      // [nhr][N]
+  const double* MtM = P.sc.MtM64;  // [N][N]
+  size_t tb = 0;
+  if (CL::STAGE) {
+    double* hs = reinterpret_cast<double*>(smem);
+    const int nh = P.nhr * N, nm = N * N;
+    for (int i = threadIdx.x; i < nh; i += blockDim.x) hs[i] = __ldg(P.sc.H64 + i);
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) hs[nh + i] = __ldg(P.sc.MtM64 + i);
+    H = hs;
+    MtM = hs + nh;
+    tb = ((size_t)(nh + nm) * 8 + 15) & ~(size_t)15;
+    __syncthreads();
+  }
+  unsigned char* mine = smem + tb + warp * CL::WARP;
+  WarpWS<N> w = carve_ws<N>(mine);
+  double* ad = reinterpret_cast<double*>(mine + warp_ws_bytes<N>());  // a_d of the set's directions
+  double* Fd = ad + kMaxHR;                                            // F in FP64
+  double* slot = P.fp64_scratch + (size_t)(blockIdx.x * (blockDim.x >> 5) + warp) * Dims<N>::WSZ;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+  const long long nwt = (long long)gridDim.x * (blockDim.x >> 5);
+  unsigned long long checked = 0, resolved = 0;
+  for (long long v = gw; v < n; v += nwt) {
+    const uint8_t st = P.status[v];
+    const int outcome = st & 0x0F;
+    if (outcome != CSD_STATUS_CONVERGED && outcome != CSD_STATUS_NITER) continue;
+    for (int c = lane; c < N; c += 32) {
+      Fd[c] = (double)P.F[v * Dims<N>::HS + c];
+      w.b[c] = P.b[v * N + c];
+    }
+    uint32_t bits[kMaxWords];
+#pragma unroll
+    for (int p = 0; p < kMaxWords; ++p) bits[p] = (p < P.nw) ? P.old[v * P.nw + p] : 0u;
+    const int k = mask_to_list(bits, P.nw, w.neg, lane);
+    __syncwarp();
+    for (int q = lane; q < k; q += 32) {
+      const double* h = H + (int)w.neg[q] * N;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+      for (int i = 0; i < N; i += 4) {
+        a0 = fma(h[i], Fd[i], a0);
+        if (i + 1 < N) a1 = fma(h[i + 1], Fd[i + 1], a1);
+        if (i + 2 < N) a2 = fma(h[i + 2], Fd[i + 2], a2);
+        if (i + 3 < N) a3 = fma(h[i + 3], Fd[i + 3], a3);
+      }
+      ad[q] = (a0 + a1) + (a2 + a3);
+    }
+    __syncwarp();
+    double rmax = 0.0, bmax = 0.0;
+#pragma unroll
+    for (int c = 0; c < Dims<N>::CQ; ++c) {
+      const int i = lane + 32 * c;
+      if (i < N) {
+        double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
+        int q = 0;
+        for (; q + 3 < k; q += 4) {
+          u0 = fma(ad[q], H[(int)w.neg[q] * N + i], u0);
+          u1 = fma(ad[q + 1], H[(int)w.neg[q + 1] * N + i], u1);
+          u2 = fma(ad[q + 2], H[(int)w.neg[q + 2] * N + i], u2);
+          u3 = fma(ad[q + 3], H[(int)w.neg[q + 3] * N + i], u3);
+        }
+        for (; q < k; ++q) u0 = fma(ad[q], H[(int)w.neg[q] * N + i], u0);
+        double m0 = 0.0, m1 = 0.0;
+        const double* Mi = MtM + i * N;
+#pragma unroll
+        for (int j = 0; j < N; j += 2) {
+          m0 = fma(Mi[j], Fd[j], m0);
+          if (j + 1 < N) m1 = fma(Mi[j + 1], Fd[j + 1], m1);
+        }
+        rmax = fmax(rmax, fabs(w.b[i] - ((m0 + m1) + ((u0 + u1) + (u2 + u3)))));
+        bmax = fmax(bmax, fabs(w.b[i]));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+      bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    }
+    ++checked;
+    if (tol <= 0.0 || rmax > tol * bmax) {  // tol 0: every voxel
+      __syncwarp();
+      const bool ok = solve_fp64<N>(P.sc, k, w, slot, lane);
+      for (int c = lane; c < N; c += 32) P.F[v * Dims<N>::HS + c] = w.F[c];
+      if (lane == 0) P.status[v] = (uint8_t)(st | CSD_STATUS_FP64 | (ok ? 0 : CSD_STATUS_CHOLFAIL));
+      ++resolved;
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && (checked || resolved)) {
+    atomicAdd(ctr, checked);
+    atomicAdd(ctr + 1, resolved);
   }
 }
 
@@ -2026,6 +2084,8 @@ struct csd_state {
   size_t reuse_smem = 0;
   int* act[2] = {nullptr, nullptr};
   int* slist = nullptr;
+  int* rlist = nullptr;       // the solve list's voxels the reuse kernel leaves to the full kernel
+  int* rcount = nullptr;      // device: their count, per pass of a csd_state_run batch
   int* counter = nullptr;
   int cur = 0;
   double* fp64 = nullptr;
@@ -2038,6 +2098,8 @@ struct csd_state {
   size_t proj_smem = 0;
   long long passes = 0, projected = 0, solved = 0;  // work counters since the last set()
   unsigned long long* stats = nullptr;              // device: sum |neg|, solves
+  unsigned long long* chk = nullptr;                // device: voxels checked, re-solved (csd_state_check)
+  long long fp64_slots = 0;                         // warps' FP64 slots in fp64
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int* pcount = nullptr;                            // device: per-pass counts of csd_state_run
   cudaEvent_t bev[3 * kRunBatch + 1] = {};          // kernel boundaries of one csd_state_run batch
@@ -2087,6 +2149,7 @@ int state_shape(csd_state* st) {
                                     (int)st->gsmem[1]));
   }
   CUDA_TRY(cudaMalloc(&st->fp64, (size_t)ls.blocks * maxw * Dims<N>::WSZ * sizeof(double)));
+  st->fp64_slots = (long long)ls.blocks * maxw;
   CUDA_TRY(cudaFuncSetAttribute(csd_solve_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem));
   int dev = 0, smem_max = 0, nsm = 0;
   CUDA_TRY(cudaGetDevice(&dev));
@@ -2225,6 +2288,19 @@ int state_solve_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
   return 0;
 }
 template <int N>
+int state_check_launch(csd_state* st, double tol, cudaStream_t s) {
+  // one FP64 slot per warp of this grid: at most fp64_slots warps
+  using CL = CheckLayout<N>;
+  const int wpb = (int)std::min<long long>(CL::WARPS, st->fp64_slots);
+  const int blocks = (int)std::max<long long>(1, std::min<long long>(st->fp64_slots / wpb, 65535));
+  const int smem = (int)((CL::table_bytes(st->sh->h.nhr) + 15) / 16 * 16) + wpb * CL::WARP;
+  CUDA_TRY(cudaFuncSetAttribute(csd_state_check_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  StateParams P = state_params(st);
+  csd_state_check_kernel<N><<<blocks, wpb * 32, smem, s>>>(P, st->n, tol, st->chk);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+template <int N>
 int state_reuse_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
   const int need = (int)std::min<long long>(st->blocks, (P.n_in + st->reuse_warps - 1) / st->reuse_warps);
   csd_solve_reuse_kernel<N><<<std::max(need, 1), st->reuse_warps * 32, st->reuse_smem, s>>>(P);
@@ -2272,6 +2348,8 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->newm, (size_t)capacity * nw * sizeof(uint32_t)));
   CUDA_TRY(cudaMalloc(&st->warm, (size_t)capacity * nw * sizeof(uint32_t)));
   CUDA_TRY(cudaMalloc(&st->slist, (size_t)capacity * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&st->rlist, (size_t)capacity * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&st->rcount, (kRunBatch + 1) * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->status, (size_t)capacity));
   CUDA_TRY(cudaMalloc(&st->iters, (size_t)capacity * sizeof(uint16_t)));
   CUDA_TRY(cudaMalloc(&st->cyc, (size_t)capacity * sizeof(uint16_t)));
@@ -2279,6 +2357,7 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->act[1], (size_t)capacity * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->counter, 2 * sizeof(int)));
   CUDA_TRY(cudaMalloc(&st->stats, 4 * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMalloc(&st->chk, 2 * sizeof(unsigned long long)));
   CUDA_TRY(cudaMalloc(&st->pcount, (2 * kRunBatch + 2) * sizeof(int)));
   for (auto& e : st->ev) CUDA_TRY(cudaEventCreate(&e));
   for (auto& e : st->bev) CUDA_TRY(cudaEventCreate(&e));
@@ -2298,6 +2377,8 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->newm);
   cudaFree(st->warm);
   cudaFree(st->slist);
+  cudaFree(st->rlist);
+  cudaFree(st->rcount);
   cudaFree(st->status);
   cudaFree(st->iters);
   cudaFree(st->cyc);
@@ -2307,6 +2388,7 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->act[1]);
   cudaFree(st->counter);
   cudaFree(st->stats);
+  cudaFree(st->chk);
   cudaFree(st->fp64);
   cudaFree(st->pcount);
   for (auto& e : st->ev)
@@ -2421,15 +2503,23 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
       Q.act_out = st->act[st->cur ^ 1];
       CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
       CUDA_TRY(cudaEventRecord(st->ev[2], s));
-      // later solves of warm-started voxels from their stored factor first;
-      // the full kernel then takes every other voxel (and any the first gave up)
-      if (Q.Lst) {
-        CSD_DISPATCH(st->sh->h.nsh, rc = state_reuse_launch<NN>(st, Q, s));
+      // later solves of warm-started voxels from their stored factor first
+      // (none before the second pass); the full kernel then takes every other
+      // voxel (and any the first gave up)
+      StateParams Qf = Q;  // the full kernel's input: the solve list, or what the reuse kernel leaves of it
+      if (Q.Lst && st->passes > 0) {
+        CUDA_TRY(cudaMemsetAsync(st->rcount, 0, sizeof(int), s));
+        StateParams Qr = Q;
+        Qr.rest_out = st->rlist;
+        Qr.n_rest = st->rcount;
+        CSD_DISPATCH(st->sh->h.nsh, rc = state_reuse_launch<NN>(st, Qr, s));
         if (rc) return rc;
         st->launches += 1;
+        Qf.act_in = st->rlist;
+        Qf.n_in_dev = st->rcount;
       }
       CUDA_TRY(cudaEventRecord(st->ev[3], s));
-      CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Q, s));
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Qf, s));
       if (rc) return rc;
       CUDA_TRY(cudaEventRecord(st->ev[1], s));
       CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -2468,10 +2558,12 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
     batch *= 2;
     const int U = (int)st->n_active;
     CUDA_TRY(cudaMemsetAsync(st->pcount, 0, (2 * K + 1) * sizeof(int), s));
+    CUDA_TRY(cudaMemsetAsync(st->rcount, 0, K * sizeof(int), s));
     CUDA_TRY(cudaMemsetAsync(st->counter + 1, 0, sizeof(int), s));
     CUDA_TRY(cudaEventRecord(st->bev[0], s));
     int rc = 0;
-    bool reuse = false;
+    int reuse_launches = 0;
+    const long long pass0 = st->passes;  // passes since csd_state_set before this batch
     for (int p = 0; p < K; ++p) {
       StateParams P = state_params(st);
       P.n_in = U;  // grid size; the count itself comes from the device after the first pass
@@ -2488,15 +2580,22 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
       Q.act_in = st->slist;
       Q.act_out = st->act[st->cur ^ 1];
       Q.n_out = st->pcount + 2 * p + 2;
-      // later solves of warm-started voxels from their stored factor first;
-      // the full kernel then takes every other voxel (and any the first gave up)
-      if (Q.Lst) {
-        reuse = true;
-        CSD_DISPATCH(st->sh->h.nsh, rc = state_reuse_launch<NN>(st, Q, s));
+      // later solves of warm-started voxels from their stored factor first
+      // (none before the second pass); the full kernel then takes every other
+      // voxel (and any the first gave up)
+      StateParams Qf = Q;  // the full kernel's input: the solve list, or what the reuse kernel leaves of it
+      if (Q.Lst && pass0 + p > 0) {
+        ++reuse_launches;
+        StateParams Qr = Q;
+        Qr.rest_out = st->rlist;
+        Qr.n_rest = st->rcount + p;
+        CSD_DISPATCH(st->sh->h.nsh, rc = state_reuse_launch<NN>(st, Qr, s));
         if (rc) return rc;
+        Qf.act_in = st->rlist;
+        Qf.n_in_dev = st->rcount + p;
       }
       CUDA_TRY(cudaEventRecord(st->bev[3 * p + 2], s));
-      CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Q, s));
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Qf, s));
       if (rc) return rc;
       CUDA_TRY(cudaEventRecord(st->bev[3 * p + 3], s));
       st->cur ^= 1;
@@ -2508,7 +2607,7 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
     CUDA_TRY(cudaStreamSynchronize(s));
     if (err) return fail(CSD_ERR_TIMEOUT, "projection: a bounded wait on the tensor cores timed out");
     cnt[0] = U;
-    st->launches += (reuse ? 3 : 2) * K;  // every enqueued pass launches its kernels (empty ones return at once)
+    st->launches += 2 * K + reuse_launches;  // every enqueued pass launches its kernels (empty ones return at once)
     for (int p = 0; p < K; ++p) {
       if (cnt[2 * p] == 0) break;
       float a = 0.f, b = 0.f, c = 0.f;
@@ -2541,6 +2640,26 @@ extern "C" int csd_state_stats(const csd_state* st, double* out) {
   out[5] = st->ms_project;
   out[6] = st->ms_solve;
   out[7] = (double)st->launches;
+  return CSD_OK;
+}
+
+extern "C" int csd_state_check(csd_state* st, double tol, int64_t* n_checked, int64_t* n_resolved, void* stream) {
+  if (!st || !(tol >= 0.0)) return fail(CSD_ERR_INVALID, "csd_state_check: invalid argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemsetAsync(st->chk, 0, 2 * sizeof(unsigned long long), s));
+  if (st->n > 0) {
+    int rc = 0;
+    CSD_DISPATCH(st->sh->h.nsh, rc = state_check_launch<NN>(st, tol, s));
+    if (rc) return rc;
+    st->launches += 1;
+  }
+  if (n_checked || n_resolved) {
+    unsigned long long c[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(c, st->chk, sizeof(c), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (n_checked) *n_checked = (int64_t)c[0];
+    if (n_resolved) *n_resolved = (int64_t)c[1];
+  }
   return CSD_OK;
 }
 

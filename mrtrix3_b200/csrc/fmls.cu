@@ -4,11 +4,12 @@
 // (1281) directions in FP64 (SH -> amplitude matrix, L2-resident) into
 // shared memory and sort the direction indices by |amplitude| descending,
 // index ascending (the reference's multimap order), by a bitonic network
-// over the next power of two in shared memory.  Lane 0 then grows the lobes
-// (fmls_core.cuh: the region growing and the pending assignments) with the
-// direction labels and the lobes' state in the warp's shared memory (up to
-// kFmlsLobes lobes; a voxel that makes more is grown again from its global
-// slot).  The Newton refinements of the candidate peaks are independent of
+// over the next power of two in shared memory.  The warp then grows the
+// lobes (grow_warp: the lanes look up a direction's neighbours, lane 0
+// applies the core's steps) with the direction labels and the lobes' state
+// in the warp's shared memory (up to kFmlsLobes lobes; a voxel that makes
+// more is grown again by lane 0 on its global slot), and lane 0 makes the
+// pending assignments.  The Newton refinements of the candidate peaks are independent of
 // one another, so the lanes compute them in parallel, and lane 0 finishes
 // the lobes (thresholds, the nearest-peak test, the fixels) from those
 // results.  The core is the same source the CPU tests build for the host and
@@ -26,6 +27,18 @@
 namespace csdb200 {
 int set_error(int code, const std::string& msg);  // csd_solver.cu
 }
+
+// Optional per-phase cycle counters (build with -DCSD_PHASE_TIMERS): lane 0
+// of each warp adds clock64() deltas of amplitudes / sort / growing / pending
+// assignments / Newton refinements / finishing to g_fmls_cycles.
+#ifdef CSD_PHASE_TIMERS
+__device__ unsigned long long g_fmls_cycles[8];
+#define FMLS_T(var) const long long var = clock64()
+#define FMLS_ACC(idx, a, b) if (lane == 0) atomicAdd(&g_fmls_cycles[idx], (unsigned long long)((b) - (a)))
+#else
+#define FMLS_T(var)
+#define FMLS_ACC(idx, a, b)
+#endif
 
 namespace {
 
@@ -52,6 +65,130 @@ constexpr int kSlotInts = 8, kSlotDoubles = 8;
 __host__ __device__ inline size_t fmls_warp_bytes(int nd, int nsh, int sort_n) {
   const size_t a = ((size_t)(nd + nsh) * sizeof(double) + (size_t)(sort_n + nd) * sizeof(int) + 15) & ~(size_t)15;
   return a + (size_t)5 * kFmlsLobes * sizeof(int) + (size_t)12 * kFmlsLobes * sizeof(double);
+}
+
+// fmls::grow (fmls.cpp:178-246) with the warp: for each direction in order,
+// lane e looks up the lobe of neighbour e (its label's root, if that lobe's
+// sign matches), the lanes drop repeated lobes and rank the rest in
+// ascending order, and lane 0 applies the step -- a new lobe, an addition, the
+// merges into the first adjacent lobe in ascending order, or a pending
+// assignment -- with the arithmetic of the core's lobe constructor, lobe_add
+// and lobe_merge, so every value is computed as in fmls::grow.  The order is
+// fixed once sorted, so the global tables a step reads (the direction's
+// neighbour list, its unit vector and weight) are fetched one and two steps
+// ahead: only the labels and lobes (shared memory) depend on earlier steps.
+// Returns the lobes created, -1 past max_lobes.
+__device__ int grow_warp(const fmls::Tables& t, const fmls::Work& w, int* n_retro, int max_lobes, int lane) {
+  const int nd = t.ndir;
+  for (int d = lane; d < nd; d += 32) w.label[d] = -1;
+  __syncwarp();
+  // step k's inputs (c), step k + 1's neighbour offsets (n), step k + 2's (nn)
+  int dc = w.order[0];
+  int e0 = __ldg(t.adj_off + dc), degc = __ldg(t.adj_off + dc + 1) - e0;
+  int nbc = lane < degc ? __ldg(t.adj + e0 + lane) : 0;
+  double uc0 = __ldg(t.unit + 3 * dc), uc1 = __ldg(t.unit + 3 * dc + 1), uc2 = __ldg(t.unit + 3 * dc + 2);
+  double wc = __ldg(t.weight + dc);
+  int dn = nd > 1 ? w.order[1] : 0;
+  int e0n = __ldg(t.adj_off + dn), degn = __ldg(t.adj_off + dn + 1) - e0n;
+  int nl = 0, nr = 0;
+  for (int k = 0; k < nd; ++k) {
+    // fetch ahead: step k + 1's neighbours, direction and weight; step k + 2's offsets
+    const int nbn = (k + 1 < nd && lane < degn) ? __ldg(t.adj + e0n + lane) : 0;
+    const double un0 = __ldg(t.unit + 3 * dn), un1 = __ldg(t.unit + 3 * dn + 1), un2 = __ldg(t.unit + 3 * dn + 2);
+    const double wn = __ldg(t.weight + dn);
+    const int dnn = k + 2 < nd ? w.order[k + 2] : 0;
+    const int e0nn = __ldg(t.adj_off + dnn), degnn = __ldg(t.adj_off + dnn + 1) - e0nn;
+    // step k
+    const int d = dc;
+    const double v = w.values[d];
+    const int vneg = v <= 0.0 ? 1 : 0;
+    int r = -1;
+    if (lane < degc) {
+      const int lab = w.label[nbc];
+      if (lab >= 0) {
+        r = fmls::root(w, lab);
+        if (w.neg[r] != vneg) r = -1;
+      }
+    }
+    // one lane per adjacent lobe, ranked by lobe index
+    const unsigned same = __match_any_sync(0xffffffffu, r);
+    const bool keep = r >= 0 && lane == __ffs(same) - 1;
+    const unsigned kept = __ballot_sync(0xffffffffu, keep);
+    const int na = __popc(kept);
+    int rank = 0;
+    for (int j = 0; j < degc; ++j) {
+      const int rj = __shfl_sync(0xffffffffu, r, j);
+      if ((kept >> j) & 1u) rank += rj < r ? 1 : 0;
+    }
+    const unsigned first = __ballot_sync(0xffffffffu, keep && rank == 0);
+    const int a0 = na ? __shfl_sync(0xffffffffu, r, __ffs(first) - 1) : -1;
+    bool add = false;
+    if (na == 0) {
+      if (nl >= max_lobes) return -1;
+      if (lane == 0) {
+        // FOD_lobe constructor (fmls.h:60-72)
+        const double av = fabs(v);
+        w.parent[nl] = nl;
+        w.neg[nl] = vneg;
+        w.max_peak[nl] = av;
+        w.peak_head[nl] = w.peak_tail[nl] = nl;
+        w.peak_next[nl] = -1;
+        w.peak_dir[3 * nl] = uc0;
+        w.peak_dir[3 * nl + 1] = uc1;
+        w.peak_dir[3 * nl + 2] = uc2;
+        w.mean[3 * nl] = uc0 * av * wc;
+        w.mean[3 * nl + 1] = uc1 * av * wc;
+        w.mean[3 * nl + 2] = uc2 * av * wc;
+        w.integral[nl] = fabs(v * wc);
+        w.label[d] = nl;
+      }
+      ++nl;
+    } else if (na == 1) {
+      add = true;
+    } else {
+      const unsigned last = __ballot_sync(0xffffffffu, keep && rank == na - 1);
+      const int al = __shfl_sync(0xffffffffu, r, __ffs(last) - 1);
+      if (fabs(v) / w.max_peak[al] > t.merge_ratio) {
+        for (int q = 1; q < na; ++q) {
+          const unsigned sel = __ballot_sync(0xffffffffu, keep && rank == q);
+          const int aq = __shfl_sync(0xffffffffu, r, __ffs(sel) - 1);
+          if (lane == 0) fmls::lobe_merge(w, a0, aq);
+          __syncwarp();
+        }
+        add = true;
+      } else {
+        if (lane == 0) {
+          w.retro_dir[nr] = d;
+          w.retro_lobe[nr] = a0;
+        }
+        ++nr;
+      }
+    }
+    if (add && lane == 0) {
+      // FOD_lobe::add (fmls.h:82-91), as fmls::lobe_add
+      double* m = w.mean + 3 * a0;
+      w.label[d] = a0;
+      const double mult = (m[0] * uc0 + m[1] * uc1 + m[2] * uc2) > 0.0 ? 1.0 : -1.0;
+      const double av = fabs(v);
+      m[0] += uc0 * mult * av * wc;
+      m[1] += uc1 * mult * av * wc;
+      m[2] += uc2 * mult * av * wc;
+      w.integral[a0] += fabs(v * wc);
+    }
+    __syncwarp();
+    dc = dn;
+    degc = degn;
+    nbc = nbn;
+    uc0 = un0;
+    uc1 = un1;
+    uc2 = un2;
+    wc = wn;
+    dn = dnn;
+    e0n = e0nn;
+    degn = degnn;
+  }
+  *n_retro = nr;
+  return nl;
 }
 
 struct FmlsArgs {
@@ -129,6 +266,7 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
       if (lane == 0) a.counts[v] = 0;
       continue;
     }
+    FMLS_T(t0);
     for (int d = lane; d < nd; d += 32) {
       const double* row = a.t.sh2amp + (long long)d * nsh;
       double s = 0.0;
@@ -137,6 +275,8 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
     }
     for (int i = lane; i < a.sort_n; i += 32) keys[i] = i;
     __syncwarp();
+    FMLS_T(t1);
+    FMLS_ACC(0, t0, t1);
     // bitonic sort of keys in the segmenter's order (padding keys >= nd last)
     for (int k = 2; k <= a.sort_n; k <<= 1) {
       for (int j = k >> 1; j > 0; j >>= 1) {
@@ -154,20 +294,27 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
         __syncwarp();
       }
     }
-    // lane 0: the region growing and the pending assignments
+    // the region growing (the warp) and the pending assignments (lane 0)
+    FMLS_T(t2);
+    FMLS_ACC(1, t1, t2);
     int nl = 0;
     bool in_smem = true;
-    if (lane == 0 && values[keys[0]] > 0.0) {
+    if (values[keys[0]] > 0.0) {
       int nr = 0;
-      nl = fmls::grow(a.t, ws, &nr, kFmlsLobes);
-      if (nl < 0) {  // more lobes than the shared arrays hold
+      nl = grow_warp(a.t, ws, &nr, kFmlsLobes, lane);
+      FMLS_T(t3);
+      FMLS_ACC(2, t2, t3);
+      if (nl < 0) {  // more lobes than the shared arrays hold: lane 0 on the global slot
         in_smem = false;
-        nl = fmls::grow(a.t, wg, &nr);
+        if (lane == 0) nl = fmls::grow(a.t, wg, &nr);
+        nl = __shfl_sync(0xffffffffu, nl, 0);
+        nr = __shfl_sync(0xffffffffu, nr, 0);
       }
-      fmls::assign_pending(a.t, in_smem ? ws : wg, nr);
+      if (lane == 0) fmls::assign_pending(a.t, in_smem ? ws : wg, nr);
+      FMLS_T(t4);
+      FMLS_ACC(3, t3, t4);
     }
-    nl = __shfl_sync(0xffffffffu, nl, 0);
-    in_smem = __shfl_sync(0xffffffffu, in_smem ? 1 : 0, 0) != 0;
+    FMLS_T(t5);
     if (nl == 0) {
       if (lane == 0) a.counts[v] = 0;
       __syncwarp();
@@ -186,11 +333,15 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
       }
     }
     __syncwarp();
+    FMLS_T(t6);
+    FMLS_ACC(4, t5, t6);
     if (lane == 0)
       a.counts[v] = fmls::finish_lobes(a.t, w, sh, nl,
                                        reinterpret_cast<fmls::Fixel*>(a.fixels + v * (long long)a.max_fixels * 8),
                                        a.max_fixels, in_smem ? pre_val : nullptr, in_smem ? pre_u : nullptr);
     __syncwarp();
+    FMLS_T(t7);
+    FMLS_ACC(5, t6, t7);
   }
 }
 
@@ -208,7 +359,7 @@ cudaError_t upload(T** dst, const T* src, size_t n) {
 struct csd_fmls {
   int device = 0;
   fmls::Tables t{};  // device pointers
-  double *unit = nullptr, *weight = nullptr, *sh2amp = nullptr, *al = nullptr;
+  double *unit = nullptr, *weight = nullptr, *sh2amp = nullptr, *al = nullptr, *dsqrt = nullptr;
   int32_t *adj_off = nullptr, *adj = nullptr, *grid_off = nullptr, *grid = nullptr;
   char* scratch = nullptr;
   size_t scratch_warps = 0;
@@ -220,6 +371,7 @@ extern "C" void csd_fmls_destroy(csd_fmls* p) {
   cudaFree(p->weight);
   cudaFree(p->sh2amp);
   cudaFree(p->al);
+  cudaFree(p->dsqrt);
   cudaFree(p->adj_off);
   cudaFree(p->adj);
   cudaFree(p->grid_off);
@@ -264,15 +416,39 @@ extern "C" int csd_fmls_create(const csd_fmls_tables* c, csd_fmls** out) {
   if (e == cudaSuccess) e = upload(&p->adj, c->adj, (size_t)c->n_adj);
   if (e == cudaSuccess) e = upload(&p->grid_off, c->grid_off, (size_t)ncell + 1);
   if (e == cudaSuccess) e = upload(&p->grid, c->grid, (size_t)c->n_grid);
+  std::vector<double> dsq((size_t)fmls::dsqrt_index(c->lmax + 1, 0), 0.0);
+  for (int l = 0; l <= c->lmax; ++l)
+    for (int m = 0; m <= l; ++m)
+      for (int q = 0; q < 4; ++q) dsq[fmls::dsqrt_index(l, m) + q] = fmls::dsqrt_value(l, m, q);
+  if (e == cudaSuccess) e = upload(&p->dsqrt, dsq.data(), dsq.size());
   if (e != cudaSuccess) {
     csd_fmls_destroy(p);
     return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_fmls_create: ") + cudaGetErrorString(e));
   }
   p->t = fmls::Tables{nd, c->lmax, c->nsh, p->unit, p->weight, p->adj_off, p->adj, p->sh2amp, c->al_ndir, c->n_al,
                       c->al_inc, p->al, c->num_az, c->num_el, c->az_begin, c->el_begin, c->az_step, c->el_step,
-                      p->grid_off, p->grid, c->integral_threshold, c->peak_value_threshold, c->merge_ratio};
+                      p->grid_off, p->grid, c->integral_threshold, c->peak_value_threshold, c->merge_ratio,
+                      p->dsqrt};
   *out = p;
   return CSD_OK;
+}
+
+// Profiling hook: per-phase cycle totals of fmls_segment_kernel since the
+// last reset (only in a build with -DCSD_PHASE_TIMERS; returns -5 otherwise).
+extern "C" int csd_debug_fmls_cycles(unsigned long long* out, int reset) {
+#ifdef CSD_PHASE_TIMERS
+  if (cudaMemcpyFromSymbol(out, g_fmls_cycles, sizeof(unsigned long long) * 8) != cudaSuccess)
+    return csdb200::set_error(CSD_ERR_CUDA, "csd_debug_fmls_cycles: copy failed");
+  if (reset) {
+    unsigned long long z[8] = {};
+    cudaMemcpyToSymbol(g_fmls_cycles, z, sizeof(z));
+  }
+  return CSD_OK;
+#else
+  (void)out;
+  (void)reset;
+  return csdb200::set_error(CSD_ERR_UNSUPPORTED, "built without CSD_PHASE_TIMERS");
+#endif
 }
 
 extern "C" int csd_fmls_segment(csd_fmls* p, const float* fod, int64_t n, int64_t voxel_stride, int64_t coef_stride,

@@ -55,7 +55,26 @@ struct Tables {
   const int* grid_off;    // [num_az * num_el + 1]
   const int* grid;
   double integral_threshold, peak_value_threshold, merge_ratio;
+  // optional: the square roots derivatives() takes of integer products, per
+  // (l, m) four of them (dsqrt_index); NULL computes them on the spot (the
+  // values are the same: a correctly rounded square root of an exact integer)
+  const double* dsqrt = nullptr;
 };
+
+// Slots of Tables::dsqrt for degree l, order m (0 <= m <= l <= lmax):
+// [0] sqrt((l+m)(l-m+1)), [1] sqrt((l-m)(l+m+1)),
+// [2] sqrt((l+m)(l-m+1)(l+m-1)(l-m+2)), [3] sqrt((l-m)(l+m+1)(l-m-1)(l+m+2)).
+FMLS_HD inline int dsqrt_index(int l, int m) { return 4 * (l * (l + 1) / 2 + m); }
+FMLS_HD inline double dsqrt_value(int l, int m, int which) {
+  double x;
+  switch (which) {
+    case 0: x = (double)((l + m) * (l - m + 1)); break;
+    case 1: x = (double)((l - m) * (l + m + 1)); break;
+    case 2: x = (double)((l + m) * (l - m + 1) * (l + m - 1) * (l - m + 2)); break;
+    default: x = (double)((l - m) * (l + m + 1) * (l - m - 1) * (l + m + 2)); break;
+  }
+  return x > 0.0 ? sqrt(x) : 0.0;
+}
 
 struct Work {  // one voxel in flight; every array has ndir entries
   double* values;
@@ -207,30 +226,40 @@ FMLS_HD inline void derivatives(const Tables& t, const double* sh, double el, do
   };
   auto IDX = [](int l, int m) { return l * (l + 1) / 2 + m; };
   const int lmax = t.lmax;
+  auto SQ = [&](int l, int m, int which) {
+    return t.dsqrt ? t.dsqrt[dsqrt_index(l, m) + which] : dsqrt_value(l, m, which);
+  };
   double amp = sh[0] * AL(0, 0);
   double d_el = 0.0, d_az = 0.0, d2_el = 0.0, d2_elaz = 0.0, d2_az = 0.0;
   for (int l = 2; l <= lmax; l += 2) {
     const double v = sh[IDX(l, 0)];
     amp += v * AL(l, 0);
-    d_el += v * sqrt((double)(l * (l + 1))) * AL(l, 1);
-    d2_el += v * (sqrt((double)(l * (l + 1) * (l - 1) * (l + 2))) * AL(l, 2) - l * (l + 1) * AL(l, 0)) / 2.0;
+    d_el += v * SQ(l, 0, 1) * AL(l, 1);                                        // sqrt(l (l+1))
+    d2_el += v * (SQ(l, 0, 3) * AL(l, 2) - l * (l + 1) * AL(l, 0)) / 2.0;    // sqrt(l (l+1) (l-1) (l+2))
   }
   const double sqrt2 = 1.4142135623730951;
   for (int m = 1; m <= lmax; ++m) {
-    const double caz = sqrt2 * cos(m * az), saz = sqrt2 * sin(m * az);
+    double sm, cm;
+#ifdef __CUDA_ARCH__
+    sincos(m * az, &sm, &cm);
+#else
+    sm = sin(m * az);
+    cm = cos(m * az);
+#endif
+    const double caz = sqrt2 * cm, saz = sqrt2 * sm;
     for (int l = (m & 1) ? m + 1 : m; l <= lmax; l += 2) {
       const double vp = sh[IDX(l, m)], vm = sh[IDX(l, -m)];
       amp += (vp * caz + vm * saz) * AL(l, m);
-      double tmp = sqrt((double)((l + m) * (l - m + 1))) * AL(l, m - 1);
-      if (l > m) tmp -= sqrt((double)((l - m) * (l + m + 1))) * AL(l, m + 1);
+      double tmp = SQ(l, m, 0) * AL(l, m - 1);
+      if (l > m) tmp -= SQ(l, m, 1) * AL(l, m + 1);
       tmp /= -2.0;
       d_el += (vp * caz + vm * saz) * tmp;
       double tmp2 = -((l + m) * (l - m + 1) + (l - m) * (l + m + 1)) * AL(l, m);
       if (m == 1)
-        tmp2 -= sqrt((double)((l + m) * (l - m + 1) * (l + m - 1) * (l - m + 2))) * AL(l, 1);
+        tmp2 -= SQ(l, m, 2) * AL(l, 1);
       else
-        tmp2 += sqrt((double)((l + m) * (l - m + 1) * (l + m - 1) * (l - m + 2))) * AL(l, m - 2);
-      if (l > m + 1) tmp2 += sqrt((double)((l - m) * (l + m + 1) * (l - m - 1) * (l + m + 2))) * AL(l, m + 2);
+        tmp2 += SQ(l, m, 2) * AL(l, m - 2);
+      if (l > m + 1) tmp2 += SQ(l, m, 3) * AL(l, m + 2);
       tmp2 /= 4.0;
       d2_el += (vp * caz + vm * saz) * tmp2;
       if (atpole) {

@@ -162,6 +162,21 @@ int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream);
  * identical to calling csd_state_iterate until it reports 0.  *n_active (may
  * be NULL) receives how many voxels are still iterating (synchronises). */
 int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, void* stream);
+/* csd_state_set + (csd_state_warm when warm_negmask is not NULL) +
+ * csd_state_run as exactly `passes` passes with no host synchronisation,
+ * so that the whole method can be captured in a CUDA graph (several states
+ * on several streams: many volumes, each with its own scheme, in one graph
+ * launch).  Every kernel reads its voxel count from the device; a pass with
+ * nothing left returns at once, so passes = niter + 1 always reaches the end
+ * (at most niter + 2).  The results equal the synchronous calls'.  With warm
+ * sets, call csd_state_warm on the state once before a capture (it
+ * allocates the factor storage).  csd_state_stats is not updated. */
+int csd_state_run_async(csd_state* st, const float* dwi, int64_t n_voxels, int64_t voxel_stride,
+                        int64_t volume_stride, const uint8_t* mask, const uint32_t* warm_negmask, int passes,
+                        void* stream);
+/* After csd_state_run_async (synchronises): voxels still iterating after its
+ * last pass (0 once it ran enough passes) and whether a bounded wait timed out. */
+int csd_state_async_result(csd_state* st, int64_t* n_active, int* timed_out, void* stream);
 /* Work and device time since the last csd_state_set: out[8] = passes, voxels
  * projected, voxels solved, sum of |negative set| over the solves that
  * assembled their system (not those of csd_state_reuse_stats), then the

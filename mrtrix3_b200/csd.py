@@ -115,6 +115,8 @@ def lib():
         L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_state_reuse_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_state_check.argtypes = [vp, ctypes.c_double, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
+        L.csd_state_run_async.argtypes = [vp, vp, i64, i64, i64, vp, vp, ctypes.c_int, vp]
+        L.csd_state_async_result.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_int), vp]
         L.csd_dwi2fod_host_phased.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
         L.csd_fmls_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.csd_fmls_create_default.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -541,6 +543,25 @@ class State:
             self.warm(warm, stream=stream)
         self.iterate_all(stream=stream)
         return int(self.stats()["passes"])
+
+    def run_async(self, dwi, mask=None, warm=None, passes=None, stream=None):
+        """set (+ warm sets) and `passes` passes (default niter + 1, enough for
+        every voxel) with no host synchronisation: capturable in a CUDA graph
+        (csd_state_run_async).  With warm sets, call warm() once beforehand."""
+        self.n = dwi.shape[0]
+        if passes is None:
+            passes = self.shared.niter + 1
+        check(lib().csd_state_run_async(self._h, ctypes.c_void_p(dwi.data_ptr()), self.n, dwi.stride(0),
+                                        dwi.stride(1), ctypes.c_void_p(_ptr(mask)) if mask is not None else None,
+                                        ctypes.c_void_p(warm.data_ptr()) if warm is not None else None,
+                                        int(passes), ctypes.c_void_p(_stream_ptr(stream))))
+
+    def async_result(self, stream=None):
+        """(voxels still active, timed out) after run_async (synchronises)."""
+        n, e = ctypes.c_int64(), ctypes.c_int()
+        check(lib().csd_state_async_result(self._h, ctypes.byref(n), ctypes.byref(e),
+                                           ctypes.c_void_p(_stream_ptr(stream))))
+        return n.value, bool(e.value)
 
     def check(self, tol: float = 1e-6, stream=None, counts: bool = True):
         """FP64 residual check of every finished voxel's last solve; voxels with

@@ -63,7 +63,11 @@ constexpr int kMaxVolumesPerLaunch = 48;
 #define CSD_CHOL_KK_PRAGMA _Pragma("unroll 1")
 #endif
 #ifndef CSD_BACK_CB_PRAGMA
+#ifdef CSD_BACK_ROLLED
+#define CSD_BACK_CB_PRAGMA _Pragma("unroll 1")
+#else
 #define CSD_BACK_CB_PRAGMA _Pragma("unroll")
+#endif
 #endif
 __host__ __device__ constexpr int packoff(int i) {
   return 4 * (i + 2 * (i >> 2) * ((i >> 2) - 1) + (i & 3) * (i >> 2));

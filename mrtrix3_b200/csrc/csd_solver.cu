@@ -637,21 +637,25 @@ __global__ void __launch_bounds__(ReuseLayout<N>::THREADS, 1)
       __syncwarp();
       continue;
     }
-    // the changed directions in order: added ones, then dropped ones
+    // the changed directions in order: added ones, then dropped ones.  Lane
+    // p < nw owns word p: an exclusive scan of the words' counts gives its
+    // place, then it writes its words' set bits.
     int na = 0;
     {
-      int base = 0;
-      for (int p = 0; p < P.nw; ++p) {
-        const uint32_t w = __shfl_sync(0xffffffffu, add, p);
-        if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
-        base += __popc(w);
+      const int ca = __popc(add), cr = __popc(rem);
+      int xa = ca, xr = cr;  // inclusive scans over the lanes
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+        const int ya = __shfl_up_sync(0xffffffffu, xa, o), yr = __shfl_up_sync(0xffffffffu, xr, o);
+        if (lane >= o) {
+          xa += ya;
+          xr += yr;
+        }
       }
-      na = base;
-      for (int p = 0; p < P.nw; ++p) {
-        const uint32_t w = __shfl_sync(0xffffffffu, rem, p);
-        if ((w >> lane) & 1u) dl[base + __popc(w & ((1u << lane) - 1u))] = 32 * p + lane;
-        base += __popc(w);
-      }
+      na = __shfl_sync(0xffffffffu, xa, 15);  // words live in lanes 0..15 (kMaxWords)
+      int pa = xa - ca, pr = na + xr - cr;
+      for (uint32_t w = add; w; w &= w - 1u) dl[pa++] = 32 * lane + __ffs(w) - 1;
+      for (uint32_t w = rem; w; w &= w - 1u) dl[pr++] = 32 * lane + __ffs(w) - 1;
     }
     __syncwarp();
     const int d = lane < r ? dl[lane] : 0;
@@ -2102,6 +2106,10 @@ struct csd_state {
   long long fp64_slots = 0;                         // warps' FP64 slots in fp64
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int* pcount = nullptr;                            // device: per-pass counts of csd_state_run
+  int* acount = nullptr;                            // device: per-pass counts of csd_state_run_async
+  int* arcount = nullptr;                           //   and its rest-list counts
+  int async_passes = 0;                             // passes acount has room for
+  int async_cur = 0;                                // list the last async run ended on
   cudaEvent_t bev[3 * kRunBatch + 1] = {};          // kernel boundaries of one csd_state_run batch
   double ms_set = 0, ms_project = 0, ms_solve = 0;  // device time of the kernels since the last set()
   double ms_reuse = 0;                              // of which in csd_solve_reuse_kernel
@@ -2359,6 +2367,9 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->stats, 4 * sizeof(unsigned long long)));
   CUDA_TRY(cudaMalloc(&st->chk, 2 * sizeof(unsigned long long)));
   CUDA_TRY(cudaMalloc(&st->pcount, (2 * kRunBatch + 2) * sizeof(int)));
+  st->async_passes = s->h.niter + 2;
+  CUDA_TRY(cudaMalloc(&st->acount, (2 * st->async_passes + 2) * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&st->arcount, (st->async_passes + 1) * sizeof(int)));
   for (auto& e : st->ev) CUDA_TRY(cudaEventCreate(&e));
   for (auto& e : st->bev) CUDA_TRY(cudaEventCreate(&e));
   int rc = 0;
@@ -2391,6 +2402,8 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->chk);
   cudaFree(st->fp64);
   cudaFree(st->pcount);
+  cudaFree(st->acount);
+  cudaFree(st->arcount);
   for (auto& e : st->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : st->bev)
@@ -2625,6 +2638,106 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
     st->n_active = cnt[2 * K];
   }
   if (n_active) *n_active = st->n_active;
+  return CSD_OK;
+}
+
+// The phased method with no host synchronisation, so that it can be captured
+// in a CUDA graph: set() (+ the warm sets), then exactly `passes` passes,
+// each kernel reading its voxel count from the device (the grids are sized
+// for every voxel; a pass with nothing left returns at once).  A voxel makes
+// at most niter + 1 passes, so passes = niter + 1 always reaches the end; the
+// results are those of csd_state_set + csd_state_warm + csd_state_run.  With
+// warm sets and the factor reuse on, the state's factor storage must exist
+// before a capture (csd_state_warm allocates it on first use).  The per-step
+// counters of csd_state_stats are not updated; csd_state_async_result
+// synchronises and reports the voxels still active and any time-out.
+extern "C" int csd_state_run_async(csd_state* st, const float* dwi, int64_t n_voxels, int64_t voxel_stride,
+                                   int64_t volume_stride, const uint8_t* mask, const uint32_t* warm_negmask,
+                                   int passes, void* stream) {
+  if (!st || n_voxels < 0 || n_voxels > st->cap || (n_voxels > 0 && !dwi) || passes < 1 ||
+      passes > st->async_passes)
+    return fail(CSD_ERR_INVALID, "csd_state_run_async: invalid argument (passes must be 1..niter+2)");
+  if (warm_negmask && g_reuse != 2 && st->reuse_warps > 0 && !st->Lst)
+    return fail(CSD_ERR_INVALID, "csd_state_run_async: call csd_state_warm once first (it allocates the factor storage)");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  st->n = n_voxels;
+  st->use_warm = warm_negmask ? 1 : 0;
+  st->cur = 0;
+  st->n_active = 0;
+  st->passes = st->projected = st->solved = 0;
+  st->ms_set = st->ms_project = st->ms_solve = st->ms_reuse = 0;
+  CUDA_TRY(cudaMemsetAsync(st->acount, 0, (2 * passes + 2) * sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(st->arcount, 0, (passes + 1) * sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(st->counter, 0, 2 * sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(st->stats, 0, 4 * sizeof(unsigned long long), s));
+  if (n_voxels == 0) return CSD_OK;
+  const int nw = (st->sh->h.nhr + 31) / 32;
+  int rc = 0;
+  {
+    StateParams P = state_params(st);
+    P.n_in = (int)n_voxels;
+    P.dwi = dwi;
+    P.vox_stride = voxel_stride;
+    P.vol_stride = volume_stride;
+    P.mask = mask;
+    P.act_out = st->act[0];
+    P.n_out = st->acount;
+    CSD_DISPATCH(st->sh->h.nsh, rc = state_set_launch<NN>(st, P, s));
+    if (rc) return rc;
+  }
+  if (warm_negmask) {
+    CUDA_TRY(cudaMemcpyAsync(st->warm, warm_negmask, (size_t)n_voxels * nw * sizeof(uint32_t),
+                             cudaMemcpyDeviceToDevice, s));
+    if (st->fac) CUDA_TRY(cudaMemsetAsync(st->fac, 0, (size_t)n_voxels, s));
+  }
+  int cur = 0;
+  for (int p = 0; p < passes; ++p) {
+    StateParams P = state_params(st);
+    P.n_in = (int)n_voxels;  // grid bound; the counts come from the device
+    P.n_in_dev = st->acount + 2 * p;
+    P.act_in = st->act[cur];
+    P.act_out = st->slist;
+    P.n_out = st->acount + 2 * p + 1;
+    CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+    if (rc) return rc;
+    StateParams Q = state_params(st);
+    Q.n_in = (int)n_voxels;
+    Q.n_in_dev = st->acount + 2 * p + 1;
+    Q.act_in = st->slist;
+    Q.act_out = st->act[cur ^ 1];
+    Q.n_out = st->acount + 2 * p + 2;
+    StateParams Qf = Q;
+    if (Q.Lst && p > 0) {
+      StateParams Qr = Q;
+      Qr.rest_out = st->rlist;
+      Qr.n_rest = st->arcount + p;
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_reuse_launch<NN>(st, Qr, s));
+      if (rc) return rc;
+      Qf.act_in = st->rlist;
+      Qf.n_in_dev = st->arcount + p;
+    }
+    CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Qf, s));
+    if (rc) return rc;
+    cur ^= 1;
+  }
+  st->cur = cur;
+  st->async_cur = passes;
+  return CSD_OK;
+}
+
+// After csd_state_run_async (synchronises the stream): *n_active = voxels
+// still iterating after its last pass (0 when it ran enough passes);
+// *timed_out = 1 if a bounded wait on the tensor cores gave up.
+extern "C" int csd_state_async_result(csd_state* st, int64_t* n_active, int* timed_out, void* stream) {
+  if (!st) return fail(CSD_ERR_INVALID, "csd_state_async_result: NULL state");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int cnt = 0, err = 0;
+  if (st->async_cur > 0)
+    CUDA_TRY(cudaMemcpyAsync(&cnt, st->acount + 2 * st->async_cur, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(&err, st->counter + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (n_active) *n_active = cnt;
+  if (timed_out) *timed_out = err;
   return CSD_OK;
 }
 

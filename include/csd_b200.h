@@ -69,6 +69,11 @@ typedef struct csd_params {
                                solution -- 0 never, 1 after every solve, 2 once at the
                                fixed point (then re-checked), 3 (default) only for voxels
                                whose negative set cycles in FP32, after every solve */
+  const double* shells;     /* -shells b-values (dwi/shells.cpp:100-239 with
+                               select_shells(true, false, true), csd.h:64): exactly
+                               one non-b=0 shell must match, and no b=0 shell;
+                               NULL / 0 = the largest b-value shell */
+  int n_shells;
 } csd_params;
 
 typedef struct csd_shared csd_shared;  /* immutable after creation, like CSD::Shared after init() */

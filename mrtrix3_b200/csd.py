@@ -50,7 +50,8 @@ class csd_params(ctypes.Structure):
                 ("norm_lambda", ctypes.c_double), ("threshold", ctypes.c_double),
                 ("filter", ctypes.POINTER(ctypes.c_double)), ("n_filter", ctypes.c_int),
                 ("bzero_threshold", ctypes.c_double), ("bvalue_epsilon", ctypes.c_double),
-                ("fp64_condition", ctypes.c_double), ("refine", ctypes.c_int)]
+                ("fp64_condition", ctypes.c_double), ("refine", ctypes.c_int),
+                ("shells", ctypes.POINTER(ctypes.c_double)), ("n_shells", ctypes.c_int)]
 
 
 class csd_volume(ctypes.Structure):
@@ -173,11 +174,15 @@ class Shared:
         self.bvalue_epsilon = 80.0
         self.fp64_condition = 1e6
         self.refine = 3
+        self.shells = None
         self._h = None
 
     def parse_cmdline_options(self, lmax=None, filter=None, directions=None, neg_lambda=None,
-                              norm_lambda=None, threshold=None, niter=None):
-        """The options csd.h:71-99 reads; ``directions`` is [n][2] az/el."""
+                              norm_lambda=None, threshold=None, niter=None, shells=None):
+        """The options csd.h:71-99 reads; ``directions`` is [n][2] az/el;
+        ``shells`` the -shells b-values (one non-b=0 shell, csd.h:64)."""
+        if shells is not None:
+            self.shells = np.ascontiguousarray(np.ravel(shells), np.float64)
         if lmax is not None:
             if np.ndim(lmax) and len(lmax) != 1:
                 raise CSDError("CSD algorithm expects a single lmax to be specified")
@@ -219,6 +224,9 @@ class Shared:
         p.bvalue_epsilon = self.bvalue_epsilon
         p.fp64_condition = self.fp64_condition
         p.refine = self.refine
+        if self.shells is not None and self.shells.size:
+            p.shells = _dp(self.shells)
+            p.n_shells = self.shells.size
         h = ctypes.c_void_p()
         hr = self.HR_dirs
         check(lib().csd_shared_create(ctypes.byref(p), _dp(self.grad), self.grad.shape[0], _dp(self.response),

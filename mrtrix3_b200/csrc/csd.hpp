@@ -35,6 +35,8 @@ struct CSDOptions {
   double norm_lambda = 1.0;            // -norm_lambda
   double threshold = 0.0;              // -threshold
   size_t niter = 50;                   // -niter
+  std::vector<double> shells;          // -shells (one non-b=0 shell; the constructor's
+                                       // select_shells at csd.h:64 -- applied by init())
   bool has_neg_lambda = false, has_norm_lambda = false, has_threshold = false, has_niter = false;
 };
 
@@ -71,6 +73,7 @@ class CSD {
       if (opt.has_norm_lambda) norm_lambda = opt.norm_lambda;
       if (opt.has_threshold) threshold = opt.threshold;
       if (opt.has_niter) niter = opt.niter;
+      if (!opt.shells.empty()) shells = opt.shells;
     }
 
     // csd.h:102-114
@@ -104,6 +107,8 @@ class CSD {
       p.threshold = threshold;
       p.filter = init_filter.empty() ? nullptr : init_filter.data();
       p.n_filter = int(init_filter.size());
+      p.shells = shells.empty() ? nullptr : shells.data();
+      p.n_shells = int(shells.size());
       csd_shared* h = nullptr;
       check(csd_shared_create(&p, grad.data(), int(grad.size() / 4), response.data(), int(response.size()),
                               HR_dirs.empty() ? nullptr : HR_dirs.data(), int(HR_dirs.size() / 2), &h));
@@ -124,7 +129,7 @@ class CSD {
     csd_shared* handle() const { return handle_; }
 
     // the public members of csd.h:204-211 that callers read
-    std::vector<double> grad, response, init_filter, HR_dirs;
+    std::vector<double> grad, response, init_filter, HR_dirs, shells;
     double neg_lambda = 1.0, norm_lambda = 1.0, threshold = 0.0;
     std::vector<size_t> dwis;
     uint32_t lmax_response = 0, lmax_data = 0, lmax_cmdline = 0, lmax = 0;

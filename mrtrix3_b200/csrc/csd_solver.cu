@@ -418,9 +418,50 @@ __global__ void __launch_bounds__(256) csd_state_set_tile_kernel(const __grid_co
   const int vg = tid >> 4, cg = tid & 15;
   const int nd4 = ndw & ~3;
   const long long ntiles = (P.n_in + kSetTile - 1) / kSetTile;
+  // the selected volumes' offsets of this lane's sample slots (up to 3 a lane)
+  constexpr int kSetChunks = 3;
+  long long off[kSetChunks];
+#pragma unroll
+  for (int c = 0; c < kSetChunks; ++c) {
+    const int t = lane + 32 * c;
+    off[c] = t < ndw ? (long long)__ldg(P.sc.dwis + t) * P.vol_stride : 0;
+  }
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long v0 = tile * kSetTile;
     __syncthreads();
+    if (ndw <= 32 * kSetChunks) {
+      // 1. samples: warp w stages voxels w, w + 8, ..., w + 56, every load
+      // issued before any is used (lane j < 8 reads voxel j's mask byte)
+      bool in = false;
+      if (lane < kSetTile / 8) {
+        const long long v = v0 + warp + 8 * lane;
+        in = v < P.n_in && !(P.mask && !P.mask[v]);
+      }
+      const unsigned inm = __ballot_sync(0xffffffffu, in);
+      float x[kSetTile / 8][kSetChunks];
+#pragma unroll
+      for (int j = 0; j < kSetTile / 8; ++j) {
+        const float* d = P.dwi + (v0 + warp + 8 * j) * P.vox_stride;
+#pragma unroll
+        for (int c = 0; c < kSetChunks; ++c)
+          x[j][c] = (((inm >> j) & 1u) && lane + 32 * c < ndw) ? __ldg(d + off[c]) : 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < kSetTile / 8; ++j) {
+        const int r = warp + 8 * j;
+        bool bad = false;
+#pragma unroll
+        for (int c = 0; c < kSetChunks; ++c) {
+          const int t = lane + 32 * c;
+          if (t < ndw) {
+            bad = bad || !isfinite(x[j][c]);
+            S[r * lds + t] = x[j][c] < 0.f ? 0.f : x[j][c];
+          }
+        }
+        const bool anybad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) flag[r] = ((inm >> j) & 1u) ? (anybad ? 3 : 0) : 1;
+      }
+    } else {
     // 1. samples: warp w stages voxels w, w + 8, ...
     for (int r = warp; r < kSetTile; r += 8) {
       const long long v = v0 + r;
@@ -436,6 +477,7 @@ __global__ void __launch_bounds__(256) csd_state_set_tile_kernel(const __grid_co
         f = __any_sync(0xffffffffu, bad) ? 3 : 0;
       }
       if (lane == 0) flag[r] = f;
+    }
     }
     __syncthreads();  // the flags are complete before anyone reads them (the vote's
                       // predicate is evaluated before its own barrier)
@@ -493,19 +535,20 @@ __global__ void __launch_bounds__(256) csd_state_set_tile_kernel(const __grid_co
         }
       }
     }
+    // (a voxel that is not solved -- masked or non-finite -- keeps no F, b or
+    // sets: csd_state_fod writes its zeros from the status)
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
       const int r = 4 * vg + a;
       const long long v = v0 + r;
-      if (v >= P.n_in) continue;
-      const bool ok = flag[r] == 0;
+      if (v >= P.n_in || flag[r] != 0) continue;
       float* F = P.F + v * Dims<N>::HS;
 #pragma unroll
       for (int j = 0; j < JC; ++j) {
         const int c = cg + 16 * j;
         if (c < N) {
-          F[c] = ok ? f0[a][j] + f1[a][j] : 0.f;
-          P.b[v * N + c] = ok ? (double)(b0[a][j] + b1[a][j]) : 0.0;
+          F[c] = f0[a][j] + f1[a][j];
+          P.b[v * N + c] = (double)(b0[a][j] + b1[a][j]);
         }
       }
       for (int c = N + cg; c < Dims<N>::HS; c += 16) F[c] = 0.f;
@@ -513,7 +556,7 @@ __global__ void __launch_bounds__(256) csd_state_set_tile_kernel(const __grid_co
     // 3. counters, sets and the active list
     for (int i = tid; i < kSetTile * P.nw; i += blockDim.x) {
       const long long v = v0 + i / P.nw;
-      if (v < P.n_in) {
+      if (v < P.n_in && flag[i / P.nw] == 0) {
         P.old[v0 * P.nw + i] = 0u;
         P.old2[v0 * P.nw + i] = 0u;
       }
@@ -922,6 +965,36 @@ __global__ void __launch_bounds__(256) csd_project_kernel(const __grid_constant_
         }
       }
     }
+  }
+}
+
+// First pass of a warm-started run: every active voxel's first set is the
+// supplied one (csd.h:246-250 is skipped for it, as the projection kernels
+// do at it == 0), so no amplitudes are needed: copy the set (its last word
+// masked to nhr directions), count the call, and list every voxel for its
+// first solve -- the state the projection kernels leave at it == 0.
+__global__ void __launch_bounds__(256) csd_warm_first_pass_kernel(const __grid_constant__ StateParams P) {
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
+  const int lane = threadIdx.x & 31;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e0 = (long long)blockIdx.x * blockDim.x; e0 < n_in; e0 += stride) {
+    const long long e = e0 + threadIdx.x;
+    const bool act = e < n_in;
+    long long v = 0;
+    if (act) {
+      v = P.act_in[e];
+      for (int w = 0; w < P.nw; ++w) {
+        uint32_t b = P.warm[v * P.nw + w];
+        if (w == P.nw - 1 && (P.nhr & 31)) b &= (1u << (P.nhr & 31)) - 1u;
+        P.newm[v * P.nw + w] = b;
+      }
+      P.iters[v] = 1;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, act);
+    int base = 0;
+    if (lane == 0 && bal) base = atomicAdd(P.n_out, __popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (act) P.act_out[base + __popc(bal & ((1u << lane) - 1u))] = (int)v;
   }
 }
 
@@ -1483,7 +1556,9 @@ __global__ void csd_state_fod_kernel(const float* F, const uint8_t* status, cons
   if (i >= n * N) return;
   const long long v = i / N;
   const int c = (int)(i - v * N);
-  fod[v * fod_stride + c] = F[v * Dims<N>::HS + c];
+  const uint8_t s0 = status[v] & 0x0F;
+  const bool solved = s0 != CSD_STATUS_MASKED && s0 != CSD_STATUS_NONFINITE;  // else no F is kept
+  fod[v * fod_stride + c] = solved ? F[v * Dims<N>::HS + c] : 0.f;
   if (c == 0) {
     uint8_t s = status[v];
     if ((s & 0x0F) == 0x0F) s = (uint8_t)(CSD_STATUS_NITER | (s & 0x70));  // still iterating
@@ -1491,7 +1566,7 @@ __global__ void csd_state_fod_kernel(const float* F, const uint8_t* status, cons
     if (st_out) st_out[v] = s;
     if (it_out) it_out[v] = (uint8_t)(iters[v] > 255 ? 255 : iters[v]);
     if (neg_out)
-      for (int p = 0; p < nw; ++p) neg_out[v * nw + p] = old[v * nw + p];
+      for (int p = 0; p < nw; ++p) neg_out[v * nw + p] = solved ? old[v * nw + p] : 0u;
   }
 }
 
@@ -1544,6 +1619,8 @@ extern "C" void csd_params_init(csd_params* p) {
   p->bvalue_epsilon = 80.0;
   p->fp64_condition = 1e6;
   p->refine = 3;
+  p->shells = nullptr;
+  p->n_shells = 0;
 }
 
 template <typename T>
@@ -1571,6 +1648,7 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
   if (p->filter && p->n_filter > 0) sp.filter.assign(p->filter, p->filter + p->n_filter);
   sp.bzero_threshold = p->bzero_threshold;
   sp.bvalue_epsilon = p->bvalue_epsilon;
+  if (p->shells && p->n_shells > 0) sp.shells.assign(p->shells, p->shells + p->n_shells);
   std::vector<double> hr;
   if (hr_dirs) {
     if (n_hr <= 0) return fail(CSD_ERR_INVALID, "n_hr must be positive");
@@ -2257,6 +2335,16 @@ int state_project_tc_launch(csd_state* st, const StateParams& P, cudaStream_t s)
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
+// The first pass's "projection" of a warm-started run: csd_warm_first_pass_kernel.
+int state_warm_first_launch(const StateParams& P, cudaStream_t s) {
+  int dev = 0, nsm = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const long long blocks = std::max<long long>(1, std::min<long long>((P.n_in + 255) / 256, (long long)nsm * 8));
+  csd_warm_first_pass_kernel<<<(unsigned)blocks, 256, 0, s>>>(P);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
 template <int N>
 int state_project_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
   if ((g_proj_kind ? g_proj_kind : kProjDefault) == 2 && P.Htc16) return state_project_tc_launch<N>(st, P, s);
@@ -2494,7 +2582,11 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
     P.act_out = st->slist;
     CUDA_TRY(cudaMemsetAsync(st->counter, 0, 2 * sizeof(int), s));
     CUDA_TRY(cudaEventRecord(st->ev[0], s));
-    CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+    if (st->use_warm && st->passes == 0) {
+      rc = state_warm_first_launch(P, s);  // the first sets are given: nothing to project
+    } else {
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+    }
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(st->ev[1], s));
     int cnt[2] = {0, 0};
@@ -2584,7 +2676,11 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
       P.act_in = st->act[st->cur];
       P.act_out = st->slist;
       P.n_out = st->pcount + 2 * p + 1;
-      CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+      if (st->use_warm && pass0 + p == 0) {
+        rc = state_warm_first_launch(P, s);  // the first sets are given: nothing to project
+      } else {
+        CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+      }
       if (rc) return rc;
       CUDA_TRY(cudaEventRecord(st->bev[3 * p + 1], s));
       StateParams Q = state_params(st);
@@ -2698,7 +2794,11 @@ extern "C" int csd_state_run_async(csd_state* st, const float* dwi, int64_t n_vo
     P.act_in = st->act[cur];
     P.act_out = st->slist;
     P.n_out = st->acount + 2 * p + 1;
-    CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+    if (warm_negmask && p == 0) {
+      rc = state_warm_first_launch(P, s);  // the first sets are given: nothing to project
+    } else {
+      CSD_DISPATCH(st->sh->h.nsh, rc = state_project_launch<NN>(st, P, s));
+    }
     if (rc) return rc;
     StateParams Q = state_params(st);
     Q.n_in = (int)n_voxels;

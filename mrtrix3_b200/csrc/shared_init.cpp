@@ -6,6 +6,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
+#include <sstream>
+#include <stdexcept>
+#include <string>
 
 namespace csdb200 {
 namespace {
@@ -53,13 +57,18 @@ void cholesky_solve(const std::vector<double>& L, int n, double* x) {
   }
 }
 
-struct ShellSel {
-  std::vector<int> volumes;
+// A b-value shell as Shell::Shell (dwi/shells.cpp:52-70) describes it: mean,
+// sample standard deviation, min and -- as computed there -- "max", the
+// larger of the running minimum and the last volume's b.
+struct Shell {
+  double mean, stdev, lo, hi;
+  std::vector<int> vols;
+  bool is_bzero(double b0thr) const { return mean <= b0thr; }
 };
 
-// dwi/shells.cpp:347-411 (clustering) + :300-345 (shell construction) +
-// :100-260 select_shells(true, false, true) without -shells + largest().
-std::vector<int> largest_shell(const std::vector<double>& b, double b0thr, double eps) {
+// dwi/shells.cpp:347-411 (clustering) + :300-345 (shell construction):
+// the shells by increasing mean b-value.
+std::vector<Shell> cluster_shells(const std::vector<double>& b, double b0thr, double eps) {
   const int nvol = static_cast<int>(b.size());
   std::vector<int> clusters(nvol, 0);
   std::vector<char> visited(nvol, 0);
@@ -101,27 +110,125 @@ std::vector<int> largest_shell(const std::vector<double>& b, double b0thr, doubl
     throw std::runtime_error(
         "DWI volumes could not be classified into b-value shells; gradient encoding may not represent a "
         "HARDI sequence");
-  struct S {
-    double mean;
-    std::vector<int> vols;
-  };
-  std::vector<S> shells;
+  std::vector<Shell> shells;
   for (int s = 1; s <= nshells; ++s) {
-    S sh{0.0, {}};
+    Shell sh{0.0, 0.0, std::numeric_limits<double>::max(), 0.0, {}};
     for (int v = 0; v < nvol; ++v)
       if (clusters[v] == s) {
         sh.vols.push_back(v);
         sh.mean += b[v];
+        sh.lo = std::min(sh.lo, b[v]);
+        sh.hi = std::max(sh.lo, b[v]);
       }
     if (sh.vols.empty()) continue;
     sh.mean /= sh.vols.size();
+    for (int v : sh.vols) sh.stdev += (b[v] - sh.mean) * (b[v] - sh.mean);
+    sh.stdev = std::sqrt(sh.stdev / (static_cast<double>(sh.vols.size()) - 1.0));
     shells.push_back(std::move(sh));
   }
-  std::stable_sort(shells.begin(), shells.end(), [](const S& a, const S& c) { return a.mean < c.mean; });
-  const bool has_b0 = shells.front().mean <= b0thr;
-  if (shells.size() == 1 && has_b0)
-    throw std::runtime_error("No non b=0 data found, but the command requires a non b=0 shell");
-  return shells.back().vols;
+  std::stable_sort(shells.begin(), shells.end(), [](const Shell& a, const Shell& c) { return a.mean < c.mean; });
+  return shells;
+}
+
+std::string shell_str(const Shell& s) {
+  std::ostringstream o;
+  o << s.mean << " +- " << s.stdev;
+  return o.str();
+}
+
+// csd.h:62-64: Shells(grad).select_shells(true, false, true).largest() --
+// the volumes of the one non-b=0 shell CSD uses.  Without -shells
+// (n_req == 0) that is the largest b-value shell (dwi/shells.cpp:243-260);
+// with it, the shells matching the requested b-values (dwi/shells.cpp:111-239)
+// must be exactly one non-b=0 shell and no b=0 shell.
+std::vector<int> csd_shell(const std::vector<double>& b, double b0thr, double eps, const double* req, int n_req) {
+  std::vector<Shell> shells = cluster_shells(b, b0thr, eps);
+  const bool has_b0 = shells.front().is_bzero(b0thr);
+  if (n_req <= 0) {
+    if (shells.size() == 1 && has_b0)
+      throw std::runtime_error("No non b=0 data found, but the command requires a non b=0 shell");
+    return shells.back().vols;
+  }
+  std::vector<char> keep(shells.size(), 0);
+  bool b0_selected = false;
+  int nonb0_selected = 0;
+  auto take = [&](size_t s) {
+    if (keep[s])
+      throw std::runtime_error("User selected a shell more than once: " + shell_str(shells[s]) + " with " +
+                               std::to_string(shells[s].vols.size()) + " volumes");
+    keep[s] = 1;
+    ++nonb0_selected;
+  };
+  for (int q = 0; q < n_req; ++q) {
+    const double want = req[q];
+    if (want < 0.0) throw std::runtime_error("Cannot select shells corresponding to negative b-values");
+    if (want <= b0thr) {
+      if (!has_b0) throw std::runtime_error("User selected b=0 shell, but no such data was found");
+      if (b0_selected) throw std::runtime_error("User selected b=0 shell more than once");
+      keep[0] = 1;
+      b0_selected = true;
+      continue;
+    }
+    // within a shell's [min, "max"] range
+    bool selected = false;
+    for (size_t s = 0; s < shells.size(); ++s)
+      if (want >= shells[s].lo && want <= shells[s].hi) {
+        take(s);
+        selected = true;
+      }
+    if (selected) continue;
+    // within 1 of exactly one shell's mean
+    size_t best = 0;
+    bool ambiguous = false;
+    for (size_t s = 0; s < shells.size(); ++s)
+      if (std::fabs(want - shells[s].mean) <= 1.0) {
+        if (selected) {
+          ambiguous = true;
+        } else {
+          best = s;
+          selected = true;
+        }
+      }
+    if (selected && !ambiguous) {
+      take(best);
+      continue;
+    }
+    // the clear winner in standard deviations (Poisson when a non-b=0 shell
+    // has a negligible spread)
+    bool zero_stdev = false;
+    for (const Shell& s : shells)
+      if (!s.is_bzero(b0thr) && s.stdev < 1.0) zero_stdev = true;
+    best = 0;
+    double best_n = std::numeric_limits<double>::max();
+    ambiguous = false;
+    for (size_t s = 0; s < shells.size(); ++s) {
+      const double sd = shells[s].is_bzero(b0thr) ? 0.5 * b0thr
+                                                  : (zero_stdev ? std::sqrt(shells[s].mean) : shells[s].stdev);
+      const double n = std::fabs((want - shells[s].mean) / sd);
+      if (n < best_n) {
+        ambiguous = n >= 0.1 * best_n;
+        best = s;
+        best_n = n;
+      } else {
+        ambiguous = n < 10.0 * best_n;
+      }
+    }
+    if (ambiguous) {
+      std::string all;
+      for (const Shell& s : shells) all += (all.empty() ? "" : ", ") + shell_str(s);
+      std::ostringstream o;
+      o << "Unable to robustly select desired shell b=" << want << " (detected shells are: " << all << ")";
+      throw std::runtime_error(o.str());
+    }
+    take(best);
+  }
+  if (nonb0_selected != 1)
+    throw std::runtime_error("User selected " + std::to_string(nonb0_selected) +
+                             " non b=0 shells, but the command requires single-shell data");
+  if (b0_selected) throw std::runtime_error("User selected b=0 shell, but the command is not compatible with b=0 data");
+  for (size_t s = shells.size(); s-- > 0;)
+    if (keep[s]) return shells[s].vols;
+  throw std::runtime_error("no shell selected");
 }
 
 }  // namespace
@@ -201,7 +308,7 @@ HostShared build_shared(const SharedParams& p, const double* grad_in, int nvol, 
   // csd.h:62-64: volumes of the largest non-b=0 shell
   std::vector<double> b(nvol);
   for (int r = 0; r < nvol; ++r) b[r] = s.grad[4 * r + 3];
-  s.dwis = largest_shell(b, p.bzero_threshold, p.bvalue_epsilon);
+  s.dwis = csd_shell(b, p.bzero_threshold, p.bvalue_epsilon, p.shells.data(), static_cast<int>(p.shells.size()));
   s.ndw = static_cast<int>(s.dwis.size());
 
   // gradient.h:77-95

@@ -20,6 +20,7 @@ struct SharedParams {
   std::vector<double> filter;   // -filter (empty = [1 1 1], csd.h:136-138)
   double bzero_threshold = 10.0;  // BZeroThreshold (dwi/gradient.h:30)
   double bvalue_epsilon = 80.0;   // BValueEpsilon (dwi/shells.h:34)
+  std::vector<double> shells;     // -shells b-values (empty = the largest shell, csd.h:64)
 };
 
 struct HostShared {

@@ -21,6 +21,8 @@ Options (csd.cpp:318-346, dwi2fod.cpp:38-59, gradient.cpp:36-60):
   -norm_lambda v     weight of the norm regulariser (1)
   -threshold v       amplitude below which a direction is constrained (0)
   -niter N           maximum iterate() calls per voxel (50)
+  -shells b         the non-b=0 shell to deconvolve (one b-value; default the
+                     largest shell; shells.cpp:100-239)
   -grad file         gradient table [x y z b] rows, instead of dw_scheme
   -fslgrad bvecs bvals   FSL gradient files (image-axis directions)
   -warm_start file   a warm-start network (.npz) trained for this scheme
@@ -109,8 +111,6 @@ def run(argv) -> int:
     if os.path.exists(out_path) and not opt.get("-force"):
         raise SystemExit(f"dwi2fod: output image \"{out_path}\" already exists (use -force to replace it)")
 
-    if "-shells" in opt:
-        raise SystemExit("dwi2fod csd: -shells is not provided (the largest non-b=0 shell is used)")
     from . import csd
     img = mif.read(dwi_path)
     if img.data.ndim != 4:
@@ -143,9 +143,14 @@ def run(argv) -> int:
             kw[name] = float(opt["-" + name])
     if "-niter" in opt:
         kw["niter"] = int(opt["-niter"])
+    if "-shells" in opt:
+        kw["shells"] = [float(v) for v in opt["-shells"].split(",")]
     shared.parse_cmdline_options(**kw)
     shared.set_response(mif.load_vector(resp_path))
-    shared.init()
+    try:
+        shared.init()
+    except csd.CSDError as e:
+        raise SystemExit(f"dwi2fod: {e}")
 
     net = None
     if "-warm_start" in opt:

@@ -54,3 +54,31 @@ def test_dwi2fod_csd_on_mif_files(cuda, hr_dirs, tmp_path):
     assert np.percentile(rel, 99) <= 1e-4
     with pytest.raises(SystemExit, match="already exists"):
         run(["csd", p_dwi, str(resp), out_path])
+
+
+def test_dwi2fod_csd_shells_option(cuda, hr_dirs, tmp_path):
+    """-shells on a two-shell image: the csd branch deconvolves the chosen
+    shell only (csd.h:64), so the FODs equal the oracle's on the image cut
+    down to the b=0 volumes and that shell."""
+    d1, d3 = synth.fibonacci_hemisphere(60), synth.fibonacci_hemisphere(45)
+    grad = np.array([[0, 0, 0, 0]] * 6 + [[*d, 1000.0] for d in d1] + [[*d, 3000.0] for d in d3], np.float64)
+    grad = grad[np.random.default_rng(8).permutation(len(grad))]
+    dims = (9, 8, 7)
+    n = int(np.prod(dims))
+    sig = synth.voxel_signals(np.random.default_rng(9), grad, n, 30.0)
+    data = sig.reshape(dims[2], dims[1], dims[0], -1).transpose(2, 1, 0, 3)
+    p_dwi = str(tmp_path / "dwi.mif")
+    mif.write(p_dwi, mif.Image(data=data.astype(np.float64), vox=[2.0, 2.0, 2.0, 1.0], transform=np.eye(4)[:3],
+                               keyval={"dw_scheme": mif.scheme_to_text(grad)}), datatype="Float32LE")
+    resp = tmp_path / "response.txt"
+    resp.write_text(" ".join(str(c) for c in synth.RESPONSE) + "\n")
+    for b in (1000.0, 3000.0):
+        out_path = str(tmp_path / f"fod{int(b)}.mif")
+        assert run(["csd", p_dwi, str(resp), out_path, "-shells", str(int(b))]) == 0
+        got = mif.read(out_path).data.transpose(2, 1, 0, 3).reshape(-1, 45)
+        keep = np.nonzero((grad[:, 3] == 0) | (grad[:, 3] == b))[0]
+        ref = O.OracleShared(grad[keep], synth.RESPONSE, hr_dirs).solve(sig[:, keep].astype(np.float64))
+        rel = np.abs(got - ref["F"]).max(1) / np.abs(ref["F"]).max(1)
+        assert np.percentile(rel, 99) <= 1e-4, (b, np.percentile(rel, 99))
+    with pytest.raises(SystemExit, match="2 non b=0 shells"):
+        run(["csd", p_dwi, str(resp), str(tmp_path / "x.mif"), "-shells", "1000,3000"])

@@ -111,3 +111,55 @@ def test_cpp_shim_compiles():
                             os.path.join(ROOT, "mrtrix3_b200", "csrc"), "-I", "/usr/local/cuda/include", src],
                            capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
+
+
+def _two_shell_grad(jitter=False):
+    """6 b=0, 60 directions at b=1000 and 45 at b=3000, the shells interleaved."""
+    d1 = synth.fibonacci_hemisphere(60)
+    d3 = synth.fibonacci_hemisphere(45)
+    rows = [[0, 0, 0, 0]] * 6
+    rows += [[*d1[i], 1000.0 + (5.0 * ((i % 3) - 1) if jitter else 0.0)] for i in range(60)]
+    rows += [[*d3[i], 3000.0] for i in range(45)]
+    g = np.array(rows, np.float64)
+    order = np.random.default_rng(3).permutation(len(g))
+    return g[order]
+
+
+@pytest.mark.parametrize("want,b", [([1000], 1000.0), ([3000], 3000.0), ([1000.5], 1000.0), ([2990], 3000.0),
+                                    (None, 3000.0)])
+def test_shells_option_selects_one_shell(hr_dirs, want, b):
+    """-shells picks the one non-b=0 shell (shells.cpp:111-239 under
+    select_shells(true, false, true), csd.h:64); the tables then equal the
+    oracle's on the scheme holding only that shell."""
+    g = _two_shell_grad()
+    s = csd.Shared(g)
+    s.parse_cmdline_options(shells=want)
+    s.set_response(synth.RESPONSE)
+    s.init()
+    expect = np.nonzero(g[:, 3] == b)[0]
+    assert np.array_equal(np.asarray(s.dwis), expect)
+    keep = np.nonzero((g[:, 3] == 0) | (g[:, 3] == b))[0]
+    o = O.OracleShared(g[keep], synth.RESPONSE, hr_dirs)
+    assert np.array_equal(keep[o.dwis], expect)
+    for k in ("rconv", "M", "HR_trans", "Mt_M"):
+        a, r = getattr(s, k), getattr(o, k)
+        assert np.abs(a - r).max() <= 1e-14 * max(np.abs(r).max(), 1.0), k
+
+
+def test_shells_option_range_and_errors():
+    g = _two_shell_grad(jitter=True)
+    # within the shell's [min, max] range (995..1005)
+    s = csd.make_shared(g, synth.RESPONSE, shells=[1003])
+    assert np.array_equal(np.asarray(s.dwis), np.nonzero(np.abs(g[:, 3] - 1000) <= 5)[0])
+    cases = [([-5], "negative b-values"),
+             ([0], "User selected 0 non b=0 shells"),
+             ([1000, 3000], "User selected 2 non b=0 shells"),
+             ([1000, 0], "not compatible with b=0 data"),
+             ([1000, 1001], "more than once"),
+             ([2000], "Unable to robustly select desired shell b=2000")]
+    for want, msg in cases:
+        with pytest.raises(csd.CSDError, match=msg):
+            csd.make_shared(g, synth.RESPONSE, shells=want)
+    # no b=0 volumes: a requested b=0 shell is an error of its own
+    with pytest.raises(csd.CSDError, match="no such data was found"):
+        csd.make_shared(g[g[:, 3] > 0], synth.RESPONSE, shells=[0, 1000])

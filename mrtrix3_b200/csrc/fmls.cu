@@ -42,10 +42,15 @@ __device__ unsigned long long g_fmls_cycles[8];
 
 namespace {
 
-constexpr int kFmlsWarps = 1;  // ~38 KB of shared memory a warp: five warps an SM
-constexpr int kFmlsMaxSort = 2048;  // directions at most (the sort's width)
+constexpr int kFmlsWarps = 1;       // one warp a block (occupancy is set by shared memory)
+constexpr int kFmlsMaxSort = 2048;  // directions at most (the sort's width; the keys carry 11 index bits)
 constexpr int kFmlsMaxNsh = 153;    // lmax 16
-constexpr int kFmlsLobes = 128;     // lobes a voxel may create in shared memory (more: the global slot)
+constexpr int kFmlsLobes = 120;     // lobes a voxel may create in shared memory (8-bit links; more: the global slot)
+
+// the shared-memory workspace (8-bit labels and lobe links, 16-bit order)
+// and the global slot's (32-bit), which shares the order in shared memory
+using WorkS = fmls::WorkT<int8_t, uint16_t>;
+using WorkG = fmls::WorkT<int, uint16_t>;
 
 int next_pow2(int n) {
   int p = 1;
@@ -53,32 +58,46 @@ int next_pow2(int n) {
   return p;
 }
 
-// per warp slot in global memory: ints label parent neg head tail next
-// retro_dir retro_lobe, doubles max_peak mean(3) integral peak_dir(3) -- one
-// entry per direction; the shared-memory lobes use only the retro lists
-constexpr int kSlotInts = 8, kSlotDoubles = 8;
+__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Shared memory of one warp: values [nd] and sh [nsh] doubles, the sort keys
-// [sort_n] and labels [nd] ints, then for kFmlsLobes lobes the ints parent
-// neg head tail next and the doubles max_peak integral mean(3) peak_dir(3)
-// and the refined peaks' values (1) and directions (3).
+// per warp slot in global memory: ints label parent neg head tail next
+// retro_dir retro_lobe, doubles values max_peak mean(3) integral peak_dir(3)
+// -- one entry per direction; the shared-memory path uses the values and the
+// retro lists only
+constexpr int kSlotInts = 8, kSlotDoubles = 9;
+
+// Shared memory of one warp: sh [nsh] doubles, then one region that holds
+// the sort keys [sort_n] (64-bit) while sorting and afterwards the order
+// [nd] (16-bit), the labels [nd] (8-bit), the lobes' links parent neg head
+// tail next [kFmlsLobes] (8-bit) and their doubles max_peak integral mean(3)
+// peak_dir(3) and the refined peaks' values (1) and directions (3).
+__host__ __device__ inline size_t fmls_after_sort_bytes(int nd) {
+  return align16((size_t)nd * 2) + align16((size_t)nd) + align16((size_t)5 * kFmlsLobes) +
+         (size_t)12 * kFmlsLobes * sizeof(double);
+}
+__host__ __device__ inline size_t fmls_region_bytes(int nd, int sort_n) {
+  const size_t k = (size_t)sort_n * 8, b = fmls_after_sort_bytes(nd);
+  return align16(k > b ? k : b);
+}
 __host__ __device__ inline size_t fmls_warp_bytes(int nd, int nsh, int sort_n) {
-  const size_t a = ((size_t)(nd + nsh) * sizeof(double) + (size_t)(sort_n + nd) * sizeof(int) + 15) & ~(size_t)15;
-  return a + (size_t)5 * kFmlsLobes * sizeof(int) + (size_t)12 * kFmlsLobes * sizeof(double);
+  return align16((size_t)nsh * sizeof(double)) + fmls_region_bytes(nd, sort_n);
 }
 
 // fmls::grow (fmls.cpp:178-246) with the warp: for each direction in order,
 // lane e looks up the lobe of neighbour e (its label's root, if that lobe's
-// sign matches), the lanes drop repeated lobes and rank the rest in
-// ascending order, and lane 0 applies the step -- a new lobe, an addition, the
-// merges into the first adjacent lobe in ascending order, or a pending
-// assignment -- with the arithmetic of the core's lobe constructor, lobe_add
-// and lobe_merge, so every value is computed as in fmls::grow.  The order is
-// fixed once sorted, so the global tables a step reads (the direction's
-// neighbour list, its unit vector and weight) are fetched one and two steps
-// ahead: only the labels and lobes (shared memory) depend on earlier steps.
-// Returns the lobes created, -1 past max_lobes.
-__device__ int grow_warp(const fmls::Tables& t, const fmls::Work& w, int* n_retro, int max_lobes, int lane) {
+// sign matches); two warp reductions give the smallest and largest adjacent
+// lobe, which decide the common steps (no adjacent lobe: a new one; one: an
+// addition), and lane 0 applies the step with the arithmetic of the core's
+// lobe constructor and lobe_add.  With two or more adjacent lobes the merge
+// test reads the largest (the last in ascending order), and the merges into
+// the smallest run in ascending order, each next lobe found by another
+// reduction -- the order of fmls::grow, so every value is computed as there.
+// The order is fixed once sorted, so the global tables a step reads (the
+// direction's value, neighbour list, unit vector and weight) are fetched one
+// and two steps ahead: only the labels and lobes (shared memory) depend on
+// earlier steps.  Returns the lobes created, -1 past max_lobes.
+template <class W>
+__device__ int grow_warp(const fmls::Tables& t, const W& w, int* n_retro, int max_lobes, int lane) {
   const int nd = t.ndir;
   for (int d = lane; d < nd; d += 32) w.label[d] = -1;
   __syncwarp();
@@ -88,19 +107,21 @@ __device__ int grow_warp(const fmls::Tables& t, const fmls::Work& w, int* n_retr
   int nbc = lane < degc ? __ldg(t.adj + e0 + lane) : 0;
   double uc0 = __ldg(t.unit + 3 * dc), uc1 = __ldg(t.unit + 3 * dc + 1), uc2 = __ldg(t.unit + 3 * dc + 2);
   double wc = __ldg(t.weight + dc);
+  double vc = w.values[dc];
   int dn = nd > 1 ? w.order[1] : 0;
   int e0n = __ldg(t.adj_off + dn), degn = __ldg(t.adj_off + dn + 1) - e0n;
   int nl = 0, nr = 0;
   for (int k = 0; k < nd; ++k) {
-    // fetch ahead: step k + 1's neighbours, direction and weight; step k + 2's offsets
+    // fetch ahead: step k + 1's neighbours, value, direction and weight; step k + 2's offsets
     const int nbn = (k + 1 < nd && lane < degn) ? __ldg(t.adj + e0n + lane) : 0;
     const double un0 = __ldg(t.unit + 3 * dn), un1 = __ldg(t.unit + 3 * dn + 1), un2 = __ldg(t.unit + 3 * dn + 2);
     const double wn = __ldg(t.weight + dn);
+    const double vn = w.values[dn];
     const int dnn = k + 2 < nd ? w.order[k + 2] : 0;
     const int e0nn = __ldg(t.adj_off + dnn), degnn = __ldg(t.adj_off + dnn + 1) - e0nn;
     // step k
     const int d = dc;
-    const double v = w.values[d];
+    const double v = vc;
     const int vneg = v <= 0.0 ? 1 : 0;
     int r = -1;
     if (lane < degc) {
@@ -110,20 +131,10 @@ __device__ int grow_warp(const fmls::Tables& t, const fmls::Work& w, int* n_retr
         if (w.neg[r] != vneg) r = -1;
       }
     }
-    // one lane per adjacent lobe, ranked by lobe index
-    const unsigned same = __match_any_sync(0xffffffffu, r);
-    const bool keep = r >= 0 && lane == __ffs(same) - 1;
-    const unsigned kept = __ballot_sync(0xffffffffu, keep);
-    const int na = __popc(kept);
-    int rank = 0;
-    for (int j = 0; j < degc; ++j) {
-      const int rj = __shfl_sync(0xffffffffu, r, j);
-      if ((kept >> j) & 1u) rank += rj < r ? 1 : 0;
-    }
-    const unsigned first = __ballot_sync(0xffffffffu, keep && rank == 0);
-    const int a0 = na ? __shfl_sync(0xffffffffu, r, __ffs(first) - 1) : -1;
+    const int rmax = __reduce_max_sync(0xffffffffu, r);
     bool add = false;
-    if (na == 0) {
+    int a0 = -1;
+    if (rmax < 0) {
       if (nl >= max_lobes) return -1;
       if (lane == 0) {
         // FOD_lobe constructor (fmls.h:60-72)
@@ -143,17 +154,18 @@ __device__ int grow_warp(const fmls::Tables& t, const fmls::Work& w, int* n_retr
         w.label[d] = nl;
       }
       ++nl;
-    } else if (na == 1) {
-      add = true;
     } else {
-      const unsigned last = __ballot_sync(0xffffffffu, keep && rank == na - 1);
-      const int al = __shfl_sync(0xffffffffu, r, __ffs(last) - 1);
-      if (fabs(v) / w.max_peak[al] > t.merge_ratio) {
-        for (int q = 1; q < na; ++q) {
-          const unsigned sel = __ballot_sync(0xffffffffu, keep && rank == q);
-          const int aq = __shfl_sync(0xffffffffu, r, __ffs(sel) - 1);
-          if (lane == 0) fmls::lobe_merge(w, a0, aq);
+      // the smallest adjacent lobe (no lobe reads as 0xffffffff)
+      a0 = (int)__reduce_min_sync(0xffffffffu, (unsigned)r);
+      if (a0 == rmax) {
+        add = true;
+      } else if (fabs(v) / w.max_peak[rmax] > t.merge_ratio) {
+        for (int cur = a0;;) {
+          const unsigned nx = __reduce_min_sync(0xffffffffu, r > cur ? (unsigned)r : 0xffffffffu);
+          if (nx == 0xffffffffu) break;
+          if (lane == 0) fmls::lobe_merge(w, a0, (int)nx);
           __syncwarp();
+          cur = (int)nx;
         }
         add = true;
       } else {
@@ -183,6 +195,7 @@ __device__ int grow_warp(const fmls::Tables& t, const fmls::Work& w, int* n_retr
     uc1 = un1;
     uc2 = un2;
     wc = wn;
+    vc = vn;
     dn = dnn;
     e0n = e0nn;
     degn = degnn;
@@ -190,6 +203,16 @@ __device__ int grow_warp(const fmls::Tables& t, const fmls::Work& w, int* n_retr
   *n_retro = nr;
   return nl;
 }
+
+// The sort key of direction d with amplitude v: |v|'s bits above the lowest
+// 11 (an order-preserving integer for a non-negative double), then 2047 - d,
+// so that a larger key comes first in the segmenter's order (|value|
+// descending, index ascending) whenever the truncated magnitudes differ or
+// are equal exactly.
+__device__ __forceinline__ unsigned long long sort_key(double v, int d) {
+  return ((unsigned long long)__double_as_longlong(fabs(v)) & ~0x7FFull) | (unsigned long long)(0x7FF - d);
+}
+__device__ __forceinline__ int key_dir(unsigned long long k) { return 0x7FF - (int)(k & 0x7FF); }
 
 struct FmlsArgs {
   fmls::Tables t;
@@ -207,26 +230,27 @@ struct FmlsArgs {
 __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __grid_constant__ FmlsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int nd = a.t.ndir, nsh = a.t.nsh;
-  unsigned char* base = smem_raw + wib * fmls_warp_bytes(nd, nsh, a.sort_n);
-  double* values = reinterpret_cast<double*>(base);
-  double* sh = values + nd;
-  int* keys = reinterpret_cast<int*>(sh + nsh);
-  int* slabel = keys + a.sort_n;
-  int* li = reinterpret_cast<int*>(base + (((size_t)(nd + nsh) * sizeof(double) +
-                                            (size_t)(a.sort_n + nd) * sizeof(int) + 15) & ~(size_t)15));
-  double* ld = reinterpret_cast<double*>(li + 5 * kFmlsLobes);
+  const int nd = a.t.ndir, nsh = a.t.nsh, sort_n = a.sort_n;
+  unsigned char* base = smem_raw + wib * fmls_warp_bytes(nd, nsh, sort_n);
+  double* sh = reinterpret_cast<double*>(base);
+  unsigned char* region = base + align16((size_t)nsh * sizeof(double));
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(region);
+  uint16_t* order = reinterpret_cast<uint16_t*>(region);
+  int8_t* slabel = reinterpret_cast<int8_t*>(region + align16((size_t)nd * 2));
+  int8_t* links = slabel + align16((size_t)nd);
+  double* ld = reinterpret_cast<double*>(links + align16((size_t)5 * kFmlsLobes));
   double* pre_val = ld + 8 * kFmlsLobes;
   double* pre_u = pre_val + kFmlsLobes;
 
   const long long gw = (long long)blockIdx.x * kFmlsWarps + wib;
   char* slot = a.scratch + gw * a.slot_bytes;
   int* ib = reinterpret_cast<int*>(slot);
-  double* db = reinterpret_cast<double*>(slot + (((size_t)kSlotInts * nd * sizeof(int) + 15) & ~(size_t)15));
+  double* db = reinterpret_cast<double*>(slot + align16((size_t)kSlotInts * nd * sizeof(int)));
+  double* values = db;  // the amplitudes, in the slot (read in order by the growing)
   // the global slot's workspace (every array one entry per direction)
-  fmls::Work wg;
+  WorkG wg;
   wg.values = values;
-  wg.order = keys;
+  wg.order = order;
   wg.label = ib;
   wg.parent = ib + nd;
   wg.neg = ib + 2 * nd;
@@ -235,18 +259,22 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
   wg.peak_next = ib + 5 * nd;
   wg.retro_dir = ib + 6 * nd;
   wg.retro_lobe = ib + 7 * nd;
-  wg.max_peak = db;
-  wg.mean = db + nd;
-  wg.integral = db + 4 * nd;
-  wg.peak_dir = db + 5 * nd;
+  wg.max_peak = db + nd;
+  wg.mean = db + 2 * nd;
+  wg.integral = db + 5 * nd;
+  wg.peak_dir = db + 6 * nd;
   // the shared-memory workspace: labels and up to kFmlsLobes lobes
-  fmls::Work ws = wg;
+  WorkS ws;
+  ws.values = values;
+  ws.order = order;
   ws.label = slabel;
-  ws.parent = li;
-  ws.neg = li + kFmlsLobes;
-  ws.peak_head = li + 2 * kFmlsLobes;
-  ws.peak_tail = li + 3 * kFmlsLobes;
-  ws.peak_next = li + 4 * kFmlsLobes;
+  ws.parent = links;
+  ws.neg = links + kFmlsLobes;
+  ws.peak_head = links + 2 * kFmlsLobes;
+  ws.peak_tail = links + 3 * kFmlsLobes;
+  ws.peak_next = links + 4 * kFmlsLobes;
+  ws.retro_dir = wg.retro_dir;
+  ws.retro_lobe = wg.retro_lobe;
   ws.max_peak = ld;
   ws.integral = ld + kFmlsLobes;
   ws.mean = ld + 2 * kFmlsLobes;
@@ -259,47 +287,81 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
       continue;
     }
     const float* src = a.fod + v * a.vs;
+    __syncwarp();  // the previous voxel's last reads of the region are done
     for (int k = lane; k < nsh; k += 32) sh[k] = (double)src[(long long)k * a.cs];
     __syncwarp();
     if (fmls::skip_voxel(sh, nsh)) {
-      __syncwarp();
       if (lane == 0) a.counts[v] = 0;
       continue;
     }
     FMLS_T(t0);
-    for (int d = lane; d < nd; d += 32) {
-      const double* row = a.t.sh2amp + (long long)d * nsh;
-      double s = 0.0;
-      for (int k = 0; k < nsh; ++k) s = fma(__ldg(row + k), sh[k], s);
-      values[d] = s;
+    // amplitudes (the transposed table: coalesced rows; the same FMA chain
+    // over the coefficients as a row of sh2amp) and their sort keys
+    for (int d = lane; d < sort_n; d += 32) {
+      unsigned long long key = 0ull;  // padding: after every direction
+      if (d < nd) {
+        double s = 0.0;
+        for (int k = 0; k < nsh; ++k) s = fma(__ldg(a.t.sh2amp_t + (long long)k * nd + d), sh[k], s);
+        values[d] = s;
+        key = sort_key(s, d);
+      }
+      keys[d] = key;
     }
-    for (int i = lane; i < a.sort_n; i += 32) keys[i] = i;
     __syncwarp();
     FMLS_T(t1);
     FMLS_ACC(0, t0, t1);
-    // bitonic sort of keys in the segmenter's order (padding keys >= nd last)
-    for (int k = 2; k <= a.sort_n; k <<= 1) {
+    // bitonic sort, descending keys: each lane takes pairs (i, i + j)
+    for (int k = 2; k <= sort_n; k <<= 1) {
       for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int i = lane; i < a.sort_n; i += 32) {
-          const int ixj = i ^ j;
-          if (ixj > i) {
-            const int ka = keys[i], kb = keys[ixj];
-            const bool up = (i & k) == 0;
-            if (up ? fmls::before(values, nd, kb, ka) : fmls::before(values, nd, ka, kb)) {
-              keys[i] = kb;
-              keys[ixj] = ka;
-            }
+        for (int p = lane; p < (sort_n >> 1); p += 32) {
+          const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
+          const unsigned long long ka = keys[i], kb = keys[i + j];
+          if ((i & k) == 0 ? ka < kb : ka > kb) {
+            keys[i] = kb;
+            keys[i + j] = ka;
           }
         }
         __syncwarp();
       }
+    }
+    // keys equal above the index bits may hide magnitudes that differ in
+    // their lowest 11 bits: lane 0 re-sorts such runs by the exact values
+    bool tie = false;
+    for (int k = lane; k + 1 < nd; k += 32) tie = tie || (keys[k] >> 11) == (keys[k + 1] >> 11);
+    if (__any_sync(0xffffffffu, tie)) {
+      if (lane == 0) {
+        for (int k = 1; k < nd; ++k) {
+          const unsigned long long x = keys[k];
+          const int dx = key_dir(x);
+          const double vx = fabs(values[dx]);
+          int q = k;
+          while (q > 0 && (keys[q - 1] >> 11) == (x >> 11)) {
+            const int dy = key_dir(keys[q - 1]);
+            const double vy = fabs(values[dy]);
+            if (!(vx > vy || (vx == vy && dx < dy))) break;
+            keys[q] = keys[q - 1];
+            --q;
+          }
+          keys[q] = x;
+        }
+      }
+      __syncwarp();
+    }
+    // the order, written over the keys it was read from (chunk c's entries
+    // land below the keys later chunks read)
+    for (int c = 0; c < nd; c += 32) {
+      const int k = c + lane;
+      const int d = k < nd ? key_dir(keys[k]) : 0;
+      __syncwarp();
+      if (k < nd) order[k] = (uint16_t)d;
+      __syncwarp();
     }
     // the region growing (the warp) and the pending assignments (lane 0)
     FMLS_T(t2);
     FMLS_ACC(1, t1, t2);
     int nl = 0;
     bool in_smem = true;
-    if (values[keys[0]] > 0.0) {
+    if (values[order[0]] > 0.0) {
       int nr = 0;
       nl = grow_warp(a.t, ws, &nr, kFmlsLobes, lane);
       FMLS_T(t3);
@@ -310,38 +372,41 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
         nl = __shfl_sync(0xffffffffu, nl, 0);
         nr = __shfl_sync(0xffffffffu, nr, 0);
       }
-      if (lane == 0) fmls::assign_pending(a.t, in_smem ? ws : wg, nr);
+      if (lane == 0) {
+        if (in_smem)
+          fmls::assign_pending(a.t, ws, nr);
+        else
+          fmls::assign_pending(a.t, wg, nr);
+      }
       FMLS_T(t4);
       FMLS_ACC(3, t3, t4);
     }
     FMLS_T(t5);
     if (nl == 0) {
       if (lane == 0) a.counts[v] = 0;
-      __syncwarp();
       continue;
     }
     __syncwarp();
-    const fmls::Work& w = in_smem ? ws : wg;
-    // the candidate peaks' Newton refinements, spread over the lanes (in the
-    // global slot's case lane 0 refines them itself, in finish_lobes)
+    fmls::Fixel* out = reinterpret_cast<fmls::Fixel*>(a.fixels + v * (long long)a.max_fixels * 8);
     if (in_smem) {
+      // the candidate peaks' Newton refinements, spread over the lanes
       for (int p = lane; p < nl; p += 32) {
-        if (!fmls::peak_candidate(a.t, w, p)) continue;
-        double u[3] = {w.peak_dir[3 * p], w.peak_dir[3 * p + 1], w.peak_dir[3 * p + 2]};
+        if (!fmls::peak_candidate(a.t, ws, p)) continue;
+        double u[3] = {ws.peak_dir[3 * p], ws.peak_dir[3 * p + 1], ws.peak_dir[3 * p + 2]};
         pre_val[p] = fmls::get_peak(a.t, sh, u);
         for (int k = 0; k < 3; ++k) pre_u[3 * p + k] = u[k];
       }
+      __syncwarp();
+      FMLS_T(t6);
+      FMLS_ACC(4, t5, t6);
+      if (lane == 0) a.counts[v] = fmls::finish_lobes(a.t, ws, sh, nl, out, a.max_fixels, pre_val, pre_u);
+      FMLS_T(t7);
+      FMLS_ACC(5, t6, t7);
+    } else {
+      // lane 0 refines the peaks itself, in finish_lobes
+      if (lane == 0) a.counts[v] = fmls::finish_lobes(a.t, wg, sh, nl, out, a.max_fixels);
     }
     __syncwarp();
-    FMLS_T(t6);
-    FMLS_ACC(4, t5, t6);
-    if (lane == 0)
-      a.counts[v] = fmls::finish_lobes(a.t, w, sh, nl,
-                                       reinterpret_cast<fmls::Fixel*>(a.fixels + v * (long long)a.max_fixels * 8),
-                                       a.max_fixels, in_smem ? pre_val : nullptr, in_smem ? pre_u : nullptr);
-    __syncwarp();
-    FMLS_T(t7);
-    FMLS_ACC(5, t6, t7);
   }
 }
 
@@ -359,7 +424,7 @@ cudaError_t upload(T** dst, const T* src, size_t n) {
 struct csd_fmls {
   int device = 0;
   fmls::Tables t{};  // device pointers
-  double *unit = nullptr, *weight = nullptr, *sh2amp = nullptr, *al = nullptr, *dsqrt = nullptr;
+  double *unit = nullptr, *weight = nullptr, *sh2amp = nullptr, *sh2amp_t = nullptr, *al = nullptr, *dsqrt = nullptr;
   int32_t *adj_off = nullptr, *adj = nullptr, *grid_off = nullptr, *grid = nullptr;
   char* scratch = nullptr;
   size_t scratch_warps = 0;
@@ -370,6 +435,7 @@ extern "C" void csd_fmls_destroy(csd_fmls* p) {
   cudaFree(p->unit);
   cudaFree(p->weight);
   cudaFree(p->sh2amp);
+  cudaFree(p->sh2amp_t);
   cudaFree(p->al);
   cudaFree(p->dsqrt);
   cudaFree(p->adj_off);
@@ -411,6 +477,10 @@ extern "C" int csd_fmls_create(const csd_fmls_tables* c, csd_fmls** out) {
   if (e == cudaSuccess) e = upload(&p->unit, c->unit, 3 * (size_t)nd);
   if (e == cudaSuccess) e = upload(&p->weight, c->weight, (size_t)nd);
   if (e == cudaSuccess) e = upload(&p->sh2amp, c->sh2amp, (size_t)nd * c->nsh);
+  std::vector<double> sh2amp_t((size_t)nd * c->nsh);
+  for (int d = 0; d < nd; ++d)
+    for (int k = 0; k < c->nsh; ++k) sh2amp_t[(size_t)k * nd + d] = c->sh2amp[(size_t)d * c->nsh + k];
+  if (e == cudaSuccess) e = upload(&p->sh2amp_t, sh2amp_t.data(), sh2amp_t.size());
   if (e == cudaSuccess) e = upload(&p->al, c->al, (size_t)c->al_ndir * c->n_al);
   if (e == cudaSuccess) e = upload(&p->adj_off, c->adj_off, (size_t)nd + 1);
   if (e == cudaSuccess) e = upload(&p->adj, c->adj, (size_t)c->n_adj);
@@ -428,7 +498,7 @@ extern "C" int csd_fmls_create(const csd_fmls_tables* c, csd_fmls** out) {
   p->t = fmls::Tables{nd, c->lmax, c->nsh, p->unit, p->weight, p->adj_off, p->adj, p->sh2amp, c->al_ndir, c->n_al,
                       c->al_inc, p->al, c->num_az, c->num_el, c->az_begin, c->el_begin, c->az_step, c->el_step,
                       p->grid_off, p->grid, c->integral_threshold, c->peak_value_threshold, c->merge_ratio,
-                      p->dsqrt};
+                      p->dsqrt, p->sh2amp_t};
   *out = p;
   return CSD_OK;
 }
@@ -469,7 +539,7 @@ extern "C" int csd_fmls_segment(csd_fmls* p, const float* fod, int64_t n, int64_
   if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_fmls_segment: ") + cudaGetErrorString(e));
   const long long blocks = std::max<long long>(
       1, std::min<long long>((n + kFmlsWarps - 1) / kFmlsWarps, (long long)nsm * std::max(1, per_sm)));
-  const size_t slot_bytes = ((((size_t)kSlotInts * nd * sizeof(int) + 15) & ~(size_t)15) +
+  const size_t slot_bytes = (align16((size_t)kSlotInts * nd * sizeof(int)) +
                              (size_t)kSlotDoubles * nd * sizeof(double) + 255) & ~(size_t)255;
   const size_t warps = (size_t)blocks * kFmlsWarps;
   if (warps > p->scratch_warps) {

@@ -59,6 +59,8 @@ struct Tables {
   // (l, m) four of them (dsqrt_index); NULL computes them on the spot (the
   // values are the same: a correctly rounded square root of an exact integer)
   const double* dsqrt = nullptr;
+  // optional: sh2amp transposed, [nsh][ndir] (the device reads it coalesced)
+  const double* sh2amp_t = nullptr;
 };
 
 // Slots of Tables::dsqrt for degree l, order m (0 <= m <= l <= lmax):
@@ -76,22 +78,29 @@ FMLS_HD inline double dsqrt_value(int l, int m, int which) {
   return x > 0.0 ? sqrt(x) : 0.0;
 }
 
-struct Work {  // one voxel in flight; every array has ndir entries
+// One voxel in flight.  values, order and label have one entry per
+// direction, the lobe arrays one per lobe (at most one per direction), the
+// pending lists one per direction.  I is the type of the labels and lobe
+// links (a signed type that holds -1 and every lobe index), O that of the
+// order entries.
+template <class I, class O>
+struct WorkT {
   double* values;
-  int* order;
-  int* label;
-  int* parent;
-  int* neg;
+  O* order;
+  I* label;
+  I* parent;
+  I* neg;
   double* max_peak;
-  double* mean;       // [3 ndir]
+  double* mean;       // [3 lobes]
   double* integral;
-  int* peak_head;
-  int* peak_tail;
-  int* peak_next;
-  double* peak_dir;   // [3 ndir]; peak p was created with lobe p
+  I* peak_head;
+  I* peak_tail;
+  I* peak_next;
+  double* peak_dir;   // [3 lobes]; peak p was created with lobe p
   int* retro_dir;
   int* retro_lobe;
 };
+using Work = WorkT<int, int>;
 
 struct Fixel {  // fod2fixel's per-fixel values
   float mean_dir[3], peak_dir[3], integral, max_peak;
@@ -105,12 +114,14 @@ FMLS_HD inline bool before(const double* v, int ndir, int a, int b) {
   return fa > fb || (fa == fb && a < b);
 }
 
-FMLS_HD inline int root(const Work& w, int l) {
+template <class W>
+FMLS_HD inline int root(const W& w, int l) {
   while (w.parent[l] != l) l = w.parent[l];
   return l;
 }
 
-FMLS_HD inline void lobe_add(const Tables& t, const Work& w, int r, int d, double value) {
+template <class W>
+FMLS_HD inline void lobe_add(const Tables& t, const W& w, int r, int d, double value) {
   // FOD_lobe::add (fmls.h:82-91)
   const double* u = t.unit + 3 * d;
   double* m = w.mean + 3 * r;
@@ -121,7 +132,8 @@ FMLS_HD inline void lobe_add(const Tables& t, const Work& w, int r, int d, doubl
   w.integral[r] += fabs(value * wt);
 }
 
-FMLS_HD inline void lobe_merge(const Work& w, int a, int b) {
+template <class W>
+FMLS_HD inline void lobe_merge(const W& w, int a, int b) {
   // FOD_lobe::merge (fmls.h:111-126): b into a
   if (w.max_peak[b] > w.max_peak[a]) {
     w.max_peak[a] = w.max_peak[b];
@@ -144,7 +156,8 @@ FMLS_HD inline void lobe_merge(const Work& w, int a, int b) {
 // Returns the number of lobes created; *n_retro the pending assignments.
 // max_lobes bounds the lobe arrays of w: a voxel that would create more
 // returns -1 (the caller repeats it with larger arrays).
-FMLS_HD inline int grow(const Tables& t, const Work& w, int* n_retro, int max_lobes = 1 << 30) {
+template <class W>
+FMLS_HD inline int grow(const Tables& t, const W& w, int* n_retro, int max_lobes = 1 << 30) {
   int nl = 0, nr = 0;
   for (int d = 0; d < t.ndir; ++d) w.label[d] = -1;
   for (int k = 0; k < t.ndir; ++k) {
@@ -337,7 +350,8 @@ FMLS_HD inline int select_direction(const Tables& t, const double* p) {
 }
 
 // fmls.cpp:248-256: the pending ("retrospective") assignments, in order.
-FMLS_HD inline void assign_pending(const Tables& t, const Work& w, int nr) {
+template <class W>
+FMLS_HD inline void assign_pending(const Tables& t, const W& w, int nr) {
   for (int q = 0; q < nr; ++q) {
     const int d = w.retro_dir[q];
     lobe_add(t, w, root(w, w.retro_lobe[q]), d, w.values[d]);
@@ -349,7 +363,8 @@ FMLS_HD inline void assign_pending(const Tables& t, const Work& w, int nr) {
 // threshold (fmls.cpp:258-262).  A peak's starting direction is the one the
 // growing left, which finish_lobes changes only after refining that peak, so
 // the refinements of all such peaks can be computed beforehand, in parallel.
-FMLS_HD inline bool peak_candidate(const Tables& t, const Work& w, int p) {
+template <class W>
+FMLS_HD inline bool peak_candidate(const Tables& t, const W& w, int p) {
   const int r = root(w, p);
   return !w.neg[r] && !(w.integral[r] < t.integral_threshold);
 }
@@ -358,7 +373,8 @@ FMLS_HD inline bool peak_candidate(const Tables& t, const Work& w, int p) {
 // the Newton refinement of its peaks.  pre_val / pre_u (nullable): the
 // results of get_peak for every candidate peak p, computed beforehand.
 // Writes at most max_out fixels; returns how many lobes survive.
-FMLS_HD inline int finish_lobes(const Tables& t, const Work& w, const double* sh, int nl, Fixel* out, int max_out,
+template <class W>
+FMLS_HD inline int finish_lobes(const Tables& t, const W& w, const double* sh, int nl, Fixel* out, int max_out,
                                 const double* pre_val = nullptr, const double* pre_u = nullptr) {
   int nout = 0;
   for (int r = 0; r < nl; ++r) {
@@ -410,7 +426,8 @@ FMLS_HD inline int finish_lobes(const Tables& t, const Work& w, const double* sh
 }
 
 // fmls.cpp:248-301 after the growing: the pending assignments, then the lobes.
-FMLS_HD inline int finish(const Tables& t, const Work& w, const double* sh, int nl, int nr, Fixel* out,
+template <class W>
+FMLS_HD inline int finish(const Tables& t, const W& w, const double* sh, int nl, int nr, Fixel* out,
                           int max_out) {
   assign_pending(t, w, nr);
   return finish_lobes(t, w, sh, nl, out, max_out);

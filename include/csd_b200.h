@@ -458,8 +458,10 @@ void csd_fmls_destroy(csd_fmls* segmenter);
  * max_fixels lobes of a voxel are written, so a count above max_fixels asks
  * for another pass with more room.  A voxel with a non-finite coefficient
  * has no lobes.  Returns without synchronising; grows a per-warp scratch
- * buffer on first use.  Calls on one segmenter share that buffer: run them
- * on one stream, or use one segmenter per stream. */
+ * buffer on first use, and on first use allocates the state of one round of
+ * 16,384 voxels (about 230 MB for the 1281 directions; the voxels go in
+ * rounds of three launches).  Calls on one segmenter share those buffers:
+ * run them on one stream, or use one segmenter per stream. */
 int csd_fmls_segment(csd_fmls* segmenter, const float* fod, int64_t n_voxels, int64_t voxel_stride,
                      int64_t coef_stride, const uint8_t* mask, int max_fixels, int32_t* counts, float* fixels,
                      void* stream);

@@ -1,19 +1,25 @@
 // fod2fixel's FMLS segmenter on the GPU (MRtrix3 src/dwi/fmls.cpp:118-311).
 //
-// One warp a voxel.  The lanes compute the voxel's amplitudes on the ndir
-// (1281) directions in FP64 (SH -> amplitude matrix, L2-resident) into
-// shared memory and sort the direction indices by |amplitude| descending,
-// index ascending (the reference's multimap order), by a bitonic network
-// over the next power of two in shared memory.  The warp then grows the
-// lobes (grow_warp: the lanes look up a direction's neighbours, lane 0
-// applies the core's steps) with the direction labels and the lobes' state
-// in the warp's shared memory (up to kFmlsLobes lobes; a voxel that makes
-// more is grown again by lane 0 on its global slot), and lane 0 makes the
-// pending assignments.  The Newton refinements of the candidate peaks are independent of
-// one another, so the lanes compute them in parallel, and lane 0 finishes
-// the lobes (thresholds, the nearest-peak test, the fixels) from those
-// results.  The core is the same source the CPU tests build for the host and
-// compare with the oracle.
+// The voxels go in rounds of kFmlsChunk, each round three kernels:
+// - fmls_segment_kernel, a warp a voxel: the amplitudes on the ndir (1281)
+//   directions in FP64 (the SH -> amplitude matrix transposed, L2-resident)
+//   into the warp's global slot, their 64-bit sort keys sorted by a bitonic
+//   network in shared memory into the reference's multimap order
+//   (|amplitude| descending, index ascending), the lobes grown by the warp
+//   (grow_warp: the lanes look up a direction's neighbours, warp reductions
+//   decide, lane 0 applies the core's step) with 8-bit labels and up to
+//   kFmlsLobes lobes in shared memory, and lane 0's pending assignments.
+//   It leaves the voxel's state (labels, lobes) in global memory and lists
+//   the candidate peaks.  A voxel that makes more lobes is grown again and
+//   finished by lane 0 on its global slot.
+// - fmls_peak_kernel, a thread a listed peak: the Newton refinements, which
+//   are independent of one another (a peak's start changes only when that
+//   peak itself is refined).  A thread takes the next peak as soon as its
+//   own is done, so no voxel waits for its slowest peak.
+// - fmls_finish_kernel, a thread a voxel: thresholds, the nearest-peak test
+//   and the fixels from the refined peaks.
+// The core is the same source the CPU tests build for the host and compare
+// with the oracle.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,9 +34,10 @@ namespace csdb200 {
 int set_error(int code, const std::string& msg);  // csd_solver.cu
 }
 
-// Optional per-phase cycle counters (build with -DCSD_PHASE_TIMERS): lane 0
-// of each warp adds clock64() deltas of amplitudes / sort / growing / pending
-// assignments / Newton refinements / finishing to g_fmls_cycles.
+// Optional per-phase cycle counters of fmls_segment_kernel (build with
+// -DCSD_PHASE_TIMERS): lane 0 of each warp adds clock64() deltas of
+// amplitudes / sort / growing / pending assignments / state out to
+// g_fmls_cycles.
 #ifdef CSD_PHASE_TIMERS
 __device__ unsigned long long g_fmls_cycles[8];
 #define FMLS_T(var) const long long var = clock64()
@@ -82,6 +89,41 @@ __host__ __device__ inline size_t fmls_region_bytes(int nd, int sort_n) {
 __host__ __device__ inline size_t fmls_warp_bytes(int nd, int nsh, int sort_n) {
   return align16((size_t)nsh * sizeof(double)) + fmls_region_bytes(nd, sort_n);
 }
+
+// A voxel's state between the kernels, laid out as the tail of the growing
+// kernel's shared region (from the labels on): 8-bit labels [nd], the
+// lobes' 8-bit links (5 x kFmlsLobes), their doubles max_peak integral
+// mean(3) peak_dir(3), and the refined peaks' values (1) and directions (3).
+__host__ __device__ inline size_t fmls_state_bytes(int nd) {
+  return align16((size_t)nd) + align16((size_t)5 * kFmlsLobes) + (size_t)12 * kFmlsLobes * sizeof(double);
+}
+struct StateView {
+  WorkS w;
+  double* pre_val;
+  double* pre_u;
+};
+__device__ inline StateView state_view(unsigned char* st, int nd) {
+  StateView s{};
+  s.w.label = reinterpret_cast<int8_t*>(st);
+  int8_t* links = s.w.label + align16((size_t)nd);
+  s.w.parent = links;
+  s.w.neg = links + kFmlsLobes;
+  s.w.peak_head = links + 2 * kFmlsLobes;
+  s.w.peak_tail = links + 3 * kFmlsLobes;
+  s.w.peak_next = links + 4 * kFmlsLobes;
+  double* ld = reinterpret_cast<double*>(links + align16((size_t)5 * kFmlsLobes));
+  s.w.max_peak = ld;
+  s.w.integral = ld + kFmlsLobes;
+  s.w.mean = ld + 2 * kFmlsLobes;
+  s.w.peak_dir = ld + 5 * kFmlsLobes;
+  s.pre_val = ld + 8 * kFmlsLobes;
+  s.pre_u = ld + 9 * kFmlsLobes;
+  return s;
+}
+
+constexpr int kFmlsChunk = 16384;   // voxels per round of the three kernels
+constexpr int kPeakThreads = 128;   // threads a block of the peak kernel
+constexpr int kPeakShift = 7;       // a listed peak is (voxel in the round) << 7 | peak
 
 // fmls::grow (fmls.cpp:178-246) with the warp: for each direction in order,
 // lane e looks up the lobe of neighbour e (its label's root, if that lobe's
@@ -217,14 +259,20 @@ __device__ __forceinline__ int key_dir(unsigned long long k) { return 0x7FF - (i
 struct FmlsArgs {
   fmls::Tables t;
   const float* fod;
-  long long n, vs, cs;
+  long long n, vs, cs;  // voxels, voxel stride, coefficient stride
   const uint8_t* mask;
   int max_fixels;
   int32_t* counts;
   float* fixels;
-  char* scratch;
+  char* scratch;        // per-warp slots of the growing kernel
   long long slot_bytes;
   int sort_n;
+  long long v0;         // this round's first voxel; n - v0 > nc ... the round is [v0, v0 + nc)
+  int nc;
+  unsigned char* state;  // [nc] voxel states (fmls_state_bytes each)
+  int* vnl;              // [nc] lobes left to finish (0: written already)
+  int* peaks;            // [nc * kFmlsLobes] listed candidate peaks
+  int* counters;         // [0] peaks listed, [1] peaks taken by the peak kernel
 };
 
 __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __grid_constant__ FmlsArgs a) {
@@ -239,8 +287,6 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
   int8_t* slabel = reinterpret_cast<int8_t*>(region + align16((size_t)nd * 2));
   int8_t* links = slabel + align16((size_t)nd);
   double* ld = reinterpret_cast<double*>(links + align16((size_t)5 * kFmlsLobes));
-  double* pre_val = ld + 8 * kFmlsLobes;
-  double* pre_u = pre_val + kFmlsLobes;
 
   const long long gw = (long long)blockIdx.x * kFmlsWarps + wib;
   char* slot = a.scratch + gw * a.slot_bytes;
@@ -280,8 +326,11 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
   ws.mean = ld + 2 * kFmlsLobes;
   ws.peak_dir = ld + 5 * kFmlsLobes;
 
+  const size_t sb = fmls_state_bytes(nd);
   const long long nwarps = (long long)gridDim.x * kFmlsWarps;
-  for (long long v = gw; v < a.n; v += nwarps) {
+  for (long long c = gw; c < a.nc; c += nwarps) {
+    const long long v = a.v0 + c;
+    if (lane == 0) a.vnl[c] = 0;
     if (a.mask && !a.mask[v]) {
       if (lane == 0) a.counts[v] = 0;
       continue;
@@ -389,25 +438,130 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
     __syncwarp();
     fmls::Fixel* out = reinterpret_cast<fmls::Fixel*>(a.fixels + v * (long long)a.max_fixels * 8);
     if (in_smem) {
-      // the candidate peaks' Newton refinements, spread over the lanes
-      for (int p = lane; p < nl; p += 32) {
-        if (!fmls::peak_candidate(a.t, ws, p)) continue;
-        double u[3] = {ws.peak_dir[3 * p], ws.peak_dir[3 * p + 1], ws.peak_dir[3 * p + 2]};
-        pre_val[p] = fmls::get_peak(a.t, sh, u);
-        for (int k = 0; k < 3; ++k) pre_u[3 * p + k] = u[k];
+      // the voxel's state for the peak and finishing kernels: labels and
+      // links whole, the first nl entries of the lobes' doubles
+      unsigned char* gst = a.state + (size_t)c * sb;
+      {
+        const uint4* src = reinterpret_cast<const uint4*>(slabel);
+        uint4* dst = reinterpret_cast<uint4*>(gst);
+        const int nq = (int)((align16((size_t)nd) + align16((size_t)5 * kFmlsLobes)) / 16);
+        for (int i = lane; i < nq; i += 32) dst[i] = src[i];
       }
-      __syncwarp();
+      const StateView g = state_view(gst, nd);
+      for (int i = lane; i < nl; i += 32) {
+        g.w.max_peak[i] = ws.max_peak[i];
+        g.w.integral[i] = ws.integral[i];
+      }
+      for (int i = lane; i < 3 * nl; i += 32) {
+        g.w.mean[i] = ws.mean[i];
+        g.w.peak_dir[i] = ws.peak_dir[i];
+      }
+      // the candidate peaks, listed with one atomic a group of 32
+      for (int p0 = 0; p0 < nl; p0 += 32) {
+        const int p = p0 + lane;
+        const bool cand = p < nl && fmls::peak_candidate(a.t, ws, p);
+        const unsigned bal = __ballot_sync(0xffffffffu, cand);
+        int base = 0;
+        if (lane == 0 && bal) base = atomicAdd(a.counters, __popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (cand) a.peaks[base + __popc(bal & ((1u << lane) - 1u))] = (int)(c << kPeakShift) | p;
+      }
+      if (lane == 0) a.vnl[c] = nl;
       FMLS_T(t6);
       FMLS_ACC(4, t5, t6);
-      if (lane == 0) a.counts[v] = fmls::finish_lobes(a.t, ws, sh, nl, out, a.max_fixels, pre_val, pre_u);
-      FMLS_T(t7);
-      FMLS_ACC(5, t6, t7);
     } else {
       // lane 0 refines the peaks itself, in finish_lobes
       if (lane == 0) a.counts[v] = fmls::finish_lobes(a.t, wg, sh, nl, out, a.max_fixels);
     }
     __syncwarp();
   }
+}
+
+// The Newton refinements of every listed candidate peak of the round
+// (SH::get_peak, SH.h:515-560), a thread a peak.  A thread takes the next
+// listed peak as soon as its own has converged or run its 50 steps, so the
+// lanes of a warp stay busy whatever the peaks' step counts; the taking is
+// one atomic a warp for all its lanes that need a peak.  The peak's voxel's
+// coefficients sit in the thread's column of shared memory (FP32, as
+// given); results go to the voxel's state.
+struct ShColumn {
+  const float* p;
+  __device__ double operator[](int k) const { return (double)p[k * kPeakThreads]; }
+};
+
+__global__ void __launch_bounds__(kPeakThreads) fmls_peak_kernel(const __grid_constant__ FmlsArgs a) {
+  extern __shared__ __align__(16) float shcol[];  // [nsh][kPeakThreads]
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int nd = a.t.ndir, nsh = a.t.nsh;
+  const size_t sb = fmls_state_bytes(nd);
+  const int total = a.counters[0];
+  const ShColumn sh{shcol + tid};
+  int cur = -1;  // the peak this thread refines (its list entry)
+  bool live = true;
+  int it = 0;
+  double u[3] = {0.0, 0.0, 0.0};
+  for (;;) {
+    const bool need = live && cur < 0;
+    const unsigned nm = __ballot_sync(0xffffffffu, need);
+    if (nm) {
+      const int leader = __ffs(nm) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(a.counters + 1, __popc(nm));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const int idx = base + __popc(nm & ((1u << lane) - 1u));
+        if (idx < total) {
+          cur = a.peaks[idx];
+          const long long c = cur >> kPeakShift;
+          const int p = cur & ((1 << kPeakShift) - 1);
+          const float* src = a.fod + (a.v0 + c) * a.vs;
+          for (int k = 0; k < nsh; ++k) shcol[k * kPeakThreads + tid] = src[(long long)k * a.cs];
+          const StateView g = state_view(a.state + (size_t)c * sb, nd);
+          u[0] = g.w.peak_dir[3 * p];
+          u[1] = g.w.peak_dir[3 * p + 1];
+          u[2] = g.w.peak_dir[3 * p + 2];
+          it = 0;
+        } else {
+          live = false;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, cur >= 0)) break;
+    if (cur >= 0) {
+      double val;
+      const bool conv = fmls::get_peak_step(a.t, sh, u, &val);
+      if (conv || ++it == fmls::kPeakSteps) {
+        if (!conv) {
+          u[0] = u[1] = u[2] = NAN;
+          val = NAN;
+        }
+        const long long c = cur >> kPeakShift;
+        const int p = cur & ((1 << kPeakShift) - 1);
+        const StateView g = state_view(a.state + (size_t)c * sb, nd);
+        g.pre_val[p] = val;
+        g.pre_u[3 * p] = u[0];
+        g.pre_u[3 * p + 1] = u[1];
+        g.pre_u[3 * p + 2] = u[2];
+        cur = -1;
+      }
+    }
+  }
+}
+
+// fmls.cpp:258-301 for the round's voxels left by the growing kernel, a
+// thread a voxel: thresholds, the nearest-peak test with the refined peaks,
+// the fixels.
+__global__ void __launch_bounds__(128) fmls_finish_kernel(const __grid_constant__ FmlsArgs a) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.nc) return;
+  const int nl = a.vnl[c];
+  if (nl <= 0) return;
+  const int nd = a.t.ndir;
+  const StateView g = state_view(a.state + (size_t)c * fmls_state_bytes(nd), nd);
+  const long long v = a.v0 + c;
+  fmls::Fixel* out = reinterpret_cast<fmls::Fixel*>(a.fixels + v * (long long)a.max_fixels * 8);
+  a.counts[v] = fmls::finish_lobes(a.t, g.w, static_cast<const double*>(nullptr), nl, out, a.max_fixels,
+                                   g.pre_val, g.pre_u);
 }
 
 template <class T>
@@ -428,6 +582,11 @@ struct csd_fmls {
   int32_t *adj_off = nullptr, *adj = nullptr, *grid_off = nullptr, *grid = nullptr;
   char* scratch = nullptr;
   size_t scratch_warps = 0;
+  // one round's voxel states, lobe counts, peak list and counters
+  unsigned char* state = nullptr;
+  int* vnl = nullptr;
+  int* peaks = nullptr;
+  int* counters = nullptr;
 };
 
 extern "C" void csd_fmls_destroy(csd_fmls* p) {
@@ -443,6 +602,10 @@ extern "C" void csd_fmls_destroy(csd_fmls* p) {
   cudaFree(p->grid_off);
   cudaFree(p->grid);
   cudaFree(p->scratch);
+  cudaFree(p->state);
+  cudaFree(p->vnl);
+  cudaFree(p->peaks);
+  cudaFree(p->counters);
   delete p;
 }
 
@@ -550,10 +713,37 @@ extern "C" int csd_fmls_segment(csd_fmls* p, const float* fod, int64_t n, int64_
     if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_fmls_segment: ") + cudaGetErrorString(e));
     p->scratch_warps = warps;
   }
-  FmlsArgs a{p->t, fod, n, voxel_stride, coef_stride, mask, max_fixels, counts, fixels, p->scratch,
-             (long long)slot_bytes, sort_n};
-  fmls_segment_kernel<<<(unsigned)blocks, kFmlsWarps * 32, smem, static_cast<cudaStream_t>(stream)>>>(a);
-  e = cudaGetLastError();
+  if (!p->state) {
+    e = cudaMalloc(&p->state, (size_t)kFmlsChunk * fmls_state_bytes(nd));
+    if (e == cudaSuccess) e = cudaMalloc(&p->vnl, (size_t)kFmlsChunk * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&p->peaks, (size_t)kFmlsChunk * kFmlsLobes * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&p->counters, 2 * sizeof(int));
+    if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_fmls_segment: ") + cudaGetErrorString(e));
+  }
+  // the peak kernel: a persistent grid, its blocks' coefficient columns in shared memory
+  const size_t psmem = (size_t)nsh * kPeakThreads * sizeof(float);
+  int peak_per_sm = 0;
+  e = cudaFuncSetAttribute(fmls_peak_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&peak_per_sm, fmls_peak_kernel, kPeakThreads, psmem);
+  if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_fmls_segment: ") + cudaGetErrorString(e));
+  const unsigned peak_blocks = (unsigned)(nsm * std::max(1, peak_per_sm));
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // rounds of kFmlsChunk voxels: growing (a warp a voxel), the peaks (a thread
+  // a peak), finishing (a thread a voxel)
+  for (long long v0 = 0; v0 < n; v0 += kFmlsChunk) {
+    const int nc = (int)std::min<long long>(kFmlsChunk, n - v0);
+    FmlsArgs a{p->t, fod, n, voxel_stride, coef_stride, mask, max_fixels, counts, fixels, p->scratch,
+               (long long)slot_bytes, sort_n, v0, nc, p->state, p->vnl, p->peaks, p->counters};
+    e = cudaMemsetAsync(p->counters, 0, 2 * sizeof(int), st);
+    if (e != cudaSuccess) break;
+    const unsigned gblocks = (unsigned)std::min<long long>(blocks, (nc + kFmlsWarps - 1) / kFmlsWarps);
+    fmls_segment_kernel<<<gblocks, kFmlsWarps * 32, smem, st>>>(a);
+    fmls_peak_kernel<<<peak_blocks, kPeakThreads, psmem, st>>>(a);
+    fmls_finish_kernel<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) break;
+  }
   if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_fmls_segment: ") + cudaGetErrorString(e));
   return CSD_OK;
 }

@@ -214,8 +214,11 @@ FMLS_HD inline int grow(const Tables& t, const W& w, int* n_retro, int max_lobes
   return nl;
 }
 
-// SH::derivatives with the precomputed Legendre table (SH.h:569-650).
-FMLS_HD inline void derivatives(const Tables& t, const double* sh, double el, double az, double* out6) {
+// SH::derivatives with the precomputed Legendre table (SH.h:569-650).  SH
+// is anything that gives coefficient i as sh[i] (a double pointer, or a
+// view of FP32 coefficients, which convert to double exactly).
+template <class SH>
+FMLS_HD inline void derivatives(const Tables& t, const SH& sh, double el, double az, double* out6) {
   const double sel = sin(el), cel = cos(el);
   (void)cel;
   const bool atpole = sel < 1e-4;
@@ -292,32 +295,44 @@ FMLS_HD inline void derivatives(const Tables& t, const double* sh, double el, do
   out6[0] = amp; out6[1] = d_el; out6[2] = d_az; out6[3] = d2_el; out6[4] = d2_elaz; out6[5] = d2_az;
 }
 
-// SH::get_peak (SH.h:515-560): Newton steps from u; NaN when it fails.
-FMLS_HD inline double get_peak(const Tables& t, const double* sh, double* u) {
-  for (int it = 0; it < 50; ++it) {
-    const double az = atan2(u[1], u[0]);
-    const double el = atan2(hypot(u[0], u[1]), u[2]);
-    double dv[6];
-    derivatives(t, sh, el, az, dv);
-    double del = sqrt(dv[1] * dv[1] + dv[2] * dv[2]);
-    double daz = 0.0;
-    if (del != 0.0) {
-      daz = dv[2] / del;
-      del = dv[1] / del;
-    }
-    const double dSH_dt = daz * dv[2] + del * dv[1];
-    const double d2SH_dt2 = daz * daz * dv[5] + 2.0 * daz * del * dv[4] + del * del * dv[3];
-    double dt = d2SH_dt2 != 0.0 ? (-dSH_dt / d2SH_dt2) : kMaxDirChange;
-    if (dt < 0.0) dt = -dt;
-    if (dt > kMaxDirChange) dt = kMaxDirChange;
-    del *= dt;
-    daz *= dt;
-    u[0] += del * cos(az) * cos(el) - daz * sin(az);
-    u[1] += del * sin(az) * cos(el) + daz * cos(az);
-    u[2] -= del * sin(el);
-    const double n = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-    u[0] /= n; u[1] /= n; u[2] /= n;
-    if (dt < kAngleTolerance) return dv[0];
+// One Newton step of SH::get_peak (SH.h:515-560) from u (updated in
+// place).  Returns true when the step was below the angle tolerance: the
+// peak has converged and *val is the amplitude there.
+template <class SH>
+FMLS_HD inline bool get_peak_step(const Tables& t, const SH& sh, double* u, double* val) {
+  const double az = atan2(u[1], u[0]);
+  const double el = atan2(hypot(u[0], u[1]), u[2]);
+  double dv[6];
+  derivatives(t, sh, el, az, dv);
+  double del = sqrt(dv[1] * dv[1] + dv[2] * dv[2]);
+  double daz = 0.0;
+  if (del != 0.0) {
+    daz = dv[2] / del;
+    del = dv[1] / del;
+  }
+  const double dSH_dt = daz * dv[2] + del * dv[1];
+  const double d2SH_dt2 = daz * daz * dv[5] + 2.0 * daz * del * dv[4] + del * del * dv[3];
+  double dt = d2SH_dt2 != 0.0 ? (-dSH_dt / d2SH_dt2) : kMaxDirChange;
+  if (dt < 0.0) dt = -dt;
+  if (dt > kMaxDirChange) dt = kMaxDirChange;
+  del *= dt;
+  daz *= dt;
+  u[0] += del * cos(az) * cos(el) - daz * sin(az);
+  u[1] += del * sin(az) * cos(el) + daz * cos(az);
+  u[2] -= del * sin(el);
+  const double n = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+  u[0] /= n; u[1] /= n; u[2] /= n;
+  *val = dv[0];
+  return dt < kAngleTolerance;
+}
+
+// SH::get_peak: at most kPeakSteps Newton steps from u; NaN when it fails.
+constexpr int kPeakSteps = 50;
+template <class SH>
+FMLS_HD inline double get_peak(const Tables& t, const SH& sh, double* u) {
+  for (int it = 0; it < kPeakSteps; ++it) {
+    double val;
+    if (get_peak_step(t, sh, u, &val)) return val;
   }
   u[0] = u[1] = u[2] = NAN;
   return NAN;

@@ -180,3 +180,23 @@ def test_segment_matches_c_oracle_large(kw):
     same = np.minimum(rc, 16) == counts
     assert same.mean() >= 0.99
     np.testing.assert_allclose(fx[same], rf[same], rtol=1e-4, atol=1e-4)
+
+
+def test_segment_rounds_match_c_oracle():
+    """40,000 voxels: three rounds of the growing / peak / finishing kernels
+    (16,384 voxels a round, the last one partial), masked voxels among them;
+    every 8th voxel against the C restatement."""
+    import os as _os
+
+    from oracle import fmls_ref
+    rows = _fods(40000, 8, seed=321, noise=0.01).astype(np.float32)
+    mask = np.ones(len(rows), np.uint8)
+    mask[::7] = 0
+    counts, fx = _segment(rows, 8, mask=mask, max_fixels=16)
+    assert not counts[mask == 0].any()
+    idx = np.nonzero(mask)[0][::8]
+    rc, rf = fmls_ref.segment_batch_c(fmls_ref.Segmenter(8), rows[idx].astype(np.float64), max_out=16,
+                                      nthreads=_os.cpu_count() or 1)
+    same = np.minimum(rc, 16) == counts[idx]
+    assert same.mean() >= 0.99
+    np.testing.assert_allclose(fx[idx][same], rf[same], rtol=1e-4, atol=1e-4)

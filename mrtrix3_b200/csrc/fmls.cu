@@ -275,7 +275,7 @@ struct FmlsArgs {
   int* counters;         // [0] peaks listed, [1] peaks taken by the peak kernel
 };
 
-__global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __grid_constant__ FmlsArgs a) {
+__global__ void __launch_bounds__(kFmlsWarps * 32, 12) fmls_segment_kernel(const __grid_constant__ FmlsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nd = a.t.ndir, nsh = a.t.nsh, sort_n = a.sort_n;
@@ -483,16 +483,23 @@ __global__ void __launch_bounds__(kFmlsWarps * 32) fmls_segment_kernel(const __g
 // lanes of a warp stay busy whatever the peaks' step counts; the taking is
 // one atomic a warp for all its lanes that need a peak.  The peak's voxel's
 // coefficients sit in the thread's column of shared memory (FP32, as
-// given); results go to the voxel's state.
+// given), and so do the Legendre values of each step, interpolated once
+// from the table's two rows (PrecomputedAL::get) instead of at every use;
+// results go to the voxel's state.
 struct ShColumn {
   const float* p;
   __device__ double operator[](int k) const { return (double)p[k * kPeakThreads]; }
 };
+struct AlColumn {
+  const double* p;
+  __device__ double operator()(int l, int m) const { return p[(l * l / 4 + m) * kPeakThreads]; }
+};
 
 __global__ void __launch_bounds__(kPeakThreads) fmls_peak_kernel(const __grid_constant__ FmlsArgs a) {
-  extern __shared__ __align__(16) float shcol[];  // [nsh][kPeakThreads]
+  extern __shared__ __align__(16) double alcol[];  // [n_al][kPeakThreads], then the coefficients
   const int tid = threadIdx.x, lane = tid & 31;
-  const int nd = a.t.ndir, nsh = a.t.nsh;
+  const int nd = a.t.ndir, nsh = a.t.nsh, n_al = a.t.n_al;
+  float* shcol = reinterpret_cast<float*>(alcol + (size_t)n_al * kPeakThreads);  // [nsh][kPeakThreads]
   const size_t sb = fmls_state_bytes(nd);
   const int total = a.counters[0];
   const ShColumn sh{shcol + tid};
@@ -529,7 +536,15 @@ __global__ void __launch_bounds__(kPeakThreads) fmls_peak_kernel(const __grid_co
     if (!__any_sync(0xffffffffu, cur >= 0)) break;
     if (cur >= 0) {
       double val;
-      const bool conv = fmls::get_peak_step(a.t, sh, u, &val);
+      const bool conv = fmls::newton_step(
+          [&](double el, double az, double* dv) {
+            int row;
+            double f1, f2;
+            fmls::al_weights(a.t, el, &row, &f1, &f2);
+            for (int k = 0; k < n_al; ++k) alcol[k * kPeakThreads + tid] = fmls::al_value(a.t, row, f1, f2, k);
+            fmls::derivatives_with(a.t, sh, AlColumn{alcol + tid}, el, az, dv);
+          },
+          u, &val);
       if (conv || ++it == fmls::kPeakSteps) {
         if (!conv) {
           u[0] = u[1] = u[2] = NAN;
@@ -721,7 +736,7 @@ extern "C" int csd_fmls_segment(csd_fmls* p, const float* fod, int64_t n, int64_
     if (e != cudaSuccess) return csdb200::set_error(CSD_ERR_CUDA, std::string("csd_fmls_segment: ") + cudaGetErrorString(e));
   }
   // the peak kernel: a persistent grid, its blocks' coefficient columns in shared memory
-  const size_t psmem = (size_t)nsh * kPeakThreads * sizeof(float);
+  const size_t psmem = (size_t)p->t.n_al * kPeakThreads * sizeof(double) + (size_t)nsh * kPeakThreads * sizeof(float);
   int peak_per_sm = 0;
   e = cudaFuncSetAttribute(fmls_peak_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
   if (e == cudaSuccess)

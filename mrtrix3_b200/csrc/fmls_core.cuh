@@ -214,15 +214,9 @@ FMLS_HD inline int grow(const Tables& t, const W& w, int* n_retro, int max_lobes
   return nl;
 }
 
-// SH::derivatives with the precomputed Legendre table (SH.h:569-650).  SH
-// is anything that gives coefficient i as sh[i] (a double pointer, or a
-// view of FP32 coefficients, which convert to double exactly).
-template <class SH>
-FMLS_HD inline void derivatives(const Tables& t, const SH& sh, double el, double az, double* out6) {
-  const double sel = sin(el), cel = cos(el);
-  (void)cel;
-  const bool atpole = sel < 1e-4;
-  // PrecomputedAL::set / get (SH.h:435-460)
+// PrecomputedAL::set (SH.h:435-460): the table row at or below elevation
+// el and the weights of it and of the next row.
+FMLS_HD inline void al_weights(const Tables& t, double el, int* row, double* w1, double* w2) {
   double f2 = el / t.al_inc, f1;
   int i = (int)f2;
   if (i < 0) {
@@ -232,14 +226,28 @@ FMLS_HD inline void derivatives(const Tables& t, const SH& sh, double el, double
   } else {
     f2 -= i; f1 = 1.0 - f2;
   }
-  const double* p1 = t.al + (long long)i * t.n_al;
-  const double* p2 = p1 + t.n_al;
-  auto AL = [&](int l, int m) {
-    const int k = l * l / 4 + m;
-    double v = f1 * p1[k];
-    if (f2 != 0.0) v += f2 * p2[k];
-    return v;
-  };
+  *row = i;
+  *w1 = f1;
+  *w2 = f2;
+}
+
+// PrecomputedAL::get: entry k (= l^2/4 + m) interpolated between the rows
+// (the next row is read only with a non-zero weight).
+FMLS_HD inline double al_value(const Tables& t, int row, double f1, double f2, int k) {
+  const double* p1 = t.al + (long long)row * t.n_al;
+  double v = f1 * p1[k];
+  if (f2 != 0.0) v += f2 * p1[t.n_al + k];
+  return v;
+}
+
+// SH::derivatives (SH.h:569-650) given the interpolated Legendre values as
+// AL(l, m).  SH is anything that gives coefficient i as sh[i] (a double
+// pointer, or a view of FP32 coefficients, which convert to double exactly).
+template <class SH, class ALF>
+FMLS_HD inline void derivatives_with(const Tables& t, const SH& sh, const ALF& AL, double el, double az,
+                                     double* out6) {
+  const double sel = sin(el);
+  const bool atpole = sel < 1e-4;
   auto IDX = [](int l, int m) { return l * (l + 1) / 2 + m; };
   const int lmax = t.lmax;
   auto SQ = [&](int l, int m, int which) {
@@ -295,15 +303,26 @@ FMLS_HD inline void derivatives(const Tables& t, const SH& sh, double el, double
   out6[0] = amp; out6[1] = d_el; out6[2] = d_az; out6[3] = d2_el; out6[4] = d2_elaz; out6[5] = d2_az;
 }
 
+// SH::derivatives with the precomputed Legendre table (SH.h:569-650).
+template <class SH>
+FMLS_HD inline void derivatives(const Tables& t, const SH& sh, double el, double az, double* out6) {
+  int row;
+  double f1, f2;
+  al_weights(t, el, &row, &f1, &f2);
+  auto AL = [&](int l, int m) { return al_value(t, row, f1, f2, l * l / 4 + m); };
+  derivatives_with(t, sh, AL, el, az, out6);
+}
+
 // One Newton step of SH::get_peak (SH.h:515-560) from u (updated in
 // place).  Returns true when the step was below the angle tolerance: the
 // peak has converged and *val is the amplitude there.
-template <class SH>
-FMLS_HD inline bool get_peak_step(const Tables& t, const SH& sh, double* u, double* val) {
+// DER(el, az, dv) evaluates the six derivatives there.
+template <class DER>
+FMLS_HD inline bool newton_step(const DER& der, double* u, double* val) {
   const double az = atan2(u[1], u[0]);
   const double el = atan2(hypot(u[0], u[1]), u[2]);
   double dv[6];
-  derivatives(t, sh, el, az, dv);
+  der(el, az, dv);
   double del = sqrt(dv[1] * dv[1] + dv[2] * dv[2]);
   double daz = 0.0;
   if (del != 0.0) {
@@ -324,6 +343,10 @@ FMLS_HD inline bool get_peak_step(const Tables& t, const SH& sh, double* u, doub
   u[0] /= n; u[1] /= n; u[2] /= n;
   *val = dv[0];
   return dt < kAngleTolerance;
+}
+template <class SH>
+FMLS_HD inline bool get_peak_step(const Tables& t, const SH& sh, double* u, double* val) {
+  return newton_step([&](double el, double az, double* dv) { derivatives(t, sh, el, az, dv); }, u, val);
 }
 
 // SH::get_peak: at most kPeakSteps Newton steps from u; NaN when it fails.

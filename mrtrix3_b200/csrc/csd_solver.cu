@@ -316,7 +316,7 @@ struct ReuseLayout {
   static constexpr int US = hr_stride(N);                         // column stride of U (odd number of float4s)
   static constexpr int WARP_FLOATS = LSZ + kReuseMaxR * US + kReuseMaxR * kReuseKS;
   // threads per block (bounds the registers: U's column lives in N of them)
-  static constexpr int THREADS = N <= 45 ? 512 : (N <= 66 ? 384 : 256);
+  static constexpr int THREADS = N <= 45 ? 576 : (N <= 66 ? 384 : 256);
 };
 
 struct StateParams {

@@ -522,12 +522,35 @@ __global__ void __launch_bounds__(kInfThreads, 1) mlp_infer_tc_kernel(const __gr
     // chunks [ck0, ck1) of its row.
     {
       constexpr int kLdS = kInfIn + 1;  // odd row stride: rows in distinct banks
+      constexpr int kRowsPerWarp = kInfRows / (kInfThreads / 32);  // 8
+      constexpr int kInChunks = (kInfIn + 31) / 32;                 // 3 samples a lane
       float* Sraw = reinterpret_cast<float*>(smem + kInfH);
-      for (int rr = warp; rr < kInfRows; rr += kInfThreads / 32) {
-        const long long r = e0 + rr;
-        if (r < a.n) {
-          const float* d = a.dwi + (a.index ? (long long)a.index[r] : r) * a.vs;
-          for (int t = lane; t < a.n_in; t += 32) Sraw[rr * kLdS + t] = d[(long long)t * a.ts];
+      // warp w stages rows w, w + 16, ...: lane j < 8 reads row j's voxel
+      // index, then every sample load of the warp's rows is issued before
+      // any is stored
+      long long vox = -1;
+      if (lane < kRowsPerWarp) {
+        const long long r = e0 + warp + (kInfThreads / 32) * lane;
+        if (r < a.n) vox = a.index ? (long long)a.index[r] : r;
+      }
+      float xr[kRowsPerWarp][kInChunks];
+#pragma unroll
+      for (int j = 0; j < kRowsPerWarp; ++j) {
+        const long long vj = __shfl_sync(0xffffffffu, vox, j);
+        const float* d = a.dwi + (vj < 0 ? 0 : vj) * a.vs;
+#pragma unroll
+        for (int c = 0; c < kInChunks; ++c) {
+          const int t = lane + 32 * c;
+          xr[j][c] = (vj >= 0 && t < a.n_in) ? __ldg(d + (long long)t * a.ts) : 0.f;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kRowsPerWarp; ++j) {
+        const int rr = warp + (kInfThreads / 32) * j;
+#pragma unroll
+        for (int c = 0; c < kInChunks; ++c) {
+          const int t = lane + 32 * c;
+          if (t < a.n_in) Sraw[rr * kLdS + t] = xr[j][c];
         }
       }
       __syncthreads();

@@ -396,10 +396,10 @@ __global__ void __launch_bounds__(kFmlsWarps * 32, 12) fmls_segment_kernel(const
       }
       __syncwarp();
     }
-    // the order, written over the keys it was read from (chunk c's entries
+    // the order, written over the keys it was read from (a chunk's entries
     // land below the keys later chunks read)
-    for (int c = 0; c < nd; c += 32) {
-      const int k = c + lane;
+    for (int k0 = 0; k0 < nd; k0 += 32) {
+      const int k = k0 + lane;
       const int d = k < nd ? key_dir(keys[k]) : 0;
       __syncwarp();
       if (k < nd) order[k] = (uint16_t)d;

@@ -138,8 +138,12 @@ typedef struct csd_mlp csd_mlp;  /* the warm-start network, below */
 /* The phased method on HOST buffers (same layout as csd_dwi2fod_host):
  * per slab of voxels, csd_state_set, then -- when `net` is not NULL -- the
  * network's predicted first negative sets (csd_mlp_predict + csd_state_warm),
- * then csd_state_run until no voxel is active, then csd_state_fod.  Slab
- * uploads / downloads overlap the passes of the other slab.  Synchronous. */
+ * then the passes until no voxel is active, then csd_state_fod.  The slabs
+ * alternate between two streams and are all enqueued at once (each slab's
+ * passes as csd_state_run_async's niter + 2), so one slab's copies and tail
+ * passes overlap the other's work; knob 11 = 2 drives each slab with
+ * csd_state_run instead.  Synchronous; CSD_ERR_TIMEOUT if a bounded device
+ * wait gave up. */
 int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const float* dwi, int64_t n_voxels,
                             const uint8_t* mask, float* fod, uint8_t* status, uint8_t* iterations);
 
@@ -397,8 +401,10 @@ int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t vo
  * into (0 = 4), 9 the csd_amp2sh kernel (1 a dot product a thread, 2 FP64
  * FMA tiles, 3 FP64 tensor cores where they apply: nd <= 64, nSH <= 48;
  * 0 = the fastest that applies), 10 the warm-started phased method's later
- * solves from the warm set's stored factor (0 default = 1 on, 2 off).
- * Knobs 0-5, 7 and 8 leave the outputs unchanged bit for bit; knob 6 changes
+ * solves from the warm set's stored factor (0 default = 1 on, 2 off), 11
+ * csd_dwi2fod_host_phased enqueueing every slab's passes at once with no
+ * host round trips (0 default = 1 on, 2 off: one round trip per batch).
+ * Knobs 0-5, 7, 8 and 11 leave the outputs unchanged bit for bit; knob 6 changes
  * the FP32 summation order of the logits, knob 9 the FP64 summation order of
  * the coefficients, knob 10 the FP32 arithmetic of the later solves (same
  * iteration, results within the parity tolerance). */

@@ -19,7 +19,7 @@ import numpy as np
 from . import csd
 
 (KNOB_PERSISTENT, KNOB_SOLVE, KNOB_PROJ, KNOB_TC_PROJECTION, KNOB_SOLVE_KIND, KNOB_SET_KIND, KNOB_INFER,
- KNOB_CYCLE_JUMP, KNOB_HOST_SLABS, KNOB_AMP2SH_KIND, KNOB_REUSE) = range(11)
+ KNOB_CYCLE_JUMP, KNOB_HOST_SLABS, KNOB_AMP2SH_KIND, KNOB_REUSE, KNOB_HOST_ASYNC) = range(12)
 # the projection kernel is chosen before its blocks per SM (which only the
 # mma.sync kernel uses)
 CANDIDATES = {KNOB_PERSISTENT: [8, 12, 16], KNOB_SOLVE: [12, 16, 20], KNOB_SOLVE_KIND: [1, 2], KNOB_TC_PROJECTION: [1, 2],

@@ -66,6 +66,8 @@ static int g_fast_cycles = 0;
 static int g_host_slabs = 0;  // host-buffer phased entry point: most slabs per call (knob 8; 0 = 4)
 static int g_reuse = 0;       // later solves of warm-started voxels from their warm-set factor (knob 10: 0 default
                               // = on, 1 on, 2 off)
+static int g_host_async = 0;  // host-buffer phased entry point: every slab's passes enqueued without host round
+                              // trips (knob 11: 0 default = on, 1 on, 2 off: one round trip per batch of passes)
 static constexpr int kSetDefault = 2;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
 
@@ -2111,6 +2113,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: factor reuse is 0 (default), 1 on or 2 off");
       g_reuse = value;
       break;
+    case 11:
+      if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: asynchronous host slabs are 0 (default), 1 on or 2 off");
+      g_host_async = value;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -3015,21 +3021,27 @@ extern "C" int csd_solve_noalloc(const csd_shared* s, const csd_volume* v, void*
 // so the copies of one slab overlap the passes of the other.
 
 namespace {
+constexpr int kHostBufs = 8;  // buffer sets (and streams): slabs in flight at once
 struct PhasedHostWS {
   uint64_t sh_id = 0;  // the csd_shared the states were made for (ids are never reused; addresses can be)
   int64_t cap = 0;
-  csd_state* st[2] = {nullptr, nullptr};
-  float* dwi[2] = {nullptr, nullptr};
-  float* fod[2] = {nullptr, nullptr};
-  uint8_t* small[2] = {nullptr, nullptr};   // mask | status | iterations
-  uint32_t* warm[2] = {nullptr, nullptr};
-  cudaStream_t stream[2] = {nullptr, nullptr};
+  int nbuf = 0;  // buffer sets allocated (each with its stream)
+  csd_state* st[kHostBufs] = {};
+  float* dwi[kHostBufs] = {};
+  float* fod[kHostBufs] = {};
+  uint8_t* small[kHostBufs] = {};   // mask | status | iterations
+  uint32_t* warm[kHostBufs] = {};
+  cudaStream_t stream[kHostBufs] = {};
+  int* hres = nullptr;  // pinned: per slab, voxels still active after its passes and the timed-out flag
+  int64_t hres_cap = 0;
+  uint8_t* hsi = nullptr;  // pinned staging of status and iterations (2 x voxels), copied out at the end
+  int64_t hsi_cap = 0;
 };
 std::mutex g_phws_mu;
 std::map<int, PhasedHostWS> g_phws;
 
 void release(PhasedHostWS& w) {
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < kHostBufs; ++i) {
     csd_state_destroy(w.st[i]);
     cudaFree(w.dwi[i]);
     cudaFree(w.fod[i]);
@@ -3040,6 +3052,13 @@ void release(PhasedHostWS& w) {
     w.small[i] = nullptr;
     w.warm[i] = nullptr;
   }
+  cudaFreeHost(w.hres);
+  w.hres = nullptr;
+  w.hres_cap = 0;
+  cudaFreeHost(w.hsi);
+  w.hsi = nullptr;
+  w.hsi_cap = 0;
+  w.nbuf = 0;
   w.cap = 0;
   w.sh_id = 0;
 }
@@ -3059,9 +3078,14 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
   const int nvol = s->h.nvol, nsh = s->h.nsh, nw = (s->h.nhr + 31) / 32;
   const int64_t nslab = std::min<int64_t>(g_host_slabs > 0 ? g_host_slabs : 4, std::max<int64_t>(1, n_voxels / 131072));
   const int64_t per = (n_voxels + nslab - 1) / nslab;
-  if (w.sh_id != s->id || w.cap < per) {
+  const bool async = g_host_async != 2;
+  // the asynchronous path gives every slab (up to kHostBufs) its own buffers
+  // and stream, so that all uploads can run ahead; the host-driven one
+  // alternates two
+  const int nb = async ? (int)std::max<int64_t>(2, std::min<int64_t>(nslab, kHostBufs)) : 2;
+  if (w.sh_id != s->id || w.cap < per || w.nbuf < nb) {
     release(w);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < nb; ++i) {
       int rc = csd_state_create(s, per, &w.st[i]);
       if (rc) return rc;
       CUDA_TRY(cudaMalloc(&w.dwi[i], (size_t)per * nvol * sizeof(float)));
@@ -3072,18 +3096,76 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
     }
     w.sh_id = s->id;
     w.cap = per;
+    w.nbuf = nb;
   }
-  // enqueue the first slab's upload, then per slab: enqueue the next upload
-  // on the other stream, solve this slab, enqueue its download
   auto upload = [&](int64_t k) -> int {
     const int64_t a = k * per, n = std::min(per, n_voxels - a);
-    const int b = (int)(k & 1);
+    const int b = (int)(k % nb);
     CUDA_TRY(cudaMemcpyAsync(w.dwi[b], dwi + a * nvol, (size_t)n * nvol * sizeof(float), cudaMemcpyHostToDevice,
                              w.stream[b]));
     if (mask) CUDA_TRY(cudaMemcpyAsync(w.small[b], mask + a, (size_t)n, cudaMemcpyHostToDevice, w.stream[b]));
     return 0;
   };
-  int rc = upload(0);
+  int rc = 0;
+  if (async) {
+    // every slab enqueued at once, slab k on stream k % nb with that
+    // stream's buffers (the stream orders their reuse): upload, inference,
+    // the phased run as csd_state_run_async's fixed passes (niter + 2, so
+    // complete; a pass with nothing left returns at once), FODs, download.
+    // One slab's tail of nearly empty passes then overlaps the other's work.
+    if (w.hres_cap < nslab) {
+      cudaFreeHost(w.hres);
+      w.hres = nullptr;
+      w.hres_cap = 0;
+      CUDA_TRY(cudaMallocHost(&w.hres, (size_t)nslab * 2 * sizeof(int)));
+      w.hres_cap = nslab;
+    }
+    // status and iterations go through pinned staging: a copy into pageable
+    // memory would hold the host until that slab is done
+    if ((status || iterations) && w.hsi_cap < n_voxels) {
+      cudaFreeHost(w.hsi);
+      w.hsi = nullptr;
+      w.hsi_cap = 0;
+      CUDA_TRY(cudaMallocHost(&w.hsi, (size_t)n_voxels * 2));
+      w.hsi_cap = n_voxels;
+    }
+    if (net)
+      for (int i = 0; i < nb; ++i)  // the warm-set factor storage, once
+        if (!w.st[i]->Lst && (rc = csd_state_warm(w.st[i], w.warm[i], w.stream[i]))) return rc;
+    for (int64_t k = 0; k < nslab; ++k) {
+      const int64_t a = k * per, n = std::min(per, n_voxels - a);
+      if (n <= 0) break;
+      const int b = (int)(k % nb);
+      cudaStream_t st = w.stream[b];
+      csd_state* S = w.st[b];
+      if ((rc = upload(k))) return rc;
+      const uint8_t* dmask = mask ? w.small[b] : nullptr;
+      if (net && (rc = csd_mlp_predict(net, w.dwi[b], n, nvol, 1, dmask, 0.f, w.warm[b], st))) return rc;
+      if ((rc = csd_state_run_async(S, w.dwi[b], n, nvol, 1, dmask, net ? w.warm[b] : nullptr, S->async_passes, st)))
+        return rc;
+      uint8_t* dst = w.small[b] + per;
+      uint8_t* dit = w.small[b] + 2 * per;
+      if ((rc = csd_state_fod(S, w.fod[b], nsh, status ? dst : nullptr, iterations ? dit : nullptr, nullptr, st)))
+        return rc;
+      CUDA_TRY(cudaMemcpyAsync(w.hres + 2 * k, S->acount + 2 * S->async_cur, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaMemcpyAsync(w.hres + 2 * k + 1, S->counter + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+      if (status) CUDA_TRY(cudaMemcpyAsync(w.hsi + a, dst, (size_t)n, cudaMemcpyDeviceToHost, st));
+      if (iterations) CUDA_TRY(cudaMemcpyAsync(w.hsi + n_voxels + a, dit, (size_t)n, cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaMemcpyAsync(fod + a * nsh, w.fod[b], (size_t)n * nsh * sizeof(float), cudaMemcpyDeviceToHost, st));
+    }
+    for (int i = 0; i < nb; ++i) CUDA_TRY(cudaStreamSynchronize(w.stream[i]));
+    if (status) std::memcpy(status, w.hsi, (size_t)n_voxels);
+    if (iterations) std::memcpy(iterations, w.hsi + n_voxels, (size_t)n_voxels);
+    for (int64_t k = 0; k < nslab && k * per < n_voxels; ++k) {
+      if (w.hres[2 * k + 1]) return fail(CSD_ERR_TIMEOUT, "csd_dwi2fod_host_phased: a bounded wait timed out");
+      if (w.hres[2 * k]) return fail(CSD_ERR_CUDA, "csd_dwi2fod_host_phased: voxels left iterating after niter + 2 passes");
+    }
+    return CSD_OK;
+  }
+  // host round trips: enqueue the first slab's upload, then per slab:
+  // enqueue the next upload on the other stream, solve this slab, enqueue
+  // its download
+  rc = upload(0);
   if (rc) return rc;
   for (int64_t k = 0; k < nslab; ++k) {
     const int64_t a = k * per, n = std::min(per, n_voxels - a);

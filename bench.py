@@ -43,15 +43,12 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustain
 WORKLOAD = ("140x140x96 synthetic DWI (mask ~45%: 846,816 voxels), 6 b=0 + 60 b=3000 directions, lmax 8, "
             "300 constraint directions, SNR U[15,40]")
 WEIGHTS = os.path.join(ROOT, "mrtrix3_b200", "data", "warmstart_c5.npz")
-# DRAM bytes per launch of csd_solve_kernel<45> from ncu on a 262,144-voxel
-# case (profiles/csd_solve_kernel_45.md), scaled to this workload's voxels
-# solved per launch; None until measured.
-# DRAM bytes (read + write) per solved voxel of csd_solve_kernel<45>, from
-# one ncu capture of its first launch on a 64^3 warm-started volume (262,144
-# solves: 126.4 MB read + 47.1 MB written); see
-# profiles/csd_solve_kernel_45.md.  The per-launch traffic reported below
-# scales it by the voxels each launch solves.
-SOLVE_DRAM_BYTES_PER_VOXEL = (126.449152e6 + 47.146496e6) / 262144
+# DRAM bytes (read + write) per solve of the dominant solve kernels, each
+# from one ncu capture on a 64^3 warm-started volume (profiles/): the
+# per-launch traffic reported below scales it by the solves of a launch.
+# None where no capture of the current kernel exists.
+SOLVE_DRAM_BYTES_PER_VOXEL = None   # csd_solve_kernel<45> on pre-assembled systems
+REUSE_DRAM_BYTES_PER_VOXEL = None   # csd_solve_reuse_kernel<45>
 
 
 FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
@@ -59,7 +56,8 @@ FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 # The numerics of the timed path (csd_params defaults, include/csd_b200.h).
 PRECISION = {
     "projection": "tcgen05, fp16 hi+lo splits of HR_trans and F (3 products, fp32 accumulate: 22 bits)",
-    "assembly": "mma.sync m16n8k16 on the fp16 hi+lo split of HR_trans, fp32 accumulate",
+    "assembly": ("tcgen05 (csd_assemble_tc_kernel): 0/1 set mask x HR_trans products split fp16 hi+lo, "
+                 "fp32 accumulate in tensor memory, 128 voxels a tile"),
     "factorisation": "fp32 Cholesky; fp64 re-factorisation when a pivot fails or (max L_ii/min L_ii)^2 > 1e6",
     "refine": "policy 3: one fp64-residual refinement after every solve of a voxel whose set cycles in fp32",
 }
@@ -678,29 +676,41 @@ def main():
                                                              axis=1)))}
 
     # ---- roofline of the solve kernels --------------------------------------
-    # csd_solve_kernel<45> (assembly + factorisation): per solve k n(n+1) +
-    # n^3/3 + 2n^2 (k = |negative set|); csd_solve_reuse_kernel<45> (warm-set
-    # factor + Woodbury correction by r changed directions): per solve
-    # r n(n-1) + r(r+1) n + 4 r n + n^2 + r^3.  Each against its own device time.
+    # csd_assemble_tc_kernel<45> (the rank-k assembly on tcgen05): k n(n+1)
+    # algorithmic flops per system (k = |negative set|); it issues
+    # 2 x 2 x 320 x 1120 dense FP16 flops per system (the 0/1 set mask times
+    # the hi and lo product tables, padded).  csd_solve_kernel<45> on the
+    # systems it leaves: n^3/3 + 2n^2 per solve (factorisation, substitutions).
+    # csd_solve_reuse_kernel<45> (warm-set factor + Woodbury correction by r
+    # changed directions): r n(n-1) + r(r+1) n + 4 r n + n^2 + r^3 per solve.
+    # Each against its own device time (CUDA events in the state's passes).
     n = 45
     peaks, peak_kind = load_peaks()
     full_solves = wstats["solved"] - wstats["reuse_solved"]
     full_ms = wstats["ms_solve"] - wstats["ms_reuse"]
-    full_flops = wstats["sum_neg"] * n * (n + 1) + full_solves * (n ** 3 / 3.0 + 2 * n * n)
+    asm_ms = wstats["ms_asm"]
+    asm_flops = wstats["sum_neg"] * n * (n + 1)
+    fact_flops = full_solves * (n ** 3 / 3.0 + 2 * n * n)
     rr = wstats["reuse_sum_changes"] / max(1.0, wstats["reuse_solved"])
     reuse_flops = wstats["reuse_solved"] * (rr * n * (n - 1) + rr * (rr + 1) * n + 4 * rr * n + n * n + rr ** 3)
     solve_launches = max(1.0, wstats["passes"])
     kernels = {
-        "csd_solve_kernel<45>": {"ms_per_step": full_ms, "solves": full_solves, "flops": full_flops},
+        "csd_solve_kernel<45>": {"ms_per_step": full_ms - asm_ms, "solves": full_solves,
+                                 "flops": fact_flops if asm_ms > 0 else fact_flops + asm_flops},
         "csd_solve_reuse_kernel<45>": {"ms_per_step": wstats["ms_reuse"], "solves": wstats["reuse_solved"],
                                        "flops": reuse_flops},
     }
+    if asm_ms > 0:
+        kernels["csd_assemble_tc_kernel<45>"] = {"ms_per_step": asm_ms, "solves": full_solves, "flops": asm_flops,
+                                                 "issued_tensor_flops": full_solves * 2 * 2 * 320 * 1120}
     dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
     kd = kernels[dom]
     achieved = kd["flops"] / max(1e-9, kd["ms_per_step"] / 1e3) / 1e12
     traffic = None
-    if dom == "csd_solve_kernel<45>" and SOLVE_DRAM_BYTES_PER_VOXEL is not None:
-        traffic = SOLVE_DRAM_BYTES_PER_VOXEL * full_solves / solve_launches
+    per_solve = {"csd_solve_kernel<45>": SOLVE_DRAM_BYTES_PER_VOXEL,
+                 "csd_solve_reuse_kernel<45>": REUSE_DRAM_BYTES_PER_VOXEL}.get(dom)
+    if per_solve is not None:
+        traffic = per_solve * kd["solves"] / solve_launches
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
                 "frac": achieved / peaks["bf16_tflops"], "traffic": traffic, "kernel": dom,
                 "peak_source": f"dense bf16 tensor peak, burst ({peak_kind})",
@@ -712,7 +722,13 @@ def main():
                 "fp32_simt_nominal_tflops": FP32_SIMT_NOMINAL_TFLOPS,
                 "frac_of_fp32_simt_nominal": achieved / FP32_SIMT_NOMINAL_TFLOPS,
                 "kernels": {k: {"ms_per_step": r4(v["ms_per_step"]), "solves": int(v["solves"]),
-                                "tflops": r4(v["flops"] / max(1e-9, v["ms_per_step"] / 1e3) / 1e12)}
+                                "tflops": r4(v["flops"] / max(1e-9, v["ms_per_step"] / 1e3) / 1e12),
+                                **({"issued_tensor_tflops": r4(v["issued_tensor_flops"]
+                                                               / max(1e-9, v["ms_per_step"] / 1e3) / 1e12),
+                                    "issued_frac_of_tensor_peak": r4(v["issued_tensor_flops"]
+                                                                     / max(1e-9, v["ms_per_step"] / 1e3) / 1e12
+                                                                     / peaks["bf16_tflops"])}
+                                   if "issued_tensor_flops" in v else {})}
                             for k, v in kernels.items()}}
 
     # ---- end to end through the host-buffer C ABI (pinned buffers) ---------

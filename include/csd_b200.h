@@ -202,6 +202,17 @@ int csd_state_stats(const csd_state* st, double* out);
  * only the arithmetic of each later W^-1 b differs.  csd_state_warm allocates
  * the factor storage (capacity x ~4.8 KB at lmax 8) on a state's first warm use. */
 int csd_state_reuse_stats(const csd_state* st, double* out);
+/* The phased solve's rank-k assembly (csd.h:255-262) on the tensor cores
+ * since the last csd_state_set: out[3] = launches of the assembly kernel
+ * (csd_assemble_tc_kernel: W = Mt_M + H[S]^T H[S] of 128 listed voxels at a
+ * time as the product of their 0/1 set masks with a table of HR_trans
+ * products, FP16 hi + lo, FP32 accumulation in tensor memory), their device
+ * milliseconds (recorded by csd_state_iterate / csd_state_run only; the
+ * solve time of csd_state_stats includes it), and how many systems one
+ * launch holds (the solve list runs in chunks of that many; 0: the
+ * assembly runs inside the solve kernel on mma.sync, as for more than 320
+ * constraint directions or launch knob 12 = 1). */
+int csd_state_assembly_stats(const csd_state* st, double* out);
 /* FP64 check of every finished voxel (converged or at niter): the residual
  * r = b - (Mt_M + HR_trans[S]^T HR_trans[S]) F of the voxel's final set S
  * (csd.h:255-264) in FP64; a voxel with max|r| > tol max|b| has its system
@@ -403,11 +414,15 @@ int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t vo
  * 0 = the fastest that applies), 10 the warm-started phased method's later
  * solves from the warm set's stored factor (0 default = 1 on, 2 off), 11
  * csd_dwi2fod_host_phased enqueueing every slab's passes at once with no
- * host round trips (0 default = 1 on, 2 off: one round trip per batch).
+ * host round trips (0 default = 1 on, 2 off: one round trip per batch), 12
+ * the phased solve's rank-k assembly (0 default = 2, 1 mma.sync inside the
+ * solve kernel, 2 tcgen05 ahead of it, up to 320 constraint directions;
+ * the grouped solve kernels of knob 4 always assemble with mma.sync).
  * Knobs 0-5, 7, 8 and 11 leave the outputs unchanged bit for bit; knob 6 changes
  * the FP32 summation order of the logits, knob 9 the FP64 summation order of
- * the coefficients, knob 10 the FP32 arithmetic of the later solves (same
- * iteration, results within the parity tolerance). */
+ * the coefficients, knob 10 the FP32 arithmetic of the later solves, knob
+ * 12 the FP32 summation order of the assembled systems (same iteration,
+ * results within the parity tolerance). */
 int csd_set_launch_config(int which, int value);
 
 /* ---- fod2fixel's FMLS FOD segmenter (src/dwi/fmls.cpp:118-311,

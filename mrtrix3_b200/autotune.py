@@ -19,10 +19,15 @@ import numpy as np
 from . import csd
 
 (KNOB_PERSISTENT, KNOB_SOLVE, KNOB_PROJ, KNOB_TC_PROJECTION, KNOB_SOLVE_KIND, KNOB_SET_KIND, KNOB_INFER,
- KNOB_CYCLE_JUMP, KNOB_HOST_SLABS, KNOB_AMP2SH_KIND, KNOB_REUSE, KNOB_HOST_ASYNC) = range(12)
+ KNOB_CYCLE_JUMP, KNOB_HOST_SLABS, KNOB_AMP2SH_KIND, KNOB_REUSE, KNOB_HOST_ASYNC, KNOB_ASSEMBLY) = range(13)
 # the projection kernel is chosen before its blocks per SM (which only the
-# mma.sync kernel uses)
-CANDIDATES = {KNOB_PERSISTENT: [8, 12, 16], KNOB_SOLVE: [12, 16, 20], KNOB_SOLVE_KIND: [1, 2], KNOB_TC_PROJECTION: [1, 2],
+# mma.sync kernel uses).  The solve kernel's warps per block apply to the
+# kernel the default tcgen05 assembly feeds (up to 32 warps at lmax 8; the
+# mma.sync-assembly kernel caps them at what its tables leave room for).
+# The grouped solve kernels assemble with mma.sync, whose FP32 sums differ
+# from the tcgen05 assembly's, so they are not tuning candidates: tuning
+# never changes results.
+CANDIDATES = {KNOB_PERSISTENT: [8, 12, 16], KNOB_SOLVE: [16, 24, 32], KNOB_TC_PROJECTION: [1, 2],
               KNOB_PROJ: [1, 2]}
 
 

@@ -33,7 +33,7 @@ EXPORTED = [
     "csd_shared_dwis", "csd_shared_matrix", "csd_solve", "csd_dwi2fod_host", "csd_state_create",
     "csd_state_destroy", "csd_state_set", "csd_state_warm", "csd_state_iterate", "csd_state_run",
     "csd_state_fod",
-    "csd_state_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_amp2sh_rician", "csd_icls_create",
+    "csd_state_stats", "csd_state_assembly_stats", "csd_dwi2fod_host_phased", "csd_sh2peaks", "csd_amp2sh", "csd_amp2sh_rician", "csd_icls_create",
     "csd_icls_destroy", "csd_icls_info", "csd_icls_solve", "csd_icls_solve_host", "csd_icls_create_standard", "csd_icls_solve_f64",
     "csd_amp2response_accumulate", "csd_dwi2tensor", "csd_fmls_create", "csd_fmls_create_default", "csd_fmls_destroy",
     "csd_fmls_segment",
@@ -115,6 +115,7 @@ def lib():
         L.csd_state_fod.argtypes = [vp, vp, i64, vp, vp, vp, vp]
         L.csd_state_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_state_reuse_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.csd_state_assembly_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.csd_state_check.argtypes = [vp, ctypes.c_double, ctypes.POINTER(i64), ctypes.POINTER(i64), vp]
         L.csd_state_run_async.argtypes = [vp, vp, i64, i64, i64, vp, vp, ctypes.c_int, vp]
         L.csd_state_async_result.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_int), vp]
@@ -534,6 +535,9 @@ class State:
         r = (ctypes.c_double * 3)()
         check(lib().csd_state_reuse_stats(self._h, r))
         d.update(reuse_solved=r[0], reuse_sum_changes=r[1], ms_reuse=r[2])
+        a = (ctypes.c_double * 3)()
+        check(lib().csd_state_assembly_stats(self._h, a))
+        d.update(asm_launches=a[0], ms_asm=a[1], asm_chunk=a[2])
         return d
 
     def iterate_all(self, max_passes: int = 0, stream=None) -> int:

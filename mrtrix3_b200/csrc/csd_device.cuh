@@ -1151,11 +1151,11 @@ __device__ bool solve_fp64(const Scheme& sc, int k, const WarpWS<N>& w, double* 
 // result when refine == 1.  Returns status flags (0x10 FP64 used, 0x20 the
 // FP64 factorisation failed too); bit 0x100 marks that w.W holds no usable
 // FP32 factor (the FP64 path ran).
-template <int N, bool SPLIT = false>
+template <int N, bool SPLIT = false, bool PRE = false>
 __device__ int assemble_solve(const Scheme& sc, const HTab<N>& H, int k, const WarpWS<N>& w, int lane,
                               float cond_thr, int refine, double* fp64_slot, long long* tacc = nullptr) {
   CSD_T0(t0);
-  assemble<N, SPLIT>(H, sc.MtMp, k, w, lane);
+  if constexpr (!PRE) assemble<N, SPLIT>(H, sc.MtMp, k, w, lane);  // PRE: w.W holds Mt_M + G^T G already
   // append b as row N: the factorisation then leaves y = L^-1 b in that row
   {
     float* bN = w.W + packoff(N);

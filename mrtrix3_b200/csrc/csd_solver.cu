@@ -12,6 +12,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -68,6 +69,9 @@ static int g_reuse = 0;       // later solves of warm-started voxels from their 
                               // = on, 1 on, 2 off)
 static int g_host_async = 0;  // host-buffer phased entry point: every slab's passes enqueued without host round
                               // trips (knob 11: 0 default = on, 1 on, 2 off: one round trip per batch of passes)
+static int g_asm_kind = 0;    // rank-k assembly of the phased solve (knob 12): 0 default, 1 mma.sync inside the
+                              // solve kernel, 2 tcgen05 (csd_assemble_tc_kernel) ahead of it (nhr <= 320)
+static constexpr int kAsmDefault = 2;
 static constexpr int kSetDefault = 2;
 static constexpr int kProjDefault = 2;  // tcgen05 where the table fits (nhr <= 320)
 
@@ -349,6 +353,11 @@ struct StateParams {
   int* err;             // set to 1 when a bounded wait times out
   unsigned long long* stats;  // [0] sum of |neg| over solves, [1] solves
   double* fp64_scratch;
+  // tcgen05 assembly: W of list entries [c0, c0 + ch), row e - c0 of Wg
+  float* Wg;                // [ch][packoff(N)] assembled systems
+  const __half* Ptc16;      // product table (asm_shape layout)
+  int pexp;                 // the product table holds HR_trans products * 2^-pexp
+  int c0, ch;               // list entries of this chunk (ch = INT_MAX: all)
   // set() inputs
   const float* dwi;
   long long vox_stride, vol_stride;
@@ -1210,18 +1219,266 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
 }
 
-// Solve pass: warp per voxel of the solve list (csd.h:255-266).
+// ---- tcgen05 rank-k assembly (sm_100a): W = Mt_M + H[neg]^T H[neg]
+// (csd.h:255-262) for a tile of 128 listed voxels at once, as the dense
+// product W[v][c] = Mt_M[c] + sum_d mask[v][d] P[d][c], with c = packoff(i)
+// + j the packed position of W(i, j) and P[d][c] = h_d[i] h_d[j].  The mask
+// is exact in FP16 (0 / 1), P is split into FP16 hi + lo (22 significant
+// bits), so two products per instruction pair accumulate in FP32 in tensor
+// memory: the rank-k update of every voxel of the tile in one pass over the
+// directions.  Roles (192 threads): warps 0-3 turn each voxel's set bits
+// into its row of the M=128 operand (one thread a voxel) and read the
+// accumulators back (tcgen05.ld, the warp's quarter of the lanes), adding
+// Mt_M and storing W to global memory for csd_solve_kernel<N, true>; warp 4
+// streams the product table through two shared-memory stages (bulk copies
+// completing on mbarriers); warp 5 issues the MMAs (N = NC columns a chunk,
+// K = 16 an instruction) into two tensor-memory buffers, so one chunk's
+// read-back overlaps the next chunk's products.  Every wait is bounded; a
+// time-out raises the error flag, and every role still reaches the final
+// barrier before the tensor memory is freed.
+constexpr int kAsmRows = 128;                    // voxels per tile (M)
+constexpr int kAsmK = 320;                       // directions (K), nhr <= 320
+constexpr int kAsmSlabK = 64;                    // directions per stage
+constexpr int kAsmSlabs = kAsmK / kAsmSlabK;     // stages per chunk
+constexpr int kAsmABytes = (kAsmK / 8) * kAsmRows * 16;
+
+struct AsmShape {
+  int wsz, nch, nc;   // packed W floats; column chunks of nc (a multiple of 16, <= 256)
+};
+__host__ __device__ constexpr AsmShape asm_shape(int n) {
+  return AsmShape{packoff(n), (packoff(n) + 255) / 256,
+                  (((packoff(n) + (packoff(n) + 255) / 256 - 1) / ((packoff(n) + 255) / 256)) + 15) / 16 * 16};
+}
+__host__ __device__ constexpr int asm_stage_bytes(int n) { return 2 * (kAsmSlabK / 8) * asm_shape(n).nc * 16; }
+__host__ __device__ constexpr int asm_smem_bytes(int n) { return kAsmABytes + 2 * asm_stage_bytes(n) + 128; }
+
+__device__ __forceinline__ void mbar_arrive1(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
+}
+
 template <int N>
-__global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(const __grid_constant__ StateParams P) {
+__global__ void __launch_bounds__(192, 1) csd_assemble_tc_kernel(const __grid_constant__ StateParams P) {
+  constexpr AsmShape S = asm_shape(N);
+  constexpr int NC = S.nc, NCH = S.nch, WSZ = S.wsz;
+  constexpr int STAGE = asm_stage_bytes(N);
+  constexpr uint32_t A_LBO = (kAsmRows / 8) * 128, B_LBO = NC * 16;
+  static_assert(2 * NC <= 512 && NC % 16 == 0 && NC >= 16 && NC <= 256, "chunk shape");
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + kAsmABytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + 2 * STAGE);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
+  const int end = min(n_in, P.c0 + P.ch);
+  const int ntiles = end > P.c0 ? (end - P.c0 + kAsmRows - 1) / kAsmRows : 0;
+  if ((int)blockIdx.x >= ntiles) return;  // the grid is an upper bound; before any allocation
+  const uint32_t bar0 = static_cast<uint32_t>(__cvta_generic_to_shared(bars));
+  // barriers: b_full[2], b_empty[2], acc_full[2], acc_empty[2], a_full, done
+  auto b_full = [&](int i) { return bar0 + 8u * (uint32_t)i; };
+  auto b_empty = [&](int i) { return bar0 + 8u * (uint32_t)(2 + i); };
+  auto acc_full = [&](int i) { return bar0 + 8u * (uint32_t)(4 + i); };
+  auto acc_empty = [&](int i) { return bar0 + 8u * (uint32_t)(6 + i); };
+  const uint32_t a_full = bar0 + 64u, done = bar0 + 72u;
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(b_full(i), 1);
+      mbar_init(b_empty(i), 1);
+      mbar_init(acc_full(i), 1);
+      mbar_init(acc_empty(i), kAsmRows);
+    }
+    mbar_init(a_full, kAsmRows);
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  if (warp == 0) tmem_alloc(static_cast<uint32_t>(__cvta_generic_to_shared(tmem_slot)), 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool failed = false;
+  if (warp == 4) {
+    // producer: the product table, chunk by chunk, slab by slab, for every tile
+    if (lane == 0) {
+      const unsigned char* src = reinterpret_cast<const unsigned char*>(P.Ptc16);
+      const uint32_t sB0 = static_cast<uint32_t>(__cvta_generic_to_shared(sB));
+      int it = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x)
+        for (int ch = 0; ch < NCH && !failed; ++ch)
+          for (int sl = 0; sl < kAsmSlabs; ++sl, ++it) {
+            const int st = it & 1;
+            const uint32_t ph = (uint32_t)(it >> 1) & 1u;
+            if (!mbar_wait(b_empty(st), ph ^ 1u)) {
+              failed = true;
+              break;
+            }
+            mbar_arrive_expect_tx(b_full(st), (uint32_t)STAGE);
+            bulk_copy_g2s(sB0 + (uint32_t)(st * STAGE), src + (size_t)(ch * kAsmSlabs + sl) * STAGE, (uint32_t)STAGE,
+                          b_full(st));
+          }
+      if (failed) atomicExch(P.err, 1);
+    }
+  } else if (warp == 5) {
+    // MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_f16(kAsmRows, NC);
+      const uint32_t aS = static_cast<uint32_t>(__cvta_generic_to_shared(sA));
+      const uint32_t bS = static_cast<uint32_t>(__cvta_generic_to_shared(sB));
+      int it = 0, ac = 0, tc = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x, ++tc) {
+        if (!mbar_wait(a_full, (uint32_t)tc & 1u)) {
+          failed = true;
+          break;
+        }
+        tc_fence_after();
+        for (int ch = 0; ch < NCH && !failed; ++ch, ++ac) {
+          const int buf = ac & 1;
+          if (!mbar_wait(acc_empty(buf), (((uint32_t)ac >> 1) & 1u) ^ 1u)) {
+            failed = true;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t dcol = tmem + (uint32_t)(buf * NC);
+          for (int sl = 0; sl < kAsmSlabs; ++sl, ++it) {
+            const int st = it & 1;
+            if (!mbar_wait(b_full(st), ((uint32_t)it >> 1) & 1u)) {
+              failed = true;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t bh = bS + (uint32_t)(st * STAGE), bl = bh + (uint32_t)(STAGE / 2);
+#pragma unroll
+            for (int ks = 0; ks < kAsmSlabK / 16; ++ks) {
+              const uint32_t ka = (uint32_t)(2 * (sl * (kAsmSlabK / 16) + ks)) * A_LBO;
+              const uint32_t kb = (uint32_t)(2 * ks) * B_LBO;
+              const uint64_t da = umma_smem_desc(aS + ka, A_LBO, 128);
+              umma_f16_ss(dcol, da, umma_smem_desc(bh + kb, B_LBO, 128), idesc, (sl > 0 || ks > 0) ? 1u : 0u);
+              umma_f16_ss(dcol, da, umma_smem_desc(bl + kb, B_LBO, 128), idesc, 1u);
+            }
+            umma_commit(b_empty(st));  // the stage is free once these products are done
+          }
+          if (failed) break;
+          umma_commit(acc_full(buf));  // the chunk's accumulators (and every earlier product) are done
+        }
+      }
+      if (failed) atomicExch(P.err, 1);
+      umma_commit(done);  // arrives once every product this thread issued has finished
+    }
+  } else {
+    // warps 0-3: one voxel a thread -- its operand row, then its accumulators
+    const int r = tid;
+    const float ps = pow2f(P.pexp);
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+    int ac = 0;
+    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+      const int e = P.c0 + tile * kAsmRows + r;
+      const bool live = e < end;
+      {
+        uint32_t words[kAsmK / 32];
+        const long long v = live ? (long long)P.act_in[e] : 0;
+#pragma unroll
+        for (int w = 0; w < kAsmK / 32; ++w) words[w] = (live && w < P.nw) ? P.newm[v * P.nw + w] : 0u;
+#pragma unroll
+        for (int kc = 0; kc < kAsmK / 8; ++kc) {
+          const uint32_t byte = (words[kc >> 2] >> (8 * (kc & 3))) & 0xFFu;
+          uint32_t q[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t)
+            q[t] = (((byte >> (2 * t)) & 1u) ? 0x3C00u : 0u) | (((byte >> (2 * t + 1)) & 1u) ? 0x3C000000u : 0u);
+          *reinterpret_cast<uint4*>(sA + kc * A_LBO + (r >> 3) * 128 + (r & 7) * 16) = make_uint4(q[0], q[1], q[2], q[3]);
+        }
+      }
+      fence_async_smem();
+      mbar_arrive1(a_full);
+      float* dst = P.Wg + (size_t)(e - P.c0) * WSZ;
+      for (int ch = 0; ch < NCH; ++ch, ++ac) {
+        const int buf = ac & 1;
+        const int ok = mbar_wait(acc_full(buf), ((uint32_t)ac >> 1) & 1u) ? 1 : 0;
+        if (!__all_sync(0xffffffffu, ok)) {
+          failed = true;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll 1
+        for (int j = 0; j < NC / 16; ++j) {
+          uint32_t x[16];
+          tmem_ld16(lane_base + (uint32_t)(buf * NC + 16 * j), x);
+          tmem_ld_wait();
+          const int c = ch * NC + 16 * j;
+          if (live && c < WSZ) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              if (c + 4 * q < WSZ) {
+                const float4 m = __ldg(reinterpret_cast<const float4*>(P.sc.MtMp + c + 4 * q));
+                float4 o;
+                o.x = fmaf(__uint_as_float(x[4 * q]), ps, m.x);
+                o.y = fmaf(__uint_as_float(x[4 * q + 1]), ps, m.y);
+                o.z = fmaf(__uint_as_float(x[4 * q + 2]), ps, m.z);
+                o.w = fmaf(__uint_as_float(x[4 * q + 3]), ps, m.w);
+                __stcg(reinterpret_cast<float4*>(dst + c + 4 * q), o);
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive1(acc_empty(buf));
+      }
+      if (failed) {
+        if (tid == 0) atomicExch(P.err, 1);
+        break;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    // no product may still be writing the tensor memory when it is freed (bounded)
+    mbar_wait(done, 0u);
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// Threads per block of csd_solve_kernel<N, true> (systems assembled by
+// csd_assemble_tc_kernel): no constraint tables and no assembly registers,
+// so more warps fit an SM.
+template <int N>
+struct PreSolveThreads {
+#ifdef CSD_PRE_THREADS45
+  static constexpr int value = N <= 45 ? CSD_PRE_THREADS45 : Dims<N>::THREADS;
+#else
+  static constexpr int value = N <= 45 ? 1024 : Dims<N>::THREADS;
+#endif
+};
+
+// Solve pass: warp per voxel of the solve list (csd.h:255-266).  PRE: the
+// list entries [c0, c0 + ch) whose systems csd_assemble_tc_kernel left in
+// Wg (row e - c0); otherwise every entry, assembled here (mma.sync).
+template <int N, bool PRE = false>
+__global__ void __launch_bounds__(PRE ? PreSolveThreads<N>::value : Dims<N>::SOLVE_THREADS, 1)
+    csd_solve_kernel(const __grid_constant__ StateParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int HS = Dims<N>::HS;
   const int nwarps = blockDim.x >> 5;
   const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
-  if ((long long)blockIdx.x * nwarps >= n_in) return;  // the grid is an upper bound
-  const HTab<N> H = load_htab<N>(smem, P.sc, P.nhr, false);
-  __syncthreads();
+  const int e0 = PRE ? P.c0 : 0;
+  const int end = PRE ? min(n_in, P.c0 + P.ch) : n_in;
+  if ((long long)e0 + (long long)blockIdx.x * nwarps >= end) return;  // the grid is an upper bound
+  HTab<N> H;
+  if constexpr (PRE) {
+    // only the refinement of cycling voxels reads the tables: from global memory
+    H.h32 = P.sc.H32;
+    H.hh = P.sc.H16;
+    H.hl = P.sc.H16 + (size_t)(P.nhr + 1) * Dims<N>::HS16;
+    H.nhr = P.nhr;
+    H.use32 = Dims<N>::KEEP32;
+    H.hs = P.sc.hscale;
+  } else {
+    H = load_htab<N>(smem, P.sc, P.nhr, false);
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  WarpWS<N> w = carve_ws<N>(smem + htab_bytes<N>(P.nhr, false) + warp * warp_ws_bytes<N>());
+  WarpWS<N> w = carve_ws<N>(smem + (PRE ? 0 : htab_bytes<N>(P.nhr, false)) + warp * warp_ws_bytes<N>());
   double* slot = P.fp64_scratch + (size_t)(blockIdx.x * nwarps + warp) * Dims<N>::WSZ;
   const int gw = blockIdx.x * nwarps + warp, nwt = gridDim.x * nwarps;
 #ifdef CSD_PHASE_TIMERS
@@ -1232,13 +1489,18 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
 #endif
   unsigned long long sum_k = 0, n_solved = 0;  // work counters, added once per warp
   WarpAppend app;
-  for (int e = gw; e < n_in; e += nwt) {
+  for (int e = e0 + gw; e < end; e += nwt) {
     CSD_T0(tl);
     const long long v = P.act_in[e];
     {
       uint32_t a_, r_;
       int nr_;
       if (reuse_route(P, v, lane, a_, r_, nr_)) continue;  // solved by csd_solve_reuse_kernel
+    }
+    if constexpr (PRE) {
+      const float4* src = reinterpret_cast<const float4*>(P.Wg + (size_t)(e - e0) * Dims<N>::WSZ);
+      float4* dst = reinterpret_cast<float4*>(w.W);
+      for (int i = lane; i < Dims<N>::WSZ / 4; i += 32) dst[i] = __ldcs(src + i);
     }
     for (int c = lane; c < N; c += 32) w.b[c] = P.b[v * N + c];
     for (int c = lane; c < HS; c += 32) w.F[c] = 0.f;
@@ -1252,7 +1514,7 @@ __global__ void __launch_bounds__(Dims<N>::SOLVE_THREADS, 1) csd_solve_kernel(co
     ++n_solved;
     CSD_T1(tacc, kPhList, tl);
     const int fl_all =
-        assemble_solve<N, true>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot, tacc);
+        assemble_solve<N, true, PRE>(P.sc, H, k, w, lane, P.cond_thr, (st & kCycling) ? 1 : 0, slot, tacc);
     const int fl = fl_all & 0x70;
     CSD_T0(tw);
     if (P.Lst && P.use_warm && P.warm && P.iters[v] == 1) {
@@ -1590,6 +1852,8 @@ struct csd_shared {
   std::vector<__half> H16_host;    // [2][nhr+1][HS16]: hi then lo
   std::vector<__half> Hp16_host;   // [2][npd][HS16]: projection table, hi then lo
   std::vector<__half> Htc16_host;  // tcgen05 projection table (core-matrix layout), hi then lo
+  std::vector<__half> Ptc16_host;  // tcgen05 assembly table: HR_trans products in packed-W order (AsmDims)
+  int pexp = 0;                    // the assembly table holds the products * 2^-pexp
   int npd = 0;                     // directions padded to a multiple of 320
   std::vector<float> MtMp_host;
   std::vector<float> rconvT_host;
@@ -1598,6 +1862,7 @@ struct csd_shared {
   __half* H16 = nullptr;
   __half* Hp16 = nullptr;
   __half* Htc16 = nullptr;
+  __half* Ptc16 = nullptr;
   double* H64 = nullptr;
   float* MtMp = nullptr;
   double* MtM64 = nullptr;
@@ -1726,6 +1991,32 @@ extern "C" int csd_shared_create(const csd_params* p, const double* grad, int n_
           s->Htc16_host[per + o] = s->H16_host[(size_t)(h.nhr + 1 + d) * HS16 + c];
         }
   }
+  if (h.nhr <= kAsmK) {
+    // rank-k assembly as one dense product per tile (csd_assemble_tc_kernel):
+    // column c = packoff(i) + j (j <= i) of W gets sum_d mask_d * h_d[i] h_d[j],
+    // so the table holds the products h_d[i] h_d[j] (FP64, scaled by an exact
+    // power of two that puts the largest in [2^14, 2^15)) split into FP16
+    // hi + lo, padding columns zero, laid out as the kernel's shared-memory
+    // stages: [chunk][slab][hi | lo][K chunk of 8][column][8 halves]
+    s->pexp = std::ilogb(hmax * hmax) - 14;
+    const double pdown = std::ldexp(1.0, -s->pexp);
+    const AsmShape a = asm_shape(n);
+    const size_t half_stage = (size_t)(kAsmSlabK / 8) * a.nc * 8;  // halves of one of hi / lo
+    s->Ptc16_host.assign((size_t)a.nch * kAsmSlabs * 2 * half_stage, __float2half_rn(0.f));
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j <= i; ++j) {
+        const int c = packoff(i) + j, ch = c / a.nc, cl = c % a.nc;
+        for (int d = 0; d < h.nhr; ++d) {
+          const double x = h.HR[(size_t)d * n + i] * h.HR[(size_t)d * n + j] * pdown;
+          const __half hi = __float2half_rn((float)x);
+          const __half lo = __float2half_rn((float)(x - (double)__half2float(hi)));
+          const int sl = d / kAsmSlabK, kc = (d % kAsmSlabK) / 8, e = d % 8;
+          const size_t o = ((size_t)(ch * kAsmSlabs + sl) * 2) * half_stage + ((size_t)kc * a.nc + cl) * 8 + e;
+          s->Ptc16_host[o] = hi;
+          s->Ptc16_host[o + half_stage] = lo;
+        }
+      }
+  }
   s->MtMp_host.assign((size_t)s->WSZ, 0.f);
   for (int i = 0; i < n; ++i)
     for (int j = 0; j <= i; ++j) s->MtMp_host[packoff(i) + j] = (float)h.MtM[(size_t)i * n + j];
@@ -1753,6 +2044,7 @@ static int ensure_device(const csd_shared* cs) {
   if ((rc = upload(&s->H16, s->H16_host))) return rc;
   if ((rc = upload(&s->Hp16, s->Hp16_host))) return rc;
   if (!s->Htc16_host.empty() && (rc = upload(&s->Htc16, s->Htc16_host))) return rc;
+  if (!s->Ptc16_host.empty() && (rc = upload(&s->Ptc16, s->Ptc16_host))) return rc;
   if ((rc = upload(&s->H64, h.HR))) return rc;
   if ((rc = upload(&s->MtMp, s->MtMp_host))) return rc;
   if ((rc = upload(&s->MtM64, h.MtM))) return rc;
@@ -1773,6 +2065,7 @@ extern "C" void csd_shared_destroy(csd_shared* s) {
     cudaFree(s->H16);
     cudaFree(s->Hp16);
     cudaFree(s->Htc16);
+    cudaFree(s->Ptc16);
     cudaFree(s->H64);
     cudaFree(s->MtMp);
     cudaFree(s->MtM64);
@@ -2117,6 +2410,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: asynchronous host slabs are 0 (default), 1 on or 2 off");
       g_host_async = value;
       break;
+    case 12:
+      if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: assembly is 0 (default), 1 mma.sync or 2 tcgen05");
+      g_asm_kind = value;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -2184,6 +2481,16 @@ struct csd_state {
   size_t gsmem[2] = {0, 0};
   int proj_blocks = 0;
   size_t proj_smem = 0;
+  float* Wg = nullptr;        // systems assembled by csd_assemble_tc_kernel, wg_entries rows of packoff(nSH)
+  long long wg_entries = 0;
+  int pre_warps = 0;          // launch shape of csd_solve_kernel<N, true>
+  size_t pre_smem = 0;
+  static constexpr int kAsmEv = 64;   // timed assembly launches between two host synchronisations
+  cudaEvent_t aev[2 * kAsmEv] = {};
+  int n_aev = 0;
+  bool time_asm = false;      // record events around csd_assemble_tc_kernel (synchronous runs only)
+  double ms_asm = 0;          // device time of csd_assemble_tc_kernel since the last set()
+  long long asm_launches = 0;
   long long passes = 0, projected = 0, solved = 0;  // work counters since the last set()
   unsigned long long* stats = nullptr;              // device: sum |neg|, solves
   unsigned long long* chk = nullptr;                // device: voxels checked, re-solved (csd_state_check)
@@ -2240,6 +2547,33 @@ int state_shape(csd_state* st) {
       CUDA_TRY(cudaFuncSetAttribute(csd_solve_group_kernel<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)st->gsmem[1]));
   }
+  if (st->sh->Ptc16) {
+    // tcgen05 assembly ahead of a table-free solve kernel: the solve list in
+    // chunks of wg_entries systems (at most ~4 GB of them)
+    int dev = 0, smem_max = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t wb = warp_ws_bytes<N>();
+    const size_t asm_smem = std::max<size_t>(asm_smem_bytes(N), 120 * 1024);  // one block (one TMEM owner) an SM
+    if (asm_smem <= (size_t)smem_max && wb <= (size_t)smem_max) {
+      st->pre_warps = (int)std::min<size_t>(PreSolveThreads<N>::value / 32, (size_t)smem_max / wb);
+      st->pre_smem = wb * st->pre_warps;
+      maxw = std::max(maxw, st->pre_warps);
+      const long long per = (long long)Dims<N>::WSZ * (long long)sizeof(float);
+      long long ent = std::min<long long>((st->cap + 127) / 128 * 128, std::max<long long>(4096, 4000000000LL / per));
+      if (const char* env = std::getenv("CSD_ASM_CHUNK")) {  // smaller chunks, to exercise chunking in tests
+        const long long c = std::atoll(env);
+        if (c >= 128) ent = std::min(ent, c);
+      }
+      ent = std::max<long long>(128, ent / 128 * 128);
+      CUDA_TRY(cudaMalloc(&st->Wg, (size_t)ent * per));
+      st->wg_entries = ent;
+      CUDA_TRY(cudaFuncSetAttribute(csd_solve_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)st->pre_smem));
+      CUDA_TRY(cudaFuncSetAttribute(csd_assemble_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)asm_smem));
+    }
+  }
   CUDA_TRY(cudaMalloc(&st->fp64, (size_t)ls.blocks * maxw * Dims<N>::WSZ * sizeof(double)));
   st->fp64_slots = (long long)ls.blocks * maxw;
   CUDA_TRY(cudaFuncSetAttribute(csd_solve_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem));
@@ -2275,6 +2609,19 @@ int state_shape(csd_state* st) {
   return 0;
 }
 
+// Device time of the csd_assemble_tc_kernel launches recorded since the last
+// host synchronisation (the stream has been synchronised).
+cudaError_t harvest_asm_time(csd_state* st) {
+  for (int i = 0; i < st->n_aev; ++i) {
+    float ms = 0.f;
+    const cudaError_t e = cudaEventElapsedTime(&ms, st->aev[2 * i], st->aev[2 * i + 1]);
+    if (e != cudaSuccess) return e;
+    st->ms_asm += ms;
+  }
+  st->n_aev = 0;
+  return cudaSuccess;
+}
+
 StateParams state_params(const csd_state* st) {
   StateParams P;
   std::memset(&P, 0, sizeof(P));
@@ -2305,6 +2652,7 @@ StateParams state_params(const csd_state* st) {
   P.err = st->counter + 1;
   P.stats = st->stats;
   P.fp64_scratch = st->fp64;
+  P.ch = 0x7fffffff;
   return P;
 }
 
@@ -2382,6 +2730,34 @@ int state_solve_launch(csd_state* st, const StateParams& P, cudaStream_t s) {
       CUDA_TRY(cudaGetLastError());
       return 0;
     }
+  }
+  if ((g_asm_kind ? g_asm_kind : kAsmDefault) == 2 && st->Wg && P.n_in > 0) {
+    // systems of each chunk of the list assembled on tcgen05, then solved
+    int dev = 0, nsm = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const size_t asm_smem = std::max<size_t>(asm_smem_bytes(N), 120 * 1024);
+    const int warps = g_tune_solve_warps > 0 ? std::min(st->pre_warps, g_tune_solve_warps) : st->pre_warps;
+    for (long long c0 = 0; c0 < P.n_in; c0 += st->wg_entries) {
+      StateParams Q = P;
+      Q.c0 = (int)c0;
+      Q.ch = (int)st->wg_entries;
+      Q.Wg = st->Wg;
+      Q.Ptc16 = st->sh->Ptc16;
+      Q.pexp = st->sh->pexp;
+      const long long cnt = std::min<long long>(P.n_in - c0, st->wg_entries);  // a bound: the count may be on the device
+      const int tiles = (int)((cnt + kAsmRows - 1) / kAsmRows);
+      const bool timed = st->time_asm && st->n_aev < csd_state::kAsmEv;
+      if (timed) CUDA_TRY(cudaEventRecord(st->aev[2 * st->n_aev], s));
+      csd_assemble_tc_kernel<N><<<std::max(1, std::min(tiles, nsm)), 192, asm_smem, s>>>(Q);
+      CUDA_TRY(cudaGetLastError());
+      if (timed) CUDA_TRY(cudaEventRecord(st->aev[2 * st->n_aev++ + 1], s));
+      ++st->asm_launches;
+      const int need = (int)std::min<long long>(st->blocks, (cnt + warps - 1) / warps);
+      csd_solve_kernel<N, true><<<std::max(need, 1), warps * 32, st->pre_smem, s>>>(Q);
+      CUDA_TRY(cudaGetLastError());
+    }
+    return 0;
   }
   const int warps = g_tune_solve_warps > 0 ? std::min(st->warps, g_tune_solve_warps) : st->warps;
   const int need = (int)std::min<long long>(st->blocks, (P.n_in + warps - 1) / warps);
@@ -2466,6 +2842,7 @@ extern "C" int csd_state_create(const csd_shared* s, int64_t capacity, csd_state
   CUDA_TRY(cudaMalloc(&st->arcount, (st->async_passes + 1) * sizeof(int)));
   for (auto& e : st->ev) CUDA_TRY(cudaEventCreate(&e));
   for (auto& e : st->bev) CUDA_TRY(cudaEventCreate(&e));
+  for (auto& e : st->aev) CUDA_TRY(cudaEventCreate(&e));
   int rc = 0;
   CSD_DISPATCH(n, rc = state_shape<NN>(st.get()));
   if (rc) return rc;
@@ -2495,12 +2872,15 @@ extern "C" void csd_state_destroy(csd_state* st) {
   cudaFree(st->stats);
   cudaFree(st->chk);
   cudaFree(st->fp64);
+  cudaFree(st->Wg);
   cudaFree(st->pcount);
   cudaFree(st->acount);
   cudaFree(st->arcount);
   for (auto& e : st->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : st->bev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : st->aev)
     if (e) cudaEventDestroy(e);
   delete st;
 }
@@ -2515,6 +2895,8 @@ extern "C" int csd_state_set(csd_state* st, const float* dwi, int64_t n_voxels, 
   st->cur = 0;
   st->passes = st->projected = st->solved = 0;
   st->ms_set = st->ms_project = st->ms_solve = st->ms_reuse = 0;
+  st->ms_asm = 0;
+  st->asm_launches = 0;
   st->launches = 0;
   CUDA_TRY(cudaMemsetAsync(st->counter, 0, sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(st->stats, 0, 4 * sizeof(unsigned long long), s));
@@ -2630,11 +3012,20 @@ extern "C" int csd_state_iterate(csd_state* st, int64_t* n_active, void* stream)
         Qf.n_in_dev = st->rcount;
       }
       CUDA_TRY(cudaEventRecord(st->ev[3], s));
+      const long long asm0 = st->asm_launches;
+      st->time_asm = true;
+      st->n_aev = 0;
       CSD_DISPATCH(st->sh->h.nsh, rc = state_solve_launch<NN>(st, Qf, s));
+      st->time_asm = false;
       if (rc) return rc;
       CUDA_TRY(cudaEventRecord(st->ev[1], s));
-      CUDA_TRY(cudaMemcpyAsync(&na, st->counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+      int na_err[2] = {0, 0};
+      CUDA_TRY(cudaMemcpyAsync(na_err, st->counter, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
       CUDA_TRY(cudaStreamSynchronize(s));
+      if (na_err[1]) return fail(CSD_ERR_TIMEOUT, "assembly: a bounded wait on the tensor cores timed out");
+      na = na_err[0];
+      CUDA_TRY(harvest_asm_time(st));
+      st->launches += st->asm_launches - asm0;
       float ms2 = 0.f, ms3 = 0.f;
       CUDA_TRY(cudaEventElapsedTime(&ms2, st->ev[2], st->ev[1]));
       CUDA_TRY(cudaEventElapsedTime(&ms3, st->ev[2], st->ev[3]));
@@ -2674,6 +3065,9 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
     CUDA_TRY(cudaEventRecord(st->bev[0], s));
     int rc = 0;
     int reuse_launches = 0;
+    const long long asm0 = st->asm_launches;
+    st->time_asm = true;
+    st->n_aev = 0;
     const long long pass0 = st->passes;  // passes since csd_state_set before this batch
     for (int p = 0; p < K; ++p) {
       StateParams P = state_params(st);
@@ -2720,9 +3114,12 @@ extern "C" int csd_state_run(csd_state* st, int max_passes, int64_t* n_active, v
     CUDA_TRY(cudaMemcpyAsync(cnt, st->pcount, (2 * K + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(&err, st->counter + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    if (err) return fail(CSD_ERR_TIMEOUT, "projection: a bounded wait on the tensor cores timed out");
+    st->time_asm = false;
+    if (err) return fail(CSD_ERR_TIMEOUT, "a bounded wait on the tensor cores timed out");
+    CUDA_TRY(harvest_asm_time(st));
     cnt[0] = U;
-    st->launches += 2 * K + reuse_launches;  // every enqueued pass launches its kernels (empty ones return at once)
+    // every enqueued pass launches its kernels (empty ones return at once)
+    st->launches += 2 * K + reuse_launches + (st->asm_launches - asm0);
     for (int p = 0; p < K; ++p) {
       if (cnt[2 * p] == 0) break;
       float a = 0.f, b = 0.f, c = 0.f;
@@ -2768,6 +3165,8 @@ extern "C" int csd_state_run_async(csd_state* st, const float* dwi, int64_t n_vo
   st->n_active = 0;
   st->passes = st->projected = st->solved = 0;
   st->ms_set = st->ms_project = st->ms_solve = st->ms_reuse = 0;
+  st->ms_asm = 0;
+  st->asm_launches = 0;
   CUDA_TRY(cudaMemsetAsync(st->acount, 0, (2 * passes + 2) * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(st->arcount, 0, (passes + 1) * sizeof(int), s));
   CUDA_TRY(cudaMemsetAsync(st->counter, 0, 2 * sizeof(int), s));
@@ -2859,6 +3258,14 @@ extern "C" int csd_state_stats(const csd_state* st, double* out) {
   out[5] = st->ms_project;
   out[6] = st->ms_solve;
   out[7] = (double)st->launches;
+  return CSD_OK;
+}
+
+extern "C" int csd_state_assembly_stats(const csd_state* st, double* out) {
+  if (!st || !out) return fail(CSD_ERR_INVALID, "csd_state_assembly_stats: invalid argument");
+  out[0] = (double)st->asm_launches;
+  out[1] = st->ms_asm;
+  out[2] = st->Wg ? (double)st->wg_entries : 0.0;
   return CSD_OK;
 }
 

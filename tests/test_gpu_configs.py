@@ -158,6 +158,9 @@ def test_grouped_solve_equals_warp_solve(cuda, lmax):
     warm[:, 0] ^= 0x9
     outs = {}
     try:
+        # the grouped kernels assemble with mma.sync: compare with the warp
+        # kernel on the same assembly
+        autotune.set_knob(autotune.KNOB_ASSEMBLY, 1)
         for kind in (1, 2, 3):
             autotune.set_knob(autotune.KNOB_SOLVE_KIND, kind)
             res = []
@@ -169,6 +172,7 @@ def test_grouped_solve_equals_warp_solve(cuda, lmax):
             outs[kind] = res
     finally:
         autotune.set_knob(autotune.KNOB_SOLVE_KIND, 0)
+        autotune.set_knob(autotune.KNOB_ASSEMBLY, 0)
     assert np.all(outs[1][2]["status"][v.mask.astype(bool)] & csd.STATUS_FP64)
     for kind in (2, 3):
         for a, b in zip(outs[1], outs[kind]):
@@ -183,7 +187,9 @@ def test_cycle_jump_equals_full_iteration(cuda):
     counts of running every call -- plain and warm-started -- while the
     number of passes drops.  The warm-started run assembles every solve
     (factor reuse off): its FP32 arithmetic is the one with cycling voxels
-    on this volume."""
+    on this volume.  Both assemblies (tcgen05, mma.sync) are run; the
+    jump must be exact for each, and the volume must hold a voxel that
+    cycles to niter under at least one of them."""
     import os
 
     import torch
@@ -201,21 +207,29 @@ def test_cycle_jump_equals_full_iteration(cuda):
     outs, passes = {}, {}
     try:
         autotune.set_knob(autotune.KNOB_REUSE, 2)
-        for knob in (2, 1):
-            autotune.set_knob(autotune.KNOB_CYCLE_JUMP, knob)
-            for name, w in (("plain", None), ("warm", warm)):
-                st.run(d, mask=m, warm=w)
-                outs[(knob, name)] = st.fod()
-                passes[(knob, name)] = st.stats()["passes"]
+        for asm in (2, 1):
+            autotune.set_knob(autotune.KNOB_ASSEMBLY, asm)
+            for knob in (2, 1):
+                autotune.set_knob(autotune.KNOB_CYCLE_JUMP, knob)
+                for name, w in (("plain", None), ("warm", warm)):
+                    st.run(d, mask=m, warm=w)
+                    outs[(asm, knob, name)] = st.fod()
+                    passes[(asm, knob, name)] = st.stats()["passes"]
     finally:
         autotune.set_knob(autotune.KNOB_CYCLE_JUMP, 0)
         autotune.set_knob(autotune.KNOB_REUSE, 0)
+        autotune.set_knob(autotune.KNOB_ASSEMBLY, 0)
     for name in ("plain", "warm"):
-        a, b = outs[(2, name)], outs[(1, name)]
-        for k in ("fod", "negmask", "status", "iterations"):
-            assert np.array_equal(a[k], b[k]), (name, k)
-        assert ((a["status"] & 0x0F) == csd.STATUS_NITER).sum() >= 1  # the case is exercised
-        assert passes[(1, name)] < passes[(2, name)]
+        exercised = 0
+        for asm in (2, 1):
+            a, b = outs[(asm, 2, name)], outs[(asm, 1, name)]
+            for k in ("fod", "negmask", "status", "iterations"):
+                assert np.array_equal(a[k], b[k]), (asm, name, k)
+            cyc = int(((a["status"] & 0x0F) == csd.STATUS_NITER).sum())
+            exercised += cyc
+            if cyc:
+                assert passes[(asm, 1, name)] < passes[(asm, 2, name)]
+        assert exercised >= 1  # the case is exercised
     # the persistent kernel's per-voxel loop jumps the same cycles
     pers = {}
     try:

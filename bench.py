@@ -47,7 +47,13 @@ WEIGHTS = os.path.join(ROOT, "mrtrix3_b200", "data", "warmstart_c5.npz")
 # from one ncu capture on a 64^3 warm-started volume (profiles/): the
 # per-launch traffic reported below scales it by the solves of a launch.
 # None where no capture of the current kernel exists.
-SOLVE_DRAM_BYTES_PER_VOXEL = None   # csd_solve_kernel<45> on pre-assembled systems
+# csd_solve_kernel<45> on assembled systems: the first solves of a warm-started
+# 64^3 volume (262,144 solves: 1293.9 MB read + 1307.2 MB written, the factor
+# store included), profiles/csd_solve_kernel_45.md
+SOLVE_DRAM_BYTES_PER_VOXEL = (1293.855e6 + 1307.167e6) / 262144
+# csd_assemble_tc_kernel<45>: the same pass's 262,144 systems (15.5 MB read +
+# 1104.4 MB written), profiles/csd_assemble_tc_kernel_45.md
+ASM_DRAM_BYTES_PER_SYSTEM = (15.497e6 + 1104.364e6) / 262144
 REUSE_DRAM_BYTES_PER_VOXEL = None   # csd_solve_reuse_kernel<45>
 
 
@@ -636,6 +642,14 @@ def main():
         nstats = st.stats()
     finally:
         autotune.set_knob(autotune.KNOB_REUSE, 0)
+    # ablation: both methods with the rank-k assembly inside the solve kernel
+    # (mma.sync) instead of on tcgen05 ahead of it
+    autotune.set_knob(autotune.KNOB_ASSEMBLY, 1)
+    try:
+        ms_warm_mma = timed(warm_step, args.steps)
+        ms_plain_mma = timed(plain_step, args.steps)
+    finally:
+        autotune.set_knob(autotune.KNOB_ASSEMBLY, 0)
     ms_pers_plain = timed(lambda: persistent_step(False), max(2, args.steps // 2))
     ms_pers_warm = timed(lambda: persistent_step(True), max(2, args.steps // 2))
 
@@ -659,6 +673,8 @@ def main():
                                  "solves_per_voxel": r4(nstats["solved"] / vol.n_masked)},
         "plain_phased": {"voxels_per_s": r4(rate(ms_plain)), "ms": r4(ms_plain), "passes": pstats["passes"],
                          "solves_per_voxel": r4(pstats["solved"] / vol.n_masked)},
+        "mma_sync_assembly": {"warm_ms": r4(ms_warm_mma), "plain_ms": r4(ms_plain_mma),
+                              "warm_vs_plain": r4(ms_plain_mma / ms_warm_mma)},
         "fp64_check": fp64_check,
         "persistent_plain_ms": r4(ms_pers_plain),
         "persistent_warm_ms": r4(ms_pers_warm),
@@ -676,53 +692,75 @@ def main():
                                                              axis=1)))}
 
     # ---- roofline of the solve kernels --------------------------------------
-    # csd_assemble_tc_kernel<45> (the rank-k assembly on tcgen05): k n(n+1)
-    # algorithmic flops per system (k = |negative set|); it issues
-    # 2 x 2 x 320 x 1120 dense FP16 flops per system (the 0/1 set mask times
-    # the hi and lo product tables, padded).  csd_solve_kernel<45> on the
-    # systems it leaves: n^3/3 + 2n^2 per solve (factorisation, substitutions).
-    # csd_solve_reuse_kernel<45> (warm-set factor + Woodbury correction by r
-    # changed directions): r n(n-1) + r(r+1) n + 4 r n + n^2 + r^3 per solve.
-    # Each against its own device time (CUDA events in the state's passes).
-    n = 45
+    # Per kernel, algorithmic flops and DRAM bytes per unit of work (n = 45,
+    # k = |negative set|, r = changed directions, WSZ = 1104 packed floats):
+    #   csd_assemble_tc_kernel<45>  (rank-k assembly on tcgen05) per system:
+    #     k n(n+1) flops; the set words in (40 B) and W out (4 WSZ = 4416 B).
+    #     It issues 2 x 2 x 320 x 1120 dense FP16 flops (0/1 mask x hi and lo
+    #     product tables, padded), reported beside.
+    #   csd_solve_kernel<45>  (factorisation + substitutions of assembled W)
+    #     per solve: n^3/3 + 2n^2 flops; W in (4416 B), b in (360 B), F out
+    #     (180 B), sets (80 B); a warm-started voxel's first solve also stores
+    #     its factor (4800 B).
+    #   csd_solve_reuse_kernel<45>  (stored factor + Woodbury correction) per
+    #     solve: r n(n-1) + r(r+1) n + 4 r n + n^2 + r^3 flops; the factor in
+    #     (4800 B), sets in (80 B), F out (180 B), sets out (80 B).
+    # Each against its own device time (CUDA events of the state's passes); the
+    # binding roof of a kernel is the one it comes closer to: measured HBM
+    # bandwidth for the bytes, the measured dense bf16 tensor peak for flops.
+    n, wsz = 45, 1104
     peaks, peak_kind = load_peaks()
     full_solves = wstats["solved"] - wstats["reuse_solved"]
     full_ms = wstats["ms_solve"] - wstats["ms_reuse"]
     asm_ms = wstats["ms_asm"]
-    asm_flops = wstats["sum_neg"] * n * (n + 1)
-    fact_flops = full_solves * (n ** 3 / 3.0 + 2 * n * n)
     rr = wstats["reuse_sum_changes"] / max(1.0, wstats["reuse_solved"])
-    reuse_flops = wstats["reuse_solved"] * (rr * n * (n - 1) + rr * (rr + 1) * n + 4 * rr * n + n * n + rr ** 3)
-    solve_launches = max(1.0, wstats["passes"])
     kernels = {
-        "csd_solve_kernel<45>": {"ms_per_step": full_ms - asm_ms, "solves": full_solves,
-                                 "flops": fact_flops if asm_ms > 0 else fact_flops + asm_flops},
-        "csd_solve_reuse_kernel<45>": {"ms_per_step": wstats["ms_reuse"], "solves": wstats["reuse_solved"],
-                                       "flops": reuse_flops},
+        "csd_solve_kernel<45>": {
+            "ms_per_step": full_ms - asm_ms, "solves": full_solves,
+            "flops": full_solves * (n ** 3 / 3.0 + 2 * n * n) + (0 if asm_ms > 0 else wstats["sum_neg"] * n * (n + 1)),
+            "bytes": full_solves * ((4 * wsz if asm_ms > 0 else 0) + 360 + 180 + 80) + vol.n_masked * 4800},
+        "csd_solve_reuse_kernel<45>": {
+            "ms_per_step": wstats["ms_reuse"], "solves": wstats["reuse_solved"],
+            "flops": wstats["reuse_solved"] * (rr * n * (n - 1) + rr * (rr + 1) * n + 4 * rr * n + n * n + rr ** 3),
+            "bytes": wstats["reuse_solved"] * (4800 + 80 + 180 + 80)},
     }
     if asm_ms > 0:
-        kernels["csd_assemble_tc_kernel<45>"] = {"ms_per_step": asm_ms, "solves": full_solves, "flops": asm_flops,
-                                                 "issued_tensor_flops": full_solves * 2 * 2 * 320 * 1120}
+        kernels["csd_assemble_tc_kernel<45>"] = {
+            "ms_per_step": asm_ms, "solves": full_solves, "flops": wstats["sum_neg"] * n * (n + 1),
+            "bytes": full_solves * (40 + 4 * wsz), "issued_tensor_flops": full_solves * 2 * 2 * 320 * 1120}
+    for v in kernels.values():
+        sec = max(1e-12, v["ms_per_step"] / 1e3)
+        v["tflops"] = v["flops"] / sec / 1e12
+        v["gbs"] = v["bytes"] / sec / 1e9
+        v["frac_tensor"] = v["tflops"] / peaks["bf16_tflops"]
+        v["frac_hbm"] = v["gbs"] / peaks["hbm_gbs"]
+        v["bound"] = "hbm" if v["frac_hbm"] >= v["frac_tensor"] else "tensor"
+    solve_launches = max(1.0, wstats["passes"])
     dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
     kd = kernels[dom]
-    achieved = kd["flops"] / max(1e-9, kd["ms_per_step"] / 1e3) / 1e12
-    traffic = None
     per_solve = {"csd_solve_kernel<45>": SOLVE_DRAM_BYTES_PER_VOXEL,
-                 "csd_solve_reuse_kernel<45>": REUSE_DRAM_BYTES_PER_VOXEL}.get(dom)
-    if per_solve is not None:
-        traffic = per_solve * kd["solves"] / solve_launches
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
-                "frac": achieved / peaks["bf16_tflops"], "traffic": traffic, "kernel": dom,
-                "peak_source": f"dense bf16 tensor peak, burst ({peak_kind})",
-                "algorithmic_flops_per_launch": kd["flops"] / solve_launches,
+                 "csd_solve_reuse_kernel<45>": REUSE_DRAM_BYTES_PER_VOXEL,
+                 "csd_assemble_tc_kernel<45>": ASM_DRAM_BYTES_PER_SYSTEM}.get(dom)
+    traffic = per_solve * kd["solves"] / solve_launches if per_solve is not None else None
+    if kd["bound"] == "hbm":
+        achieved, peak, unit = kd["gbs"], peaks["hbm_gbs"], "GB/s"
+        alg = {"algorithmic_bytes_per_launch": kd["bytes"] / solve_launches}
+        peak_source = f"HBM copy bandwidth ({peak_kind})"
+    else:
+        achieved, peak, unit = kd["tflops"], peaks["bf16_tflops"], "TFLOP/s"
+        alg = {"algorithmic_flops_per_launch": kd["flops"] / solve_launches}
+        peak_source = f"dense bf16 tensor peak, burst ({peak_kind})"
+    roofline = {"bound": kd["bound"], "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
+                "traffic": traffic, "kernel": dom, "peak_source": peak_source, **alg,
                 "avg_launch_ms": kd["ms_per_step"] / solve_launches,
                 "kernel_share_of_step": kd["ms_per_step"] / ms_warm,
                 # context: the factorisations and substitutions run on the FP32 SIMT pipes
                 # (148 SMs x 128 FMA lanes x 2 flops x 1.965 GHz, nominal, not measured)
                 "fp32_simt_nominal_tflops": FP32_SIMT_NOMINAL_TFLOPS,
-                "frac_of_fp32_simt_nominal": achieved / FP32_SIMT_NOMINAL_TFLOPS,
                 "kernels": {k: {"ms_per_step": r4(v["ms_per_step"]), "solves": int(v["solves"]),
-                                "tflops": r4(v["flops"] / max(1e-9, v["ms_per_step"] / 1e3) / 1e12),
+                                "bound": v["bound"], "tflops": r4(v["tflops"]), "gbs": r4(v["gbs"]),
+                                "frac_hbm": r4(v["frac_hbm"]), "frac_tensor": r4(v["frac_tensor"]),
+                                "frac_of_fp32_simt_nominal": r4(v["tflops"] / FP32_SIMT_NOMINAL_TFLOPS),
                                 **({"issued_tensor_tflops": r4(v["issued_tensor_flops"]
                                                                / max(1e-9, v["ms_per_step"] / 1e3) / 1e12),
                                     "issued_frac_of_tensor_peak": r4(v["issued_tensor_flops"]

@@ -195,7 +195,7 @@ int csd_state_stats(const csd_state* st, double* out);
 /* Factor reuse of a warm-started state since the last csd_state_set: out[3]
  * = solves that went through the warm set's stored Cholesky factor (a
  * Woodbury correction by the directions added to / dropped from the warm set,
- * at most 24; more, a voxel whose set cycles, or a first solve that needed
+ * at most 16; more, a voxel whose set cycles, or a first solve that needed
  * FP64 take the full assembly + factorisation), the sum of those changed-
  * direction counts, and the device milliseconds of that kernel.  No
  * counterpart in the reference: the iteration and its sets are csd.h:245-269's,

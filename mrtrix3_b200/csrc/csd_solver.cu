@@ -313,8 +313,14 @@ struct WarpAppend {
 // diagonal without pivoting.  The iteration, its sets and its stopping rule
 // are the plain method's; only the way each later W_S^-1 b is computed
 // changes (r^2 n + r n^2 / 2 + n^2 operations instead of k n^2 / 2 + n^3 / 3).
-constexpr int kReuseMaxR = 24;   // more changed directions than this: full solve
-constexpr int kReuseKS = 25;     // row stride of [K | rhs] in shared memory (rhs in column 24)
+#ifndef CSD_REUSE_MAXR
+#define CSD_REUSE_MAXR 16
+#endif
+#ifndef CSD_REUSE_THREADS45
+#define CSD_REUSE_THREADS45 768
+#endif
+constexpr int kReuseMaxR = CSD_REUSE_MAXR;  // more changed directions than this: full solve
+constexpr int kReuseKS = kReuseMaxR + 1;    // row stride of [K | rhs] in shared memory (rhs in the last column)
 
 template <int N>
 struct ReuseLayout {
@@ -322,7 +328,7 @@ struct ReuseLayout {
   static constexpr int US = hr_stride(N);                         // column stride of U (odd number of float4s)
   static constexpr int WARP_FLOATS = LSZ + kReuseMaxR * US + kReuseMaxR * kReuseKS;
   // threads per block (bounds the registers: U's column lives in N of them)
-  static constexpr int THREADS = N <= 45 ? 576 : (N <= 66 ? 384 : 256);
+  static constexpr int THREADS = N <= 45 ? CSD_REUSE_THREADS45 : (N <= 66 ? 384 : 256);
 };
 
 struct StateParams {
@@ -712,48 +718,88 @@ __global__ void __launch_bounds__(ReuseLayout<N>::THREADS, 1)
       for (uint32_t w = rem; w; w &= w - 1u) dl[pr++] = 32 * lane + __ffs(w) - 1;
     }
     __syncwarp();
-    const int d = lane < r ? dl[lane] : 0;
-    __syncwarp();
-    // U = L0^-1 C, column `lane` in registers
-    float u[N];
+    // U = L0^-1 C in shared memory (column j of U at Ub + j US), blocked by
+    // 8 rows: the r column lanes solve a block's diagonal part, then every
+    // lane takes one of the rows below it and subtracts the block's
+    // contribution from that row of every column.  (One column a lane over
+    // all 45 rows left 23 of 32 lanes idle for most of the kernel.)
     {
-      const float4* h = reinterpret_cast<const float4*>(P.sc.H32 + (size_t)d * HS);
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        const float4 x = lane < r ? __ldg(h + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-        if (4 * q < N) u[4 * q] = x.x;
-        if (4 * q + 1 < N) u[4 * q + 1] = x.y;
-        if (4 * q + 2 < N) u[4 * q + 2] = x.z;
-        if (4 * q + 3 < N) u[4 * q + 3] = x.w;
+      constexpr int Q4 = RL::US / 4;
+      for (int it = lane; it < r * Q4; it += 32) {
+        const int j = it / Q4, q = it - j * Q4;
+        const int dj = dl[j];
+        reinterpret_cast<float4*>(Ub + j * RL::US)[q] =
+            4 * q < HS ? __ldg(reinterpret_cast<const float4*>(P.sc.H32 + (size_t)dj * HS) + q)
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
+    __syncwarp();
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-      const float* Li = Lb + packoff(i);
-      float s0 = u[i], s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    for (int i0 = 0; i0 < N; i0 += 8) {
+      constexpr int BW = 8;
+      const int nb = N - i0 < BW ? N - i0 : BW;  // rows of this block (compile-time after unrolling)
+      if (lane < r) {
+        float* uc = Ub + lane * RL::US + i0;
+        float v[BW];
 #pragma unroll
-      for (int k4 = 0; k4 < i; k4 += 4) {
-        const float4 l = *reinterpret_cast<const float4*>(Li + k4);
-        s0 = fmaf(-l.x, u[k4], s0);
-        if (k4 + 1 < i) s1 = fmaf(-l.y, u[k4 + 1], s1);
-        if (k4 + 2 < i) s2 = fmaf(-l.z, u[k4 + 2], s2);
-        if (k4 + 3 < i) s3 = fmaf(-l.w, u[k4 + 3], s3);
+        for (int t = 0; t < BW; ++t) {
+          if (t < nb) {
+            const float* Li = Lb + packoff(i0 + t) + i0;
+            float s0 = uc[t], s1 = 0.f;
+#pragma unroll
+            for (int e = 0; e < t; e += 2) {
+              s0 = fmaf(-Li[e], v[e], s0);
+              if (e + 1 < t) s1 = fmaf(-Li[e + 1], v[e + 1], s1);
+            }
+            v[t] = (s0 + s1) * rd[i0 + t];
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < BW; ++t)
+          if (t < nb) uc[t] = v[t];
       }
-      u[i] = ((s0 + s1) + (s2 + s3)) * rd[i];
+      __syncwarp();
+      if (i0 + BW < N) {
+        // rows i0 + 8 .. N - 1: lane l takes rows i0 + 8 + l (+ 32)
+#pragma unroll
+        for (int rb = i0 + BW; rb < N; rb += 32) {
+          const int i = rb + lane;
+          if (i < N) {
+            const float4 la = *reinterpret_cast<const float4*>(Lb + packoff(i) + i0);
+            const float4 lb = *reinterpret_cast<const float4*>(Lb + packoff(i) + i0 + 4);
+            for (int j = 0; j < r; ++j) {
+              const float* uc = Ub + j * RL::US;
+              const float4 ua = *reinterpret_cast<const float4*>(uc + i0);
+              const float4 ub = *reinterpret_cast<const float4*>(uc + i0 + 4);
+              float s0 = uc[i], s1 = 0.f;
+              s0 = fmaf(-la.x, ua.x, s0);
+              s1 = fmaf(-la.y, ua.y, s1);
+              s0 = fmaf(-la.z, ua.z, s0);
+              s1 = fmaf(-la.w, ua.w, s1);
+              s0 = fmaf(-lb.x, ub.x, s0);
+              s1 = fmaf(-lb.y, ub.y, s1);
+              s0 = fmaf(-lb.z, ub.z, s0);
+              s1 = fmaf(-lb.w, ub.w, s1);
+              Ub[j * RL::US + i] = s0 + s1;
+            }
+          }
+        }
+      }
+      __syncwarp();
     }
-    // rhs_j = u_j . y0; U's columns to shared memory (zero padded to US)
+    // rhs_j = u_j . y0
     float rhs0 = 0.f, rhs1 = 0.f;
-#pragma unroll
-    for (int i = 0; i < N; i += 2) {
-      rhs0 = fmaf(u[i], y0[i], rhs0);
-      if (i + 1 < N) rhs1 = fmaf(u[i + 1], y0[i + 1], rhs1);
-    }
     if (lane < r) {
-      float4* uc = reinterpret_cast<float4*>(Ub + lane * RL::US);
+      const float4* uc = reinterpret_cast<const float4*>(Ub + lane * RL::US);
+      const float4* y4 = reinterpret_cast<const float4*>(y0);
 #pragma unroll
-      for (int q = 0; q < RL::US / 4; ++q)
-        uc[q] = make_float4(4 * q < N ? u[4 * q] : 0.f, 4 * q + 1 < N ? u[4 * q + 1] : 0.f,
-                            4 * q + 2 < N ? u[4 * q + 2] : 0.f, 4 * q + 3 < N ? u[4 * q + 3] : 0.f);
+      for (int q = 0; q < NQ; ++q) {  // only rows < N: y0's padding is not cleared
+        const float4 x = uc[q], y = y4[q];
+        rhs0 = fmaf(x.x, y.x, rhs0);
+        if (4 * q + 1 < N) rhs1 = fmaf(x.y, y.y, rhs1);
+        if (4 * q + 2 < N) rhs0 = fmaf(x.z, y.z, rhs0);
+        if (4 * q + 3 < N) rhs1 = fmaf(x.w, y.w, rhs1);
+      }
     }
     __syncwarp();
     // K = D + U^T U: pair p = j (j + 1) / 2 + i, i <= j, spread over the lanes

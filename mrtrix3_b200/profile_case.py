@@ -4,6 +4,7 @@
         [--method warm|plain|persistent|persistent_warm|predict|peaks|fod2fixel|amp2sh|msmt|tensor|amp2response]
         [--reps 2]
         [--projection mma|tcgen05] [--solve warp|group16|group8] [--amp2sh-kernel auto|row|tile|mma]
+        [--passes N]
 
 Every voxel is inside the volume (no mask); the scheme is 6 b=0 + 60 DW
 (lmax 8) or 8 b=0 + 90 DW (lmax 10).  Prints the state's work / time
@@ -26,6 +27,9 @@ def main():
     ap.add_argument("--projection", default="tcgen05", choices=["mma", "tcgen05"])
     ap.add_argument("--solve", default="warp", choices=["warp", "group16", "group8"])
     ap.add_argument("--amp2sh-kernel", default="auto", choices=["auto", "row", "tile", "mma"])
+    ap.add_argument("--passes", type=int, default=0,
+                    help="warm / plain: stop the phased run after this many passes (0: run to the end), so "
+                         "that the state's counters describe exactly the launches a profiler captured")
     a = ap.parse_args()
     import torch
 
@@ -140,6 +144,12 @@ def main():
             net.predict(d)
         elif a.method == "peaks":
             csd.sh2peaks(fod)
+        elif st is not None and a.passes > 0:
+            w = net.predict(d) if net is not None else None
+            st.set(d)
+            if w is not None:
+                st.warm(w)
+            st.iterate_all(max_passes=a.passes)
         elif st is not None:
             st.run(d, warm=net.predict(d) if net is not None else None)
         else:

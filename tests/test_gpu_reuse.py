@@ -85,7 +85,9 @@ def test_reuse_matches_oracle_and_full_solves(cuda, hr_dirs, lmax, nb0, ndw):
 
 def test_reuse_on_the_shipped_network(cuda, hr_dirs):
     """The benchmark's scheme warm-started by the shipped network: the reuse
-    takes most later solves and leaves the results on the oracle's."""
+    takes most later solves (>= 90%: a voxel whose set changed by more than
+    16 directions takes the full solve) and leaves the results on the
+    oracle's."""
     import torch
 
     from mrtrix3_b200.warmstart import WarmStartNet
@@ -105,7 +107,7 @@ def test_reuse_on_the_shipped_network(cuda, hr_dirs):
     finally:
         st.close()
     later = stt["solved"] - len(dwi)
-    assert stt["reuse_solved"] >= 0.95 * later, (stt["reuse_solved"], later)
+    assert stt["reuse_solved"] >= 0.90 * later, (stt["reuse_solved"], later)
     r = _rel(out["fod"], ref["F"])
     assert np.percentile(r, 99) <= 1e-4, (np.percentile(r, 99), r.max())
     assert np.mean(np.all(out["negmask"].view(np.uint32) == ref["negmask"], axis=1)) >= 0.995

@@ -54,7 +54,9 @@ SOLVE_DRAM_BYTES_PER_VOXEL = (1293.855e6 + 1307.167e6) / 262144
 # csd_assemble_tc_kernel<45>: the same pass's 262,144 systems (15.5 MB read +
 # 1104.4 MB written), profiles/csd_assemble_tc_kernel_45.md
 ASM_DRAM_BYTES_PER_SYSTEM = (15.497e6 + 1104.364e6) / 262144
-REUSE_DRAM_BYTES_PER_VOXEL = None   # csd_solve_reuse_kernel<45>
+# csd_solve_reuse_kernel<45>: its pass-2 launch on the same volume (247,196
+# reuse solves: 1304.8 MB read + 24.6 MB written), profiles/csd_solve_reuse_kernel_45.md
+REUSE_DRAM_BYTES_PER_VOXEL = (1304.825e6 + 24.625e6) / 247196
 
 
 FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12

@@ -326,7 +326,9 @@ template <int N>
 struct ReuseLayout {
   static constexpr int LSZ = packoff(N + 1) + ((N + 3) / 4) * 4;  // factor rows 0..N (row N = y0), then 1/L_ii
   static constexpr int US = hr_stride(N);                         // column stride of U (odd number of float4s)
-  static constexpr int WARP_FLOATS = LSZ + kReuseMaxR * US + kReuseMaxR * kReuseKS;
+  // a warp's block, rounded to 16 bytes: the next warp's factor is read as float4s
+  static constexpr int WARP_FLOATS = (LSZ + kReuseMaxR * US + kReuseMaxR * kReuseKS + 3) / 4 * 4;
+  static_assert(LSZ % 4 == 0 && US % 4 == 0 && WARP_FLOATS % 4 == 0, "float4 alignment of the warp blocks");
   // threads per block (bounds the registers: U's column lives in N of them)
   static constexpr int THREADS = N <= 45 ? CSD_REUSE_THREADS45 : (N <= 66 ? 384 : 256);
 };

@@ -139,11 +139,16 @@ typedef struct csd_mlp csd_mlp;  /* the warm-start network, below */
  * per slab of voxels, csd_state_set, then -- when `net` is not NULL -- the
  * network's predicted first negative sets (csd_mlp_predict + csd_state_warm),
  * then the passes until no voxel is active, then csd_state_fod.  The slabs
- * alternate between two streams and are all enqueued at once (each slab's
- * passes as csd_state_run_async's niter + 2), so one slab's copies and tail
- * passes overlap the other's work; knob 11 = 2 drives each slab with
- * csd_state_run instead.  Synchronous; CSD_ERR_TIMEOUT if a bounded device
- * wait gave up. */
+ * (at most 8 by default, knob 8) each get their own buffers and stream and
+ * are all enqueued at once, so the uploads run ahead and one slab's copies
+ * and tail passes overlap the others' work: each slab's passes are
+ * csd_state_run_async's, 16 of them (niter + 2 when slabs share buffers),
+ * and a slab with voxels still iterating after them is finished by
+ * csd_state_run on its own state after one host synchronisation (the same
+ * iteration, so the same outputs).  Knob 11 = 2 drives each slab with
+ * csd_state_run instead; knob 13 > 0 makes slab k's compute wait for slab
+ * k - knob's.  Synchronous; CSD_ERR_TIMEOUT if a bounded device wait gave
+ * up. */
 int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const float* dwi, int64_t n_voxels,
                             const uint8_t* mask, float* fod, uint8_t* status, uint8_t* iterations);
 
@@ -409,7 +414,7 @@ int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t vo
  * built-in default, 7 the jump of exactly periodic two-cycles to their
  * last call (1 on, 2 off; by default on in the phased method, off in the
  * persistent kernel), 8 the most slabs csd_dwi2fod_host_phased cuts a volume
- * into (0 = 4), 9 the csd_amp2sh kernel (1 a dot product a thread, 2 FP64
+ * into (0 = 8), 9 the csd_amp2sh kernel (1 a dot product a thread, 2 FP64
  * FMA tiles, 3 FP64 tensor cores where they apply: nd <= 64, nSH <= 48;
  * 0 = the fastest that applies), 10 the warm-started phased method's later
  * solves from the warm set's stored factor (0 default = 1 on, 2 off), 11
@@ -417,8 +422,10 @@ int csd_icls_solve_host(csd_icls* problem, const float* b, int64_t n, int64_t vo
  * host round trips (0 default = 1 on, 2 off: one round trip per batch), 12
  * the phased solve's rank-k assembly (0 default = 2, 1 mma.sync inside the
  * solve kernel, 2 tcgen05 ahead of it, up to 320 constraint directions;
- * the grouped solve kernels of knob 4 always assemble with mma.sync).
- * Knobs 0-5, 7, 8 and 11 leave the outputs unchanged bit for bit; knob 6 changes
+ * the grouped solve kernels of knob 4 always assemble with mma.sync), 13
+ * csd_dwi2fod_host_phased's slabs computing at once (0 default = all; k:
+ * slab j's compute waits for slab j - k's).
+ * Knobs 0-5, 7, 8, 11 and 13 leave the outputs unchanged bit for bit; knob 6 changes
  * the FP32 summation order of the logits, knob 9 the FP64 summation order of
  * the coefficients, knob 10 the FP32 arithmetic of the later solves, knob
  * 12 the FP32 summation order of the assembled systems (same iteration,

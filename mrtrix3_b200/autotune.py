@@ -19,7 +19,8 @@ import numpy as np
 from . import csd
 
 (KNOB_PERSISTENT, KNOB_SOLVE, KNOB_PROJ, KNOB_TC_PROJECTION, KNOB_SOLVE_KIND, KNOB_SET_KIND, KNOB_INFER,
- KNOB_CYCLE_JUMP, KNOB_HOST_SLABS, KNOB_AMP2SH_KIND, KNOB_REUSE, KNOB_HOST_ASYNC, KNOB_ASSEMBLY) = range(13)
+ KNOB_CYCLE_JUMP, KNOB_HOST_SLABS, KNOB_AMP2SH_KIND, KNOB_REUSE, KNOB_HOST_ASYNC, KNOB_ASSEMBLY,
+ KNOB_HOST_CONC) = range(14)
 # the projection kernel is chosen before its blocks per SM (which only the
 # mma.sync kernel uses).  The solve kernel's warps per block apply to the
 # kernel the default tcgen05 assembly feeds (up to 32 warps at lmax 8; the

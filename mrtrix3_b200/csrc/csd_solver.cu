@@ -64,11 +64,14 @@ static int g_set_kind = 0;    // phased set kernel: 0 default, 1 warp per voxel,
 // where a cycling voxel only holds its own warp and the extra checks in every iteration cost more (83.8 vs
 // 87.9 ms per benchmark volume)
 static int g_fast_cycles = 0;
-static int g_host_slabs = 0;  // host-buffer phased entry point: most slabs per call (knob 8; 0 = 4)
+static int g_host_slabs = 0;  // host-buffer phased entry point: most slabs per call (knob 8; 0 = 8)
 static int g_reuse = 0;       // later solves of warm-started voxels from their warm-set factor (knob 10: 0 default
                               // = on, 1 on, 2 off)
 static int g_host_async = 0;  // host-buffer phased entry point: every slab's passes enqueued without host round
                               // trips (knob 11: 0 default = on, 1 on, 2 off: one round trip per batch of passes)
+static int g_host_conc = 0;   // host-buffer phased entry point (asynchronous form): slabs computing at once (knob 13;
+                              // 0 = all); slab k's compute waits for slab k - conc's, so the slabs finish one after
+                              // another and their downloads overlap the later slabs' compute
 static int g_asm_kind = 0;    // rank-k assembly of the phased solve (knob 12): 0 default, 1 mma.sync inside the
                               // solve kernel, 2 tcgen05 (csd_assemble_tc_kernel) ahead of it (nhr <= 320)
 static constexpr int kAsmDefault = 2;
@@ -2462,6 +2465,10 @@ extern "C" int csd_set_launch_config(int which, int value) {
       if (value > 2) return fail(CSD_ERR_INVALID, "csd_set_launch_config: assembly is 0 (default), 1 mma.sync or 2 tcgen05");
       g_asm_kind = value;
       break;
+    case 13:
+      if (value > 16) return fail(CSD_ERR_INVALID, "csd_set_launch_config: at most 16 slabs computing at once");
+      g_host_conc = value;
+      break;
     default: return fail(CSD_ERR_INVALID, "csd_set_launch_config: unknown knob");
   }
   return CSD_OK;
@@ -3477,6 +3484,12 @@ extern "C" int csd_solve_noalloc(const csd_shared* s, const csd_volume* v, void*
 
 namespace {
 constexpr int kHostBufs = 8;  // buffer sets (and streams): slabs in flight at once
+constexpr int kHostConcDefault = 1 << 20;  // slabs computing at once by default (all)
+// passes enqueued per slab when every slab has its own state: the benchmark
+// volume needs 7 (warm) / 10 (plain); a slab with voxels still active after
+// them is finished by csd_state_run (same iteration) after one host sync,
+// instead of enqueueing niter + 2 passes whose empty launches cost ~40 us each
+constexpr int kHostAsyncPasses = 16;
 struct PhasedHostWS {
   uint64_t sh_id = 0;  // the csd_shared the states were made for (ids are never reused; addresses can be)
   int64_t cap = 0;
@@ -3491,6 +3504,7 @@ struct PhasedHostWS {
   int64_t hres_cap = 0;
   uint8_t* hsi = nullptr;  // pinned staging of status and iterations (2 x voxels), copied out at the end
   int64_t hsi_cap = 0;
+  cudaEvent_t cev[16] = {};  // per slab: its compute is done (orders the next slabs' compute)
 };
 std::mutex g_phws_mu;
 std::map<int, PhasedHostWS> g_phws;
@@ -3531,7 +3545,7 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
   std::lock_guard<std::mutex> lk(g_phws_mu);
   PhasedHostWS& w = g_phws[dev];
   const int nvol = s->h.nvol, nsh = s->h.nsh, nw = (s->h.nhr + 31) / 32;
-  const int64_t nslab = std::min<int64_t>(g_host_slabs > 0 ? g_host_slabs : 4, std::max<int64_t>(1, n_voxels / 131072));
+  const int64_t nslab = std::min<int64_t>(g_host_slabs > 0 ? g_host_slabs : 8, std::max<int64_t>(1, n_voxels / 131072));
   const int64_t per = (n_voxels + nslab - 1) / nslab;
   const bool async = g_host_async != 2;
   // the asynchronous path gives every slab (up to kHostBufs) its own buffers
@@ -3587,6 +3601,17 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
     if (net)
       for (int i = 0; i < nb; ++i)  // the warm-set factor storage, once
         if (!w.st[i]->Lst && (rc = csd_state_warm(w.st[i], w.warm[i], w.stream[i]))) return rc;
+    const int64_t conc = g_host_conc > 0 ? g_host_conc : kHostConcDefault;
+    // fewer passes than niter + 2 only when no state is reused by a later slab
+    int host_passes = kHostAsyncPasses;
+    if (const char* env = std::getenv("CSD_HOST_PASSES")) {  // fewer, to exercise the finishing path in tests
+      const int v = std::atoi(env);
+      if (v >= 1) host_passes = v;
+    }
+    auto passes0 = [&](const csd_state* S) { return nslab <= nb ? std::min(S->async_passes, host_passes)
+                                                                : S->async_passes; };
+    for (auto& e : w.cev)
+      if (!e) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (int64_t k = 0; k < nslab; ++k) {
       const int64_t a = k * per, n = std::min(per, n_voxels - a);
       if (n <= 0) break;
@@ -3594,14 +3619,17 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
       cudaStream_t st = w.stream[b];
       csd_state* S = w.st[b];
       if ((rc = upload(k))) return rc;
+      // the upload above runs ahead; the compute waits for slab k - conc's
+      if (conc < nslab && k >= conc) CUDA_TRY(cudaStreamWaitEvent(st, w.cev[k - conc], 0));
       const uint8_t* dmask = mask ? w.small[b] : nullptr;
       if (net && (rc = csd_mlp_predict(net, w.dwi[b], n, nvol, 1, dmask, 0.f, w.warm[b], st))) return rc;
-      if ((rc = csd_state_run_async(S, w.dwi[b], n, nvol, 1, dmask, net ? w.warm[b] : nullptr, S->async_passes, st)))
+      if ((rc = csd_state_run_async(S, w.dwi[b], n, nvol, 1, dmask, net ? w.warm[b] : nullptr, passes0(S), st)))
         return rc;
       uint8_t* dst = w.small[b] + per;
       uint8_t* dit = w.small[b] + 2 * per;
       if ((rc = csd_state_fod(S, w.fod[b], nsh, status ? dst : nullptr, iterations ? dit : nullptr, nullptr, st)))
         return rc;
+      CUDA_TRY(cudaEventRecord(w.cev[k], st));
       CUDA_TRY(cudaMemcpyAsync(w.hres + 2 * k, S->acount + 2 * S->async_cur, sizeof(int), cudaMemcpyDeviceToHost, st));
       CUDA_TRY(cudaMemcpyAsync(w.hres + 2 * k + 1, S->counter + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
       if (status) CUDA_TRY(cudaMemcpyAsync(w.hsi + a, dst, (size_t)n, cudaMemcpyDeviceToHost, st));
@@ -3609,12 +3637,35 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
       CUDA_TRY(cudaMemcpyAsync(fod + a * nsh, w.fod[b], (size_t)n * nsh * sizeof(float), cudaMemcpyDeviceToHost, st));
     }
     for (int i = 0; i < nb; ++i) CUDA_TRY(cudaStreamSynchronize(w.stream[i]));
-    if (status) std::memcpy(status, w.hsi, (size_t)n_voxels);
-    if (iterations) std::memcpy(iterations, w.hsi + n_voxels, (size_t)n_voxels);
+    bool finished = false;
     for (int64_t k = 0; k < nslab && k * per < n_voxels; ++k) {
       if (w.hres[2 * k + 1]) return fail(CSD_ERR_TIMEOUT, "csd_dwi2fod_host_phased: a bounded wait timed out");
-      if (w.hres[2 * k]) return fail(CSD_ERR_CUDA, "csd_dwi2fod_host_phased: voxels left iterating after niter + 2 passes");
+      if (!w.hres[2 * k]) continue;
+      const int b = (int)(k % nb);
+      csd_state* S = w.st[b];
+      if (nslab > nb || passes0(S) >= S->async_passes)
+        return fail(CSD_ERR_CUDA, "csd_dwi2fod_host_phased: voxels left iterating after niter + 2 passes");
+      // voxels still iterating after the enqueued passes: the rest of the
+      // iteration by csd_state_run on the same state, then this slab's
+      // outputs again
+      const int64_t a = k * per, n = std::min(per, n_voxels - a);
+      cudaStream_t st = w.stream[b];
+      S->n_active = w.hres[2 * k];
+      S->passes = passes0(S);
+      if ((rc = csd_state_run(S, 0, nullptr, st))) return rc;
+      uint8_t* dst = w.small[b] + per;
+      uint8_t* dit = w.small[b] + 2 * per;
+      if ((rc = csd_state_fod(S, w.fod[b], nsh, status ? dst : nullptr, iterations ? dit : nullptr, nullptr, st)))
+        return rc;
+      if (status) CUDA_TRY(cudaMemcpyAsync(w.hsi + a, dst, (size_t)n, cudaMemcpyDeviceToHost, st));
+      if (iterations) CUDA_TRY(cudaMemcpyAsync(w.hsi + n_voxels + a, dit, (size_t)n, cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaMemcpyAsync(fod + a * nsh, w.fod[b], (size_t)n * nsh * sizeof(float), cudaMemcpyDeviceToHost, st));
+      finished = true;
     }
+    if (finished)
+      for (int i = 0; i < nb; ++i) CUDA_TRY(cudaStreamSynchronize(w.stream[i]));
+    if (status) std::memcpy(status, w.hsi, (size_t)n_voxels);
+    if (iterations) std::memcpy(iterations, w.hsi + n_voxels, (size_t)n_voxels);
     return CSD_OK;
   }
   // host round trips: enqueue the first slab's upload, then per slab:

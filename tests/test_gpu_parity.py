@@ -360,3 +360,36 @@ def test_host_phased_after_shared_objects_are_replaced(cuda):
         assert np.array_equal(host["status"], dev["status"]), lmax
         del s, st
         gc.collect()
+
+
+@pytest.mark.parametrize("passes", [None, "2"])
+def test_host_phased_finishes_slabs_left_iterating(cuda, monkeypatch, passes):
+    """The host-buffer entry point enqueues a bounded number of passes per
+    slab (16 by default; 2 here to force the case) and finishes any slab
+    whose voxels are still iterating with the synchronous run on the same
+    state: outputs equal the device-buffer method's bit for bit, plain and
+    warm-started by the shipped network, over several slabs."""
+    import os
+
+    import torch
+
+    from mrtrix3_b200.warmstart import WarmStartNet
+    if passes:
+        monkeypatch.setenv("CSD_HOST_PASSES", passes)
+    else:
+        monkeypatch.delenv("CSD_HOST_PASSES", raising=False)
+    net = WarmStartNet.load(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                         "mrtrix3_b200", "data", "warmstart_c5.npz"))
+    grad = synth.config5_scheme()
+    dwi = synth.voxel_signals(np.random.default_rng(95), grad, 300_000, (15.0, 40.0))
+    s = csd.make_shared(grad, synth.RESPONSE)
+    d = torch.from_numpy(dwi).cuda()
+    st = csd.State(s, len(dwi))
+    for w in (None, net):
+        host = csd.dwi2fod_csd_host_phased(s, dwi, None, net=w)
+        st.run(d, warm=w.predict(d) if w is not None else None)
+        dev = st.fod()
+        assert np.array_equal(host["fod"], dev["fod"]), w
+        assert np.array_equal(host["status"], dev["status"]), w
+        assert np.array_equal(host["iterations"], dev["iterations"].astype(np.uint8)), w
+    st.close()

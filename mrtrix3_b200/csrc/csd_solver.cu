@@ -3561,7 +3561,16 @@ extern "C" int csd_dwi2fod_host_phased(const csd_shared* s, csd_mlp* net, const 
       CUDA_TRY(cudaMalloc(&w.fod[i], (size_t)per * nsh * sizeof(float)));
       CUDA_TRY(cudaMalloc(&w.small[i], (size_t)per * 3));
       CUDA_TRY(cudaMalloc(&w.warm[i], (size_t)per * nw * sizeof(uint32_t)));
-      if (!w.stream[i]) CUDA_TRY(cudaStreamCreateWithFlags(&w.stream[i], cudaStreamNonBlocking));
+      if (!w.stream[i]) {
+        // earlier slabs at higher priority: they finish first, so their
+        // downloads overlap the later slabs' compute, which fills the SMs
+        // the earlier ones leave idle in their tail passes
+        int lo = 0, hi = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        const int levels = lo - hi + 1;
+        const int prio = hi + std::min(levels - 1, i * levels / kHostBufs);
+        CUDA_TRY(cudaStreamCreateWithPriority(&w.stream[i], cudaStreamNonBlocking, prio));
+      }
     }
     w.sh_id = s->id;
     w.cap = per;

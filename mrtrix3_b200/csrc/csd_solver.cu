@@ -1281,7 +1281,7 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
 // into its row of the M=128 operand (one thread a voxel) and read the
 // accumulators back (tcgen05.ld, the warp's quarter of the lanes), adding
 // Mt_M and storing W to global memory for csd_solve_kernel<N, true>; warp 4
-// streams the product table through two shared-memory stages (bulk copies
+// streams the product table through kAsmStages shared-memory stages (bulk copies
 // completing on mbarriers); warp 5 issues the MMAs (N = NC columns a chunk,
 // K = 16 an instruction) into two tensor-memory buffers, so one chunk's
 // read-back overlaps the next chunk's products.  Every wait is bounded; a
@@ -1289,8 +1289,21 @@ __global__ void __launch_bounds__(128, 1) csd_project_tc_kernel(const __grid_con
 // barrier before the tensor memory is freed.
 constexpr int kAsmRows = 128;                    // voxels per tile (M)
 constexpr int kAsmK = 320;                       // directions (K), nhr <= 320
-constexpr int kAsmSlabK = 64;                    // directions per stage
+#ifndef CSD_ASM_SLAB_K
+#define CSD_ASM_SLAB_K 64
+#endif
+#ifndef CSD_ASM_STAGES
+#define CSD_ASM_STAGES 2
+#endif
+// The product table streams through kAsmStages shared-memory stages of
+// kAsmSlabK directions; while the MMAs read one stage the others are in
+// flight.  Two stages of 64, four of 32 and eight of 16 directions measure
+// the same (2.52 / 2.53 / 2.61 ms of assembly a benchmark step, outputs
+// bit-identical): the copies in flight do not bound the kernel.
+constexpr int kAsmSlabK = CSD_ASM_SLAB_K;        // directions per stage
 constexpr int kAsmSlabs = kAsmK / kAsmSlabK;     // stages per chunk
+constexpr int kAsmStages = CSD_ASM_STAGES;       // stages in shared memory
+static_assert(kAsmK % kAsmSlabK == 0 && kAsmSlabK % 16 == 0 && kAsmStages >= 2 && kAsmStages <= 8, "stages");
 constexpr int kAsmABytes = (kAsmK / 8) * kAsmRows * 16;
 
 struct AsmShape {
@@ -1301,7 +1314,7 @@ __host__ __device__ constexpr AsmShape asm_shape(int n) {
                   (((packoff(n) + (packoff(n) + 255) / 256 - 1) / ((packoff(n) + 255) / 256)) + 15) / 16 * 16};
 }
 __host__ __device__ constexpr int asm_stage_bytes(int n) { return 2 * (kAsmSlabK / 8) * asm_shape(n).nc * 16; }
-__host__ __device__ constexpr int asm_smem_bytes(int n) { return kAsmABytes + 2 * asm_stage_bytes(n) + 128; }
+__host__ __device__ constexpr int asm_smem_bytes(int n) { return kAsmABytes + kAsmStages * asm_stage_bytes(n) + 256; }
 
 __device__ __forceinline__ void mbar_arrive1(uint32_t mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(mbar) : "memory");
@@ -1317,24 +1330,27 @@ __global__ void __launch_bounds__(192, 1) csd_assemble_tc_kernel(const __grid_co
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* sA = smem;
   unsigned char* sB = smem + kAsmABytes;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + 2 * STAGE);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + kAsmStages * STAGE);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kAsmStages + 6);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n_in = P.n_in_dev ? *P.n_in_dev : P.n_in;
   const int end = min(n_in, P.c0 + P.ch);
   const int ntiles = end > P.c0 ? (end - P.c0 + kAsmRows - 1) / kAsmRows : 0;
   if ((int)blockIdx.x >= ntiles) return;  // the grid is an upper bound; before any allocation
   const uint32_t bar0 = static_cast<uint32_t>(__cvta_generic_to_shared(bars));
-  // barriers: b_full[2], b_empty[2], acc_full[2], acc_empty[2], a_full, done
+  // barriers: b_full[kAsmStages], b_empty[kAsmStages], acc_full[2], acc_empty[2], a_full, done
+  constexpr uint32_t NS = kAsmStages;
   auto b_full = [&](int i) { return bar0 + 8u * (uint32_t)i; };
-  auto b_empty = [&](int i) { return bar0 + 8u * (uint32_t)(2 + i); };
-  auto acc_full = [&](int i) { return bar0 + 8u * (uint32_t)(4 + i); };
-  auto acc_empty = [&](int i) { return bar0 + 8u * (uint32_t)(6 + i); };
-  const uint32_t a_full = bar0 + 64u, done = bar0 + 72u;
+  auto b_empty = [&](int i) { return bar0 + 8u * (NS + (uint32_t)i); };
+  auto acc_full = [&](int i) { return bar0 + 8u * (2 * NS + (uint32_t)i); };
+  auto acc_empty = [&](int i) { return bar0 + 8u * (2 * NS + 2 + (uint32_t)i); };
+  const uint32_t a_full = bar0 + 8u * (2 * NS + 4), done = bar0 + 8u * (2 * NS + 5);
   if (tid == 0) {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kAsmStages; ++i) {
       mbar_init(b_full(i), 1);
       mbar_init(b_empty(i), 1);
+    }
+    for (int i = 0; i < 2; ++i) {
       mbar_init(acc_full(i), 1);
       mbar_init(acc_empty(i), kAsmRows);
     }
@@ -1357,8 +1373,8 @@ __global__ void __launch_bounds__(192, 1) csd_assemble_tc_kernel(const __grid_co
       for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x)
         for (int ch = 0; ch < NCH && !failed; ++ch)
           for (int sl = 0; sl < kAsmSlabs; ++sl, ++it) {
-            const int st = it & 1;
-            const uint32_t ph = (uint32_t)(it >> 1) & 1u;
+            const int st = it % kAsmStages;
+            const uint32_t ph = (uint32_t)(it / kAsmStages) & 1u;
             if (!mbar_wait(b_empty(st), ph ^ 1u)) {
               failed = true;
               break;
@@ -1391,8 +1407,8 @@ __global__ void __launch_bounds__(192, 1) csd_assemble_tc_kernel(const __grid_co
           tc_fence_after();
           const uint32_t dcol = tmem + (uint32_t)(buf * NC);
           for (int sl = 0; sl < kAsmSlabs; ++sl, ++it) {
-            const int st = it & 1;
-            if (!mbar_wait(b_full(st), ((uint32_t)it >> 1) & 1u)) {
+            const int st = it % kAsmStages;
+            if (!mbar_wait(b_full(st), (uint32_t)(it / kAsmStages) & 1u)) {
               failed = true;
               break;
             }

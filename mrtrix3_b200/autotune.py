@@ -2,8 +2,8 @@
 
 Times candidate values of the launch knobs of csd_set_launch_config (warps
 per block of the persistent kernel and of the phased solve kernel, the
-phased solve kernel's lanes per voxel, the projection kernel -- mma.sync or
-tcgen05 -- and its blocks per SM) on a probe volume, keeps the fastest, and caches
+projection kernel -- mma.sync or tcgen05 -- and its blocks per SM) on a
+probe volume, keeps the fastest, and caches
 the choice per (GPU name, nSH, constraint directions, DW directions) in a
 JSON file (default ~/.cache/mrtrix3_b200/launch.json, or $CSD_TUNE_CACHE).
 Outputs do not depend on the knobs, so tuning never changes results.

@@ -97,6 +97,22 @@ def test_errors_follow_reference_messages():
     assert L.csd_shared_nsh(None) == csd.lib().csd_shared_nsh(None) < 0
 
 
+def test_state_queries_and_launch_knobs_reject_bad_arguments():
+    """The state queries refuse NULL arguments and the launch knobs refuse
+    values out of range (no device work: both checks come first)."""
+    L = csd.lib()
+    out = (ctypes.c_double * 8)()
+    for name in ("csd_state_stats", "csd_state_reuse_stats", "csd_state_assembly_stats"):
+        fn = getattr(L, name)
+        fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        assert fn(None, out) == csd.CSD_ERR_INVALID, name
+    L.csd_set_launch_config.argtypes = [ctypes.c_int, ctypes.c_int]
+    assert L.csd_set_launch_config(12, 3) == csd.CSD_ERR_INVALID   # assembly: 0, 1 or 2
+    assert L.csd_set_launch_config(13, 17) == csd.CSD_ERR_INVALID  # at most 16 slabs at once
+    assert L.csd_set_launch_config(14, 0) == csd.CSD_ERR_INVALID   # no such knob
+    assert L.csd_set_launch_config(12, 0) == csd.CSD_OK and L.csd_set_launch_config(13, 0) == csd.CSD_OK
+
+
 def test_cpp_shim_compiles():
     """The C++ drop-in headers (CSD::Shared / CSD, csd.h:46-271; ICLS::Problem
     / Solver, constrained_least_squares.h:71-370; FMLS::Segmenter, fmls.h:60-291)

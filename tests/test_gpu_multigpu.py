@@ -1,6 +1,6 @@
 """The slab-sharding driver (mrtrix3_b200/multigpu.py) with the GPU solve on
 every rank: two gloo ranks, each deconvolving its mask-balanced z-slab with
-csd_dwi2fod_host_phased on cuda:0 (the only GPU of this run; the ranks'
+csd_dwi2fod_host_phased, both on cuda:0 (one GPU is enough: the ranks'
 kernels never wait on one another, and the one collective, the final
 gather, runs on host tensors), gathered on rank 0.  Voxels are independent,
 so the gathered volume equals one process's result bit for bit."""

@@ -13,7 +13,7 @@
 #include "../mrtrix3_b200/csrc/fmls_core.cuh"
 #include "../mrtrix3_b200/csrc/fmls_tables.hpp"
 
-// the library's error recorder and device upload are not part of this build
+// the library's error recorder and device upload are not compiled into this harness
 namespace csdb200 {
 int set_error(int code, const std::string&) { return code; }
 }
